@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Energy-point solve throughput of the per-energy-point transport solve.
+
+Workload (default): the batched-FP64 nanowire -- 100 principal layers of 256
+orbitals, complex128, 10 % random non-zeros, S = I + 0.05 R, 2048 energies in
+[-2, 2] eV x 16 transverse k-points, contact self-energies at E + i*1e-6,
+outputs T(E,k) and the diagonal spectral density of every orbital.  Seeded
+synthetic data (libNEGF ships no benchmark inputs).
+
+A step is one persistent launch over a batch of (E, k) points of this rank.
+  value  device-resident inputs and outputs (negf_b200_transmission_dos_dev),
+         CUDA events on the launching stream, max over ranks.
+  e2e    the same batches through the host-buffer C-ABI call
+         (negf_b200_transmission_dos), host<->device copies inside the timing.
+Multi-GPU: (E, k) points shard across ranks with no data-path collective
+(weak scaling: fixed points per rank per step).
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle restatement, LAPACK zgetrf/zgetrs + zgemm, OpenMP over points) on the
+host cores on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    # name: (nbl, n, nE, emin, emax, nk, eta, dos)
+    "c1": dict(nbl=100, n=256, nE=2048, emin=-2.0, emax=2.0, nk=16, eta=1e-6, dos=True, gen="c1"),
+    "c0": dict(nbl=20, n=32, nE=512, emin=-3.0, emax=3.0, nk=1, eta=1e-6, dos=False, gen="c0"),
+    "c2": dict(nbl=60, n=512, nE=1024, emin=-2.0, emax=2.0, nk=8, eta=1e-6, dos=False, gen="c1"),
+    # small case of the c1 kernel for profiler captures (few GB on the device)
+    "prof": dict(nbl=8, n=256, nE=256, emin=-2.0, emax=2.0, nk=1, eta=1e-6, dos=True, gen="c1"),
+}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    p.add_argument("--points-per-step", type=int, default=0, help="0 = 2 x resident CTAs")
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline points (0 = auto)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--trace", action="store_true", help="one extra untimed step with per-phase cycle tracing")
+    return p.parse_args()
+
+
+def devices_for(wl):
+    from libnegf_b200 import generators as G
+    if wl["gen"] == "c0":
+        return [G.transport_c0(nbl=wl["nbl"], n=wl["n"], seed=0)], [0.0]
+    ks = [np.pi * j / wl["nk"] for j in range(wl["nk"])]
+    return G.transport_c1_kpoints(ks, nbl=wl["nbl"], n=wl["n"], seed=1), ks
+
+
+def point_list(wl, seed=11):
+    from libnegf_b200 import generators as G
+    E = G.energy_grid(wl["emin"], wl["emax"], wl["nE"])
+    kk, ee = np.meshgrid(np.arange(wl["nk"]), E, indexing="ij")
+    ids = kk.ravel().astype(np.int32)
+    en = ee.ravel().astype(np.float64)
+    perm = np.random.default_rng(seed).permutation(ids.size)   # mix k and E inside every batch
+    return ids[perm], en[perm]
+
+
+def flops_per_point(wl, ncyc_total, ncont=2):
+    """Algorithmic FP64 flops of one point, as the engine computes it
+    (uniform PL size n = lead PL size): complex GEMM m*n*k = 8mnk flops,
+    Gauss-Jordan inverse = 8 n^3 flops.
+      decimation, per contact with c iterations: c inverses, 6(c-1)+2 GEMMs,
+        one final inverse  -> 8 n^3 (7c - 3)
+      self-energy: 2 GEMMs per contact
+      gsmr sweep + Gr(1,1): N inverses, 2(N-1) GEMMs
+      diagonal retarded sweep (DOS): 4 GEMMs per layer 2..N
+      2-contact trace: 2 GEMMs"""
+    n, N = wl["n"], wl["nbl"]
+    u = 8.0 * n ** 3
+    dec = u * (7.0 * ncyc_total - 3.0 * ncont)
+    sig = u * 2 * ncont
+    sweep = u * (N + 2 * (N - 1))
+    dos = u * 4 * (N - 1) if wl["dos"] else 0.0
+    tr = u * 2
+    return dec + sig + sweep + dos + tr
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.FIELDS, "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def fp64_peak_tflops(torch, dev):
+    """Measured FP64 denominator: cuBLAS ZGEMM (complex128 matmul, 8 n^3)."""
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.complex128, device=dev)
+    b = torch.randn(n, n, dtype=torch.complex128, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    return 8.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
+    """Oracle restatement (LAPACK/BLAS per point, OpenMP over points) on a
+    bounded sample of the workload's points.  Returns (solves/s, T sample)."""
+    from oracle import oracle as O
+    O.lib()
+    T = np.zeros(nsamp)
+    t0 = time.perf_counter()
+    done = 0
+    for k in sorted(set(ids[:nsamp].tolist())):
+        sel = np.nonzero(ids[:nsamp] == k)[0]
+        if wl["dos"]:
+            t, _, _, _ = O.transmission_dos(devs[k], E[sel], eta=wl["eta"], dos_delta=0.0, nthreads=nthreads)
+        else:
+            t, _, _ = O.transmission(devs[k], E[sel], eta=wl["eta"], nthreads=nthreads)
+        T[sel] = t
+        done += sel.size
+    dt = time.perf_counter() - t0
+    return done / dt, T, dt
+
+
+def run_reference(args, wl, rank, world):
+    if rank != 0:
+        return
+    devs, _ = devices_for(wl)
+    ids, E = point_list(wl)
+    cores = os.cpu_count() or 1
+    nsamp = args.cpu_sample or max(cores, 8) * (1 if wl["n"] >= 256 else 8)
+    vals = []
+    for s in range(args.warmup + args.steps):
+        k0 = ids[s % ids.size]
+        sel = np.nonzero(ids == k0)[0]
+        sel = sel[(s * nsamp) % max(1, sel.size - nsamp):][:nsamp]
+        v, _, _ = cpu_baseline(wl, devs, ids[sel], E[sel], sel.size, cores)
+        if s >= args.warmup:
+            vals.append(v)
+    value = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": "energy_point_solves_per_s", "value": value, "unit": "solves/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * nsamp / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": config_of(args, wl, nsamp),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                         "sample": "%d points of the workload per step (LAPACK zgetrf/zgetrs + zgemm per point, "
+                                   "OpenMP over points, single-threaded BLAS)" % nsamp},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(args, wl, pts):
+    return {"workload": "transport_%s: N=%d PLs x n=%d, complex128, %d energies x %d k-points%s" % (
+        args.workload, wl["nbl"], wl["n"], wl["nE"], wl["nk"], ", T(E,k) + diagonal DOS" if wl["dos"] else
+        ", T(E,k)"), "points_per_step": pts, "eta": wl["eta"], "sgf_tol": 1e-9,
+        "l2": "inputs and workspace larger than L2 (126 MB)", "parallelism": "dp%d (E,k shards)" % args.gpus}
+
+
+def main():
+    args = parse()
+    wl = WORKLOADS[args.workload]
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, wl, rank, world)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from libnegf_b200 import native
+    L = native.load()
+
+    peak = fp64_peak_tflops(torch, "cuda:%d" % local)
+    devs, ks = devices_for(wl)
+    ids_all, E_all = point_list(wl)
+    shard = np.arange(rank, ids_all.size, world)     # round-robin, as tunneling_int_def
+    ids_r, E_r = ids_all[shard], E_all[shard]
+
+    ctx = native.Context(local)
+    dids = [ctx.upload(d) for d in devs]
+    norb = devs[0].norb
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    P = args.points_per_step or 4 * sms
+    nsteps = args.warmup + args.steps
+    need = P * nsteps
+    reps = int(np.ceil(need / ids_r.size))
+    ids_run = np.tile(ids_r, reps)[:need]
+    E_run = np.tile(E_r, reps)[:need]
+    d_ids = torch.from_numpy(np.asarray(dids, dtype=np.int32)[ids_run]).cuda()
+    d_E = torch.from_numpy(E_run).cuda()
+    d_T = torch.zeros(need, dtype=torch.float64, device="cuda")
+    d_dos = torch.zeros((P, norb), dtype=torch.float64, device="cuda") if wl["dos"] else None
+    d_nc = torch.zeros(need, dtype=torch.int32, device="cuda")
+    d_st = torch.zeros(need, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()          # a real stream: NULL would mean the context's own stream
+    sh = ctypes.c_void_p(stream.cuda_stream)
+
+    def step(s):
+        o = s * P
+        if wl["dos"]:
+            rc = L.negf_b200_transmission_dos_dev(
+                ctx.handle, P, d_ids.data_ptr() + 4 * o, d_E.data_ptr() + 8 * o, wl["eta"], 0.0, 1, 2,
+                d_T.data_ptr() + 8 * o, d_dos.data_ptr(), norb, d_nc.data_ptr() + 4 * o, d_st.data_ptr() + 4 * o, sh)
+        else:
+            rc = L.negf_b200_transmission_dev(
+                ctx.handle, P, d_ids.data_ptr() + 4 * o, d_E.data_ptr() + 8 * o, wl["eta"], 1, 2,
+                d_T.data_ptr() + 8 * o, d_nc.data_ptr() + 4 * o, d_st.data_ptr() + 4 * o, sh)
+        if rc != 0:
+            raise RuntimeError("solve failed: %d %s" % (rc, ctx.last_error()))
+
+    for s in range(args.warmup):
+        step(s)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    with ClockSampler(local) as clk:
+        ev[0].record(stream)
+        for j in range(args.steps):
+            step(args.warmup + j)
+            ev[j + 1].record(stream)
+        torch.cuda.synchronize()
+    per_step = [ev[j].elapsed_time(ev[j + 1]) for j in range(args.steps)]
+    ms = ev[0].elapsed_time(ev[-1])
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    trace = None
+    if args.trace:
+        ctx.set_tracing(True)
+        ctx.get_trace()
+        step(args.warmup)
+        torch.cuda.synchronize()
+        tr = ctx.get_trace()
+        ctx.set_tracing(False)
+        tot = max(tr["total"], 1)
+        trace = {k: tr[k] / tot for k in ("gemm", "inv_panel", "inv_update", "inv_other", "elementwise")}
+        trace["other"] = 1.0 - sum(trace.values())
+        trace["points"] = tr["points"]
+    st = d_st.cpu().numpy()
+    nc = d_nc.cpu().numpy()
+    Tgpu = d_T.cpu().numpy()
+    timed = slice(args.warmup * P, nsteps * P)
+    flops = float(sum(flops_per_point(wl, int(c)) for c in nc[timed]))
+    points_total = args.steps * P * world
+    value = points_total / (ms * 1e-3)
+
+    # e2e: same batches through the host-buffer C-ABI call
+    e2e_steps = max(1, args.e2e_steps)
+    h_ids = np.asarray(dids, dtype=np.int32)[ids_run]
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for j in range(e2e_steps):
+        o = (args.warmup + j % args.steps) * P
+        if wl["dos"]:
+            ctx.transmission_dos(h_ids[o:o + P], E_run[o:o + P], eta=wl["eta"], dos_delta=0.0, check=False)
+        else:
+            ctx.transmission(h_ids[o:o + P], E_run[o:o + P], eta=wl["eta"], check=False)
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = e2e_steps * P * world / e2e_s
+    h2d = P * (4 + 8)
+    d2h = P * (8 + 4 + 4 + (8 * norb if wl["dos"] else 0))
+
+    if rank == 0:
+        achieved = flops / (ms * 1e-3) / 1e12 / 1.0
+        line = {
+            "metric": "energy_point_solves_per_s", "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": config_of(args, wl, P),
+            "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured in-run: cuBLAS ZGEMM 4096^3 complex128 (FP64 DMMA pipe)",
+                         "flops_per_step": flops / args.steps},
+            "clocks": clk.summary(),
+            "status_counts": {str(k): int(v) for k, v in zip(*np.unique(st[timed], return_counts=True))},
+            "ncyc_mean": float(nc[timed].mean()),
+            "step_ms": per_step,
+        }
+        if trace:
+            line["trace_phase_share"] = trace
+        if world == 1 and not args.no_cpu_baseline:
+            cores = os.cpu_count() or 1
+            nsamp = args.cpu_sample or (cores if wl["n"] >= 256 else 8 * cores)
+            o = args.warmup * P
+            # points of the timed batches at one k-point (all k share structure and cost), so that
+            # OpenMP spreads the sample over every host core
+            k0 = ids_run[o]
+            sel = o + np.nonzero(ids_run[o:] == k0)[0][:nsamp]
+            nsamp = sel.size
+            v, Tc, dt = cpu_baseline(wl, devs, ids_run[sel], E_run[sel], nsamp, cores)
+            err = np.abs(Tgpu[sel] - Tc)
+            line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                                    "sample": "%d points of the timed batches, %.1f s" % (nsamp, dt)}
+            line["parity_sample"] = {"points": int(nsamp), "max_abs_dT": float(err.max()),
+                                     "max_rel_dT_T_gt_1e-6": float((err / np.maximum(np.abs(Tc), 1e-300))[
+                                         np.abs(Tc) > 1e-6].max()) if (np.abs(Tc) > 1e-6).any() else 0.0}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

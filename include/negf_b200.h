@@ -1,0 +1,269 @@
+/*
+ * negf_b200.h -- C-ABI of the B200 per-energy-point transport solve.
+ *
+ * Drop-in seam: libNEGF selects its RGF backend at build time
+ * (src/iterative.F90:38-43: `use iterative_gpu` | `use iterative_cpu`) and
+ * reaches CUDA through `bind(C)` interfaces (src/cudautils.F90:236-431) to the
+ * `extern "C"` functions of src/gpuroutines.cu.  This header is the
+ * replacement of that seam.  It keeps the reference's conventions:
+ *
+ *   - matrices are column-major complex128 (interleaved re,im doubles), the
+ *     layout of `z_DNS%val` (src/mat_def.F90:199-204);
+ *   - sizes are plain integers, pointers are plain pointers, no C++ types;
+ *   - every function returns an `int` status (0 = OK), the convention of the
+ *     `cu_*` functions (src/gpuroutines.cu:248-996), but never traps or exits:
+ *     where the reference stops (`error stop`, `__trap()`), these functions
+ *     return a NEGF_B200_ERR_* code and fill a per-point status array.
+ *
+ * Two levels are exported:
+ *   1. batched per-energy-point solves over a device description that stays
+ *      resident in HBM (the context API below) -- the hot path;
+ *   2. device-pointer primitives that mirror the reference's cuBLAS/cuSOLVER
+ *      wrappers one-for-one (cu_ZmultMat, cu_Zinverse, cu_Zdecimation).
+ *
+ * Energies are in the units of H (libNEGF does not rescale them).
+ */
+#ifndef NEGF_B200_H
+#define NEGF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define NEGF_B200_OK 0
+#define NEGF_B200_ERR_SINGULAR 1      /* exact zero pivot in a block inversion
+                                         (zgetrf info>0, src/inversions.F90:823) */
+#define NEGF_B200_ERR_NOT_CONVERGED 2 /* decimation reached the iteration cap
+                                         (src/contselfenergy.F90:289) */
+#define NEGF_B200_ERR_NONFINITE 3     /* NaN/Inf in an output */
+#define NEGF_B200_ERR_NOMEM 4         /* device allocation failed */
+#define NEGF_B200_ERR_BAD_ARG 5       /* shape / pointer / index error */
+#define NEGF_B200_ERR_CUDA 6          /* CUDA runtime error */
+#define NEGF_B200_ERR_TIMEOUT 7       /* a bounded device wait expired */
+#define NEGF_B200_ERR_ADMISSION 8     /* request exceeds the HBM budget */
+#define NEGF_B200_ERR_NO_GPU 9        /* no CUDA device / extension not built */
+#define NEGF_B200_ERR_SCBA_NOT_CONVERGED 10 /* SCBA stopped at scba_niter
+                                               (informational, results valid) */
+
+#define NEGF_B200_MAXNCONT 10 /* src/api/lnParams.h:10 */
+
+/* ---- device description ------------------------------------------------
+ * The block-tridiagonal device of libNEGF after `zcsr2blk_sod`
+ * (src/sparsekit_drv.F90:3409-3436) and the contact blocks after
+ * `extract_cont` (src/ln_extract.F90:37-75).  All blocks are dense,
+ * column-major complex128, concatenated in layer order.
+ *
+ *   h_diag : H(i,i),   n_i x n_i,       i = 0..nbl-1
+ *   h_upper: H(i,i+1), n_i x n_{i+1},   i = 0..nbl-2
+ *   h_lower: H(i+1,i), n_{i+1} x n_i,   i = 0..nbl-2
+ *   s_*    : same for S; all three NULL means S = I (set_S_id,
+ *            src/libnegf.F90:408).
+ * Contacts (surfdim = 0, two principal layers per contact as in
+ * src/contselfenergy.F90:184-207):
+ *   cblk[c]      : 1-based device block the contact couples to (TStruct cblk)
+ *   lead_size[c] : L_c, orbitals of one contact principal layer
+ *   lead_h00/s00 : contact PL1 on-site block, L_c x L_c (concatenated over c)
+ *   lead_h01/s01 : contact PL1 -> PL2 coupling, L_c x L_c
+ *   hmc/smc      : device block cblk[c] -> contact PL1, n_cblk x L_c
+ *   lead_s00/lead_s01/smc NULL means identity / zero overlap.
+ */
+typedef struct negf_b200_device {
+  int32_t nbl;
+  const int32_t* pl_size;
+  const double* h_diag;
+  const double* h_upper;
+  const double* h_lower;
+  const double* s_diag;
+  const double* s_upper;
+  const double* s_lower;
+  int32_t ncont;
+  const int32_t* cblk;
+  const int32_t* lead_size;
+  const double* lead_h00;
+  const double* lead_h01;
+  const double* lead_s00;
+  const double* lead_s01;
+  const double* hmc;
+  const double* smc;
+} negf_b200_device;
+
+/* ---- solver options ------------------------------------------------------
+ * Defaults (negf_b200_default_options) are the reference's:
+ *   sgf_tol = SGFACC = 1e-9          src/ln_precision.F90:40
+ *   sgf_max_iter = 300               src/contselfenergy.F90:289
+ *   eps_drop = 0 (EPS is never set inside libNEGF, src/ln_precision.F90:36)
+ *   scba_tol = 1e-7                  src/lib_param.F90:653
+ */
+typedef struct negf_b200_options {
+  double sgf_tol;
+  int32_t sgf_max_iter;
+  double eps_drop;
+  double scba_tol;
+  int32_t scba_niter;
+  /* 0 = plain complex FP64 (the parity form). */
+  int32_t precision;
+  /* Resident CTAs per SM for the persistent point engine (0 = auto). */
+  int32_t ctas_per_sm;
+} negf_b200_options;
+
+typedef struct negf_b200_ctx negf_b200_ctx;
+
+void negf_b200_default_options(negf_b200_options* opt);
+
+/* Library and build identification (never fails). */
+const char* negf_b200_version(void);
+
+/* Creates a context bound to CUDA device `cuda_device`: one stream, a
+ * resident device arena and the persistent-kernel workspace.  Mirrors the
+ * GPU part of init_negf (src/libnegf.F90:160-170). */
+int negf_b200_ctx_create(int32_t cuda_device, negf_b200_ctx** ctx);
+int negf_b200_ctx_destroy(negf_b200_ctx* ctx);
+int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* opt);
+/* Last error message of this context (empty if none). */
+const char* negf_b200_last_error(const negf_b200_ctx* ctx);
+
+/* Uploads a device description to HBM once (H/S blocks, contact blocks) and
+ * returns a handle.  One description per k-point: libNEGF keeps one H(k),S(k)
+ * pair per local k (negf%HS(iK), src/integrations.F90:1868-1870).  The host
+ * arrays may be freed after the call. */
+int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dev,
+                            int32_t* device_id);
+int negf_b200_release_device(negf_b200_ctx* ctx, int32_t device_id);
+/* Bytes of HBM the device description holds. */
+int negf_b200_device_bytes(const negf_b200_ctx* ctx, int32_t device_id,
+                           size_t* bytes);
+
+/* ---- batched per-energy-point solves (host buffers) ----------------------
+ * A point is (device_id[p], energy[p]).  All points of one call run in one
+ * persistent launch.  `status` (npts) receives a per-point NEGF_B200_* code;
+ * the return value is the first non-OK point status (or a call error).
+ * `ncyc` (npts, optional) receives the total decimation iteration count over
+ * all contacts at that point (src/integrations.F90:1751 prints the average
+ * over contacts). */
+
+/* Coherent transmission T(E) between contacts ni -> nf (1-based).
+ * Replaces compute_contacts(E+i*eta) + calculate_transmissions(E)
+ * (src/integrations.F90:1747-1755, src/iterative.F90:1669-1780): contact
+ * self-energies at E + i*eta, ES-H at real E, gsmr sweep, Caroli trace.
+ * Uses the 2-contact fast path when the reference does (ncont == 2 and
+ * min(cblk) == 1, src/iterative.F90:1697-1713), else the N-contact column
+ * sweep (src/iterative_cpu.F90:477-583). */
+int negf_b200_transmission(negf_b200_ctx* ctx, int32_t npts,
+                           const int32_t* device_id, const double* energy,
+                           double eta, int32_t ni, int32_t nf, double* T,
+                           int32_t* ncyc, int32_t* status);
+
+/* Transmission plus the diagonal spectral density -Im Gr_ii / pi of every
+ * device orbital (dos: npts x norb, row-major by point).  Replaces
+ * calculate_transmissions_and_dos(E + i*dos_delta) with contact
+ * self-energies at E + i*eta (src/integrations.F90:1757-1770,
+ * src/iterative.F90:1821-1952).  Projection on LDOS index sets is a host
+ * reduction of `dos`. */
+int negf_b200_transmission_dos(negf_b200_ctx* ctx, int32_t npts,
+                               const int32_t* device_id, const double* energy,
+                               double eta, double dos_delta, int32_t ni,
+                               int32_t nf, double* T, double* dos,
+                               int32_t* ncyc, int32_t* status);
+
+/* Non-equilibrium solve with local elastic dephasing, one SCBA loop per
+ * point (src/iterative.F90:289-363, src/elphdd.F90:108-276,
+ * src/scba.F90:120-147), then the Meir-Wingreen contact currents
+ * (src/iterative.F90:382-414) and the layer currents / layer densities
+ * (src/iterative.F90:427-461).
+ *   frm       : npts x ncont contact occupations f_c(E) (reference f = 0)
+ *   coupling  : norb dephasing couplings (NOT squared; squared on device as
+ *               in ElPhonDephD_init, src/elphdd.F90:95); NULL = no dephasing
+ *   curr      : npts x ncont  I_c(E)   (optional)
+ *   layer_curr: npts x (nbl-1) J_{i,i+1}(E) (optional)
+ *   layer_dens: npts x nbl     Tr Gn_ii (optional)
+ *   scba_iter : npts iterations run (optional); scba_err: npts last error */
+int negf_b200_meir_wingreen(negf_b200_ctx* ctx, int32_t npts,
+                            const int32_t* device_id, const double* energy,
+                            double eta, const double* frm,
+                            const double* coupling, double* curr,
+                            double* layer_curr, double* layer_dens,
+                            int32_t* scba_iter, double* scba_err,
+                            int32_t* ncyc, int32_t* status);
+
+/* ---- batched solves on device buffers ------------------------------------
+ * Same as negf_b200_transmission / _transmission_dos with every per-point
+ * array already resident in HBM (device pointers) and no host
+ * synchronisation: the launch is enqueued on `stream` (NULL = the context's
+ * stream) and the call returns.  Workspace sizing covers every uploaded
+ * device.  `dos_stride` is the row stride of d_dos in doubles. */
+int negf_b200_transmission_dev(negf_b200_ctx* ctx, int32_t npts,
+                               const int32_t* d_device_id,
+                               const double* d_energy, double eta, int32_t ni,
+                               int32_t nf, double* d_T, int32_t* d_ncyc,
+                               int32_t* d_status, void* stream);
+int negf_b200_transmission_dos_dev(negf_b200_ctx* ctx, int32_t npts,
+                                   const int32_t* d_device_id,
+                                   const double* d_energy, double eta,
+                                   double dos_delta, int32_t ni, int32_t nf,
+                                   double* d_T, double* d_dos,
+                                   int64_t dos_stride, int32_t* d_ncyc,
+                                   int32_t* d_status, void* stream);
+
+/* ---- tracing ---------------------------------------------------------------
+ * libNEGF times phases with a stack of host wall clocks (src/clock.F90:35-93,
+ * printed when verbose > 70).  Here every CTA of the persistent engine
+ * accumulates SM cycles per phase; negf_b200_get_trace synchronises the
+ * device, returns the sums over all CTAs since the previous call and resets
+ * them.  Phases:
+ *   0 block products (decimation, self-energies, sweeps)
+ *   1 inversion panel factorisation (pivot search, row exchanges)
+ *   2 inversion trailing update
+ *   3 inversion copies / final column permutation
+ *   4 ES-H assembly and elementwise passes
+ *   5 whole kernel (per CTA)      6 points processed (a count)   7 unused */
+#define NEGF_B200_TRACE_NPHASE 8
+int negf_b200_set_tracing(negf_b200_ctx* ctx, int32_t enable);
+int negf_b200_get_trace(negf_b200_ctx* ctx, uint64_t* cycles);
+
+/* ---- device-pointer primitives (mirror src/gpuroutines.cu) ---------------
+ * All pointers are device pointers, `stream` is a cudaStream_t (NULL =
+ * legacy default stream); `batch` independent problems with the given
+ * element strides.  No allocation inside except where stated. */
+
+/* C = alpha*op(A)*op(B) + beta*C, complex128.  dagger: 0 = (N,N),
+ * 1 = (C,N), 2 = (N,C) -- the `dagger` argument of cu_ZmultMat
+ * (src/gpuroutines.cu:395-446).  alpha/beta are {re, im}. */
+int negf_b200_zgemm_batched(int32_t batch, int32_t m, int32_t n, int32_t k,
+                            const double* alpha, const double* A,
+                            int64_t strideA, const double* B, int64_t strideB,
+                            const double* beta, double* C, int64_t strideC,
+                            int32_t dagger, void* stream);
+
+/* Ainv = A^-1 (n x n) by Gauss-Jordan elimination with partial pivoting
+ * (pivot = max |Re|+|Im|, the izamax rule of zgetrf).  Replaces cu_Zinverse
+ * = cusolverDnZgetrf + Zgetrs against the identity (src/gpuroutines.cu:
+ * 449-523) and zinv (src/inversions.F90:807-839).  `work` is a device buffer
+ * of negf_b200_zinv_work_bytes(batch, n) bytes; info[b] = 0 or the 1-based
+ * column of the first zero pivot. */
+size_t negf_b200_zinv_work_bytes(int32_t batch, int32_t n);
+int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A,
+                           double* Ainv, int32_t* info, void* work,
+                           void* stream);
+
+/* Sancho-Rubio decimation, batched, device-side convergence: replaces
+ * cu_Zdecimation (src/gpuroutines.cu:742-986) with the CPU rule of
+ * decimation (src/contselfenergy.F90:271-340): converged when
+ * max|C1| <= tol on two consecutive iterations, at most max_iter
+ * iterations.  Ao/Bo/Co/Go: batch x n x n; ncyc: batch (as in the
+ * reference, max_iter+1 when the cap is reached).  `work` holds
+ * negf_b200_decimation_work_bytes(batch, n) bytes. */
+size_t negf_b200_decimation_work_bytes(int32_t batch, int32_t n);
+int negf_b200_decimation_batched(int32_t batch, int32_t n, const double* Ao,
+                                 const double* Bo, const double* Co,
+                                 double* Go, int32_t* ncyc, double tol,
+                                 int32_t max_iter, void* work, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NEGF_B200_H */

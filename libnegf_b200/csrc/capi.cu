@@ -1,0 +1,610 @@
+// C-ABI of the B200 per-energy-point transport solve (include/negf_b200.h).
+//
+// Host side of the drop-in seam: a context owns one CUDA stream, the
+// HBM-resident device descriptions (the counterpart of the H/S blocks and
+// contact blocks libNEGF re-copies to the GPU at every energy point,
+// src/iterative_gpu.F90:185-217), the persistent-kernel workspace and the
+// per-call staging buffers.  Errors are returned as status codes; nothing
+// here exits or traps (the reference stops on every error:
+// src/ln_messages.F90:9-22, src/gpuroutines.cu:38-81).
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/negf_b200.h"
+#include "engine.cuh"
+
+using negf::DevDesc;
+
+namespace {
+
+struct DeviceRec {
+  bool live = false;
+  void* blob = nullptr;
+  size_t bytes = 0;
+  DevDesc desc{};
+  int nbl = 0, ncont = 0, norb = 0, nmax = 0;
+  int cblk[negf::kMaxCont] = {0};
+  bool has_s = false;
+};
+
+}  // namespace
+
+struct negf_b200_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  negf_b200_options opt{};
+  std::string err;
+  std::vector<DeviceRec> devs;
+  DevDesc* d_descs = nullptr;
+  size_t d_descs_cap = 0;
+  bool descs_dirty = true;
+  void* ws = nullptr;
+  size_t ws_bytes = 0;
+  void* io = nullptr;
+  size_t io_bytes = 0;
+  int sms = 0;
+  bool trace = false;
+  unsigned long long* d_trace = nullptr;
+  std::mutex mu;
+};
+
+namespace {
+
+int fail(negf_b200_ctx* ctx, int code, const std::string& msg) {
+  if (ctx) ctx->err = msg;
+  return code;
+}
+
+int cuda_fail(negf_b200_ctx* ctx, cudaError_t e, const char* where) {
+  return fail(ctx, NEGF_B200_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define CK(call)                                                        \
+  do {                                                                  \
+    cudaError_t e_ = (call);                                            \
+    if (e_ != cudaSuccess) return cuda_fail(ctx, e_, #call);            \
+  } while (0)
+
+int grow(negf_b200_ctx* ctx, void** p, size_t* cap, size_t need) {
+  if (need <= *cap) return NEGF_B200_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  cudaError_t e = cudaMalloc(p, need);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(ctx, NEGF_B200_ERR_NOMEM, "device allocation of " + std::to_string(need) + " bytes failed");
+  }
+  *cap = need;
+  return NEGF_B200_OK;
+}
+
+int sync_descs(negf_b200_ctx* ctx) {
+  if (!ctx->descs_dirty) return NEGF_B200_OK;
+  size_t need = std::max<size_t>(1, ctx->devs.size()) * sizeof(DevDesc);
+  int st = grow(ctx, reinterpret_cast<void**>(&ctx->d_descs), &ctx->d_descs_cap, need);
+  if (st) return st;
+  std::vector<DevDesc> h(ctx->devs.size());
+  for (size_t i = 0; i < ctx->devs.size(); ++i) h[i] = ctx->devs[i].desc;
+  if (!h.empty())
+    CK(cudaMemcpy(ctx->d_descs, h.data(), h.size() * sizeof(DevDesc), cudaMemcpyHostToDevice));
+  ctx->descs_dirty = false;
+  return NEGF_B200_OK;
+}
+
+struct LaunchShape {
+  int nmax = 0, nbl_max = 0, ncont_max = 0, norb_max = 0;
+};
+
+int shape_of(negf_b200_ctx* ctx, int npts, const int32_t* ids, LaunchShape& sh) {
+  for (int p = 0; p < npts; ++p) {
+    int id = ids ? ids[p] : -1;
+    if (ids && (id < 0 || id >= (int)ctx->devs.size() || !ctx->devs[id].live))
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "point " + std::to_string(p) + ": unknown device id " +
+                                                   std::to_string(id));
+  }
+  for (size_t i = 0; i < ctx->devs.size(); ++i) {
+    const DeviceRec& r = ctx->devs[i];
+    if (!r.live) continue;
+    sh.nmax = std::max(sh.nmax, r.nmax);
+    sh.nbl_max = std::max(sh.nbl_max, r.nbl);
+    sh.ncont_max = std::max(sh.ncont_max, r.ncont);
+    sh.norb_max = std::max(sh.norb_max, r.norb);
+  }
+  return NEGF_B200_OK;
+}
+
+int grid_for(negf_b200_ctx* ctx, int npts) {
+  int per_sm = ctx->opt.ctas_per_sm > 0 ? ctx->opt.ctas_per_sm : 2;
+  return std::max(1, std::min(npts, per_sm * ctx->sms));
+}
+
+// Runs one launch with device-resident inputs/outputs (all pointers device).
+int run_device(negf_b200_ctx* ctx, negf::EngineArgs a, const LaunchShape& sh, cudaStream_t s) {
+  if (sh.nmax > negf::kMaxOrder)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "block order " + std::to_string(sh.nmax) + " exceeds " +
+                                                std::to_string(negf::kMaxOrder));
+  int st = sync_descs(ctx);
+  if (st) return st;
+  const int grid = grid_for(ctx, a.npts);
+  const int64_t per = negf::engine_ws_elems(a.mode, sh.nbl_max, sh.ncont_max, sh.nmax);
+  // counter lives at the start of the workspace allocation
+  const size_t need = 256 + (size_t)grid * per * sizeof(double2);
+  st = grow(ctx, &ctx->ws, &ctx->ws_bytes, need);
+  if (st) return st;
+  a.counter = reinterpret_cast<int*>(ctx->ws);
+  a.ws = reinterpret_cast<double2*>(reinterpret_cast<char*>(ctx->ws) + 256);
+  a.ws_per_cta = per;
+  a.Q = (int64_t)sh.nmax * sh.nmax;
+  a.nmax = sh.nmax;
+  a.nbl_max = sh.nbl_max;
+  a.ncont_max = sh.ncont_max;
+  a.devs = ctx->d_descs;
+  a.trace = ctx->trace ? ctx->d_trace : nullptr;
+  CK(cudaMemsetAsync(a.counter, 0, sizeof(int), s));
+  cudaError_t e = negf::launch_engine(a, grid, s);
+  if (e != cudaSuccess) return cuda_fail(ctx, e, "launch_engine");
+  return NEGF_B200_OK;
+}
+
+negf::EngineArgs base_args(negf_b200_ctx* ctx, int mode, int npts) {
+  negf::EngineArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.mode = mode;
+  a.npts = npts;
+  a.sgf_tol = ctx->opt.sgf_tol;
+  a.sgf_max_iter = ctx->opt.sgf_max_iter;
+  a.eps = ctx->opt.eps_drop;
+  a.scba_niter = ctx->opt.scba_niter;
+  a.scba_tol = ctx->opt.scba_tol;
+  return a;
+}
+
+int first_status(const int32_t* status, int npts) {
+  for (int p = 0; p < npts; ++p)
+    if (status[p] != NEGF_B200_OK) return status[p];
+  return NEGF_B200_OK;
+}
+
+// Staging area carve-out on ctx->io
+struct Carve {
+  char* base;
+  size_t off = 0;
+  template <class T>
+  T* take(size_t n) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += n * sizeof(T);
+    return p;
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+void negf_b200_default_options(negf_b200_options* o) {
+  if (!o) return;
+  o->sgf_tol = 1e-9;
+  o->sgf_max_iter = 300;
+  o->eps_drop = 0.0;
+  o->scba_tol = 1e-7;
+  o->scba_niter = 0;
+  o->precision = 0;
+  o->ctas_per_sm = 0;
+}
+
+const char* negf_b200_version(void) { return "negf_b200 0.1 (sm_100a, complex FP64)"; }
+
+int negf_b200_ctx_create(int32_t cuda_device, negf_b200_ctx** out) {
+  if (!out) return NEGF_B200_ERR_BAD_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return NEGF_B200_ERR_NO_GPU;
+  }
+  if (cuda_device < 0 || cuda_device >= ndev) return NEGF_B200_ERR_BAD_ARG;
+  negf_b200_ctx* ctx = new negf_b200_ctx();
+  ctx->device = cuda_device;
+  negf_b200_default_options(&ctx->opt);
+  cudaError_t e = cudaSetDevice(cuda_device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->sms, cudaDevAttrMultiProcessorCount, cuda_device);
+  if (e != cudaSuccess) {
+    delete ctx;
+    return NEGF_B200_ERR_CUDA;
+  }
+  *out = ctx;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_ctx_destroy(negf_b200_ctx* ctx) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  cudaSetDevice(ctx->device);
+  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  for (auto& r : ctx->devs)
+    if (r.blob) cudaFree(r.blob);
+  if (ctx->d_descs) cudaFree(ctx->d_descs);
+  if (ctx->ws) cudaFree(ctx->ws);
+  if (ctx->io) cudaFree(ctx->io);
+  if (ctx->d_trace) cudaFree(ctx->d_trace);
+  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* o) {
+  if (!ctx || !o) return NEGF_B200_ERR_BAD_ARG;
+  if (o->sgf_tol <= 0.0 || o->sgf_max_iter < 1 || o->scba_niter < 0 || o->ctas_per_sm < 0 ||
+      o->ctas_per_sm > 2)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "invalid options");
+  if (o->precision != 0) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "only precision 0 (complex FP64) is built");
+  ctx->opt = *o;
+  return NEGF_B200_OK;
+}
+
+const char* negf_b200_last_error(const negf_b200_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_id) {
+  if (!ctx || !dv || !device_id) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  const int nbl = dv->nbl, ncont = dv->ncont;
+  if (nbl < 1 || !dv->pl_size || !dv->h_diag || (nbl > 1 && (!dv->h_upper || !dv->h_lower)))
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "device needs nbl >= 1 and H blocks");
+  if (ncont < 1 || ncont > negf::kMaxCont || !dv->cblk || !dv->lead_size || !dv->lead_h00 || !dv->lead_h01 ||
+      !dv->hmc)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "device needs 1..10 contacts with lead and coupling blocks");
+  const bool has_s = dv->s_diag != nullptr;
+  if (has_s && nbl > 1 && (!dv->s_upper || !dv->s_lower))
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "S blocks must be all given or all NULL");
+  std::vector<int32_t> pl(dv->pl_size, dv->pl_size + nbl), pstart(nbl);
+  std::vector<int64_t> od(nbl), oo(std::max(1, nbl - 1));
+  int64_t nd = 0, no = 0;
+  int norb = 0, nmax = 0;
+  for (int i = 0; i < nbl; ++i) {
+    if (pl[i] < 1) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "PL size must be >= 1");
+    pstart[i] = norb;
+    norb += pl[i];
+    nmax = std::max(nmax, pl[i]);
+    od[i] = nd;
+    nd += (int64_t)pl[i] * pl[i];
+    if (i + 1 < nbl) {
+      oo[i] = no;
+      no += (int64_t)pl[i] * pl[i + 1];
+    }
+  }
+  int64_t nl = 0, nm = 0;
+  std::vector<int64_t> olead(ncont), omc(ncont);
+  for (int c = 0; c < ncont; ++c) {
+    const int cb = dv->cblk[c], L = dv->lead_size[c];
+    if (cb < 1 || cb > nbl || L < 1)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "contact " + std::to_string(c + 1) + ": bad cblk or lead size");
+    nmax = std::max(nmax, L);
+    olead[c] = nl;
+    nl += (int64_t)L * L;
+    omc[c] = nm;
+    nm += (int64_t)pl[cb - 1] * L;
+  }
+  if (nmax > negf::kMaxOrder)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "block order above " + std::to_string(negf::kMaxOrder));
+  // blob layout (complex elements): hd sd | hu hl su sl | h00 h01 s00 s01 | hmc smc | ints
+  const int64_t ns = has_s ? 1 : 0;
+  const int64_t has00 = dv->lead_s00 ? 1 : 0, has01 = dv->lead_s01 ? 1 : 0, hasmc = dv->smc ? 1 : 0;
+  int64_t elems = nd * (1 + ns) + no * (2 + 2 * ns) + nl * (2 + has00 + has01) + nm * (1 + hasmc);
+  size_t bytes = (size_t)elems * 16 + (size_t)nbl * (4 + 4 + 8) + (size_t)std::max(1, nbl - 1) * 8 + 64;
+  int st;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  void* blob = nullptr;
+  if (cudaMalloc(&blob, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, NEGF_B200_ERR_NOMEM, "device allocation of the device description failed");
+  }
+  char* b = reinterpret_cast<char*>(blob);
+  size_t off = 0;
+  auto put = [&](const void* src, size_t nbytes) -> void* {
+    void* dst = b + off;
+    off += (nbytes + 15) & ~size_t(15);
+    if (src && nbytes) cudaMemcpy(dst, src, nbytes, cudaMemcpyHostToDevice);
+    return dst;
+  };
+  DevDesc d{};
+  d.nbl = nbl; d.ncont = ncont; d.norb = norb; d.has_s = has_s ? 1 : 0;
+  d.has_s00 = (int)has00; d.has_s01 = (int)has01; d.has_smc = (int)hasmc;
+  d.hd = (const double2*)put(dv->h_diag, nd * 16);
+  d.sd = has_s ? (const double2*)put(dv->s_diag, nd * 16) : nullptr;
+  d.hu = (const double2*)put(nbl > 1 ? dv->h_upper : nullptr, no * 16);
+  d.hl = (const double2*)put(nbl > 1 ? dv->h_lower : nullptr, no * 16);
+  d.su = has_s ? (const double2*)put(nbl > 1 ? dv->s_upper : nullptr, no * 16) : nullptr;
+  d.sl = has_s ? (const double2*)put(nbl > 1 ? dv->s_lower : nullptr, no * 16) : nullptr;
+  d.h00 = (const double2*)put(dv->lead_h00, nl * 16);
+  d.h01 = (const double2*)put(dv->lead_h01, nl * 16);
+  d.s00 = has00 ? (const double2*)put(dv->lead_s00, nl * 16) : nullptr;
+  d.s01 = has01 ? (const double2*)put(dv->lead_s01, nl * 16) : nullptr;
+  d.hmc = (const double2*)put(dv->hmc, nm * 16);
+  d.smc = hasmc ? (const double2*)put(dv->smc, nm * 16) : nullptr;
+  d.pl = (const int*)put(pl.data(), nbl * 4);
+  d.pstart = (const int*)put(pstart.data(), nbl * 4);
+  d.od = (const int64_t*)put(od.data(), nbl * 8);
+  d.oo = (const int64_t*)put(oo.data(), oo.size() * 8);
+  for (int c = 0; c < ncont; ++c) {
+    d.cblk[c] = dv->cblk[c];
+    d.L[c] = dv->lead_size[c];
+    d.olead[c] = olead[c];
+    d.omc[c] = omc[c];
+  }
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess || off > bytes) {
+    cudaFree(blob);
+    return fail(ctx, NEGF_B200_ERR_CUDA, "upload of the device description failed");
+  }
+  DeviceRec r;
+  r.live = true; r.blob = blob; r.bytes = bytes; r.desc = d;
+  r.nbl = nbl; r.ncont = ncont; r.norb = norb; r.nmax = nmax; r.has_s = has_s;
+  for (int c = 0; c < ncont; ++c) r.cblk[c] = dv->cblk[c];
+  int id = -1;
+  for (size_t i = 0; i < ctx->devs.size(); ++i)
+    if (!ctx->devs[i].live) { id = (int)i; break; }
+  if (id < 0) { id = (int)ctx->devs.size(); ctx->devs.push_back(r); } else ctx->devs[id] = r;
+  ctx->descs_dirty = true;
+  *device_id = id;
+  (void)st;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_release_device(negf_b200_ctx* ctx, int32_t id) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (id < 0 || id >= (int)ctx->devs.size() || !ctx->devs[id].live)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaFree(ctx->devs[id].blob);
+  ctx->devs[id] = DeviceRec();
+  ctx->descs_dirty = true;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_device_bytes(const negf_b200_ctx* ctx, int32_t id, size_t* bytes) {
+  if (!ctx || !bytes || id < 0 || id >= (int)ctx->devs.size() || !ctx->devs[id].live)
+    return NEGF_B200_ERR_BAD_ARG;
+  *bytes = ctx->devs[id].bytes;
+  return NEGF_B200_OK;
+}
+
+// ---- host-buffer solves ----------------------------------------------------
+static int check_pair(negf_b200_ctx* ctx, int npts, const int32_t* ids, int ni, int nf) {
+  for (int p = 0; p < npts; ++p) {
+    const DeviceRec& r = ctx->devs[ids[p]];
+    if (ni < 1 || nf < 1 || ni > r.ncont || nf > r.ncont || (r.ncont > 1 && ni == nf))
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "contact pair (ni, nf) outside 1..ncont");
+  }
+  return NEGF_B200_OK;
+}
+
+static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t* ids, const double* E,
+                      double eta, double dos_delta, int32_t ni, int32_t nf, double* T, double* dos, int32_t* ncyc,
+                      int32_t* status, const double* frm, const double* coupling, double* curr, double* lcurr,
+                      double* ldens, int32_t* scba_iter, double* scba_err) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  if (npts < 0 || (npts > 0 && (!ids || !E))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
+  if (npts == 0) return NEGF_B200_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  LaunchShape sh;
+  int st = shape_of(ctx, npts, ids, sh);
+  if (st) return st;
+  int ncont_pts = 0, nbl_pts = 0, norb_pts = 0;
+  for (int p = 0; p < npts; ++p) {
+    const DeviceRec& r = ctx->devs[ids[p]];
+    ncont_pts = std::max(ncont_pts, r.ncont);
+    nbl_pts = std::max(nbl_pts, r.nbl);
+    norb_pts = std::max(norb_pts, r.norb);
+  }
+  if (mode != negf::MODE_GN) {
+    st = check_pair(ctx, npts, ids, ni, nf);
+    if (st) return st;
+  } else {
+    for (int p = 0; p < npts; ++p)
+      if (ctx->devs[ids[p]].nbl < 2) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the Gn solve needs nbl >= 2");
+    if (!frm) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "frm is required");
+  }
+  // staging
+  size_t need = 0;
+  {
+    Carve c{nullptr};
+    c.take<int32_t>(npts); c.take<double>(npts); c.take<double>(npts); c.take<int32_t>(npts);
+    c.take<int32_t>(npts);
+    if (dos) c.take<double>((size_t)npts * norb_pts);
+    if (frm) c.take<double>((size_t)npts * ncont_pts);
+    if (coupling) c.take<double>((size_t)norb_pts);
+    if (curr) c.take<double>((size_t)npts * ncont_pts);
+    if (lcurr) c.take<double>((size_t)npts * std::max(1, nbl_pts - 1));
+    if (ldens) c.take<double>((size_t)npts * nbl_pts);
+    c.take<int32_t>(npts); c.take<double>(npts);
+    need = c.off + 256;
+  }
+  st = grow(ctx, &ctx->io, &ctx->io_bytes, need);
+  if (st) return st;
+  Carve c{reinterpret_cast<char*>(ctx->io)};
+  int32_t* d_ids = c.take<int32_t>(npts);
+  double* d_E = c.take<double>(npts);
+  double* d_T = c.take<double>(npts);
+  int32_t* d_ncyc = c.take<int32_t>(npts);
+  int32_t* d_st = c.take<int32_t>(npts);
+  double* d_dos = dos ? c.take<double>((size_t)npts * norb_pts) : nullptr;
+  double* d_frm = frm ? c.take<double>((size_t)npts * ncont_pts) : nullptr;
+  double* d_cpl = coupling ? c.take<double>((size_t)norb_pts) : nullptr;
+  double* d_curr = curr ? c.take<double>((size_t)npts * ncont_pts) : nullptr;
+  double* d_lcurr = lcurr ? c.take<double>((size_t)npts * std::max(1, nbl_pts - 1)) : nullptr;
+  double* d_ldens = ldens ? c.take<double>((size_t)npts * nbl_pts) : nullptr;
+  int32_t* d_it = c.take<int32_t>(npts);
+  double* d_err = c.take<double>(npts);
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(d_ids, ids, npts * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_E, E, npts * 8, cudaMemcpyHostToDevice, s));
+  if (d_frm) CK(cudaMemcpyAsync(d_frm, frm, (size_t)npts * ncont_pts * 8, cudaMemcpyHostToDevice, s));
+  if (d_cpl) CK(cudaMemcpyAsync(d_cpl, coupling, (size_t)norb_pts * 8, cudaMemcpyHostToDevice, s));
+  negf::EngineArgs a = base_args(ctx, mode, npts);
+  a.dev_id = d_ids; a.energy = d_E; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
+  a.T = d_T; a.ncyc = d_ncyc; a.status = d_st;
+  a.dos = d_dos; a.dos_stride = norb_pts;
+  a.frm = d_frm; a.frm_stride = ncont_pts; a.coupling = d_cpl;
+  a.curr = d_curr; a.curr_stride = ncont_pts;
+  a.lcurr = d_lcurr; a.lcurr_stride = std::max(1, nbl_pts - 1);
+  a.ldens = d_ldens; a.ldens_stride = nbl_pts;
+  a.scba_iter = d_it; a.scba_err = d_err;
+  st = run_device(ctx, a, sh, s);
+  if (st) return st;
+  std::vector<int32_t> hst(npts);
+  if (T) CK(cudaMemcpyAsync(T, d_T, npts * 8, cudaMemcpyDeviceToHost, s));
+  if (ncyc) CK(cudaMemcpyAsync(ncyc, d_ncyc, npts * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
+  if (dos) CK(cudaMemcpyAsync(dos, d_dos, (size_t)npts * norb_pts * 8, cudaMemcpyDeviceToHost, s));
+  if (curr) CK(cudaMemcpyAsync(curr, d_curr, (size_t)npts * ncont_pts * 8, cudaMemcpyDeviceToHost, s));
+  if (lcurr)
+    CK(cudaMemcpyAsync(lcurr, d_lcurr, (size_t)npts * std::max(1, nbl_pts - 1) * 8, cudaMemcpyDeviceToHost, s));
+  if (ldens) CK(cudaMemcpyAsync(ldens, d_ldens, (size_t)npts * nbl_pts * 8, cudaMemcpyDeviceToHost, s));
+  if (scba_iter) CK(cudaMemcpyAsync(scba_iter, d_it, npts * 4, cudaMemcpyDeviceToHost, s));
+  if (scba_err) CK(cudaMemcpyAsync(scba_err, d_err, npts * 8, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (status) std::memcpy(status, hst.data(), npts * 4);
+  return first_status(hst.data(), npts);
+}
+
+int negf_b200_transmission(negf_b200_ctx* ctx, int32_t npts, const int32_t* device_id, const double* energy,
+                           double eta, int32_t ni, int32_t nf, double* T, int32_t* ncyc, int32_t* status) {
+  return solve_host(ctx, negf::MODE_T, npts, device_id, energy, eta, 0.0, ni, nf, T, nullptr, ncyc, status,
+                    nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+}
+
+int negf_b200_transmission_dos(negf_b200_ctx* ctx, int32_t npts, const int32_t* device_id, const double* energy,
+                               double eta, double dos_delta, int32_t ni, int32_t nf, double* T, double* dos,
+                               int32_t* ncyc, int32_t* status) {
+  return solve_host(ctx, negf::MODE_DOS, npts, device_id, energy, eta, dos_delta, ni, nf, T, dos, ncyc, status,
+                    nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+}
+
+int negf_b200_meir_wingreen(negf_b200_ctx* ctx, int32_t npts, const int32_t* device_id, const double* energy,
+                            double eta, const double* frm, const double* coupling, double* curr,
+                            double* layer_curr, double* layer_dens, int32_t* scba_iter, double* scba_err,
+                            int32_t* ncyc, int32_t* status) {
+  return solve_host(ctx, negf::MODE_GN, npts, device_id, energy, eta, 0.0, 1, 2, nullptr, nullptr, ncyc, status,
+                    frm, coupling, curr, layer_curr, layer_dens, scba_iter, scba_err);
+}
+
+// ---- device-pointer solve (inputs already resident in HBM) ------------------
+int negf_b200_transmission_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_device_id,
+                               const double* d_energy, double eta, int32_t ni, int32_t nf, double* d_T,
+                               int32_t* d_ncyc, int32_t* d_status, void* stream) {
+  if (!ctx || npts < 0) return NEGF_B200_ERR_BAD_ARG;
+  if (npts == 0) return NEGF_B200_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  LaunchShape sh;
+  int st = shape_of(ctx, npts, nullptr, sh);
+  if (st) return st;
+  negf::EngineArgs a = base_args(ctx, negf::MODE_T, npts);
+  a.dev_id = d_device_id; a.energy = d_energy; a.eta = eta; a.ni = ni; a.nf = nf;
+  a.T = d_T; a.ncyc = d_ncyc; a.status = d_status;
+  return run_device(ctx, a, sh, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+int negf_b200_transmission_dos_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_device_id,
+                                   const double* d_energy, double eta, double dos_delta, int32_t ni, int32_t nf,
+                                   double* d_T, double* d_dos, int64_t dos_stride, int32_t* d_ncyc,
+                                   int32_t* d_status, void* stream) {
+  if (!ctx || npts < 0) return NEGF_B200_ERR_BAD_ARG;
+  if (npts == 0) return NEGF_B200_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  LaunchShape sh;
+  int st = shape_of(ctx, npts, nullptr, sh);
+  if (st) return st;
+  negf::EngineArgs a = base_args(ctx, negf::MODE_DOS, npts);
+  a.dev_id = d_device_id; a.energy = d_energy; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
+  a.T = d_T; a.dos = d_dos; a.dos_stride = dos_stride; a.ncyc = d_ncyc; a.status = d_status;
+  return run_device(ctx, a, sh, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+// ---- tracing ----------------------------------------------------------------
+int negf_b200_set_tracing(negf_b200_ctx* ctx, int32_t enable) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  if (enable && !ctx->d_trace) {
+    if (cudaMalloc(&ctx->d_trace, NEGF_B200_TRACE_NPHASE * sizeof(unsigned long long)) != cudaSuccess) {
+      cudaGetLastError();
+      ctx->d_trace = nullptr;
+      return fail(ctx, NEGF_B200_ERR_NOMEM, "trace buffer");
+    }
+    CK(cudaMemset(ctx->d_trace, 0, NEGF_B200_TRACE_NPHASE * sizeof(unsigned long long)));
+  }
+  ctx->trace = enable != 0;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_get_trace(negf_b200_ctx* ctx, uint64_t* cycles) {
+  if (!ctx || !cycles) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  std::memset(cycles, 0, NEGF_B200_TRACE_NPHASE * sizeof(uint64_t));
+  if (!ctx->d_trace) return NEGF_B200_OK;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  CK(cudaDeviceSynchronize());
+  CK(cudaMemcpy(cycles, ctx->d_trace, NEGF_B200_TRACE_NPHASE * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+  CK(cudaMemset(ctx->d_trace, 0, NEGF_B200_TRACE_NPHASE * sizeof(unsigned long long)));
+  return NEGF_B200_OK;
+}
+
+// ---- primitives -------------------------------------------------------------
+int negf_b200_zgemm_batched(int32_t batch, int32_t m, int32_t n, int32_t k, const double* alpha, const double* A,
+                            int64_t strideA, const double* B, int64_t strideB, const double* beta, double* C,
+                            int64_t strideC, int32_t dagger, void* stream) {
+  if (batch < 0 || m < 0 || n < 0 || k < 0 || !alpha || !beta || (dagger < 0 || dagger > 2))
+    return NEGF_B200_ERR_BAD_ARG;
+  if (batch == 0 || m == 0 || n == 0) return NEGF_B200_OK;
+  if (!A || !B || !C) return NEGF_B200_ERR_BAD_ARG;
+  cudaError_t e = negf::launch_zgemm_batched(
+      batch, m, n, k, make_double2(alpha[0], alpha[1]), (const double2*)A, strideA / 2, (const double2*)B,
+      strideB / 2, make_double2(beta[0], beta[1]), (double2*)C, strideC / 2, dagger, (cudaStream_t)stream);
+  return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;
+}
+
+size_t negf_b200_zinv_work_bytes(int32_t batch, int32_t n) {
+  if (batch <= 0 || n <= 0) return 0;
+  return (size_t)batch * negf::zinv_batched_work_elems(n) * 16 + 16;
+}
+
+int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A, double* Ainv, int32_t* info, void* work,
+                           void* stream) {
+  if (batch < 0 || n < 0 || n > negf::kMaxOrder) return NEGF_B200_ERR_BAD_ARG;
+  if (batch == 0 || n == 0) return NEGF_B200_OK;
+  if (!A || !Ainv || (negf::zinv_batched_work_elems(n) > 0 && !work)) return NEGF_B200_ERR_BAD_ARG;
+  cudaError_t e = negf::launch_zinv_batched(batch, n, (const double2*)A, (double2*)Ainv, info, (double2*)work,
+                                            (cudaStream_t)stream);
+  return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;
+}
+
+size_t negf_b200_decimation_work_bytes(int32_t batch, int32_t n) {
+  if (batch <= 0 || n <= 0) return 0;
+  return (size_t)batch * negf::decimation_batched_work_elems(n) * 16 + 16;
+}
+
+int negf_b200_decimation_batched(int32_t batch, int32_t n, const double* Ao, const double* Bo, const double* Co,
+                                 double* Go, int32_t* ncyc, double tol, int32_t max_iter, void* work,
+                                 void* stream) {
+  if (batch < 0 || n < 0 || n > negf::kMaxOrder || tol <= 0.0 || max_iter < 1) return NEGF_B200_ERR_BAD_ARG;
+  if (batch == 0 || n == 0) return NEGF_B200_OK;
+  if (!Ao || !Bo || !Co || !Go || !work) return NEGF_B200_ERR_BAD_ARG;
+  cudaError_t e = negf::launch_decimation_batched(batch, n, (const double2*)Ao, (const double2*)Bo,
+                                                  (const double2*)Co, (double2*)Go, ncyc, tol, max_iter,
+                                                  (double2*)work, (cudaStream_t)stream);
+  return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,568 @@
+// CTA-level complex128 block operations for sm_100a.
+//
+// Every routine here is executed cooperatively by all threads of one CTA on
+// blocks that live in global memory (HBM, L2-resident while hot).  They are
+// the building blocks of the persistent per-energy-point engine: one CTA
+// owns one (energy, k) point at a time and runs its whole recursive
+// Green's-function solve with these operations.
+//
+//   cta_gemm  C = epilogue(op(A) op(B)) on the FP64 tensor pipe
+//             (mma.sync m16n8k4 .f64, 4 real products per complex product),
+//             operands staged through shared memory with cp.async.
+//   cta_zinv  in-place-style blocked Gauss-Jordan inversion with partial
+//             pivoting (pivot = max |Re|+|Im|, the izamax rule of zgetrf):
+//             panel factorisation in shared memory, trailing update as a
+//             gathered GEMM on the tensor pipe, out-of-place ping-pong so
+//             that row interchanges need no in-place hazards.
+//
+// Layout: column-major complex128 (double2 = {re, im}), leading dimension
+// = number of rows, the layout of libNEGF's z_DNS%val.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace negf {
+
+constexpr int kThreads = 256;          // threads per CTA (8 warps)
+constexpr int TM = 64, TN = 64, TK = 16;
+constexpr int A_LD = TM + 2;           // sA[k][m], padded: conflict-free fragment loads
+constexpr int B_LD = TK + 4;           // sB[n][k]
+constexpr int kGemmSmemBytes = 2 * (TK * A_LD + TN * B_LD) * 16;
+constexpr int kSmallInvMax = 64;       // n <= 64: whole matrix in shared memory
+
+// ---------------------------------------------------------------- complex
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+// 1/z by Smith's algorithm (scaled, avoids overflow for large |z|)
+__device__ __forceinline__ double2 crecip(double2 z) {
+  if (fabs(z.x) >= fabs(z.y)) {
+    double r = z.y / z.x, den = z.x + z.y * r;
+    return make_double2(1.0 / den, -r / den);
+  } else {
+    double r = z.x / z.y, den = z.y + z.x * r;
+    return make_double2(r / den, -1.0 / den);
+  }
+}
+__device__ __forceinline__ double cabs1(double2 z) { return fabs(z.x) + fabs(z.y); }
+__device__ __forceinline__ double cabs(double2 z) { return hypot(z.x, z.y); }
+
+// ---------------------------------------------------------------- async copy
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, bool valid) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(sdst)),
+               "l"(gsrc), "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma_16x8x4(double (&d)[4], double a0, double a1, double b0) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+      "{%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a0), "d"(a1), "d"(b0));
+}
+
+// ---------------------------------------------------------------- operands
+enum OpMode : int {
+  OP_N = 0,       // X(r,c) = p[r + c*ld]
+  OP_C = 1,       // X(r,c) = conj(p[c + r*ld])   (conjugate transpose)
+  OP_GATHER = 2,  // X(r,c) = p[perm[r] + c*ld]   (row gather, perm in smem)
+};
+
+struct Operand {
+  const double2* p;
+  int ld;
+  int mode;
+  const int* perm;  // OP_GATHER only (shared memory), already offset
+};
+
+__device__ __forceinline__ Operand opN(const double2* p, int ld) { return Operand{p, ld, OP_N, nullptr}; }
+__device__ __forceinline__ Operand opC(const double2* p, int ld) { return Operand{p, ld, OP_C, nullptr}; }
+
+// ---------------------------------------------------------------- epilogues
+enum EpiMode : int {
+  EPI_STORE = 0,   // C = alpha*acc + beta*C   (beta==0: C not read)
+  EPI_GJ = 1,      // Gauss-Jordan trailing update (see cta_zinv)
+};
+
+struct Epilogue {
+  int mode;
+  double2* C;
+  int ldc;
+  double2 alpha, beta;
+  // EPI_GJ
+  const double2* xcur;  // previous iterate, read with row permutation
+  int ldx;
+  const int* perm;      // smem, full-length row permutation of this panel
+  const double2* W;     // panel (n x jb), ld = n
+  int k0, jb;
+  // optional reduction of max |C| over stored elements
+  double* maxabs;       // smem accumulator (nullptr = off)
+};
+
+__device__ __forceinline__ Epilogue epi_store(double2* C, int ldc, double2 alpha, double2 beta) {
+  Epilogue e;
+  e.mode = EPI_STORE; e.C = C; e.ldc = ldc; e.alpha = alpha; e.beta = beta;
+  e.xcur = nullptr; e.ldx = 0; e.perm = nullptr; e.W = nullptr; e.k0 = 0; e.jb = 0;
+  e.maxabs = nullptr;
+  return e;
+}
+
+// ---------------------------------------------------------------- tile loads
+// A tile: rows [m0, m0+TM) x cols [k0, k0+TK) of op(A) (M x K) into sA[k][m]
+__device__ __forceinline__ void load_a_tile(const Operand& A, int M, int K, int m0, int k0, double2* sA) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < (TM * TK) / kThreads; ++j) {
+    int idx = tid + j * kThreads;
+    int m, k;
+    const double2* src;
+    bool ok;
+    if (A.mode == OP_C) {
+      k = idx & (TK - 1); m = idx / TK;
+      ok = (m0 + m < M) && (k0 + k < K);
+      src = ok ? A.p + (size_t)(k0 + k) + (size_t)(m0 + m) * A.ld : A.p;
+    } else {
+      m = idx & (TM - 1); k = idx / TM;
+      ok = (m0 + m < M) && (k0 + k < K);
+      int row = (A.mode == OP_GATHER && ok) ? A.perm[m0 + m] : m0 + m;
+      src = ok ? A.p + (size_t)row + (size_t)(k0 + k) * A.ld : A.p;
+    }
+    cp_async16(&sA[k * A_LD + m], src, ok);
+  }
+}
+
+// B tile: rows [k0, k0+TK) x cols [n0, n0+TN) of op(B) (K x N) into sB[n][k]
+__device__ __forceinline__ void load_b_tile(const Operand& B, int K, int N, int k0, int n0, double2* sB) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int j = 0; j < (TK * TN) / kThreads; ++j) {
+    int idx = tid + j * kThreads;
+    int k, n;
+    const double2* src;
+    bool ok;
+    if (B.mode == OP_C) {
+      n = idx & (TN - 1); k = idx / TN;
+      ok = (k0 + k < K) && (n0 + n < N);
+      src = ok ? B.p + (size_t)(n0 + n) + (size_t)(k0 + k) * B.ld : B.p;
+    } else {
+      k = idx & (TK - 1); n = idx / TK;
+      ok = (k0 + k < K) && (n0 + n < N);
+      int row = (B.mode == OP_GATHER && ok) ? B.perm[k0 + k] : k0 + k;
+      src = ok ? B.p + (size_t)row + (size_t)(n0 + n) * B.ld : B.p;
+    }
+    cp_async16(&sB[n * B_LD + k], src, ok);
+  }
+}
+
+// ---------------------------------------------------------------- epilogue
+__device__ __forceinline__ void epi_apply(const Epilogue& e, int r, int c, double re, double im, int M,
+                                          int N, double& lmax) {
+  if (r >= M || c >= N) return;
+  double2 out;
+  if (e.mode == EPI_STORE) {
+    out = make_double2(e.alpha.x * re - e.alpha.y * im, e.alpha.x * im + e.alpha.y * re);
+    if (e.beta.x != 0.0 || e.beta.y != 0.0) out = cadd(out, cmul(e.beta, e.C[(size_t)r + (size_t)c * e.ldc]));
+  } else {  // EPI_GJ
+    if (c >= e.k0 && c < e.k0 + e.jb) {
+      out = e.W[(size_t)r + (size_t)(c - e.k0) * M];
+    } else {
+      out = make_double2(re, im);
+      if (r < e.k0 || r >= e.k0 + e.jb) out = cadd(out, e.xcur[(size_t)e.perm[r] + (size_t)c * e.ldx]);
+    }
+  }
+  e.C[(size_t)r + (size_t)c * e.ldc] = out;
+  lmax = fmax(lmax, cabs(out));
+}
+
+// ---------------------------------------------------------------- GEMM
+// C(MxN) = epilogue( op(A)(MxK) * op(B)(KxN) ).  All threads of the CTA must
+// call it.  `smem` must hold kGemmSmemBytes.  Ends with __syncthreads().
+__device__ __noinline__ void cta_gemm(int M, int N, int K, const Operand& A, const Operand& B, const Epilogue& e,
+                         double2* smem) {
+  double2* sA0 = smem;
+  double2* sA1 = sA0 + TK * A_LD;
+  double2* sB0 = sA1 + TK * A_LD;
+  double2* sB1 = sB0 + TN * B_LD;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = warp & 1, wn = warp >> 1;
+  const double ca = (A.mode == OP_C) ? -1.0 : 1.0;
+  const double cb = (B.mode == OP_C) ? -1.0 : 1.0;
+  const int tilesM = (M + TM - 1) / TM, tilesN = (N + TN - 1) / TN;
+  const int nk = (K + TK - 1) / TK;
+  double lmax = 0.0;
+
+  for (int tile = 0; tile < tilesM * tilesN; ++tile) {
+    const int m0 = (tile % tilesM) * TM, n0 = (tile / tilesM) * TN;
+    double accR[2][2][4], accI[2][2][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) { accR[i][j][q] = 0.0; accI[i][j][q] = 0.0; }
+
+    if (nk > 0) {
+      load_a_tile(A, M, K, m0, 0, sA0);
+      load_b_tile(B, K, N, 0, n0, sB0);
+      cp_async_commit();
+    }
+    for (int kt = 0; kt < nk; ++kt) {
+      double2* sA = (kt & 1) ? sA1 : sA0;
+      double2* sB = (kt & 1) ? sB1 : sB0;
+      if (kt + 1 < nk) {
+        load_a_tile(A, M, K, m0, (kt + 1) * TK, (kt & 1) ? sA0 : sA1);
+        load_b_tile(B, K, N, (kt + 1) * TK, n0, (kt & 1) ? sB0 : sB1);
+        cp_async_commit();
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+      __syncthreads();
+#pragma unroll
+      for (int ks = 0; ks < TK / 4; ++ks) {
+        const int k = ks * 4 + t;
+        double are[2][2], aim[2][2], nai[2][2], bre[2], bim[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+          const int r0 = wm * 32 + i * 16 + g;
+          double2 v0 = sA[k * A_LD + r0];
+          double2 v1 = sA[k * A_LD + r0 + 8];
+          are[i][0] = v0.x; are[i][1] = v1.x;
+          aim[i][0] = ca * v0.y; aim[i][1] = ca * v1.y;
+          nai[i][0] = -aim[i][0]; nai[i][1] = -aim[i][1];
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+          const int c = wn * 16 + j * 8 + g;
+          double2 v = sB[c * B_LD + k];
+          bre[j] = v.x; bim[j] = cb * v.y;
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+          for (int j = 0; j < 2; ++j) {
+            dmma_16x8x4(accR[i][j], are[i][0], are[i][1], bre[j]);
+            dmma_16x8x4(accR[i][j], nai[i][0], nai[i][1], bim[j]);
+            dmma_16x8x4(accI[i][j], are[i][0], are[i][1], bim[j]);
+            dmma_16x8x4(accI[i][j], aim[i][0], aim[i][1], bre[j]);
+          }
+      }
+      __syncthreads();
+    }
+    // epilogue
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int r = m0 + wm * 32 + i * 16 + g + ((q >> 1) << 3);
+          const int c = n0 + wn * 16 + j * 8 + 2 * t + (q & 1);
+          epi_apply(e, r, c, accR[i][j][q], accI[i][j][q], M, N, lmax);
+        }
+  }
+  if (e.maxabs) {
+    // warp max then one atomic per warp on the shared accumulator
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
+    if (lane == 0) {
+      unsigned long long* a = reinterpret_cast<unsigned long long*>(e.maxabs);
+      atomicMax(a, (unsigned long long)__double_as_longlong(lmax));  // lmax >= 0: bit order == value order
+    }
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- elementwise
+// All loops stride by blockDim; callers __syncthreads() between dependent ops.
+
+// D(r,c) = s_e * S(r,c) - H(r,c)  (S == nullptr: identity if diag else zero)
+// optionally minus a full block `sub` (contact self-energy) and minus a
+// diagonal vector `subdiag` (dephasing sigma_r).  op == OP_C builds the
+// conjugate transpose of (s_e*S - H) instead (rows/cols refer to the result).
+__device__ __noinline__ void cta_esh(double2* D, int rows, int cols, const double2* H, const double2* S, double2 s_e,
+                        bool diag, const double2* sub, const double2* subdiag, int op) {
+  const int n = rows * cols;
+  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+    const int r = idx % rows, c = idx / rows;
+    // source element of the un-transposed matrix
+    const int sr = (op == OP_C) ? c : r, sc = (op == OP_C) ? r : c;
+    const int sld = (op == OP_C) ? cols : rows;
+    const size_t s = (size_t)sr + (size_t)sc * sld;
+    double2 sv = S ? S[s] : make_double2((diag && sr == sc) ? 1.0 : 0.0, 0.0);
+    double2 v = csub(cmul(s_e, sv), H[s]);
+    if (op == OP_C) v = cconj(v);
+    if (sub) v = csub(v, sub[idx]);
+    if (subdiag && r == c) v = csub(v, subdiag[r]);
+    D[idx] = v;
+  }
+}
+
+__device__ void cta_copy(double2* D, const double2* S, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) D[i] = S[i];
+}
+
+// D = i*(A - A^dag)   (zspectral_dns), A square n x n
+__device__ void cta_spectral(double2* D, const double2* A, int n) {
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int r = idx % n, c = idx / n;
+    double2 a = A[idx], b = cconj(A[(size_t)c + (size_t)r * n]);
+    double2 d = csub(a, b);
+    D[idx] = make_double2(-d.y, d.x);
+  }
+}
+
+// block-wide sum of doubles, result valid in all threads; `red` smem >= 32 doubles
+__device__ double cta_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[w];
+  __syncthreads();
+  return s;
+}
+
+__device__ double cta_max(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double s = 0.0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s = fmax(s, red[w]);
+  __syncthreads();
+  return s;
+}
+
+// Re Tr(X Y) = sum_{i,j} Re(X(i,j) Y(j,i)); op applies to Y (OP_C: Y = Z^dag)
+__device__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red) {
+  double acc = 0.0;
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int i = idx % n, j = idx / n;
+    double2 x = X[idx];
+    double2 y = (opY == OP_C) ? cconj(Y[(size_t)i + (size_t)j * n]) : Y[(size_t)j + (size_t)i * n];
+    acc += x.x * y.x - x.y * y.y;
+  }
+  return cta_sum(acc, red);
+}
+
+// ---------------------------------------------------------------- tracing
+// Per-CTA cycle accumulators (shared memory, thread 0 writes), summed into a
+// global array at kernel exit when tracing is on.
+enum TracePhase : int {
+  TR_GEMM = 0,        // sweep / decimation / self-energy products
+  TR_INV_PANEL = 1,   // Gauss-Jordan panel factorisation (pivoting)
+  TR_INV_UPDATE = 2,  // Gauss-Jordan trailing update (tensor-pipe GEMM)
+  TR_INV_OTHER = 3,   // inversion copies / final column permutation
+  TR_ELEM = 4,        // ES-H assembly and other elementwise passes
+  TR_TOTAL = 5,       // whole kernel, per CTA
+  TR_POINTS = 6,      // points processed (count, not cycles)
+  TR_NPHASE = 8,
+};
+
+struct Trace {
+  long long* acc;  // smem [TR_NPHASE] or nullptr
+  __device__ __forceinline__ long long start() const { return acc ? clock64() : 0; }
+  __device__ __forceinline__ void stop(int ph, long long t0) const {
+    if (acc && threadIdx.x == 0) acc[ph] += clock64() - t0;
+  }
+};
+
+// ---------------------------------------------------------------- inversion
+// Shared-memory scratch of cta_zinv (besides the GEMM staging area).
+struct InvScratch {
+  int* piv;    // n
+  int* perm;   // n
+  int* cperm;  // n
+  double* redv; int* redi;  // >= 32 each
+  int* flag;   // info
+  Trace tr;
+};
+
+// Pivot search on a column in shared memory: rows [j, n) of col[] -> index
+// of max |Re|+|Im| (first occurrence, as izamax).  All threads call.
+__device__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double best = -1.0;
+  int bi = n;
+  for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
+    double v = cabs1(col[i]);
+    if (v > best) { best = v; bi = i; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    double ov = __shfl_xor_sync(0xffffffffu, best, o);
+    int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+  }
+  if (lane == 0) { s.redv[warp] = best; s.redi[warp] = bi; }
+  __syncthreads();
+  best = s.redv[0]; bi = s.redi[0];
+  for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+    double ov = s.redv[w];
+    int oi = s.redi[w];
+    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+  }
+  __syncthreads();
+  return bi;
+}
+
+// One Gauss-Jordan step on a column panel P (n rows x w cols, ld = n) held in
+// shared memory: pivot row j (global row index), panel column jj.
+// f[] is an n-vector of scratch.  Returns the pivot row chosen.
+__device__ __noinline__ int gj_step(double2* P, int n, int w, int j, int jj, double2* f, InvScratch& s, int* info) {
+  double2* colj = P + (size_t)jj * n;
+  int p = cta_pivot(colj, j, n, s);
+  if (p >= n) p = j;
+  // swap rows j and p across the panel
+  if (p != j)
+    for (int c = threadIdx.x; c < w; c += blockDim.x) {
+      double2 a = P[j + (size_t)c * n], b = P[p + (size_t)c * n];
+      P[j + (size_t)c * n] = b; P[p + (size_t)c * n] = a;
+    }
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x) f[i] = colj[i];
+  __syncthreads();
+  double2 piv = f[j];
+  if (piv.x == 0.0 && piv.y == 0.0 && threadIdx.x == 0 && *info == 0) *info = j + 1;
+  const double2 d = crecip(piv);
+  for (int c = threadIdx.x; c < w; c += blockDim.x)
+    P[j + (size_t)c * n] = (c == jj) ? d : cmul(P[j + (size_t)c * n], d);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < n * w; idx += blockDim.x) {
+    const int i = idx % n, c = idx / n;
+    if (i == j) continue;
+    if (c == jj) P[idx] = make_double2(-(f[i].x * d.x - f[i].y * d.y), -(f[i].x * d.y + f[i].y * d.x));
+    else P[idx] = csub(P[idx], cmul(f[i], P[j + (size_t)c * n]));
+  }
+  __syncthreads();
+  return p;
+}
+
+// Panel width of the blocked path for an n x n inversion within `smem_bytes`
+__host__ __device__ inline int zinv_panel(int n, int smem_bytes) {
+  int jb = 32;
+  while (jb > 4 && (size_t)n * (jb + 1) * 16 > (size_t)smem_bytes) jb >>= 1;
+  return jb;
+}
+
+// Workspace (complex elements) for cta_zinv of order n.
+__host__ __device__ inline size_t zinv_ws_elems(int n, int smem_bytes) {
+  if (n <= kSmallInvMax) return 0;
+  return 2 * (size_t)n * n + (size_t)n * zinv_panel(n, smem_bytes);
+}
+
+// out = A^-1 (n x n).  A is read only (out may alias A).  `ws` holds
+// zinv_ws_elems(n) elements.  `smem` holds smem_bytes.  Returns info
+// (0 or the 1-based column of the first exactly-zero pivot) in all threads.
+__device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, double2* ws, double2* smem, int smem_bytes,
+                        InvScratch& s) {
+  if (threadIdx.x == 0) *s.flag = 0;
+  __syncthreads();
+  if (n <= kSmallInvMax) {
+    double2* P = smem;
+    double2* f = smem + (size_t)n * n;
+    long long t0 = s.tr.start();
+    for (int i = threadIdx.x; i < n * n; i += blockDim.x) P[i] = A[i];
+    __syncthreads();
+    for (int j = 0; j < n; ++j) {
+      int p = gj_step(P, n, n, j, j, f, s, s.flag);
+      if (threadIdx.x == 0) s.piv[j] = p;
+    }
+    __syncthreads();
+    s.tr.stop(TR_INV_PANEL, t0);
+    t0 = s.tr.start();
+    if (threadIdx.x == 0) {
+      for (int c = 0; c < n; ++c) s.cperm[c] = c;
+      for (int j = n - 1; j >= 0; --j) {
+        int p = s.piv[j];
+        int tmp = s.cperm[j]; s.cperm[j] = s.cperm[p]; s.cperm[p] = tmp;
+      }
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+      const int r = idx % n, c = idx / n;
+      out[idx] = P[r + (size_t)s.cperm[c] * n];
+    }
+    __syncthreads();
+    s.tr.stop(TR_INV_OTHER, t0);
+    int info = *s.flag;
+    __syncthreads();
+    return info;
+  }
+  const int jb_max = zinv_panel(n, smem_bytes);
+  double2* X0 = ws;
+  double2* X1 = ws + (size_t)n * n;
+  double2* W = ws + 2 * (size_t)n * n;
+  const double2* xcur = A;
+  double2* xnext = X0;
+  for (int k0 = 0; k0 < n; k0 += jb_max) {
+    const int jb = min(jb_max, n - k0);
+    double2* P = smem;
+    double2* f = smem + (size_t)n * jb;
+    long long t0 = s.tr.start();
+    for (int idx = threadIdx.x; idx < n * jb; idx += blockDim.x)
+      P[idx] = xcur[(size_t)(idx % n) + (size_t)(k0 + idx / n) * n];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s.perm[i] = i;
+    __syncthreads();
+    for (int jj = 0; jj < jb; ++jj) {
+      const int j = k0 + jj;
+      int p = gj_step(P, n, jb, j, jj, f, s, s.flag);
+      if (threadIdx.x == 0) {
+        s.piv[j] = p;
+        int tmp = s.perm[j]; s.perm[j] = s.perm[p]; s.perm[p] = tmp;
+      }
+      __syncthreads();
+    }
+    for (int idx = threadIdx.x; idx < n * jb; idx += blockDim.x) W[idx] = P[idx];
+    __syncthreads();
+    s.tr.stop(TR_INV_PANEL, t0);
+    t0 = s.tr.start();
+    // X_next = mask_J(X_cur[perm,:]) + W * X_cur[perm[J],:] ; X_next[:,J] = W
+    Operand Aop = opN(W, n);
+    Operand Bop{xcur, n, OP_GATHER, s.perm + k0};
+    Epilogue e;
+    e.mode = EPI_GJ; e.C = xnext; e.ldc = n; e.alpha = make_double2(1, 0); e.beta = make_double2(0, 0);
+    e.xcur = xcur; e.ldx = n; e.perm = s.perm; e.W = W; e.k0 = k0; e.jb = jb; e.maxabs = nullptr;
+    cta_gemm(n, n, jb, Aop, Bop, e, smem);
+    s.tr.stop(TR_INV_UPDATE, t0);
+    xcur = xnext;
+    xnext = (xnext == X0) ? X1 : X0;
+  }
+  long long t1 = s.tr.start();
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < n; ++c) s.cperm[c] = c;
+    for (int j = n - 1; j >= 0; --j) {
+      int p = s.piv[j];
+      int tmp = s.cperm[j]; s.cperm[j] = s.cperm[p]; s.cperm[p] = tmp;
+    }
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
+    const int r = idx % n, c = idx / n;
+    out[idx] = xcur[r + (size_t)s.cperm[c] * n];
+  }
+  __syncthreads();
+  s.tr.stop(TR_INV_OTHER, t1);
+  int info = *s.flag;
+  __syncthreads();
+  return info;
+}
+
+}  // namespace negf

@@ -1,0 +1,90 @@
+// Persistent per-energy-point engine: shared declarations between the CUDA
+// translation unit and the C-ABI host layer.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace negf {
+
+constexpr int kMaxCont = 10;           // MAXNCONT (src/api/lnParams.h:10)
+constexpr int kMaxOrder = 1024;        // largest PL / contact PL size supported
+constexpr int kSmemMain = 96 * 1024;   // GEMM staging / inversion panel region
+
+enum Mode : int { MODE_T = 0, MODE_DOS = 1, MODE_GN = 2 };
+
+// Status codes (identical to include/negf_b200.h)
+enum Status : int {
+  ST_OK = 0, ST_SINGULAR = 1, ST_NOT_CONVERGED = 2, ST_NONFINITE = 3, ST_NOMEM = 4,
+  ST_BAD_ARG = 5, ST_CUDA = 6, ST_TIMEOUT = 7, ST_ADMISSION = 8, ST_NO_GPU = 9,
+  ST_SCBA_NOT_CONVERGED = 10,
+};
+
+// One uploaded device description, as the kernels see it (device memory).
+struct DevDesc {
+  int nbl, ncont, norb, has_s;
+  int has_s00, has_s01, has_smc, pad;
+  const int* pl;            // [nbl] PL sizes
+  const int* pstart;        // [nbl] first orbital of each PL
+  const int64_t* od;        // [nbl] element offset of block (i,i) in hd/sd
+  const int64_t* oo;        // [nbl-1] element offset of block (i,i+1)/(i+1,i)
+  const double2* hd; const double2* hu; const double2* hl;
+  const double2* sd; const double2* su; const double2* sl;
+  int cblk[kMaxCont];       // 1-based
+  int L[kMaxCont];
+  int64_t olead[kMaxCont];  // offset of lead blocks (L x L)
+  int64_t omc[kMaxCont];    // offset of hmc/smc blocks (n_cb x L)
+  const double2* h00; const double2* h01; const double2* s00; const double2* s01;
+  const double2* hmc; const double2* smc;
+};
+
+struct EngineArgs {
+  int mode;
+  int npts;
+  const int* dev_id;
+  const double* energy;
+  const DevDesc* devs;
+  double eta, dos_delta;
+  int ni, nf;
+  double sgf_tol;
+  int sgf_max_iter;
+  double eps;
+  // outputs
+  double* T;
+  double* dos; int64_t dos_stride;
+  int* ncyc;
+  int* status;
+  // non-equilibrium (MODE_GN)
+  const double* frm; int frm_stride;
+  const double* coupling;       // norb (unsquared) or null
+  int scba_niter; double scba_tol;
+  double* curr; int curr_stride;
+  double* lcurr; int lcurr_stride;
+  double* ldens; int ldens_stride;
+  int* scba_iter; double* scba_err;
+  // workspace
+  double2* ws; int64_t ws_per_cta; int64_t Q;  // slot size in complex elements
+  int nmax;                      // max PL/contact PL order over the launch
+  int nbl_max;
+  int ncont_max;                 // contacts per device, max over the launch
+  int* counter;                  // work-queue head (zeroed before launch)
+  unsigned long long* trace;     // TR_NPHASE phase cycle sums, or null (tracing off)
+};
+
+// Workspace slot counts of the engine for a launch
+int64_t engine_slots(int mode, int nbl_max, int ncont_max);
+int64_t engine_ws_elems(int mode, int nbl_max, int ncont_max, int nmax);
+size_t engine_smem_bytes(int nmax);
+
+cudaError_t launch_engine(const EngineArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_zgemm_batched(int batch, int m, int n, int k, double2 alpha, const double2* A,
+                                 int64_t sA, const double2* B, int64_t sB, double2 beta, double2* C,
+                                 int64_t sC, int dagger, cudaStream_t s);
+cudaError_t launch_zinv_batched(int batch, int n, const double2* A, double2* Ainv, int* info, double2* work,
+                                cudaStream_t s);
+size_t zinv_batched_work_elems(int n);
+cudaError_t launch_decimation_batched(int batch, int n, const double2* Ao, const double2* Bo, const double2* Co,
+                                      double2* Go, int* ncyc, double tol, int max_iter, double2* work,
+                                      cudaStream_t s);
+size_t decimation_batched_work_elems(int n);
+
+}  // namespace negf

@@ -1,0 +1,236 @@
+"""ctypes binding of libnegf_b200.so (the C-ABI of include/negf_b200.h).
+
+The CUDA extension is the only implementation: there is no CPU fallback.
+Importing this module without a built libnegf_b200.so raises, and creating a
+context without a GPU raises NegfError(NO_GPU).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .device import Device
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnegf_b200.so")
+
+OK, SINGULAR, NOT_CONVERGED, NONFINITE, NOMEM, BAD_ARG, CUDA, TIMEOUT, ADMISSION, NO_GPU = range(10)
+SCBA_NOT_CONVERGED = 10
+STATUS_NAMES = {0: "OK", 1: "SINGULAR", 2: "NOT_CONVERGED", 3: "NONFINITE", 4: "NOMEM", 5: "BAD_ARG",
+                6: "CUDA", 7: "TIMEOUT", 8: "ADMISSION", 9: "NO_GPU", 10: "SCBA_NOT_CONVERGED"}
+
+# every symbol include/negf_b200.h declares
+EXPORTED = [
+    "negf_b200_default_options", "negf_b200_version", "negf_b200_ctx_create", "negf_b200_ctx_destroy",
+    "negf_b200_set_options", "negf_b200_last_error", "negf_b200_upload_device", "negf_b200_release_device",
+    "negf_b200_device_bytes", "negf_b200_transmission", "negf_b200_transmission_dos",
+    "negf_b200_meir_wingreen", "negf_b200_transmission_dev", "negf_b200_transmission_dos_dev",
+    "negf_b200_zgemm_batched", "negf_b200_zinv_work_bytes", "negf_b200_zinv_batched",
+    "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
+    "negf_b200_get_trace",
+]
+TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
+
+
+class NegfError(RuntimeError):
+    def __init__(self, code: int, msg: str = ""):
+        self.code = code
+        super().__init__("%s (%d)%s" % (STATUS_NAMES.get(code, "?"), code, (": " + msg) if msg else ""))
+
+
+class Options(ctypes.Structure):
+    """Mirror of negf_b200_options."""
+    _fields_ = [("sgf_tol", ctypes.c_double), ("sgf_max_iter", ctypes.c_int32), ("eps_drop", ctypes.c_double),
+                ("scba_tol", ctypes.c_double), ("scba_niter", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("ctas_per_sm", ctypes.c_int32)]
+
+
+_lib = None
+
+
+def load():
+    """Loads the extension; raises if it was not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libnegf_b200.so is not built (run __graft_entry__.build() or "
+                          "python libnegf_b200/build.py); there is no CPU fallback")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, dp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int32)
+    i32, f64 = ctypes.c_int32, ctypes.c_double
+    L.negf_b200_version.restype = ctypes.c_char_p
+    L.negf_b200_last_error.restype = ctypes.c_char_p
+    L.negf_b200_last_error.argtypes = [vp]
+    L.negf_b200_default_options.argtypes = [ctypes.POINTER(Options)]
+    L.negf_b200_ctx_create.argtypes = [i32, ctypes.POINTER(vp)]
+    L.negf_b200_ctx_destroy.argtypes = [vp]
+    L.negf_b200_set_options.argtypes = [vp, ctypes.POINTER(Options)]
+    L.negf_b200_upload_device.argtypes = [vp, vp, ip]
+    L.negf_b200_release_device.argtypes = [vp, i32]
+    L.negf_b200_device_bytes.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_size_t)]
+    L.negf_b200_transmission.argtypes = [vp, i32, ip, dp, f64, i32, i32, dp, ip, ip]
+    L.negf_b200_transmission_dos.argtypes = [vp, i32, ip, dp, f64, f64, i32, i32, dp, dp, ip, ip]
+    L.negf_b200_meir_wingreen.argtypes = [vp, i32, ip, dp, f64, dp, dp, dp, dp, dp, ip, dp, ip, ip]
+    L.negf_b200_transmission_dev.argtypes = [vp, i32, vp, vp, f64, i32, i32, vp, vp, vp, vp]
+    L.negf_b200_transmission_dos_dev.argtypes = [vp, i32, vp, vp, f64, f64, i32, i32, vp, vp, ctypes.c_int64,
+                                                 vp, vp, vp]
+    L.negf_b200_zgemm_batched.argtypes = [i32, i32, i32, i32, dp, vp, ctypes.c_int64, vp, ctypes.c_int64, dp, vp,
+                                          ctypes.c_int64, i32, vp]
+    L.negf_b200_zinv_work_bytes.restype = ctypes.c_size_t
+    L.negf_b200_zinv_work_bytes.argtypes = [i32, i32]
+    L.negf_b200_zinv_batched.argtypes = [i32, i32, vp, vp, vp, vp, vp]
+    L.negf_b200_decimation_work_bytes.restype = ctypes.c_size_t
+    L.negf_b200_decimation_work_bytes.argtypes = [i32, i32]
+    L.negf_b200_decimation_batched.argtypes = [i32, i32, vp, vp, vp, vp, vp, f64, i32, vp, vp]
+    L.negf_b200_set_tracing.argtypes = [vp, i32]
+    L.negf_b200_get_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+    _lib = L
+    return L
+
+
+def _d(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if a is not None else ctypes.POINTER(ctypes.c_double)()
+
+
+def _i(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)) if a is not None else ctypes.POINTER(ctypes.c_int32)()
+
+
+class Context:
+    """One CUDA device, its stream, the HBM-resident device descriptions and
+    the persistent-kernel workspace (negf_b200_ctx)."""
+
+    def __init__(self, cuda_device: int = 0, **options):
+        L = load()
+        h = ctypes.c_void_p()
+        rc = L.negf_b200_ctx_create(cuda_device, ctypes.byref(h))
+        if rc != OK:
+            raise NegfError(rc, "negf_b200_ctx_create")
+        self._h = h
+        self._L = L
+        self.devices = {}
+        if options:
+            self.set_options(**options)
+
+    # -- lifecycle
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.negf_b200_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def last_error(self) -> str:
+        return self._L.negf_b200_last_error(self._h).decode()
+
+    def _check(self, rc, what):
+        if rc not in (OK,):
+            raise NegfError(rc, "%s: %s" % (what, self.last_error()))
+
+    def set_options(self, **kw):
+        o = Options()
+        self._L.negf_b200_default_options(ctypes.byref(o))
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise TypeError("unknown option %s" % k)
+            setattr(o, k, v)
+        self._check(self._L.negf_b200_set_options(self._h, ctypes.byref(o)), "set_options")
+
+    def set_tracing(self, enable=True):
+        self._check(self._L.negf_b200_set_tracing(self._h, 1 if enable else 0), "set_tracing")
+
+    def get_trace(self) -> dict:
+        """Per-phase SM cycles summed over CTAs since the last call (reset)."""
+        buf = (ctypes.c_uint64 * 8)()
+        self._check(self._L.negf_b200_get_trace(self._h, buf), "get_trace")
+        return {k: int(v) for k, v in zip(TRACE_PHASES, buf)}
+
+    def upload(self, dev: Device) -> int:
+        st = dev.to_struct()
+        did = ctypes.c_int32()
+        self._check(self._L.negf_b200_upload_device(self._h, ctypes.byref(st), ctypes.byref(did)), "upload")
+        self.devices[did.value] = dev
+        return did.value
+
+    def release(self, device_id: int):
+        self._check(self._L.negf_b200_release_device(self._h, device_id), "release")
+        self.devices.pop(device_id, None)
+
+    # -- solves (host buffers)
+    @staticmethod
+    def _ids(device_id, npts):
+        return np.ascontiguousarray(np.broadcast_to(np.asarray(device_id, dtype=np.int32), (npts,)))
+
+    def transmission(self, device_id, energies, eta=1e-4, ni=1, nf=2, check=True):
+        E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
+        n = E.size
+        ids = self._ids(device_id, n)
+        T = np.zeros(n)
+        ncyc = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        rc = self._L.negf_b200_transmission(self._h, n, _i(ids), _d(E), eta, ni, nf, _d(T), _i(ncyc), _i(st))
+        if check and rc not in (OK, NOT_CONVERGED):
+            raise NegfError(rc, "transmission: " + self.last_error())
+        return T, ncyc, st
+
+    def transmission_dos(self, device_id, energies, eta=1e-4, dos_delta=1e-4, ni=1, nf=2, check=True):
+        E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
+        n = E.size
+        ids = self._ids(device_id, n)
+        norb = max(self.devices[int(i)].norb for i in set(ids.tolist()))
+        T = np.zeros(n)
+        dos = np.zeros((n, norb))
+        ncyc = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        rc = self._L.negf_b200_transmission_dos(self._h, n, _i(ids), _d(E), eta, dos_delta, ni, nf, _d(T), _d(dos),
+                                                _i(ncyc), _i(st))
+        if check and rc not in (OK, NOT_CONVERGED):
+            raise NegfError(rc, "transmission_dos: " + self.last_error())
+        return T, dos, ncyc, st
+
+    def meir_wingreen(self, device_id, energies, frm, coupling=None, eta=1e-4, check=True):
+        E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
+        n = E.size
+        ids = self._ids(device_id, n)
+        devs = [self.devices[int(i)] for i in set(ids.tolist())]
+        ncont = max(d.ncont for d in devs)
+        nbl = max(d.nbl for d in devs)
+        norb = max(d.norb for d in devs)
+        frm = np.ascontiguousarray(np.broadcast_to(np.asarray(frm, dtype=np.float64), (n, ncont)))
+        cp = None if coupling is None else np.ascontiguousarray(
+            np.broadcast_to(np.asarray(coupling, dtype=np.float64), (norb,)))
+        curr = np.zeros((n, ncont))
+        lcurr = np.zeros((n, max(nbl - 1, 1)))
+        ldens = np.zeros((n, nbl))
+        it = np.zeros(n, dtype=np.int32)
+        err = np.zeros(n)
+        ncyc = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        rc = self._L.negf_b200_meir_wingreen(self._h, n, _i(ids), _d(E), eta, _d(frm), _d(cp), _d(curr), _d(lcurr),
+                                             _d(ldens), _i(it), _d(err), _i(ncyc), _i(st))
+        if check and rc not in (OK, NOT_CONVERGED):
+            raise NegfError(rc, "meir_wingreen: " + self.last_error())
+        return dict(curr=curr, layer_curr=lcurr[:, :nbl - 1], layer_dens=ldens, scba_iter=it, scba_err=err,
+                    ncyc=ncyc, status=st)
+
+
+def version() -> str:
+    return load().negf_b200_version().decode()

@@ -1,0 +1,138 @@
+"""ctypes front-end of the CPU oracle (test infrastructure only).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module; the product path never imports it.  See negf_oracle.cpp for the
+reference routines each entry point restates.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(HERE))
+
+from libnegf_b200.device import Device  # noqa: E402
+
+_lib = None
+KB_HARTREE_PER_K = 3.166811389002312e-6   # src/ln_constants.F90:36
+KB_EV_PER_K = 8.617332411853536e-5        # src/ln_constants.F90:39
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        from oracle import build as _b   # noqa: E402
+        path = _b.build()
+        L = ctypes.CDLL(path)
+        dp = ctypes.POINTER(ctypes.c_double)
+        ip = ctypes.POINTER(ctypes.c_int)
+        vp = ctypes.c_void_p
+        L.oracle_decimation.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp, ip]
+        L.oracle_zinv.argtypes = [ctypes.c_int, dp, dp]
+        L.oracle_transmission.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, ip, ip, ctypes.c_int]
+        L.oracle_transmission_dos.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                              ctypes.c_double, dp, dp, ip, ip, ctypes.c_int]
+        L.oracle_meir_wingreen.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, dp, dp, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                           dp, dp, dp, ip, dp, ip, ip, ctypes.c_int]
+        L.oracle_fermi.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        L.oracle_fermi.restype = ctypes.c_double
+        L.oracle_integrate_el.argtypes = [dp, ctypes.c_int] + [ctypes.c_double] * 8
+        L.oracle_integrate_el.restype = ctypes.c_double
+        _lib = L
+    return _lib
+
+
+def _d(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _i(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+
+
+def _flatF(x):
+    return np.ascontiguousarray(np.asarray(x, dtype=np.complex128).ravel(order="F"))
+
+
+def decimation(Ao, Bo, Co, tol=1e-9, max_iter=300):
+    n = Ao.shape[0]
+    a, b, c = (_flatF(x) for x in (Ao, Bo, Co))
+    g = np.zeros(n * n, dtype=np.complex128)
+    ncyc = np.zeros(1, dtype=np.int32)
+    st = lib().oracle_decimation(n, _d(a.view(np.float64)), _d(b.view(np.float64)), _d(c.view(np.float64)),
+                                 tol, max_iter, _d(g.view(np.float64)), _i(ncyc))
+    return g.reshape((n, n), order="F"), int(ncyc[0]), st
+
+
+def zinv(A):
+    n = A.shape[0]
+    a = _flatF(A)
+    x = np.zeros(n * n, dtype=np.complex128)
+    st = lib().oracle_zinv(n, _d(a.view(np.float64)), _d(x.view(np.float64)))
+    return x.reshape((n, n), order="F"), st
+
+
+def transmission(dev: Device, energies, eta=1e-4, ni=1, nf=2, sgf_tol=1e-9, sgf_max_iter=300,
+                 eps=0.0, nthreads=0):
+    E = np.ascontiguousarray(energies, dtype=np.float64)
+    npts = E.size
+    T = np.zeros(npts)
+    ncyc = np.zeros(npts, dtype=np.int32)
+    status = np.zeros(npts, dtype=np.int32)
+    st = dev.to_struct()
+    lib().oracle_transmission(ctypes.addressof(st), npts, _d(E), eta, ni, nf, sgf_tol, sgf_max_iter, eps,
+                              _d(T), _i(ncyc), _i(status), nthreads)
+    return T, ncyc, status
+
+
+def transmission_dos(dev: Device, energies, eta=1e-4, dos_delta=1e-4, ni=1, nf=2, sgf_tol=1e-9,
+                     sgf_max_iter=300, eps=0.0, nthreads=0):
+    E = np.ascontiguousarray(energies, dtype=np.float64)
+    npts = E.size
+    T = np.zeros(npts)
+    dos = np.zeros((npts, dev.norb))
+    ncyc = np.zeros(npts, dtype=np.int32)
+    status = np.zeros(npts, dtype=np.int32)
+    st = dev.to_struct()
+    lib().oracle_transmission_dos(ctypes.addressof(st), npts, _d(E), eta, dos_delta, ni, nf, sgf_tol,
+                                  sgf_max_iter, eps, _d(T), _d(dos), _i(ncyc), _i(status), nthreads)
+    return T, dos, ncyc, status
+
+
+def meir_wingreen(dev: Device, energies, frm, coupling=None, eta=1e-4, scba_niter=5, scba_tol=1e-7,
+                  sgf_tol=1e-9, sgf_max_iter=300, eps=0.0, nthreads=0):
+    E = np.ascontiguousarray(energies, dtype=np.float64)
+    npts = E.size
+    frm = np.ascontiguousarray(np.broadcast_to(frm, (npts, dev.ncont)), dtype=np.float64)
+    cp = None if coupling is None else np.ascontiguousarray(np.broadcast_to(coupling, (dev.norb,)),
+                                                             dtype=np.float64)
+    curr = np.zeros((npts, dev.ncont))
+    lcurr = np.zeros((npts, max(dev.nbl - 1, 1)))
+    ldens = np.zeros((npts, dev.nbl))
+    it = np.zeros(npts, dtype=np.int32)
+    err = np.zeros(npts)
+    ncyc = np.zeros(npts, dtype=np.int32)
+    status = np.zeros(npts, dtype=np.int32)
+    st = dev.to_struct()
+    lib().oracle_meir_wingreen(ctypes.addressof(st), npts, _d(E), eta, _d(frm),
+                               _d(cp) if cp is not None else ctypes.POINTER(ctypes.c_double)(),
+                               scba_niter, scba_tol, sgf_tol, sgf_max_iter, eps,
+                               _d(curr), _d(lcurr), _d(ldens), _i(it), _d(err), _i(ncyc), _i(status), nthreads)
+    return dict(curr=curr, layer_curr=lcurr[:, :dev.nbl - 1], layer_dens=ldens, scba_iter=it,
+                scba_err=err, ncyc=ncyc, status=status)
+
+
+def fermi(E, Ef, kT):
+    return lib().oracle_fermi(E, Ef, kT)
+
+
+def integrate_el(tun, mu1, mu2, kT1, kT2, emin, emax, estep, kb_1K=KB_HARTREE_PER_K):
+    t = np.ascontiguousarray(tun, dtype=np.float64)
+    return lib().oracle_integrate_el(_d(t), t.size, mu1, mu2, kT1, kT2, emin, emax, estep, kb_1K)

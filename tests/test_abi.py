@@ -1,0 +1,50 @@
+"""The C-ABI library loads and exports every symbol include/negf_b200.h
+declares (no GPU needed, no compute calls)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from libnegf_b200 import native
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "negf_b200.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(negf_b200_\w+)\s*\(", src)))
+
+
+def test_header_and_binding_agree():
+    assert declared_symbols() == sorted(native.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    L = native.load()
+    for name in declared_symbols():
+        assert hasattr(L, name), name
+
+
+def test_version_and_defaults():
+    assert "sm_100a" in native.version()
+    o = native.Options()
+    native.load().negf_b200_default_options(ctypes.byref(o))
+    assert o.sgf_tol == 1e-9 and o.sgf_max_iter == 300 and o.scba_tol == 1e-7 and o.eps_drop == 0.0
+
+
+def test_no_gpu_is_an_error_not_a_fallback():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("GPU present")
+    with pytest.raises(native.NegfError) as ei:
+        native.Context(0)
+    assert ei.value.code == native.NO_GPU
+
+
+def test_bad_arguments_are_rejected_without_gpu():
+    L = native.load()
+    assert L.negf_b200_ctx_create(0, None) == native.BAD_ARG
+    assert L.negf_b200_zinv_batched(1, -1, None, None, None, None, None) == native.BAD_ARG
+    assert L.negf_b200_decimation_batched(1, 4, None, None, None, None, None, -1.0, 10, None, None) == native.BAD_ARG

@@ -1,0 +1,259 @@
+"""GPU parity: the CUDA path (through the C-ABI) against the CPU oracle on
+the same seeded inputs.  Bound: |T - T_oracle| <= max(1e-10 |T_oracle|, 1e-13)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from libnegf_b200 import generators as G
+from libnegf_b200 import native
+from oracle import oracle as O
+from conftest import assert_T_close, oracle_spread
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _rand(rng, shape):
+    return rng.standard_normal(shape) + 1j * rng.standard_normal(shape)
+
+
+def _dev(a):
+    """complex128 numpy (column-major semantics) -> device tensor of the
+    Fortran-ordered data"""
+    flat = np.ascontiguousarray(np.asarray(a, dtype=np.complex128).reshape(a.shape[0], -1, a.shape[-1])
+                                .transpose(0, 2, 1))   # batch x cols x rows == column-major per item
+    return torch.from_numpy(flat).cuda()
+
+
+def _host(t, rows, cols):
+    return t.cpu().numpy().transpose(0, 2, 1).reshape(-1, rows, cols)
+
+
+@pytest.mark.parametrize("m,n,k,dagger", [(1, 1, 1, 0), (8, 8, 8, 0), (32, 32, 32, 0), (64, 64, 64, 0),
+                                          (17, 33, 65, 0), (130, 70, 100, 0), (48, 40, 24, 1), (48, 40, 24, 2),
+                                          (256, 256, 256, 0), (100, 100, 100, 2)])
+def test_zgemm_batched(m, n, k, dagger):
+    rng = np.random.default_rng(m * 1000 + n * 10 + k + dagger)
+    b = 3
+    A = _rand(rng, (b, k, m)) if dagger == 1 else _rand(rng, (b, m, k))
+    B = _rand(rng, (b, n, k)) if dagger == 2 else _rand(rng, (b, k, n))
+    C = _rand(rng, (b, m, n))
+    alpha, beta = np.array([0.7, -0.3]), np.array([0.25, 0.5])
+    dA, dB, dC = _dev(A), _dev(B), _dev(C)
+    L = native.load()
+    dp = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rc = L.negf_b200_zgemm_batched(b, m, n, k, dp(alpha), dA.data_ptr(), 2 * A[0].size, dB.data_ptr(),
+                                   2 * B[0].size, dp(beta), dC.data_ptr(), 2 * m * n, dagger, None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    opA = A.conj().transpose(0, 2, 1) if dagger == 1 else A
+    opB = B.conj().transpose(0, 2, 1) if dagger == 2 else B
+    ref = (0.7 - 0.3j) * (opA @ opB) + (0.25 + 0.5j) * C
+    got = _host(dC, m, n)
+    assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max()) * np.sqrt(k)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 16, 33, 64, 65, 100, 128, 200, 256, 512])
+def test_zinv_batched(n):
+    rng = np.random.default_rng(n)
+    b = 2
+    A = _rand(rng, (b, n, n)) + 2.0 * np.sqrt(n) * np.eye(n) * (rng.random() < 2)
+    A[1] = _rand(rng, (n, n))   # general (pivoting exercised)
+    dA = _dev(A)
+    dX = torch.empty_like(dA)
+    info = torch.zeros(b, dtype=torch.int32, device="cuda")
+    L = native.load()
+    wb = L.negf_b200_zinv_work_bytes(b, n)
+    work = torch.empty(max(wb, 16), dtype=torch.uint8, device="cuda")
+    rc = L.negf_b200_zinv_batched(b, n, dA.data_ptr(), dX.data_ptr(), info.data_ptr(), work.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(info.abs().sum()) == 0
+    X = _host(dX, n, n)
+    for i in range(b):
+        Xr = np.linalg.inv(A[i])
+        cond = np.linalg.cond(A[i])
+        assert np.abs(X[i] - Xr).max() <= 1e-14 * cond * max(1.0, np.abs(Xr).max()) * n
+
+
+def test_zinv_singular_reports_info():
+    n = 8
+    A = np.eye(n, dtype=np.complex128)[None]
+    A[0, 3, 3] = 0.0
+    dA = _dev(A)
+    dX = torch.empty_like(dA)
+    info = torch.zeros(1, dtype=torch.int32, device="cuda")
+    L = native.load()
+    rc = L.negf_b200_zinv_batched(1, n, dA.data_ptr(), dX.data_ptr(), info.data_ptr(), None, None)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(info[0]) == 4
+
+
+@pytest.mark.parametrize("n", [1, 4, 32, 80])
+def test_decimation_batched(n):
+    dev = G.transport_c0(nbl=3, n=n, seed=n)
+    Es = [-1.3, 0.2, 2.2]
+    b = len(Es)
+    Ao, Bo, Co = [], [], []
+    for e in Es:
+        Ec = e + 1e-6j
+        Ao.append(Ec * np.eye(n) - dev.lead_h00[1])
+        Bo.append(-dev.lead_h01[1])
+        Co.append(-dev.lead_h01[1].conj().T)
+    Ao, Bo, Co = np.array(Ao), np.array(Bo), np.array(Co)
+    dAo, dBo, dCo = _dev(Ao), _dev(Bo), _dev(Co)
+    dG = torch.empty_like(dAo)
+    ncyc = torch.zeros(b, dtype=torch.int32, device="cuda")
+    L = native.load()
+    work = torch.empty(L.negf_b200_decimation_work_bytes(b, n), dtype=torch.uint8, device="cuda")
+    rc = L.negf_b200_decimation_batched(b, n, dAo.data_ptr(), dBo.data_ptr(), dCo.data_ptr(), dG.data_ptr(),
+                                        ncyc.data_ptr(), 1e-9, 300, work.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    Gd = _host(dG, n, n)
+    for i in range(b):
+        g, nc, st = O.decimation(Ao[i], Bo[i], Co[i], tol=1e-9)
+        assert abs(int(ncyc[i]) - nc) <= 1
+        assert np.abs(Gd[i] - g).max() <= 1e-9 * max(1.0, np.abs(g).max())
+
+
+CASES = {
+    "chain1": lambda: (G.chain(1, 4), np.linspace(-1.9, 1.9, 9)),
+    "chain3_rev": lambda: (G.chain(3, 5, cblk=[5, 1]), np.linspace(-1.9, 1.9, 9)),
+    "nbl1": lambda: (G.transport_c0(nbl=1, n=6, seed=1), np.linspace(-3, 3, 9)),
+    "nbl2": lambda: (G.transport_c0(nbl=2, n=6, seed=1), np.linspace(-3, 3, 9)),
+    "c0_small": lambda: (G.transport_c0(nbl=6, n=8, seed=0), np.linspace(-3, 3, 17)),
+    "c0_n32": lambda: (G.transport_c0(nbl=20, n=32, seed=0), G.energy_grid(-3, 3, 512)[::16]),
+    "c1_S": lambda: (G.transport_c1(nbl=5, n=12, seed=2, density=0.3), np.linspace(-2, 2, 9)),
+    "uneven": lambda: (G.uneven([5, 7, 3, 6], seed=4), np.linspace(-2, 2, 9)),
+    "ncont": lambda: (G.transport_c0(nbl=6, n=8, seed=1, cblk=[2, 5]), np.linspace(-3, 3, 13)),
+    "n80": lambda: (G.transport_c0(nbl=4, n=80, seed=6), np.linspace(-3, 3, 5)),
+    "n130_S": lambda: (G.transport_c1(nbl=3, n=130, seed=7, density=0.1), np.linspace(-2, 2, 3)),
+}
+
+
+def _o_T(E, **kw):
+    def run(d):
+        T, nc, st = O.transmission(d, E, **kw)
+        return {"T": T, "ncyc": nc, "status": st}
+    return run
+
+
+def _o_dos(E, **kw):
+    def run(d):
+        T, dos, nc, st = O.transmission_dos(d, E, **kw)
+        return {"T": T, "dos": dos, "ncyc": nc, "status": st}
+    return run
+
+
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_transmission_parity(gpu_ctx, case):
+    dev, E = CASES[case]()
+    did = gpu_ctx.upload(dev)
+    try:
+        T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6)
+        ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev)
+        assert np.all(st == ref["status"])
+        assert np.all(np.abs(ncyc - ref["ncyc"]) <= 4)
+        assert_T_close(T, ref["T"], spread=spread["T"])
+    finally:
+        gpu_ctx.release(did)
+
+
+@pytest.mark.parametrize("case", ["chain1", "c0_small", "c0_n32"])
+def test_transmission_parity_default_eta(gpu_ctx, case):
+    """At libNEGF's default broadening delta = 1e-4 (lib_param.F90:628)."""
+    dev, E = CASES[case]()
+    did = gpu_ctx.upload(dev)
+    try:
+        T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-4)
+        ref, spread = oracle_spread(_o_T(E, eta=1e-4), dev)
+        assert np.all(st == ref["status"])
+        assert_T_close(T, ref["T"], spread=spread["T"])
+    finally:
+        gpu_ctx.release(did)
+
+
+@pytest.mark.parametrize("case", ["chain3_rev", "c0_small", "c1_S", "uneven", "ncont", "n80"])
+def test_transmission_dos_parity(gpu_ctx, case):
+    dev, E = CASES[case]()
+    did = gpu_ctx.upload(dev)
+    try:
+        T, dos, ncyc, st = gpu_ctx.transmission_dos(did, E, eta=1e-6, dos_delta=1e-4)
+        ref, spread = oracle_spread(_o_dos(E, eta=1e-6, dos_delta=1e-4), dev)
+        assert np.all(st == ref["status"])
+        assert_T_close(T, ref["T"], spread=spread["T"])
+        scale = max(np.abs(ref["dos"]).max(), 1.0)
+        bound = np.maximum(1e-10 * scale, 10 * spread["dos"])
+        assert np.all(np.abs(dos - ref["dos"]) <= bound)
+    finally:
+        gpu_ctx.release(did)
+
+
+def test_multi_device_batch(gpu_ctx):
+    """Points of different devices (k-points / requests) in one launch."""
+    d1, E1 = CASES["c0_small"]()
+    d2, E2 = CASES["uneven"]()
+    i1, i2 = gpu_ctx.upload(d1), gpu_ctx.upload(d2)
+    try:
+        ids = np.array([i1] * len(E1) + [i2] * len(E2), dtype=np.int32)
+        E = np.concatenate([E1, E2])
+        T, _, st = gpu_ctx.transmission(ids, E, eta=1e-6)
+        r1, s1 = oracle_spread(_o_T(E1, eta=1e-6), d1)
+        r2, s2 = oracle_spread(_o_T(E2, eta=1e-6), d2)
+        assert_T_close(T[:len(E1)], r1["T"], spread=s1["T"])
+        assert_T_close(T[len(E1):], r2["T"], spread=s2["T"])
+    finally:
+        gpu_ctx.release(i1)
+        gpu_ctx.release(i2)
+
+
+@pytest.mark.parametrize("case", ["elph", "c0_deph", "c1_S_deph"])
+def test_meir_wingreen_parity(gpu_ctx, case):
+    if case == "elph":
+        dev = G.chain(10, 6, cblk=[6, 1])
+        E = np.arange(-2.0, 2.0 + 1e-9, 0.1)
+        cpl = np.full(dev.norb, 0.05)
+        frm = [1.0, 0.0]
+    elif case == "c0_deph":
+        dev = G.transport_c0(nbl=5, n=8, seed=3)
+        E = np.linspace(-1, 1, 7)
+        cpl = np.full(dev.norb, 0.1)
+        frm = np.stack([[0.9, 0.2]] * len(E))
+    else:
+        dev = G.transport_c1(nbl=4, n=10, seed=4, density=0.3)
+        E = np.linspace(-1, 1, 5)
+        cpl = np.full(dev.norb, 0.1)
+        frm = [1.0, 0.0]
+    did = gpu_ctx.upload(dev)
+    gpu_ctx.set_options(scba_niter=5)
+    try:
+        r = gpu_ctx.meir_wingreen(did, E, frm, coupling=cpl, eta=1e-4)
+        o, spread = oracle_spread(lambda d: O.meir_wingreen(d, E, frm, coupling=cpl, eta=1e-4, scba_niter=5), dev)
+        assert np.all(r["status"] == o["status"])
+        assert np.all(np.abs(r["scba_iter"] - o["scba_iter"]) <= 1)
+        for key in ("curr", "layer_curr", "layer_dens"):
+            a, b = r[key], o[key]
+            bound = np.maximum(1e-10 * max(1.0, np.abs(b).max()), 10 * spread[key])
+            assert np.all(np.abs(a - b) <= bound), key
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
+
+
+def test_elph_current_known_answer(gpu_ctx):
+    """tests/f90elph_deph: zero coupling -> 2.0 +- 1e-4, coupling 0.05 -> [1.90, 1.95]"""
+    dev = G.chain(10, 6, cblk=[6, 1])
+    E = np.arange(-2.0, 2.0 + 1e-9, 0.1)
+    did = gpu_ctx.upload(dev)
+    gpu_ctx.set_options(scba_niter=5)
+    try:
+        r0 = gpu_ctx.meir_wingreen(did, E, [1.0, 0.0], coupling=np.zeros(60), eta=1e-4)
+        c0 = O.integrate_el(r0["curr"][:, 0], -0.5, 0.5, 1e-3, 1e-3, -2.0, 2.0, 0.1) * 2
+        r1 = gpu_ctx.meir_wingreen(did, E, [1.0, 0.0], coupling=np.full(60, 0.05), eta=1e-4)
+        c1 = abs(O.integrate_el(r1["curr"][:, 0], -0.5, 0.5, 1e-3, 1e-3, -2.0, 2.0, 0.1) * 2)
+        assert abs(c0 - 2.0) < 1e-4
+        assert 1.90 <= c1 <= 1.95
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
