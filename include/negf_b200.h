@@ -262,6 +262,25 @@ int negf_b200_decimation_batched(int32_t batch, int32_t n, const double* Ao,
                                  double* Go, int32_t* ncyc, double tol,
                                  int32_t max_iter, void* work, void* stream);
 
+/* Same as negf_b200_decimation_batched, but allocates no device memory and
+ * takes no work buffer.  It has no counterpart in the reference.
+ * For callers that cannot allocate: codes whose device memory belongs to
+ * another allocator (a framework's caching pool, a host that passes only
+ * the arrays it owns) and solver loops that cannot afford the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  Ao/Bo/Co/Go/ncyc are still the
+ * caller's device buffers.
+ * Scratch comes from one fixed 64 MiB array compiled into the library:
+ * batch * 15 * n * n * 16 bytes must fit (e.g. up to 4 problems of order
+ * 256, 68 of order 64); larger requests return NEGF_B200_ERR_ADMISSION and
+ * print the limit.  The first call on each device resolves the array's
+ * address for that device; make it before any stream capture.  All calls
+ * share the array: calls that can overlap on the GPU race, so serialise
+ * them. */
+int negf_b200_decimation_noalloc(int32_t batch, int32_t n, const double* Ao,
+                                 const double* Bo, const double* Co,
+                                 double* Go, int32_t* ncyc, double tol,
+                                 int32_t max_iter, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

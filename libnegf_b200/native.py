@@ -30,7 +30,7 @@ EXPORTED = [
     "negf_b200_meir_wingreen", "negf_b200_transmission_dev", "negf_b200_transmission_dos_dev",
     "negf_b200_zgemm_batched", "negf_b200_zinv_work_bytes", "negf_b200_zinv_batched",
     "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
-    "negf_b200_get_trace",
+    "negf_b200_get_trace", "negf_b200_decimation_noalloc",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -88,6 +88,7 @@ def load():
     L.negf_b200_decimation_batched.argtypes = [i32, i32, vp, vp, vp, vp, vp, f64, i32, vp, vp]
     L.negf_b200_set_tracing.argtypes = [vp, i32]
     L.negf_b200_get_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.negf_b200_decimation_noalloc.argtypes = [i32, i32, vp, vp, vp, vp, vp, f64, i32, vp]
     _lib = L
     return L
 
