@@ -26,8 +26,10 @@ namespace negf {
 constexpr int kThreads = 256;          // threads per CTA (8 warps)
 constexpr int TM = 64, TN = 64, TK = 16;
 constexpr int A_LD = TM + 2;           // sA[k][m], padded: conflict-free fragment loads
-constexpr int B_LD = TK + 4;           // sB[n][k]
-constexpr int kGemmSmemBytes = 2 * (TK * A_LD + TN * B_LD) * 16;
+constexpr int B_LD = TK + 4;           // sB[n][k], padded: conflict-free fragment loads
+constexpr int kStages = 2;             // cp.async double buffer
+constexpr int kStageElems = TK * A_LD + TN * B_LD;
+constexpr int kGemmSmemBytes = kStages * kStageElems * 16;
 constexpr int kSmallInvMax = 64;       // n <= 64: whole matrix in shared memory
 
 // ---------------------------------------------------------------- complex
@@ -119,6 +121,7 @@ __device__ __forceinline__ Epilogue epi_store(double2* C, int ldc, double2 alpha
 
 // ---------------------------------------------------------------- tile loads
 // A tile: rows [m0, m0+TM) x cols [k0, k0+TK) of op(A) (M x K) into sA[k][m]
+template <int MODE>
 __device__ __forceinline__ void load_a_tile(const Operand& A, int M, int K, int m0, int k0, double2* sA) {
   const int tid = threadIdx.x;
 #pragma unroll
@@ -127,14 +130,14 @@ __device__ __forceinline__ void load_a_tile(const Operand& A, int M, int K, int 
     int m, k;
     const double2* src;
     bool ok;
-    if (A.mode == OP_C) {
+    if (MODE == OP_C) {
       k = idx & (TK - 1); m = idx / TK;
       ok = (m0 + m < M) && (k0 + k < K);
       src = ok ? A.p + (size_t)(k0 + k) + (size_t)(m0 + m) * A.ld : A.p;
     } else {
       m = idx & (TM - 1); k = idx / TM;
       ok = (m0 + m < M) && (k0 + k < K);
-      int row = (A.mode == OP_GATHER && ok) ? A.perm[m0 + m] : m0 + m;
+      int row = (MODE == OP_GATHER && ok) ? A.perm[m0 + m] : m0 + m;
       src = ok ? A.p + (size_t)row + (size_t)(k0 + k) * A.ld : A.p;
     }
     cp_async16(&sA[k * A_LD + m], src, ok);
@@ -142,6 +145,7 @@ __device__ __forceinline__ void load_a_tile(const Operand& A, int M, int K, int 
 }
 
 // B tile: rows [k0, k0+TK) x cols [n0, n0+TN) of op(B) (K x N) into sB[n][k]
+template <int MODE>
 __device__ __forceinline__ void load_b_tile(const Operand& B, int K, int N, int k0, int n0, double2* sB) {
   const int tid = threadIdx.x;
 #pragma unroll
@@ -150,14 +154,14 @@ __device__ __forceinline__ void load_b_tile(const Operand& B, int K, int N, int 
     int k, n;
     const double2* src;
     bool ok;
-    if (B.mode == OP_C) {
+    if (MODE == OP_C) {
       n = idx & (TN - 1); k = idx / TN;
       ok = (k0 + k < K) && (n0 + n < N);
       src = ok ? B.p + (size_t)(n0 + n) + (size_t)(k0 + k) * B.ld : B.p;
     } else {
       k = idx & (TK - 1); n = idx / TK;
       ok = (k0 + k < K) && (n0 + n < N);
-      int row = (B.mode == OP_GATHER && ok) ? B.perm[k0 + k] : k0 + k;
+      int row = (MODE == OP_GATHER && ok) ? B.perm[k0 + k] : k0 + k;
       src = ok ? B.p + (size_t)row + (size_t)(n0 + n) * B.ld : B.p;
     }
     cp_async16(&sB[n * B_LD + k], src, ok);
@@ -165,114 +169,156 @@ __device__ __forceinline__ void load_b_tile(const Operand& B, int K, int N, int 
 }
 
 // ---------------------------------------------------------------- epilogue
-__device__ __forceinline__ void epi_apply(const Epilogue& e, int r, int c, double re, double im, int M,
-                                          int N, double& lmax) {
+// The value the epilogue combines with the product at (r, c): C(r,c) for
+// EPI_STORE with beta != 0, the permuted previous iterate (or the panel) for
+// EPI_GJ.  Loaded for a whole fragment before any store, so that the loads
+// of one fragment are in flight together instead of each waiting behind the
+// previous element's store.
+template <int EMODE>
+__device__ __forceinline__ double2 epi_old(const Epilogue& e, int r, int c, int M, int N) {
+  if (r >= M || c >= N) return make_double2(0.0, 0.0);
+  if (EMODE == EPI_STORE) {
+    if (e.beta.x == 0.0 && e.beta.y == 0.0) return make_double2(0.0, 0.0);
+    return e.C[(size_t)r + (size_t)c * e.ldc];
+  }
+  if (c >= e.k0 && c < e.k0 + e.jb) return e.W[(size_t)r + (size_t)(c - e.k0) * M];
+  if (r >= e.k0 && r < e.k0 + e.jb) return make_double2(0.0, 0.0);
+  return e.xcur[(size_t)e.perm[r] + (size_t)c * e.ldx];
+}
+
+template <int EMODE>
+__device__ __forceinline__ void epi_store_one(const Epilogue& e, int r, int c, double re, double im, double2 old,
+                                              int M, int N, double& lmax, bool want_max) {
   if (r >= M || c >= N) return;
   double2 out;
-  if (e.mode == EPI_STORE) {
+  if (EMODE == EPI_STORE) {
     out = make_double2(e.alpha.x * re - e.alpha.y * im, e.alpha.x * im + e.alpha.y * re);
-    if (e.beta.x != 0.0 || e.beta.y != 0.0) out = cadd(out, cmul(e.beta, e.C[(size_t)r + (size_t)c * e.ldc]));
-  } else {  // EPI_GJ
-    if (c >= e.k0 && c < e.k0 + e.jb) {
-      out = e.W[(size_t)r + (size_t)(c - e.k0) * M];
-    } else {
-      out = make_double2(re, im);
-      if (r < e.k0 || r >= e.k0 + e.jb) out = cadd(out, e.xcur[(size_t)e.perm[r] + (size_t)c * e.ldx]);
-    }
+    out = cadd(out, cmul(e.beta, old));
+  } else {
+    out = (c >= e.k0 && c < e.k0 + e.jb) ? old : make_double2(re + old.x, im + old.y);
   }
   e.C[(size_t)r + (size_t)c * e.ldc] = out;
-  lmax = fmax(lmax, cabs(out));
+  if (want_max) lmax = fmax(lmax, cabs(out));
 }
 
 // ---------------------------------------------------------------- GEMM
 // C(MxN) = epilogue( op(A)(MxK) * op(B)(KxN) ).  All threads of the CTA must
 // call it.  `smem` must hold kGemmSmemBytes.  Ends with __syncthreads().
-__device__ __noinline__ void cta_gemm(int M, int N, int K, const Operand& A, const Operand& B, const Epilogue& e,
-                         double2* smem) {
-  double2* sA0 = smem;
-  double2* sA1 = sA0 + TK * A_LD;
-  double2* sB0 = sA1 + TK * A_LD;
-  double2* sB1 = sB0 + TN * B_LD;
+//
+// The operand pipeline runs over the flattened sequence of (output tile,
+// K-tile) steps, so the next output tile's first operands are in flight
+// while the current tile's epilogue runs; K = 16 products (the Gauss-Jordan
+// updates) are as pipelined as long ones.  One specialisation per operand /
+// epilogue combination keeps the live state of the main loop in registers.
+template <int AM, int BM, int EM>
+__device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, const Operand B, const Epilogue& e,
+                                        double2* smem) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp & 1, wn = warp >> 1;
-  const double ca = (A.mode == OP_C) ? -1.0 : 1.0;
-  const double cb = (B.mode == OP_C) ? -1.0 : 1.0;
+  constexpr double ca = (AM == OP_C) ? -1.0 : 1.0;
+  constexpr double cb = (BM == OP_C) ? -1.0 : 1.0;
+  const bool want_max = e.maxabs != nullptr;
   const int tilesM = (M + TM - 1) / TM, tilesN = (N + TN - 1) / TN;
-  const int nk = (K + TK - 1) / TK;
+  const int nk = max(1, (K + TK - 1) / TK);
+  const int total = tilesM * tilesN * nk;
   double lmax = 0.0;
+  double accR[2][2][4], accI[2][2][4];
+  int ld_tile = 0, ld_kt = 0;   // (tile, K-tile) of the next step to load
 
-  for (int tile = 0; tile < tilesM * tilesN; ++tile) {
-    const int m0 = (tile % tilesM) * TM, n0 = (tile / tilesM) * TN;
-    double accR[2][2][4], accI[2][2][4];
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) { accR[i][j][q] = 0.0; accI[i][j][q] = 0.0; }
+  auto issue = [&](int buf) {
+    const int m0 = (ld_tile % tilesM) * TM, n0 = (ld_tile / tilesM) * TN;
+    double2* st = smem + buf * kStageElems;
+    load_a_tile<AM>(A, M, K, m0, ld_kt * TK, st);
+    load_b_tile<BM>(B, K, N, ld_kt * TK, n0, st + TK * A_LD);
+    cp_async_commit();
+    if (++ld_kt == nk) { ld_kt = 0; ++ld_tile; }
+  };
 
-    if (nk > 0) {
-      load_a_tile(A, M, K, m0, 0, sA0);
-      load_b_tile(B, K, N, 0, n0, sB0);
-      cp_async_commit();
+  issue(0);
+  int tile = 0, kt = 0;
+  for (int step = 0; step < total; ++step) {
+    if (kt == 0) {
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) { accR[i][j][q] = 0.0; accI[i][j][q] = 0.0; }
     }
-    for (int kt = 0; kt < nk; ++kt) {
-      double2* sA = (kt & 1) ? sA1 : sA0;
-      double2* sB = (kt & 1) ? sB1 : sB0;
-      if (kt + 1 < nk) {
-        load_a_tile(A, M, K, m0, (kt + 1) * TK, (kt & 1) ? sA0 : sA1);
-        load_b_tile(B, K, N, (kt + 1) * TK, n0, (kt & 1) ? sB0 : sB1);
-        cp_async_commit();
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
+    if (step + 1 < total) {
+      issue((step + 1) & 1);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+    const double2* sA = smem + (step & 1) * kStageElems;
+    const double2* sB = sA + TK * A_LD;
+#pragma unroll
+    for (int ks = 0; ks < TK / 4; ++ks) {
+      const int k = ks * 4 + t;
+      double are[2][2], aim[2][2], nai[2][2], bre[2], bim[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int r0 = wm * 32 + i * 16 + g;
+        double2 v0 = sA[k * A_LD + r0];
+        double2 v1 = sA[k * A_LD + r0 + 8];
+        are[i][0] = v0.x; are[i][1] = v1.x;
+        aim[i][0] = ca * v0.y; aim[i][1] = ca * v1.y;
+        nai[i][0] = -aim[i][0]; nai[i][1] = -aim[i][1];
       }
-      __syncthreads();
 #pragma unroll
-      for (int ks = 0; ks < TK / 4; ++ks) {
-        const int k = ks * 4 + t;
-        double are[2][2], aim[2][2], nai[2][2], bre[2], bim[2];
+      for (int j = 0; j < 2; ++j) {
+        const int c = wn * 16 + j * 8 + g;
+        double2 v = sB[c * B_LD + k];
+        bre[j] = v.x; bim[j] = cb * v.y;
+      }
+      // four independent accumulators between two updates of the same one
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-          const int r0 = wm * 32 + i * 16 + g;
-          double2 v0 = sA[k * A_LD + r0];
-          double2 v1 = sA[k * A_LD + r0 + 8];
-          are[i][0] = v0.x; are[i][1] = v1.x;
-          aim[i][0] = ca * v0.y; aim[i][1] = ca * v1.y;
-          nai[i][0] = -aim[i][0]; nai[i][1] = -aim[i][1];
-        }
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 2; ++j) {
-          const int c = wn * 16 + j * 8 + g;
-          double2 v = sB[c * B_LD + k];
-          bre[j] = v.x; bim[j] = cb * v.y;
-        }
+        for (int j = 0; j < 2; ++j) dmma_16x8x4(accR[i][j], are[i][0], are[i][1], bre[j]);
 #pragma unroll
-        for (int i = 0; i < 2; ++i)
+      for (int i = 0; i < 2; ++i)
 #pragma unroll
-          for (int j = 0; j < 2; ++j) {
-            dmma_16x8x4(accR[i][j], are[i][0], are[i][1], bre[j]);
-            dmma_16x8x4(accR[i][j], nai[i][0], nai[i][1], bim[j]);
-            dmma_16x8x4(accI[i][j], are[i][0], are[i][1], bim[j]);
-            dmma_16x8x4(accI[i][j], aim[i][0], aim[i][1], bre[j]);
+        for (int j = 0; j < 2; ++j) dmma_16x8x4(accI[i][j], are[i][0], are[i][1], bim[j]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_16x8x4(accR[i][j], nai[i][0], nai[i][1], bim[j]);
+#pragma unroll
+      for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) dmma_16x8x4(accI[i][j], aim[i][0], aim[i][1], bre[j]);
+    }
+    __syncthreads();
+    if (kt == nk - 1) {
+      const int m0 = (tile % tilesM) * TM, n0 = (tile / tilesM) * TN;
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        double2 old[2][4];
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = m0 + wm * 32 + i * 16 + g + ((q >> 1) << 3);
+            const int c = n0 + wn * 16 + j * 8 + 2 * t + (q & 1);
+            old[j][q] = epi_old<EM>(e, r, c, M, N);
+          }
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int r = m0 + wm * 32 + i * 16 + g + ((q >> 1) << 3);
+            const int c = n0 + wn * 16 + j * 8 + 2 * t + (q & 1);
+            epi_store_one<EM>(e, r, c, accR[i][j][q], accI[i][j][q], old[j][q], M, N, lmax, want_max);
           }
       }
-      __syncthreads();
     }
-    // epilogue
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 2; ++j)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const int r = m0 + wm * 32 + i * 16 + g + ((q >> 1) << 3);
-          const int c = n0 + wn * 16 + j * 8 + 2 * t + (q & 1);
-          epi_apply(e, r, c, accR[i][j][q], accI[i][j][q], M, N, lmax);
-        }
+    if (++kt == nk) { kt = 0; ++tile; }
   }
-  if (e.maxabs) {
+  if (want_max) {
     // warp max then one atomic per warp on the shared accumulator
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
@@ -282,6 +328,20 @@ __device__ __noinline__ void cta_gemm(int M, int N, int K, const Operand& A, con
     }
   }
   __syncthreads();
+}
+
+// Runtime dispatch to the specialisations in use.
+__device__ __forceinline__ void cta_gemm(int M, int N, int K, const Operand& A, const Operand& B, const Epilogue& e,
+                                         double2* smem) {
+  if (e.mode == EPI_GJ) {
+    cta_gemm_t<OP_N, OP_GATHER, EPI_GJ>(M, N, K, A, B, e, smem);
+  } else if (A.mode == OP_N && B.mode == OP_N) {
+    cta_gemm_t<OP_N, OP_N, EPI_STORE>(M, N, K, A, B, e, smem);
+  } else if (A.mode == OP_N && B.mode == OP_C) {
+    cta_gemm_t<OP_N, OP_C, EPI_STORE>(M, N, K, A, B, e, smem);
+  } else {
+    cta_gemm_t<OP_C, OP_N, EPI_STORE>(M, N, K, A, B, e, smem);
+  }
 }
 
 // ---------------------------------------------------------------- elementwise
@@ -294,23 +354,71 @@ __device__ __noinline__ void cta_gemm(int M, int N, int K, const Operand& A, con
 __device__ __noinline__ void cta_esh(double2* D, int rows, int cols, const double2* H, const double2* S, double2 s_e,
                         bool diag, const double2* sub, const double2* subdiag, int op) {
   const int n = rows * cols;
-  for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-    const int r = idx % rows, c = idx / rows;
-    // source element of the un-transposed matrix
-    const int sr = (op == OP_C) ? c : r, sc = (op == OP_C) ? r : c;
-    const int sld = (op == OP_C) ? cols : rows;
-    const size_t s = (size_t)sr + (size_t)sc * sld;
-    double2 sv = S ? S[s] : make_double2((diag && sr == sc) ? 1.0 : 0.0, 0.0);
-    double2 v = csub(cmul(s_e, sv), H[s]);
-    if (op == OP_C) v = cconj(v);
-    if (sub) v = csub(v, sub[idx]);
-    if (subdiag && r == c) v = csub(v, subdiag[r]);
-    D[idx] = v;
+  const int sld = (op == OP_C) ? cols : rows;
+  constexpr int U = 4;  // elements per thread per round: loads of a round are in flight together
+  for (int base = threadIdx.x; base < n; base += U * blockDim.x) {
+    double2 hv[U], sv[U], bv[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < n) {
+        const int r = idx % rows, c = idx / rows;
+        // source element of the un-transposed matrix
+        const int sr = (op == OP_C) ? c : r, sc = (op == OP_C) ? r : c;
+        const size_t sidx = (size_t)sr + (size_t)sc * sld;
+        hv[u] = H[sidx];
+        sv[u] = S ? S[sidx] : make_double2((diag && sr == sc) ? 1.0 : 0.0, 0.0);
+        bv[u] = sub ? sub[idx] : make_double2(0.0, 0.0);
+        if (subdiag && r == c) bv[u] = cadd(bv[u], subdiag[r]);
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < n) {
+        double2 v = csub(cmul(s_e, sv[u]), hv[u]);
+        if (op == OP_C) v = cconj(v);
+        D[idx] = csub(v, bv[u]);
+      }
+    }
   }
 }
 
 __device__ void cta_copy(double2* D, const double2* S, int n) {
-  for (int i = threadIdx.x; i < n; i += blockDim.x) D[i] = S[i];
+  constexpr int U = 4;
+  for (int base = threadIdx.x; base < n; base += U * blockDim.x) {
+    double2 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (base + u * (int)blockDim.x < n) v[u] = S[base + u * blockDim.x];
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (base + u * (int)blockDim.x < n) D[base + u * blockDim.x] = v[u];
+  }
+}
+
+// D(r, c) = S(r, cperm[c]) for an n x n matrix (column gather)
+__device__ void cta_copy_colperm(double2* D, const double2* S, int n, const int* cperm) {
+  constexpr int U = 4;
+  const int nn = n * n;
+  for (int base = threadIdx.x; base < nn; base += U * blockDim.x) {
+    double2 v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < nn) v[u] = S[(size_t)(idx % n) + (size_t)cperm[idx / n] * n];
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int idx = base + u * blockDim.x;
+      if (idx < nn) D[idx] = v[u];
+    }
+  }
+}
+
+// D (n x w, ld n) = columns [k0, k0+w) of S (ld n)
+__device__ void cta_copy_cols(double2* D, const double2* S, int n, int k0, int w) {
+  cta_copy(D, S + (size_t)k0 * n, n * w);
 }
 
 // D = i*(A - A^dag)   (zspectral_dns), A square n x n
@@ -425,32 +533,51 @@ __device__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
 
 // One Gauss-Jordan step on a column panel P (n rows x w cols, ld = n) held in
 // shared memory: pivot row j (global row index), panel column jj.
-// f[] is an n-vector of scratch.  Returns the pivot row chosen.
-__device__ __noinline__ int gj_step(double2* P, int n, int w, int j, int jj, double2* f, InvScratch& s, int* info) {
-  double2* colj = P + (size_t)jj * n;
+// f[] (n) and rowj[] (2w) are shared scratch.  Returns the pivot row chosen.
+// Four barriers per step: pivot search (2), exchange + capture (1),
+// scale + rank-1 update (1).
+__device__ __noinline__ int gj_step(double2* P, int n, int w, int j, int jj, double2* f, double2* rowj,
+                                    InvScratch& s, int* info) {
+  const double2* colj = P + (size_t)jj * n;
   int p = cta_pivot(colj, j, n, s);
   if (p >= n) p = j;
-  // swap rows j and p across the panel
-  if (p != j)
-    for (int c = threadIdx.x; c < w; c += blockDim.x) {
-      double2 a = P[j + (size_t)c * n], b = P[p + (size_t)c * n];
-      P[j + (size_t)c * n] = b; P[p + (size_t)c * n] = a;
-    }
+  // Read-only capture: f = pivot column after the exchange of rows j and p,
+  // rowj = new row j (old row p), rowo = new row p (old row j).
+  double2* rowo = rowj + w;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int src = (i == j) ? p : ((i == p) ? j : i);
+    f[i] = colj[src];
+  }
+  for (int c = threadIdx.x; c < w; c += blockDim.x) {
+    rowj[c] = P[p + (size_t)c * n];
+    rowo[c] = P[j + (size_t)c * n];
+  }
   __syncthreads();
-  for (int i = threadIdx.x; i < n; i += blockDim.x) f[i] = colj[i];
-  __syncthreads();
-  double2 piv = f[j];
+  const double2 piv = f[j];
   if (piv.x == 0.0 && piv.y == 0.0 && threadIdx.x == 0 && *info == 0) *info = j + 1;
   const double2 d = crecip(piv);
-  for (int c = threadIdx.x; c < w; c += blockDim.x)
-    P[j + (size_t)c * n] = (c == jj) ? d : cmul(P[j + (size_t)c * n], d);
-  __syncthreads();
-  for (int idx = threadIdx.x; idx < n * w; idx += blockDim.x) {
-    const int i = idx % n, c = idx / n;
-    if (i == j) continue;
-    if (c == jj) P[idx] = make_double2(-(f[i].x * d.x - f[i].y * d.y), -(f[i].x * d.y + f[i].y * d.x));
-    else P[idx] = csub(P[idx], cmul(f[i], P[j + (size_t)c * n]));
-  }
+  // rows are spread over threads, columns looped inside: no integer divide
+  const int rows_per_pass = blockDim.x >= (unsigned)n ? n : (int)blockDim.x;
+  const int cgroups = max(1, (int)blockDim.x / rows_per_pass);
+  const int i0 = threadIdx.x % rows_per_pass, c0 = threadIdx.x / rows_per_pass;
+  if (c0 < cgroups)
+    for (int i = i0; i < n; i += rows_per_pass) {
+      const double2 fi = f[i];
+      const double2 fd = cmul(fi, d);
+      for (int c = c0; c < w; c += cgroups) {
+        double2* el = P + i + (size_t)c * n;
+        double2 v;
+        if (i == j) {
+          v = (c == jj) ? d : cmul(rowj[c], d);
+        } else if (c == jj) {
+          v = make_double2(-fd.x, -fd.y);
+        } else {
+          const double2 base = (i == p) ? rowo[c] : *el;
+          v = csub(base, cmul(fd, rowj[c]));
+        }
+        *el = v;
+      }
+    }
   __syncthreads();
   return p;
 }
@@ -458,7 +585,7 @@ __device__ __noinline__ int gj_step(double2* P, int n, int w, int j, int jj, dou
 // Panel width of the blocked path for an n x n inversion within `smem_bytes`
 __host__ __device__ inline int zinv_panel(int n, int smem_bytes) {
   int jb = 32;
-  while (jb > 4 && (size_t)n * (jb + 1) * 16 > (size_t)smem_bytes) jb >>= 1;
+  while (jb > 4 && (size_t)n * (jb + 2) * 16 > (size_t)smem_bytes) jb >>= 1;
   return jb;
 }
 
@@ -478,11 +605,12 @@ __device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, doub
   if (n <= kSmallInvMax) {
     double2* P = smem;
     double2* f = smem + (size_t)n * n;
+    double2* rowj = f + n;
     long long t0 = s.tr.start();
-    for (int i = threadIdx.x; i < n * n; i += blockDim.x) P[i] = A[i];
+    cta_copy(P, A, n * n);
     __syncthreads();
     for (int j = 0; j < n; ++j) {
-      int p = gj_step(P, n, n, j, j, f, s, s.flag);
+      int p = gj_step(P, n, n, j, j, f, rowj, s, s.flag);
       if (threadIdx.x == 0) s.piv[j] = p;
     }
     __syncthreads();
@@ -496,10 +624,7 @@ __device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, doub
       }
     }
     __syncthreads();
-    for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-      const int r = idx % n, c = idx / n;
-      out[idx] = P[r + (size_t)s.cperm[c] * n];
-    }
+    cta_copy_colperm(out, P, n, s.cperm);
     __syncthreads();
     s.tr.stop(TR_INV_OTHER, t0);
     int info = *s.flag;
@@ -516,21 +641,21 @@ __device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, doub
     const int jb = min(jb_max, n - k0);
     double2* P = smem;
     double2* f = smem + (size_t)n * jb;
+    double2* rowj = f + n;
     long long t0 = s.tr.start();
-    for (int idx = threadIdx.x; idx < n * jb; idx += blockDim.x)
-      P[idx] = xcur[(size_t)(idx % n) + (size_t)(k0 + idx / n) * n];
+    cta_copy_cols(P, xcur, n, k0, jb);
     for (int i = threadIdx.x; i < n; i += blockDim.x) s.perm[i] = i;
     __syncthreads();
     for (int jj = 0; jj < jb; ++jj) {
       const int j = k0 + jj;
-      int p = gj_step(P, n, jb, j, jj, f, s, s.flag);
+      int p = gj_step(P, n, jb, j, jj, f, rowj, s, s.flag);
       if (threadIdx.x == 0) {
         s.piv[j] = p;
         int tmp = s.perm[j]; s.perm[j] = s.perm[p]; s.perm[p] = tmp;
       }
       __syncthreads();
     }
-    for (int idx = threadIdx.x; idx < n * jb; idx += blockDim.x) W[idx] = P[idx];
+    cta_copy(W, P, n * jb);
     __syncthreads();
     s.tr.stop(TR_INV_PANEL, t0);
     t0 = s.tr.start();
@@ -554,10 +679,7 @@ __device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, doub
     }
   }
   __syncthreads();
-  for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
-    const int r = idx % n, c = idx / n;
-    out[idx] = xcur[r + (size_t)s.cperm[c] * n];
-  }
+  cta_copy_colperm(out, xcur, n, s.cperm);
   __syncthreads();
   s.tr.stop(TR_INV_OTHER, t1);
   int info = *s.flag;

@@ -21,6 +21,10 @@
 
 namespace negf {
 
+static_assert(kGemmSmemBytes <= kSmemMain, "GEMM staging ring must fit the main shared-memory region");
+static_assert((kSmallInvMax * kSmallInvMax + 3 * kSmallInvMax) * 16 <= kSmemMain,
+              "small inversion must fit the main shared-memory region");
+
 // ---------------------------------------------------------------- smem map
 struct SmemMap {
   double2* main;

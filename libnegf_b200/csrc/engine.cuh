@@ -8,7 +8,7 @@ namespace negf {
 
 constexpr int kMaxCont = 10;           // MAXNCONT (src/api/lnParams.h:10)
 constexpr int kMaxOrder = 1024;        // largest PL / contact PL size supported
-constexpr int kSmemMain = 96 * 1024;   // GEMM staging / inversion panel region
+constexpr int kSmemMain = 100 * 1024;  // GEMM staging ring / inversion panel region
 
 enum Mode : int { MODE_T = 0, MODE_DOS = 1, MODE_GN = 2 };
 
