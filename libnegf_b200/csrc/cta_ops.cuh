@@ -93,7 +93,7 @@ __device__ __forceinline__ Operand opC(const double2* p, int ld) { return Operan
 // ---------------------------------------------------------------- epilogues
 enum EpiMode : int {
   EPI_STORE = 0,   // C = alpha*acc + beta*C   (beta==0: C not read)
-  EPI_GJ = 1,      // Gauss-Jordan trailing update (see cta_zinv)
+  EPI_GJ = 1,      // Gauss-Jordan delayed update: C = acc + rowmask(X[perm,:]) (see cta_zinv)
 };
 
 struct Epilogue {
@@ -102,11 +102,11 @@ struct Epilogue {
   int ldc;
   double2 alpha, beta;
   // EPI_GJ
-  const double2* xcur;  // previous iterate, read with row permutation
+  const double2* xcur;  // target columns before the update, read with row permutation
   int ldx;
-  const int* perm;      // smem, full-length row permutation of this panel
-  const double2* W;     // panel (n x jb), ld = n
-  int k0, jb;
+  const int* perm;      // smem, full-length row permutation of the applied block
+  const double2* W;     // unused
+  int k0, jb;           // pivot rows [k0, k0+jb) of the applied block (masked)
   // optional reduction of max |C| over stored elements
   double* maxabs;       // smem accumulator (nullptr = off)
 };
@@ -181,7 +181,6 @@ __device__ __forceinline__ double2 epi_old(const Epilogue& e, int r, int c, int 
     if (e.beta.x == 0.0 && e.beta.y == 0.0) return make_double2(0.0, 0.0);
     return e.C[(size_t)r + (size_t)c * e.ldc];
   }
-  if (c >= e.k0 && c < e.k0 + e.jb) return e.W[(size_t)r + (size_t)(c - e.k0) * M];
   if (r >= e.k0 && r < e.k0 + e.jb) return make_double2(0.0, 0.0);
   return e.xcur[(size_t)e.perm[r] + (size_t)c * e.ldx];
 }
@@ -195,7 +194,7 @@ __device__ __forceinline__ void epi_store_one(const Epilogue& e, int r, int c, d
     out = make_double2(e.alpha.x * re - e.alpha.y * im, e.alpha.x * im + e.alpha.y * re);
     out = cadd(out, cmul(e.beta, old));
   } else {
-    out = (c >= e.k0 && c < e.k0 + e.jb) ? old : make_double2(re + old.x, im + old.y);
+    out = make_double2(re + old.x, im + old.y);
   }
   e.C[(size_t)r + (size_t)c * e.ldc] = out;
   if (want_max) lmax = fmax(lmax, cabs(out));
@@ -210,8 +209,17 @@ __device__ __forceinline__ void epi_store_one(const Epilogue& e, int r, int c, d
 // while the current tile's epilogue runs; K = 16 products (the Gauss-Jordan
 // updates) are as pipelined as long ones.  One specialisation per operand /
 // epilogue combination keeps the live state of the main loop in registers.
+template <int AM, int BM>
+__device__ __forceinline__ void gemm_issue(const Operand& A, const Operand& B, int M, int N, int K, int tilesM,
+                                           int ld_tile, int ld_kt, double2* st) {
+  const int m0 = (ld_tile % tilesM) * TM, n0 = (ld_tile / tilesM) * TN;
+  load_a_tile<AM>(A, M, K, m0, ld_kt * TK, st);
+  load_b_tile<BM>(B, K, N, ld_kt * TK, n0, st + TK * A_LD);
+  cp_async_commit();
+}
+
 template <int AM, int BM, int EM>
-__device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, const Operand B, const Epilogue& e,
+__device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, const Operand B, const Epilogue e,
                                         double2* smem) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -226,16 +234,8 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
   double accR[2][2][4], accI[2][2][4];
   int ld_tile = 0, ld_kt = 0;   // (tile, K-tile) of the next step to load
 
-  auto issue = [&](int buf) {
-    const int m0 = (ld_tile % tilesM) * TM, n0 = (ld_tile / tilesM) * TN;
-    double2* st = smem + buf * kStageElems;
-    load_a_tile<AM>(A, M, K, m0, ld_kt * TK, st);
-    load_b_tile<BM>(B, K, N, ld_kt * TK, n0, st + TK * A_LD);
-    cp_async_commit();
-    if (++ld_kt == nk) { ld_kt = 0; ++ld_tile; }
-  };
-
-  issue(0);
+  gemm_issue<AM, BM>(A, B, M, N, K, tilesM, ld_tile, ld_kt, smem);
+  if (++ld_kt == nk) { ld_kt = 0; ++ld_tile; }
   int tile = 0, kt = 0;
   for (int step = 0; step < total; ++step) {
     if (kt == 0) {
@@ -247,7 +247,8 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
           for (int q = 0; q < 4; ++q) { accR[i][j][q] = 0.0; accI[i][j][q] = 0.0; }
     }
     if (step + 1 < total) {
-      issue((step + 1) & 1);
+      gemm_issue<AM, BM>(A, B, M, N, K, tilesM, ld_tile, ld_kt, smem + ((step + 1) & 1) * kStageElems);
+      if (++ld_kt == nk) { ld_kt = 0; ++ld_tile; }
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -536,7 +537,7 @@ __device__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
 // f[] (n) and rowj[] (2w) are shared scratch.  Returns the pivot row chosen.
 // Four barriers per step: pivot search (2), exchange + capture (1),
 // scale + rank-1 update (1).
-__device__ __noinline__ int gj_step(double2* P, int n, int w, int j, int jj, double2* f, double2* rowj,
+__device__ __forceinline__ int gj_step(double2* P, int n, int w, int j, int jj, double2* f, double2* rowj,
                                     InvScratch& s, int* info) {
   const double2* colj = P + (size_t)jj * n;
   int p = cta_pivot(colj, j, n, s);
@@ -582,24 +583,51 @@ __device__ __noinline__ int gj_step(double2* P, int n, int w, int j, int jj, dou
   return p;
 }
 
-// Panel width of the blocked path for an n x n inversion within `smem_bytes`
-__host__ __device__ inline int zinv_panel(int n, int smem_bytes) {
-  int jb = 32;
-  while (jb > 4 && (size_t)n * (jb + 2) * 16 > (size_t)smem_bytes) jb >>= 1;
-  return jb;
+// Widest leaf (columns factorised in shared memory at once) for order n.
+__host__ __device__ inline int zinv_leaf_max(int n, int smem_bytes) {
+  int w = 16;
+  while (w > 2 && (size_t)n * (w + 2) * 16 > (size_t)smem_bytes) --w;
+  return w;
 }
 
-// Workspace (complex elements) for cta_zinv of order n.
+// Workspace (complex elements) for cta_zinv of order n: two n x n buffers.
 __host__ __device__ inline size_t zinv_ws_elems(int n, int smem_bytes) {
+  (void)smem_bytes;
   if (n <= kSmallInvMax) return 0;
-  return 2 * (size_t)n * n + (size_t)n * zinv_panel(n, smem_bytes);
+  return 2 * (size_t)n * n;
+}
+
+// Row permutation of the pivots of columns [c0, c1), composed in order
+// (position i of the transformed block holds row perm[i] of the input).
+__device__ void gj_block_perm(int* perm, const int* piv, int n, int c0, int c1) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int j = c0; j < c1; ++j) {
+      const int p = piv[j];
+      const int t = perm[j]; perm[j] = perm[p]; perm[p] = t;
+    }
+  __syncthreads();
 }
 
 // out = A^-1 (n x n).  A is read only (out may alias A).  `ws` holds
 // zinv_ws_elems(n) elements.  `smem` holds smem_bytes.  Returns info
 // (0 or the 1-based column of the first exactly-zero pivot) in all threads.
-__device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, double2* ws, double2* smem, int smem_bytes,
-                        InvScratch& s) {
+//
+// n <= kSmallInvMax: Gauss-Jordan with partial pivoting on the whole matrix
+// in shared memory.  Larger n: the same elimination with delayed updates
+// over a perfect binary tree of 2^d column leaves.  A leaf is factorised in
+// shared memory once every earlier pivot has been applied to it; after the
+// left half of a node is done, its pivots are applied to the right half,
+// and after the right half, the right half's pivots to the left half, each
+// as one product X' = rowmask(X[perm,:]) + W * X[perm[J],:] with K equal to
+// the half's width (n/2, n/4, ...).  Every column is rewritten once per tree
+// level, so the matrix makes d ~ log2(n/16) trips through memory instead of
+// n/16.  Products are out of place between two buffers (row exchanges then
+// have no hazards); a perfect tree keeps every leaf of a node in the same
+// buffer.
+__device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, double2* ws, double2* smem,
+                                     int smem_bytes, InvScratch& s) {
   if (threadIdx.x == 0) *s.flag = 0;
   __syncthreads();
   if (n <= kSmallInvMax) {
@@ -631,57 +659,78 @@ __device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, doub
     __syncthreads();
     return info;
   }
-  const int jb_max = zinv_panel(n, smem_bytes);
-  double2* X0 = ws;
-  double2* X1 = ws + (size_t)n * n;
-  double2* W = ws + 2 * (size_t)n * n;
-  const double2* xcur = A;
-  double2* xnext = X0;
-  for (int k0 = 0; k0 < n; k0 += jb_max) {
-    const int jb = min(jb_max, n - k0);
+  const int wmax = zinv_leaf_max(n, smem_bytes);
+  int d = 0;
+  while ((n + (1 << d) - 1) >> d > wmax) ++d;
+  const int nl = 1 << d;
+  double2* buf[2] = {ws, ws + (size_t)n * n};
+  unsigned char* par = reinterpret_cast<unsigned char*>(s.cperm);   // per-leaf buffer index (nl <= n)
+  long long t0 = s.tr.start();
+  cta_copy(buf[0], A, n * n);
+  for (int k = threadIdx.x; k < nl; k += blockDim.x) par[k] = 0;
+  __syncthreads();
+  s.tr.stop(TR_INV_OTHER, t0);
+  for (int k = 0; k < nl; ++k) {
+    // ---- factorise leaf k in shared memory
+    t0 = s.tr.start();
+    const int c0 = (k * n) >> d, c1 = ((k + 1) * n) >> d, w = c1 - c0;
     double2* P = smem;
-    double2* f = smem + (size_t)n * jb;
+    double2* f = smem + (size_t)n * w;
     double2* rowj = f + n;
-    long long t0 = s.tr.start();
-    cta_copy_cols(P, xcur, n, k0, jb);
-    for (int i = threadIdx.x; i < n; i += blockDim.x) s.perm[i] = i;
+    double2* src = buf[par[k]] + (size_t)c0 * n;
+    cta_copy(P, src, n * w);
     __syncthreads();
-    for (int jj = 0; jj < jb; ++jj) {
-      const int j = k0 + jj;
-      int p = gj_step(P, n, jb, j, jj, f, rowj, s, s.flag);
-      if (threadIdx.x == 0) {
-        s.piv[j] = p;
-        int tmp = s.perm[j]; s.perm[j] = s.perm[p]; s.perm[p] = tmp;
-      }
-      __syncthreads();
+    for (int jj = 0; jj < w; ++jj) {
+      const int j = c0 + jj;
+      int p = gj_step(P, n, w, j, jj, f, rowj, s, s.flag);
+      if (threadIdx.x == 0) s.piv[j] = p;
     }
-    cta_copy(W, P, n * jb);
+    cta_copy(src, P, n * w);
     __syncthreads();
     s.tr.stop(TR_INV_PANEL, t0);
-    t0 = s.tr.start();
-    // X_next = mask_J(X_cur[perm,:]) + W * X_cur[perm[J],:] ; X_next[:,J] = W
-    Operand Aop = opN(W, n);
-    Operand Bop{xcur, n, OP_GATHER, s.perm + k0};
-    Epilogue e;
-    e.mode = EPI_GJ; e.C = xnext; e.ldc = n; e.alpha = make_double2(1, 0); e.beta = make_double2(0, 0);
-    e.xcur = xcur; e.ldx = n; e.perm = s.perm; e.W = W; e.k0 = k0; e.jb = jb; e.maxabs = nullptr;
-    cta_gemm(n, n, jb, Aop, Bop, e, smem);
-    s.tr.stop(TR_INV_UPDATE, t0);
-    xcur = xnext;
-    xnext = (xnext == X0) ? X1 : X0;
+    // ---- delayed updates of the tree nodes this leaf closes
+    for (int l = 1; l <= d; ++l) {
+      const int size = 1 << l, half = size >> 1;
+      const int r = (k + 1) & (size - 1);
+      if (r != half && r != 0) break;
+      const int lo = (k >> l) << l;
+      const int fa = (r == half) ? lo : lo + half;       // leaves whose pivots are applied
+      const int ta = (r == half) ? lo + half : lo;       // leaves that receive them
+      const int j0 = (fa * n) >> d, j1 = ((fa + half) * n) >> d;
+      const int a0 = (ta * n) >> d, a1 = ((ta + half) * n) >> d;
+      t0 = s.tr.start();
+      gj_block_perm(s.perm, s.piv, n, j0, j1);
+      const int pw = par[fa], pt = par[ta];
+      double2* W = buf[pw] + (size_t)j0 * n;
+      const double2* X = buf[pt] + (size_t)a0 * n;
+      double2* Y = buf[pt ^ 1] + (size_t)a0 * n;
+      Operand Aop = opN(W, n);
+      Operand Bop{X, n, OP_GATHER, s.perm + j0};
+      Epilogue e;
+      e.mode = EPI_GJ; e.C = Y; e.ldc = n; e.alpha = make_double2(1, 0); e.beta = make_double2(0, 0);
+      e.xcur = X; e.ldx = n; e.perm = s.perm; e.W = nullptr; e.k0 = j0; e.jb = j1 - j0; e.maxabs = nullptr;
+      cta_gemm(n, a1 - a0, j1 - j0, Aop, Bop, e, smem);
+      for (int q = threadIdx.x; q < half; q += blockDim.x) par[ta + q] ^= 1;
+      __syncthreads();
+      s.tr.stop(TR_INV_UPDATE, t0);
+      if (r == half) break;
+    }
   }
-  long long t1 = s.tr.start();
+  // every leaf went through one update per level: all sit in buf[par[0]]
+  t0 = s.tr.start();
+  const double2* X = buf[par[0]];
+  __syncthreads();
   if (threadIdx.x == 0) {
-    for (int c = 0; c < n; ++c) s.cperm[c] = c;
+    for (int c = 0; c < n; ++c) s.perm[c] = c;
     for (int j = n - 1; j >= 0; --j) {
       int p = s.piv[j];
-      int tmp = s.cperm[j]; s.cperm[j] = s.cperm[p]; s.cperm[p] = tmp;
+      int tmp = s.perm[j]; s.perm[j] = s.perm[p]; s.perm[p] = tmp;
     }
   }
   __syncthreads();
-  cta_copy_colperm(out, xcur, n, s.cperm);
+  cta_copy_colperm(out, X, n, s.perm);
   __syncthreads();
-  s.tr.stop(TR_INV_OTHER, t1);
+  s.tr.stop(TR_INV_OTHER, t0);
   int info = *s.flag;
   __syncthreads();
   return info;
