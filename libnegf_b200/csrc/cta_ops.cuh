@@ -78,6 +78,7 @@ enum OpMode : int {
   OP_N = 0,       // X(r,c) = p[r + c*ld]
   OP_C = 1,       // X(r,c) = conj(p[c + r*ld])   (conjugate transpose)
   OP_GATHER = 2,  // X(r,c) = p[perm[r] + c*ld]   (row gather, perm in smem)
+  OP_RT = -1,     // template argument only: the mode is read from the descriptor
 };
 
 struct Operand {
@@ -94,6 +95,7 @@ __device__ __forceinline__ Operand opC(const double2* p, int ld) { return Operan
 enum EpiMode : int {
   EPI_STORE = 0,   // C = alpha*acc + beta*C   (beta==0: C not read)
   EPI_GJ = 1,      // Gauss-Jordan delayed update: C = acc + rowmask(X[perm,:]) (see cta_zinv)
+  EPI_RT = -1,     // template argument only: the mode is read from the descriptor
 };
 
 struct Epilogue {
@@ -209,33 +211,106 @@ __device__ __forceinline__ void epi_store_one(const Epilogue& e, int r, int c, d
 // while the current tile's epilogue runs; K = 16 products (the Gauss-Jordan
 // updates) are as pipelined as long ones.  One specialisation per operand /
 // epilogue combination keeps the live state of the main loop in registers.
+// GEMM parameters, written to shared memory by the caller and re-read by the
+// product loop after each barrier.  Parameters that only sit in memory cost
+// the loop no registers; the accumulators and fragments get them all.
+struct GemmDesc {
+  const double2* A;
+  const double2* B;
+  double2* C;
+  const int* aperm;
+  const int* bperm;
+  const double2* xcur;
+  const int* perm;
+  double* maxabs;
+  double2 alpha, beta;
+  int M, N, K, lda, ldb, ldc, ldx, k0, jb, tilesM, nk, total;
+  int amode, bmode, emode;
+};
+constexpr int kGemmDescOffset = kStages * kStageElems;   // in double2 units, after the staging ring
+
 template <int AM, int BM>
-__device__ __forceinline__ void gemm_issue(const Operand& A, const Operand& B, int M, int N, int K, int tilesM,
-                                           int ld_tile, int ld_kt, double2* st) {
+__device__ __forceinline__ void gemm_issue(const GemmDesc* d, int ld_tile, int ld_kt, double2* st) {
+  const int tilesM = d->tilesM;
   const int m0 = (ld_tile % tilesM) * TM, n0 = (ld_tile / tilesM) * TN;
-  load_a_tile<AM>(A, M, K, m0, ld_kt * TK, st);
-  load_b_tile<BM>(B, K, N, ld_kt * TK, n0, st + TK * A_LD);
+  const Operand A{d->A, d->lda, AM, d->aperm};
+  const Operand B{d->B, d->ldb, BM, d->bperm};
+  if constexpr (AM >= 0) {
+    load_a_tile<AM>(A, d->M, d->K, m0, ld_kt * TK, st);
+  } else {
+    const int am = d->amode;
+    if (am == OP_C) load_a_tile<OP_C>(A, d->M, d->K, m0, ld_kt * TK, st);
+    else if (am == OP_GATHER) load_a_tile<OP_GATHER>(A, d->M, d->K, m0, ld_kt * TK, st);
+    else load_a_tile<OP_N>(A, d->M, d->K, m0, ld_kt * TK, st);
+  }
+  if constexpr (BM >= 0) {
+    load_b_tile<BM>(B, d->K, d->N, ld_kt * TK, n0, st + TK * A_LD);
+  } else {
+    const int bm = d->bmode;
+    if (bm == OP_C) load_b_tile<OP_C>(B, d->K, d->N, ld_kt * TK, n0, st + TK * A_LD);
+    else if (bm == OP_GATHER) load_b_tile<OP_GATHER>(B, d->K, d->N, ld_kt * TK, n0, st + TK * A_LD);
+    else load_b_tile<OP_N>(B, d->K, d->N, ld_kt * TK, n0, st + TK * A_LD);
+  }
   cp_async_commit();
 }
 
+// x with its sign bit flipped when m == 0x80000000 (integer pipe, no FP64 op)
+__device__ __forceinline__ double flip_sign(double x, unsigned m) {
+  return __hiloint2double(__double2hiint(x) ^ (int)m, __double2loint(x));
+}
+
+template <int EMODE>
+__device__ __forceinline__ double2 epi_old_d(const GemmDesc* d, int r, int c) {
+  if (r >= d->M || c >= d->N) return make_double2(0.0, 0.0);
+  if (EMODE == EPI_STORE || (EMODE == EPI_RT && d->emode == EPI_STORE)) {
+    const double2 be = d->beta;
+    if (be.x == 0.0 && be.y == 0.0) return make_double2(0.0, 0.0);
+    return d->C[(size_t)r + (size_t)c * d->ldc];
+  }
+  if (r >= d->k0 && r < d->k0 + d->jb) return make_double2(0.0, 0.0);
+  return d->xcur[(size_t)d->perm[r] + (size_t)c * d->ldx];
+}
+
+template <int EMODE>
+__device__ __forceinline__ void epi_store_d(const GemmDesc* d, int r, int c, double re, double im, double2 old,
+                                            double& lmax) {
+  if (r >= d->M || c >= d->N) return;
+  double2 out;
+  if (EMODE == EPI_STORE || (EMODE == EPI_RT && d->emode == EPI_STORE)) {
+    const double2 al = d->alpha;
+    out = make_double2(al.x * re - al.y * im, al.x * im + al.y * re);
+    out = cadd(out, cmul(d->beta, old));
+  } else {
+    out = make_double2(re + old.x, im + old.y);
+  }
+  d->C[(size_t)r + (size_t)c * d->ldc] = out;
+  if (d->maxabs) lmax = fmax(lmax, cabs(out));
+}
+
+// The product loop.  All threads of the CTA call it after the descriptor at
+// smem + kGemmDescOffset has been written and published by a barrier.
+//
+// Out-of-line device functions here are kept leaves (none calls another
+// out-of-line function): with a call chain of depth two anywhere in a
+// kernel, the compiler gives every callee the full save/restore calling
+// convention and this loop spills (measured: 30 % slower).  cta_gemm_t is the
+// out-of-line copy for the engine's top level; cta_gemm_body is inlined into
+// the inversion.
 template <int AM, int BM, int EM>
-__device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, const Operand B, const Epilogue e,
-                                        double2* smem) {
+__device__ __forceinline__ void cta_gemm_body(const GemmDesc* d, double2* smem) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
   const int wm = warp & 1, wn = warp >> 1;
-  constexpr double ca = (AM == OP_C) ? -1.0 : 1.0;
-  constexpr double cb = (BM == OP_C) ? -1.0 : 1.0;
-  const bool want_max = e.maxabs != nullptr;
-  const int tilesM = (M + TM - 1) / TM, tilesN = (N + TN - 1) / TN;
-  const int nk = max(1, (K + TK - 1) / TK);
-  const int total = tilesM * tilesN * nk;
+  // sign masks of the imaginary parts (conjugated operands)
+  const unsigned sa = (AM >= 0) ? (AM == OP_C ? 0x80000000u : 0u) : (d->amode == OP_C ? 0x80000000u : 0u);
+  const unsigned sb = (BM >= 0) ? (BM == OP_C ? 0x80000000u : 0u) : (d->bmode == OP_C ? 0x80000000u : 0u);
+  const int total = d->total;
   double lmax = 0.0;
   double accR[2][2][4], accI[2][2][4];
   int ld_tile = 0, ld_kt = 0;   // (tile, K-tile) of the next step to load
 
-  gemm_issue<AM, BM>(A, B, M, N, K, tilesM, ld_tile, ld_kt, smem);
-  if (++ld_kt == nk) { ld_kt = 0; ++ld_tile; }
+  gemm_issue<AM, BM>(d, ld_tile, ld_kt, smem);
+  if (++ld_kt == d->nk) { ld_kt = 0; ++ld_tile; }
   int tile = 0, kt = 0;
   for (int step = 0; step < total; ++step) {
     if (kt == 0) {
@@ -247,8 +322,8 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
           for (int q = 0; q < 4; ++q) { accR[i][j][q] = 0.0; accI[i][j][q] = 0.0; }
     }
     if (step + 1 < total) {
-      gemm_issue<AM, BM>(A, B, M, N, K, tilesM, ld_tile, ld_kt, smem + ((step + 1) & 1) * kStageElems);
-      if (++ld_kt == nk) { ld_kt = 0; ++ld_tile; }
+      gemm_issue<AM, BM>(d, ld_tile, ld_kt, smem + ((step + 1) & 1) * kStageElems);
+      if (++ld_kt == d->nk) { ld_kt = 0; ++ld_tile; }
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
@@ -266,14 +341,14 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
         double2 v0 = sA[k * A_LD + r0];
         double2 v1 = sA[k * A_LD + r0 + 8];
         are[i][0] = v0.x; are[i][1] = v1.x;
-        aim[i][0] = ca * v0.y; aim[i][1] = ca * v1.y;
-        nai[i][0] = -aim[i][0]; nai[i][1] = -aim[i][1];
+        aim[i][0] = flip_sign(v0.y, sa); aim[i][1] = flip_sign(v1.y, sa);
+        nai[i][0] = flip_sign(v0.y, sa ^ 0x80000000u); nai[i][1] = flip_sign(v1.y, sa ^ 0x80000000u);
       }
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
         const int c = wn * 16 + j * 8 + g;
         double2 v = sB[c * B_LD + k];
-        bre[j] = v.x; bim[j] = cb * v.y;
+        bre[j] = v.x; bim[j] = flip_sign(v.y, sb);
       }
       // four independent accumulators between two updates of the same one
 #pragma unroll
@@ -294,7 +369,8 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
         for (int j = 0; j < 2; ++j) dmma_16x8x4(accI[i][j], aim[i][0], aim[i][1], bre[j]);
     }
     __syncthreads();
-    if (kt == nk - 1) {
+    if (kt == d->nk - 1) {
+      const int tilesM = d->tilesM;
       const int m0 = (tile % tilesM) * TM, n0 = (tile / tilesM) * TN;
 #pragma unroll
       for (int i = 0; i < 2; ++i) {
@@ -305,7 +381,7 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
           for (int q = 0; q < 4; ++q) {
             const int r = m0 + wm * 32 + i * 16 + g + ((q >> 1) << 3);
             const int c = n0 + wn * 16 + j * 8 + 2 * t + (q & 1);
-            old[j][q] = epi_old<EM>(e, r, c, M, N);
+            old[j][q] = epi_old_d<EM>(d, r, c);
           }
 #pragma unroll
         for (int j = 0; j < 2; ++j)
@@ -313,36 +389,60 @@ __device__ __noinline__ void cta_gemm_t(int M, int N, int K, const Operand A, co
           for (int q = 0; q < 4; ++q) {
             const int r = m0 + wm * 32 + i * 16 + g + ((q >> 1) << 3);
             const int c = n0 + wn * 16 + j * 8 + 2 * t + (q & 1);
-            epi_store_one<EM>(e, r, c, accR[i][j][q], accI[i][j][q], old[j][q], M, N, lmax, want_max);
+            epi_store_d<EM>(d, r, c, accR[i][j][q], accI[i][j][q], old[j][q], lmax);
           }
       }
     }
-    if (++kt == nk) { kt = 0; ++tile; }
+    if (++kt == d->nk) { kt = 0; ++tile; }
   }
-  if (want_max) {
+  if (d->maxabs) {
     // warp max then one atomic per warp on the shared accumulator
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) lmax = fmax(lmax, __shfl_xor_sync(0xffffffffu, lmax, o));
     if (lane == 0) {
-      unsigned long long* a = reinterpret_cast<unsigned long long*>(e.maxabs);
+      unsigned long long* a = reinterpret_cast<unsigned long long*>(d->maxabs);
       atomicMax(a, (unsigned long long)__double_as_longlong(lmax));  // lmax >= 0: bit order == value order
     }
   }
   __syncthreads();
 }
 
-// Runtime dispatch to the specialisations in use.
+template <int AM, int BM, int EM>
+__device__ __noinline__ void cta_gemm_t(const GemmDesc* d, double2* smem) {
+  cta_gemm_body<AM, BM, EM>(d, smem);
+}
+
+__device__ __forceinline__ GemmDesc* gemm_desc_publish(int M, int N, int K, const Operand& A, const Operand& B,
+                                                       const Epilogue& e, double2* smem) {
+  GemmDesc* d = reinterpret_cast<GemmDesc*>(smem + kGemmDescOffset);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    d->A = A.p; d->lda = A.ld; d->aperm = A.perm;
+    d->B = B.p; d->ldb = B.ld; d->bperm = B.perm;
+    d->C = e.C; d->ldc = e.ldc; d->alpha = e.alpha; d->beta = e.beta;
+    d->xcur = e.xcur; d->ldx = e.ldx; d->perm = e.perm; d->k0 = e.k0; d->jb = e.jb;
+    d->maxabs = e.maxabs;
+    d->M = M; d->N = N; d->K = K;
+    d->amode = A.mode; d->bmode = B.mode; d->emode = e.mode;
+    d->tilesM = (M + TM - 1) / TM;
+    d->nk = max(1, (K + TK - 1) / TK);
+    d->total = d->tilesM * ((N + TN - 1) / TN) * d->nk;
+  }
+  __syncthreads();
+  return d;
+}
+
+// C(MxN) = epilogue( op(A)(MxK) * op(B)(KxN) ).  All threads of the CTA must
+// call it.  `smem` must hold kGemmSmemBytes + sizeof(GemmDesc).  Ends with
+// __syncthreads().
+//
+// The operand pipeline runs over the flattened sequence of (output tile,
+// K-tile) steps, so the next output tile's first operands are in flight
+// while the current tile's epilogue runs; K = 16 products are as pipelined
+// as long ones.  One specialisation per operand / epilogue combination.
 __device__ __forceinline__ void cta_gemm(int M, int N, int K, const Operand& A, const Operand& B, const Epilogue& e,
                                          double2* smem) {
-  if (e.mode == EPI_GJ) {
-    cta_gemm_t<OP_N, OP_GATHER, EPI_GJ>(M, N, K, A, B, e, smem);
-  } else if (A.mode == OP_N && B.mode == OP_N) {
-    cta_gemm_t<OP_N, OP_N, EPI_STORE>(M, N, K, A, B, e, smem);
-  } else if (A.mode == OP_N && B.mode == OP_C) {
-    cta_gemm_t<OP_N, OP_C, EPI_STORE>(M, N, K, A, B, e, smem);
-  } else {
-    cta_gemm_t<OP_C, OP_N, EPI_STORE>(M, N, K, A, B, e, smem);
-  }
+  cta_gemm_t<OP_RT, OP_RT, EPI_RT>(gemm_desc_publish(M, N, K, A, B, e, smem), smem);
 }
 
 // ---------------------------------------------------------------- elementwise
@@ -385,7 +485,7 @@ __device__ __noinline__ void cta_esh(double2* D, int rows, int cols, const doubl
   }
 }
 
-__device__ void cta_copy(double2* D, const double2* S, int n) {
+__device__ __forceinline__ void cta_copy(double2* D, const double2* S, int n) {
   constexpr int U = 4;
   for (int base = threadIdx.x; base < n; base += U * blockDim.x) {
     double2 v[U];
@@ -399,7 +499,7 @@ __device__ void cta_copy(double2* D, const double2* S, int n) {
 }
 
 // D(r, c) = S(r, cperm[c]) for an n x n matrix (column gather)
-__device__ void cta_copy_colperm(double2* D, const double2* S, int n, const int* cperm) {
+__device__ __forceinline__ void cta_copy_colperm(double2* D, const double2* S, int n, const int* cperm) {
   constexpr int U = 4;
   const int nn = n * n;
   for (int base = threadIdx.x; base < nn; base += U * blockDim.x) {
@@ -418,12 +518,12 @@ __device__ void cta_copy_colperm(double2* D, const double2* S, int n, const int*
 }
 
 // D (n x w, ld n) = columns [k0, k0+w) of S (ld n)
-__device__ void cta_copy_cols(double2* D, const double2* S, int n, int k0, int w) {
+__device__ __forceinline__ void cta_copy_cols(double2* D, const double2* S, int n, int k0, int w) {
   cta_copy(D, S + (size_t)k0 * n, n * w);
 }
 
 // D = i*(A - A^dag)   (zspectral_dns), A square n x n
-__device__ void cta_spectral(double2* D, const double2* A, int n) {
+__device__ __forceinline__ void cta_spectral(double2* D, const double2* A, int n) {
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     const int r = idx % n, c = idx / n;
     double2 a = A[idx], b = cconj(A[(size_t)c + (size_t)r * n]);
@@ -433,7 +533,7 @@ __device__ void cta_spectral(double2* D, const double2* A, int n) {
 }
 
 // block-wide sum of doubles, result valid in all threads; `red` smem >= 32 doubles
-__device__ double cta_sum(double v, double* red) {
+__device__ __forceinline__ double cta_sum(double v, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -446,7 +546,7 @@ __device__ double cta_sum(double v, double* red) {
   return s;
 }
 
-__device__ double cta_max(double v, double* red) {
+__device__ __forceinline__ double cta_max(double v, double* red) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -460,7 +560,7 @@ __device__ double cta_max(double v, double* red) {
 }
 
 // Re Tr(X Y) = sum_{i,j} Re(X(i,j) Y(j,i)); op applies to Y (OP_C: Y = Z^dag)
-__device__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red) {
+__device__ __forceinline__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red) {
   double acc = 0.0;
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     const int i = idx % n, j = idx / n;
@@ -506,7 +606,7 @@ struct InvScratch {
 
 // Pivot search on a column in shared memory: rows [j, n) of col[] -> index
 // of max |Re|+|Im| (first occurrence, as izamax).  All threads call.
-__device__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
+__device__ __forceinline__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double best = -1.0;
   int bi = n;
@@ -599,7 +699,7 @@ __host__ __device__ inline size_t zinv_ws_elems(int n, int smem_bytes) {
 
 // Row permutation of the pivots of columns [c0, c1), composed in order
 // (position i of the transformed block holds row perm[i] of the input).
-__device__ void gj_block_perm(int* perm, const int* piv, int n, int c0, int c1) {
+__device__ __forceinline__ void gj_block_perm(int* perm, const int* piv, int n, int c0, int c1) {
   for (int i = threadIdx.x; i < n; i += blockDim.x) perm[i] = i;
   __syncthreads();
   if (threadIdx.x == 0)
@@ -709,7 +809,7 @@ __device__ __noinline__ int cta_zinv(int n, const double2* A, double2* out, doub
       Epilogue e;
       e.mode = EPI_GJ; e.C = Y; e.ldc = n; e.alpha = make_double2(1, 0); e.beta = make_double2(0, 0);
       e.xcur = X; e.ldx = n; e.perm = s.perm; e.W = nullptr; e.k0 = j0; e.jb = j1 - j0; e.maxabs = nullptr;
-      cta_gemm(n, a1 - a0, j1 - j0, Aop, Bop, e, smem);
+      cta_gemm_t<OP_RT, OP_RT, EPI_RT>(gemm_desc_publish(n, a1 - a0, j1 - j0, Aop, Bop, e, smem), smem);
       for (int q = threadIdx.x; q < half; q += blockDim.x) par[ta + q] ^= 1;
       __syncthreads();
       s.tr.stop(TR_INV_UPDATE, t0);

@@ -1,0 +1,815 @@
+// The per-point program of the persistent engine, written as a resumable
+// generator.
+//
+// A CTA's work alternates between control (which block operation comes
+// next, convergence decisions, bookkeeping) and the block operations
+// themselves (GEMM on the FP64 tensor pipe, Gauss-Jordan inversion, ES-H
+// assembly, traces).  Calling the block operations from deep inside the
+// control code made every heavy routine run under the register pressure of
+// its callers.  Here the control code is a generator: next_op() runs until
+// it has filled one Op descriptor and returns; the kernel's top level then
+// executes the op with exec_op() in a clean register context and calls
+// next_op() again, which resumes where it stopped.  The generator keeps all
+// state that must survive an op in a Prog struct (local memory), switch-
+// based resumption points (PT_EMIT) mark where it yields.  Op results the
+// control code needs (max|C1|, pivot info, traces) come back in shared
+// memory.  All threads of the CTA run the generator identically.
+//
+// The operation sequence is the one of libNEGF's per-point solve:
+// decimation src/contselfenergy.F90:271-340, contact self-energies :445-491,
+// build_ESH src/iterative.F90:1956, gsmr/Gr/Gn sweeps
+// src/iterative_cpu.F90:51-372, transmissions :399-583, DOS
+// src/iterative.F90:1821-1952, elastic SCBA :289-363 with
+// src/elphdd.F90:108-276 and src/scba.F90:120-147, Meir-Wingreen and layer
+// currents src/iterative.F90:382-461.
+#pragma once
+#include "cta_ops.cuh"
+#include "engine.cuh"
+
+namespace negf {
+
+// ---------------------------------------------------------------- smem map
+struct SmemMap {
+  double2* main;
+  InvScratch inv;
+  double* red;
+  double* maxv;
+  double* res;      // op results read by the control code
+  int* ires;
+  int* item;
+  Trace tr;
+};
+
+__device__ __forceinline__ SmemMap map_smem(char* base, int nmax) {
+  SmemMap m;
+  m.main = reinterpret_cast<double2*>(base);
+  char* p = base + kSmemMain;
+  m.red = reinterpret_cast<double*>(p); p += 32 * sizeof(double);
+  m.maxv = reinterpret_cast<double*>(p); p += 2 * sizeof(double);
+  m.res = reinterpret_cast<double*>(p); p += 8 * sizeof(double);
+  m.inv.redv = reinterpret_cast<double*>(p); p += 32 * sizeof(double);
+  m.inv.redi = reinterpret_cast<int*>(p); p += 32 * sizeof(int);
+  m.inv.flag = reinterpret_cast<int*>(p); p += 4 * sizeof(int);
+  m.item = reinterpret_cast<int*>(p); p += 4 * sizeof(int);
+  m.ires = reinterpret_cast<int*>(p); p += 4 * sizeof(int);
+  m.inv.piv = reinterpret_cast<int*>(p); p += nmax * sizeof(int);
+  m.inv.perm = reinterpret_cast<int*>(p); p += nmax * sizeof(int);
+  m.inv.cperm = reinterpret_cast<int*>(p); p += nmax * sizeof(int);
+  p = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(p) + 7) & ~uintptr_t(7));
+  m.tr.acc = reinterpret_cast<long long*>(p);   // TR_NPHASE entries; enabled by the caller
+  m.inv.tr.acc = nullptr;
+  return m;
+}
+
+inline size_t smem_bytes_for(int nmax) {
+  return kSmemMain + 32 * 8 + 2 * 8 + 8 * 8 + 32 * 8 + 32 * 4 + 4 * 4 + 4 * 4 + 4 * 4 + 3 * (size_t)nmax * 4 + 8 +
+         TR_NPHASE * 8;
+}
+
+__device__ __forceinline__ double2 cz(double re, double im) { return make_double2(re, im); }
+
+// Workspace slots: 0..11 scratch (0..7 also the decimation buffers),
+// 12..14 inversion workspace, 15.. one self-energy per contact, then the
+// per-layer arrays.
+enum : int { S_INV = 12, S_SIG = 15 };
+
+struct Ws {
+  double2* base;
+  int64_t Q;
+  int ncont;
+  __device__ double2* slot(int k) const { return base + (int64_t)k * Q; }
+  __device__ double2* inv() const { return slot(S_INV); }
+  __device__ double2* sig(int c) const { return slot(S_SIG + c); }
+  __device__ double2* layer(int arr, int i, int nbl) const { return slot(S_SIG + ncont + arr * nbl + i); }
+};
+
+// ---------------------------------------------------------------- ops
+enum OpKind : int {
+  K_NONE = 0,
+  K_GEMM,      // C = alpha op(A) op(B) + beta C   (flag: reduce max|C| into sm.maxv)
+  K_ZINV,      // C = A^-1, order n                 (info -> ires[0])
+  K_ESH,       // C (m x n) = s_e S - H - sub - diag(subdiag)   (A = H, X = S, Y = sub, V = subdiag)
+  K_COPY,      // C = A, m elements
+  K_SUB,       // C -= A, m elements
+  K_DECUPD,    // C -= A and D -= A, m elements (decimation Ao_s, Ao update)
+  K_SPECTRAL,  // C = i (A - A^dag), order m
+  K_TRACE,     // res[slot] = Re Tr(A op(B)), order m
+  K_TRACEC,    // res[slot], res[slot+1] = Tr(A op(B)), A m x n
+  K_TRACEN,    // res[slot] = Re Tr(A B^dag), A and B m x n
+  K_DOS,       // out[k] = -Im A_kk / pi, k < m
+  K_SIGDIAG,   // C[k] = cpl[k]^2 A_kk, k < m
+  K_SNINIT,    // C (m x m) = diag(A) or 0
+  K_SNGAMMA,   // C += scal * i (A - A^dag), order m
+  K_DAGGER,    // C (m x n) = A^dag, A is n x m
+  K_ERRDIAG,   // res[slot] = max(res[slot], max_k |A_kk - B_kk|), order m
+  K_ERRPAT,    // res[slot] = max(res[slot], max_{X(q) != 0} |A(q) - B(q)|), m x n;
+               //   Y (n x m) adds the pattern of Y at transposed positions
+  K_MAXABS,    // res[slot] = max |A(q)|, m elements
+  K_TRDIAG,    // res[slot] = Re Tr A, order m
+};
+
+struct Op {
+  int kind;
+  int m, n, k;
+  int opa, opb, flag, slot;
+  int lda, ldb, ldc, pad;
+  const double2* A;
+  const double2* B;
+  double2* C;
+  double2* D;
+  const double2* X;
+  const double2* Y;
+  const double2* V;
+  const double* cpl;
+  double* out;
+  double2 alpha, beta;
+  double scal;
+};
+
+__device__ __forceinline__ void set_gemm(Op& o, int M, int N, int K, const double2* A, int lda, int opa,
+                                         const double2* B, int ldb, int opb, double2* C, int ldc, double2 al,
+                                         double2 be, int want_max = 0) {
+  o.kind = K_GEMM; o.m = M; o.n = N; o.k = K; o.A = A; o.lda = lda; o.opa = opa; o.B = B; o.ldb = ldb;
+  o.opb = opb; o.C = C; o.ldc = ldc; o.alpha = al; o.beta = be; o.flag = want_max;
+}
+
+__device__ __forceinline__ void set_esh(Op& o, double2* D, int rows, int cols, const double2* H, const double2* S,
+                                        double2 se, int diag, const double2* sub, const double2* subdiag, int opm) {
+  o.kind = K_ESH; o.C = D; o.m = rows; o.n = cols; o.A = H; o.X = S; o.alpha = se; o.flag = diag; o.Y = sub;
+  o.V = subdiag; o.opa = opm;
+}
+
+__device__ __forceinline__ void set_simple(Op& o, int kind, int m, const double2* A, double2* C) {
+  o.kind = kind; o.m = m; o.A = A; o.C = C;
+}
+
+// ---------------------------------------------------------------- executor
+__device__ __forceinline__ void exec_op(const Op& o, SmemMap& sm, double2* invws) {
+  const int tid = threadIdx.x;
+  long long t0 = sm.tr.start();
+  switch (o.kind) {
+    case K_GEMM: {
+      Epilogue e = epi_store(o.C, o.ldc, o.alpha, o.beta);
+      if (o.flag) {
+        if (tid == 0) *sm.maxv = 0.0;
+        __syncthreads();
+        e.maxabs = sm.maxv;
+      }
+      cta_gemm(o.m, o.n, o.k, Operand{o.A, o.lda, o.opa, nullptr}, Operand{o.B, o.ldb, o.opb, nullptr}, e, sm.main);
+      sm.tr.stop(TR_GEMM, t0);
+      return;
+    }
+    case K_ZINV: {
+      const int info = cta_zinv(o.m, o.A, o.C, invws, sm.main, kSmemMain, sm.inv);
+      if (tid == 0) sm.ires[0] = info;
+      __syncthreads();
+      return;
+    }
+    case K_ESH:
+      cta_esh(o.C, o.m, o.n, o.A, o.X, o.alpha, o.flag != 0, o.Y, o.V, o.opa);
+      break;
+    case K_COPY:
+      cta_copy(o.C, o.A, o.m);
+      break;
+    case K_SUB:
+      for (int q = tid; q < o.m; q += blockDim.x) o.C[q] = csub(o.C[q], o.A[q]);
+      break;
+    case K_DECUPD:
+      for (int q = tid; q < o.m; q += blockDim.x) {
+        const double2 s = o.A[q];
+        o.C[q] = csub(o.C[q], s);
+        o.D[q] = csub(o.D[q], s);
+      }
+      break;
+    case K_SPECTRAL:
+      cta_spectral(o.C, o.A, o.m);
+      break;
+    case K_TRACE: {
+      const double r = cta_re_trace_prod(o.A, o.B, o.m, o.opb, sm.red);
+      if (tid == 0) sm.res[o.slot] = r;
+      break;
+    }
+    case K_TRACEC: {
+      const int n = o.m, m = o.n;   // A is n x m, op(B) is m x n
+      double re = 0.0, im = 0.0;
+      for (int idx = tid; idx < n * m; idx += blockDim.x) {
+        const int i = idx % n, j = idx / n;   // A(i,j) * opB(j,i)
+        const double2 x = o.A[idx];
+        const double2 y = (o.opb == OP_C) ? cconj(o.B[(size_t)i + (size_t)j * n]) : o.B[(size_t)j + (size_t)i * m];
+        re += x.x * y.x - x.y * y.y;
+        im += x.x * y.y + x.y * y.x;
+      }
+      re = cta_sum(re, sm.red);
+      im = cta_sum(im, sm.red);
+      if (tid == 0) { sm.res[o.slot] = re; sm.res[o.slot + 1] = im; }
+      break;
+    }
+    case K_TRACEN: {
+      const int n2 = o.m, n1 = o.n;
+      double acc = 0.0;
+      for (int idx = tid; idx < n2 * n1; idx += blockDim.x) {
+        const double2 x = o.A[idx], y = o.B[idx];   // W2(r,c) * conj(G21(r,c))
+        acc += x.x * y.x + x.y * y.y;
+      }
+      acc = cta_sum(acc, sm.red);
+      if (tid == 0) sm.res[o.slot] = acc;
+      break;
+    }
+    case K_DOS: {
+      const double pi = 3.14159265358979323846;
+      for (int k = tid; k < o.m; k += blockDim.x) o.out[k] = -(1.0 / pi) * o.A[(size_t)k * (o.m + 1)].y;
+      break;
+    }
+    case K_SIGDIAG:
+      for (int k = tid; k < o.m; k += blockDim.x) {
+        const double c = o.cpl[k];
+        o.C[k] = cscale(c * c, o.A[(size_t)k * (o.m + 1)]);
+      }
+      break;
+    case K_SNINIT:
+      for (int q = tid; q < o.m * o.m; q += blockDim.x) {
+        const int r = q % o.m, c = q / o.m;
+        o.C[q] = (o.A && r == c) ? o.A[r] : cz(0.0, 0.0);
+      }
+      break;
+    case K_SNGAMMA:
+      for (int q = tid; q < o.m * o.m; q += blockDim.x) {
+        const int r = q % o.m, c = q / o.m;
+        const double2 a1 = o.A[q], b1 = cconj(o.A[(size_t)c + (size_t)r * o.m]);
+        const double2 gam = cz(-(a1.y - b1.y), a1.x - b1.x);   // i (S - S^dag)
+        o.C[q] = cadd(o.C[q], cscale(o.scal, gam));
+      }
+      break;
+    case K_DAGGER:
+      for (int q = tid; q < o.m * o.n; q += blockDim.x) {
+        const int r = q % o.m, c = q / o.m;
+        o.C[q] = cconj(o.A[(size_t)c + (size_t)r * o.n]);
+      }
+      break;
+    case K_ERRDIAG: {
+      double e = 0.0;
+      for (int k = tid; k < o.m; k += blockDim.x)
+        e = fmax(e, cabs(csub(o.A[(size_t)k * (o.m + 1)], o.B[(size_t)k * (o.m + 1)])));
+      e = cta_max(e, sm.red);
+      if (tid == 0) sm.res[o.slot] = fmax(sm.res[o.slot], e);
+      break;
+    }
+    case K_ERRPAT: {
+      double e = 0.0;
+      for (int q = tid; q < o.m * o.n; q += blockDim.x) {
+        const int r = q % o.m, c = q / o.m;
+        const double diff = cabs(csub(o.A[q], o.B[q]));
+        const double2 sp = o.X[q];
+        if (sp.x != 0.0 || sp.y != 0.0) e = fmax(e, diff);
+        if (o.Y) {
+          const double2 st = o.Y[(size_t)c + (size_t)r * o.n];
+          if (st.x != 0.0 || st.y != 0.0) e = fmax(e, diff);
+        }
+      }
+      e = cta_max(e, sm.red);
+      if (tid == 0) sm.res[o.slot] = fmax(sm.res[o.slot], e);
+      break;
+    }
+    case K_MAXABS: {
+      double e = 0.0;
+      for (int q = tid; q < o.m; q += blockDim.x) e = fmax(e, cabs(o.A[q]));
+      e = cta_max(e, sm.red);
+      if (tid == 0) sm.res[o.slot] = e;
+      break;
+    }
+    case K_TRDIAG: {
+      double tr = 0.0;
+      for (int k = tid; k < o.m; k += blockDim.x) tr += o.A[(size_t)k * (o.m + 1)].x;
+      tr = cta_sum(tr, sm.red);
+      if (tid == 0) sm.res[o.slot] = tr;
+      break;
+    }
+    default:
+      break;
+  }
+  __syncthreads();
+  sm.tr.stop(TR_ELEM, t0);
+}
+
+// ---------------------------------------------------------------- generator
+struct Prog {
+  int pc;
+  int p;                // current point
+  const DevDesc* d;
+  double E;
+  int st, ncyc;
+  double2 ec, ecs;      // ES-H energy, contact energy
+  // contacts / decimation
+  int c, L, ncb, it, ok, done, ib, ix, ic, ic1;
+  // sweeps
+  int i, j, sub_first, cur, cc, last, tiny, pp, lo;
+  double2* gnext;
+  double2* gsv;         // target of gr_first
+  int keep;
+  const double2* sr;    // dephasing sigma_r in effect (or null)
+  // transmission bookkeeping
+  int fast, ct1, ct2, bl1, bl2;
+  double T;
+  // SCBA
+  int sit, conv, have_old, par;
+  double err;
+  double2* vec;
+};
+
+#define PT_EMIT(s) do { (s).pc = __LINE__; return true; case __LINE__:; } while (0)
+
+__device__ __forceinline__ const double2* sig_on_block(const DevDesc* d, const Ws& w, int i, int& first) {
+  first = -1;
+  for (int c = 0; c < d->ncont; ++c)
+    if (d->cblk[c] == i + 1) { first = c; return w.sig(c); }
+  return nullptr;
+}
+
+// ESH(i,i) = ec S - H - Sigma_first - diag(sigr)
+__device__ __forceinline__ void op_esh_diag(Op& o, const DevDesc* d, int i, double2 ec, double2* dst, const Ws& w,
+                                            const double2* sigr, int& first) {
+  const double2* sub = sig_on_block(d, w, i, first);
+  set_esh(o, dst, d->pl[i], d->pl[i], d->hd + d->od[i], d->has_s ? d->sd + d->od[i] : nullptr, ec, 1, sub,
+          sigr ? sigr + d->pstart[i] : nullptr, OP_N);
+}
+__device__ __forceinline__ void op_esh_up(Op& o, const DevDesc* d, int i, double2 ec, double2* dst) {
+  set_esh(o, dst, d->pl[i], d->pl[i + 1], d->hu + d->oo[i], d->has_s ? d->su + d->oo[i] : nullptr, ec, 0, nullptr,
+          nullptr, OP_N);
+}
+__device__ __forceinline__ void op_esh_lo(Op& o, const DevDesc* d, int i, double2 ec, double2* dst) {
+  set_esh(o, dst, d->pl[i + 1], d->pl[i], d->hl + d->oo[i], d->has_s ? d->sl + d->oo[i] : nullptr, ec, 0, nullptr,
+          nullptr, OP_N);
+}
+
+__device__ __forceinline__ void put_status(int& st, int s) { if (st == ST_OK) st = s; }
+
+// Fills `o` with the next block operation of this CTA and returns true, or
+// returns false when the work queue is exhausted.
+__device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& sm, const Ws& w, Op& o) {
+  const double2 one = cz(1, 0), zero = cz(0, 0), mone = cz(-1, 0);
+  double mx;
+  switch (s.pc) {
+    case 0:
+    for (;;) {
+      // ---------------------------------------------------------- next point
+      if (threadIdx.x == 0) *sm.item = atomicAdd(a.counter, 1);
+      __syncthreads();
+      s.p = *sm.item;
+      __syncthreads();
+      if (s.p >= a.npts) break;
+      s.d = a.devs + a.dev_id[s.p];
+      s.E = a.energy[s.p];
+      s.st = ST_OK;
+      s.ncyc = 0;
+      s.T = 0.0;
+      s.ecs = cz(s.E, a.eta);
+      s.ec = (a.mode == MODE_DOS) ? cz(s.E, a.dos_delta) : cz(s.E, 0.0);
+      if (threadIdx.x == 0 && sm.tr.acc) sm.tr.acc[TR_POINTS] += 1;
+
+      // ------------------------------------------ contacts (compute_contacts_dns)
+      for (s.c = 0; s.c < s.d->ncont; ++s.c) {
+        s.L = s.d->L[s.c];
+        s.ncb = s.d->pl[s.d->cblk[s.c] - 1];
+        set_esh(o, w.slot(0), s.L, s.L, s.d->h00 + s.d->olead[s.c], s.d->has_s00 ? s.d->s00 + s.d->olead[s.c] : nullptr,
+                s.ecs, 1, nullptr, nullptr, OP_N);                                          // Ao
+        PT_EMIT(s);
+        set_esh(o, w.slot(2), s.L, s.L, s.d->h01 + s.d->olead[s.c], s.d->has_s01 ? s.d->s01 + s.d->olead[s.c] : nullptr,
+                s.ecs, 0, nullptr, nullptr, OP_N);                                          // Bo
+        PT_EMIT(s);
+        set_esh(o, w.slot(3), s.L, s.L, s.d->h01 + s.d->olead[s.c], s.d->has_s01 ? s.d->s01 + s.d->olead[s.c] : nullptr,
+                cconj(s.ecs), 0, nullptr, nullptr, OP_C);                                   // Co = (E* S01 - H01)^dag
+        PT_EMIT(s);
+        // ---- decimation (src/contselfenergy.F90:271-340): Ao 0, Aos 1, Go 4, Sf 6
+        set_simple(o, K_COPY, s.L * s.L, w.slot(0), w.slot(1));
+        PT_EMIT(s);
+        s.ok = 0; s.done = 0; s.ib = 2; s.ix = 5; s.ic = 3; s.ic1 = 7;
+        for (s.it = 1; s.it <= a.sgf_max_iter; ++s.it) {
+          o.kind = K_ZINV; o.m = s.L; o.A = w.slot(0); o.C = w.slot(4);
+          PT_EMIT(s);
+          if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          set_gemm(o, s.L, s.L, s.L, w.slot(4), s.L, OP_N, w.slot(s.ic), s.L, OP_N, w.slot(s.ix), s.L, one, zero);
+          PT_EMIT(s);                                                                    // GoXCo
+          set_gemm(o, s.L, s.L, s.L, w.slot(s.ic), s.L, OP_N, w.slot(s.ix), s.L, OP_N, w.slot(s.ic1), s.L, one,
+                   zero, 1);
+          PT_EMIT(s);                                                                    // C1 = Co GoXCo
+          mx = *sm.maxv;
+          if (mx <= a.sgf_tol) {
+            if (s.ok) { s.done = 1; break; }
+            s.ok = 1;
+          } else {
+            s.ok = 0;
+          }
+          set_gemm(o, s.L, s.L, s.L, w.slot(s.ib), s.L, OP_N, w.slot(s.ix), s.L, OP_N, w.slot(6), s.L, one, zero);
+          PT_EMIT(s);                                                                    // Self = Bo GoXCo
+          o.kind = K_DECUPD; o.m = s.L * s.L; o.A = w.slot(6); o.C = w.slot(1); o.D = w.slot(0);
+          PT_EMIT(s);                                                                    // Ao_s -= Self, Ao -= Self
+          set_gemm(o, s.L, s.L, s.L, w.slot(4), s.L, OP_N, w.slot(s.ib), s.L, OP_N, w.slot(6), s.L, one, zero);
+          PT_EMIT(s);                                                                    // GoXBo
+          set_gemm(o, s.L, s.L, s.L, w.slot(s.ib), s.L, OP_N, w.slot(6), s.L, OP_N, w.slot(s.ix), s.L, one, zero);
+          PT_EMIT(s);                                                                    // B1 = Bo GoXBo
+          set_gemm(o, s.L, s.L, s.L, w.slot(s.ic), s.L, OP_N, w.slot(6), s.L, OP_N, w.slot(0), s.L, mone, one);
+          PT_EMIT(s);                                                                    // Ao -= Co GoXBo
+          { int t = s.ib; s.ib = s.ix; s.ix = t; t = s.ic; s.ic = s.ic1; s.ic1 = t; }   // Bo = B1, Co = C1
+        }
+        if (!s.done) put_status(s.st, ST_NOT_CONVERGED);
+        s.ncyc += s.done ? s.it : a.sgf_max_iter + 1;
+        o.kind = K_ZINV; o.m = s.L; o.A = w.slot(1); o.C = w.slot(4);
+        PT_EMIT(s);                                                                      // gs = Ao_s^-1
+        if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+        // ---- self-energy: Tlc = E SMC - HMC, Tcl = (E^* SMC - HMC)^dag, Sigma = Tlc gs Tcl
+        set_esh(o, w.slot(0), s.ncb, s.L, s.d->hmc + s.d->omc[s.c], s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr,
+                s.ecs, 0, nullptr, nullptr, OP_N);
+        PT_EMIT(s);
+        set_esh(o, w.slot(1), s.L, s.ncb, s.d->hmc + s.d->omc[s.c], s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr,
+                cconj(s.ecs), 0, nullptr, nullptr, OP_C);
+        PT_EMIT(s);
+        set_gemm(o, s.ncb, s.L, s.L, w.slot(0), s.ncb, OP_N, w.slot(4), s.L, OP_N, w.slot(2), s.ncb, one, zero);
+        PT_EMIT(s);
+        set_gemm(o, s.ncb, s.ncb, s.L, w.slot(2), s.ncb, OP_N, w.slot(1), s.L, OP_N, w.sig(s.c), s.ncb, one, zero);
+        PT_EMIT(s);
+      }
+
+      // ------------------------------------------------ transmission bookkeeping
+      {
+        const int ni = a.ni - 1, nf = a.nf - 1;
+        const int cbi = s.d->cblk[ni < s.d->ncont ? ni : 0], cbf = s.d->cblk[nf < s.d->ncont ? nf : 0];
+        s.ct1 = (cbi < cbf) ? ni : nf;
+        s.ct2 = (cbi < cbf) ? nf : ni;
+        s.bl1 = s.d->cblk[s.ct1 < s.d->ncont ? s.ct1 : 0];
+        s.bl2 = s.d->cblk[s.ct2 < s.d->ncont ? s.ct2 : 0];
+        s.fast = (a.mode == MODE_T) && s.d->ncont == 2 && min(cbi, cbf) == 1;
+      }
+      if (a.mode == MODE_T && s.d->ncont == 1) goto point_done;
+
+      // ------------------------------------------------ SCBA loop (once for T / DOS)
+      s.sit = 0; s.conv = 0; s.have_old = 0; s.err = 0.0; s.par = 0;
+      s.vec = w.slot(S_SIG + a.ncont_max + 8 * a.nbl_max);
+      for (;;) {
+        if (a.mode == MODE_GN && (s.conv || s.sit > a.scba_niter)) break;
+        s.sr = (a.mode == MODE_GN && s.sit > 0 && a.coupling) ? s.vec : nullptr;
+        s.keep = !s.fast;
+        // -------------------------------------- gsmr sweep (calculate_gsmr_blocks)
+        if (s.d->nbl > 1) {
+          op_esh_diag(o, s.d, s.d->nbl - 1, s.ec, w.slot(0), w, s.sr, s.sub_first);
+          PT_EMIT(s);
+          for (s.j = s.sub_first + 1; s.sub_first >= 0 && s.j < s.d->ncont; ++s.j)
+            if (s.d->cblk[s.j] == s.d->nbl) {
+              set_simple(o, K_SUB, s.d->pl[s.d->nbl - 1] * s.d->pl[s.d->nbl - 1], w.sig(s.j), w.slot(0));
+              PT_EMIT(s);
+            }
+          s.gnext = s.keep ? w.layer(0, s.d->nbl - 1, s.d->nbl) : w.slot(4);
+          o.kind = K_ZINV; o.m = s.d->pl[s.d->nbl - 1]; o.A = w.slot(0); o.C = s.gnext;
+          PT_EMIT(s);
+          if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          s.pp = 1;
+          for (s.i = s.d->nbl - 2; s.i >= 1; --s.i) {
+            op_esh_up(o, s.d, s.i, s.ec, w.slot(1));
+            PT_EMIT(s);
+            op_esh_lo(o, s.d, s.i, s.ec, w.slot(2));
+            PT_EMIT(s);
+            op_esh_diag(o, s.d, s.i, s.ec, w.slot(0), w, s.sr, s.sub_first);
+            PT_EMIT(s);
+            for (s.j = s.sub_first + 1; s.sub_first >= 0 && s.j < s.d->ncont; ++s.j)
+              if (s.d->cblk[s.j] == s.i + 1) {
+                set_simple(o, K_SUB, s.d->pl[s.i] * s.d->pl[s.i], w.sig(s.j), w.slot(0));
+                PT_EMIT(s);
+              }
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.slot(1), s.d->pl[s.i], OP_N, s.gnext,
+                     s.d->pl[s.i + 1], OP_N, w.slot(3), s.d->pl[s.i], mone, zero);   // -ESH(i,i+1) gsmr(i+1)
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i + 1], w.slot(3), s.d->pl[s.i], OP_N, w.slot(2),
+                     s.d->pl[s.i + 1], OP_N, w.slot(0), s.d->pl[s.i], one, one);    // ESH(i,i) + W ESH(i+1,i)
+            PT_EMIT(s);
+            o.kind = K_ZINV; o.m = s.d->pl[s.i]; o.A = w.slot(0);
+            o.C = s.keep ? w.layer(0, s.i, s.d->nbl) : w.slot(4 + s.pp);
+            s.pp ^= 1;
+            s.gnext = o.C;
+            PT_EMIT(s);
+            if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          }
+        }
+        // -------------------------------------- Gr(1,1)
+        s.gsv = (a.mode == MODE_GN) ? w.layer(1, 0, s.d->nbl) : w.slot(11);
+        op_esh_diag(o, s.d, 0, s.ec, w.slot(0), w, s.sr, s.sub_first);
+        PT_EMIT(s);
+        for (s.j = s.sub_first + 1; s.sub_first >= 0 && s.j < s.d->ncont; ++s.j)
+          if (s.d->cblk[s.j] == 1) {
+            set_simple(o, K_SUB, s.d->pl[0] * s.d->pl[0], w.sig(s.j), w.slot(0));
+            PT_EMIT(s);
+          }
+        if (s.d->nbl > 1) {
+          op_esh_up(o, s.d, 0, s.ec, w.slot(1));
+          PT_EMIT(s);
+          op_esh_lo(o, s.d, 0, s.ec, w.slot(2));
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[0], s.d->pl[1], s.d->pl[1], w.slot(1), s.d->pl[0], OP_N, s.gnext, s.d->pl[1], OP_N,
+                   w.slot(3), s.d->pl[0], one, zero);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[0], s.d->pl[0], s.d->pl[1], w.slot(3), s.d->pl[0], OP_N, w.slot(2), s.d->pl[1], OP_N,
+                   w.slot(0), s.d->pl[0], mone, one);
+          PT_EMIT(s);
+        }
+        o.kind = K_ZINV; o.m = s.d->pl[0]; o.A = w.slot(0); o.C = s.gsv;
+        PT_EMIT(s);
+        if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+        if (s.fast) {
+          // ------------------------------------ 2-contact trace (iterative_cpu.F90:399-470)
+          s.lo = s.d->pl[0];
+          goto trans2;
+        }
+        // -------------------------------------- forward retarded sweep
+        // T / DOS: Gr(i,i) ping-pongs in slots 11/10, Gr(bl1,bl1) kept in slot 9.
+        // GN: Gr(i,i) -> layer 1, Gr(i-1,i) -> layer 2.
+        s.cur = 0;
+        s.last = (a.mode == MODE_T) ? s.bl1 - 1 : s.d->nbl - 1;
+        for (s.i = 0; s.i <= s.last; ++s.i) {
+          if (s.i > 0) {
+            // gr_step(i): E1 = ESH(i-1,i) slot 0, E2 = ESH(i,i-1) slot 1, X slot 2, W2 slot 3, GL slot 6
+            op_esh_up(o, s.d, s.i - 1, s.ec, w.slot(0));
+            PT_EMIT(s);
+            op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(1));
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
+                     w.slot(1), s.d->pl[s.i], OP_N, w.slot(2), s.d->pl[s.i], one, zero);          // gsmr(i) ESH(i,i-1)
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i - 1], w.slot(2), s.d->pl[s.i], OP_N,
+                     (a.mode == MODE_GN) ? w.layer(1, s.i - 1, s.d->nbl) : w.slot(11 - s.cur), s.d->pl[s.i - 1], OP_N,
+                     w.slot(6), s.d->pl[s.i], mone, zero);                                         // Gr(i,i-1)
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i - 1], s.d->pl[s.i], s.d->pl[s.i], w.slot(0), s.d->pl[s.i - 1], OP_N,
+                     w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(3), s.d->pl[s.i - 1], one, zero);  // ESH gsmr
+            PT_EMIT(s);
+            if (a.mode == MODE_GN) {
+              set_gemm(o, s.d->pl[s.i - 1], s.d->pl[s.i], s.d->pl[s.i - 1], w.layer(1, s.i - 1, s.d->nbl),
+                       s.d->pl[s.i - 1], OP_N, w.slot(3), s.d->pl[s.i - 1], OP_N, w.layer(2, s.i - 1, s.d->nbl),
+                       s.d->pl[s.i - 1], mone, zero);                                              // Gr(i-1,i)
+              PT_EMIT(s);
+            }
+            set_simple(o, K_COPY, s.d->pl[s.i] * s.d->pl[s.i], w.layer(0, s.i, s.d->nbl),
+                       (a.mode == MODE_GN) ? w.layer(1, s.i, s.d->nbl) : w.slot(11 - (s.cur ^ 1)));
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i - 1], w.slot(6), s.d->pl[s.i], OP_N, w.slot(3),
+                     s.d->pl[s.i - 1], OP_N,
+                     (a.mode == MODE_GN) ? w.layer(1, s.i, s.d->nbl) : w.slot(11 - (s.cur ^ 1)), s.d->pl[s.i], mone,
+                     one);                                                                         // Gr(i,i)
+            PT_EMIT(s);
+            s.cur ^= 1;
+          }
+          if (a.mode == MODE_DOS && a.dos) {
+            set_simple(o, K_DOS, s.d->pl[s.i], w.slot(11 - s.cur), nullptr);
+            o.out = a.dos + (int64_t)s.p * a.dos_stride + s.d->pstart[s.i];
+            PT_EMIT(s);
+          }
+          if (a.mode != MODE_GN && s.i == s.bl1 - 1) {
+            set_simple(o, K_COPY, s.d->pl[s.i] * s.d->pl[s.i], w.slot(11 - s.cur), w.slot(9));
+            PT_EMIT(s);
+          }
+        }
+        if (a.mode != MODE_GN) {
+          if (s.d->ncont == 1) { s.T = 0.0; goto point_done; }
+          if (a.mode == MODE_DOS && s.d->ncont == 2) {
+            s.lo = s.d->pl[s.bl1 - 1];
+            s.gsv = w.slot(9);
+            goto trans2;
+          }
+          // ------------------------------------ column sweep Gr(i,bl1) (iterative_cpu.F90:507-538)
+          s.cc = 0;
+          s.tiny = 0;
+          for (s.i = s.bl1; s.i <= s.bl2 - 1; ++s.i) {
+            set_simple(o, K_MAXABS, s.d->pl[s.i - 1] * s.d->pl[s.bl1 - 1], s.cc ? w.slot(6) : w.slot(9), nullptr);
+            o.slot = 0;
+            PT_EMIT(s);
+            if (sm.res[0] < a.eps) { s.tiny = 1; break; }
+            op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(0));
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
+                     w.slot(0), s.d->pl[s.i], OP_N, w.slot(1), s.d->pl[s.i], mone, zero);
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.bl1 - 1], s.d->pl[s.i - 1], w.slot(1), s.d->pl[s.i], OP_N,
+                     s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.i - 1], OP_N, s.cc ? w.slot(9) : w.slot(6), s.d->pl[s.i],
+                     one, zero);
+            PT_EMIT(s);
+            s.cc ^= 1;
+          }
+          if (s.tiny) { s.T = a.eps * a.eps; goto point_done; }
+          // ------------------------------------ N-contact trace |Re Tr[Gam2 G21 Gam1 G21^dag]|
+          // Gam1 slot 7, Gam2 slot 8, W1 slot 2, W2 slot 3; G21 in slot 9 or 6
+          set_simple(o, K_SPECTRAL, s.d->pl[s.bl1 - 1], w.sig(s.ct1), w.slot(7));
+          PT_EMIT(s);
+          set_simple(o, K_SPECTRAL, s.d->pl[s.bl2 - 1], w.sig(s.ct2), w.slot(8));
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.bl2 - 1], s.d->pl[s.bl1 - 1], s.d->pl[s.bl2 - 1], w.slot(8), s.d->pl[s.bl2 - 1], OP_N,
+                   s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.bl2 - 1], OP_N, w.slot(2), s.d->pl[s.bl2 - 1], one, zero);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.bl2 - 1], s.d->pl[s.bl1 - 1], s.d->pl[s.bl1 - 1], w.slot(2), s.d->pl[s.bl2 - 1],
+                   OP_N, w.slot(7), s.d->pl[s.bl1 - 1], OP_N, w.slot(3), s.d->pl[s.bl2 - 1], one, zero);
+          PT_EMIT(s);
+          o.kind = K_TRACEN; o.m = s.d->pl[s.bl2 - 1]; o.n = s.d->pl[s.bl1 - 1]; o.A = w.slot(3);
+          o.B = s.cc ? w.slot(6) : w.slot(9); o.slot = 0;
+          PT_EMIT(s);
+          s.T = fabs(sm.res[0]);
+          goto point_done;
+        }
+        // ================================== elastic SCBA: lesser sweep (GN)
+        // sigma_r = D diag(Gr)
+        if (a.coupling)
+          for (s.i = 0; s.i < s.d->nbl; ++s.i) {
+            set_simple(o, K_SIGDIAG, s.d->pl[s.i], w.layer(1, s.i, s.d->nbl), s.vec + s.d->pstart[s.i]);
+            o.cpl = a.coupling + s.d->pstart[s.i];
+            PT_EMIT(s);
+          }
+        // Sigma_n(i,i) = dephasing (it > 0) + contacts (f_c - f_ref) Gam_c, f_ref = 0
+        for (s.i = 0; s.i < s.d->nbl; ++s.i) {
+          set_simple(o, K_SNINIT, s.d->pl[s.i],
+                     (s.sit > 0 && a.coupling) ? s.vec + s.d->norb + s.d->pstart[s.i] : nullptr,
+                     w.layer(3, s.i, s.d->nbl));
+          PT_EMIT(s);
+        }
+        for (s.c = 0; s.c < s.d->ncont; ++s.c) {
+          if (fabs(a.frm[(int64_t)s.p * a.frm_stride + s.c]) > a.eps) {
+            set_simple(o, K_SNGAMMA, s.d->pl[s.d->cblk[s.c] - 1], w.sig(s.c), w.layer(3, s.d->cblk[s.c] - 1, s.d->nbl));
+            o.scal = a.frm[(int64_t)s.p * a.frm_stride + s.c];
+            PT_EMIT(s);
+          }
+        }
+        // upward fold of Sigma_n (calculate_sigma_n); gns slot 6, T1 slot 7, E1 slot 8
+        s.i = s.d->nbl - 1;
+        set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
+                 w.layer(3, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i], one, zero);
+        PT_EMIT(s);
+        set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i], w.slot(7), s.d->pl[s.i], OP_N,
+                 w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_C, w.slot(6), s.d->pl[s.i], one, zero);
+        PT_EMIT(s);
+        for (s.i = s.d->nbl - 2; s.i >= 0; --s.i) {
+          op_esh_up(o, s.d, s.i, s.ec, w.slot(8));
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.slot(8), s.d->pl[s.i], OP_N, w.slot(6),
+                   s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i], one, zero);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i + 1], w.slot(7), s.d->pl[s.i], OP_N, w.slot(8),
+                   s.d->pl[s.i], OP_C, w.layer(3, s.i, s.d->nbl), s.d->pl[s.i], one, one);
+          PT_EMIT(s);
+          if (s.i > 0) {
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
+                     w.layer(3, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i], one, zero);
+            PT_EMIT(s);
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i], w.slot(7), s.d->pl[s.i], OP_N,
+                     w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_C, w.slot(6), s.d->pl[s.i], one, zero);
+            PT_EMIT(s);
+          }
+        }
+        // Gn(1,1) = Gr(1,1) Sigma_n(1,1) Gr(1,1)^dag
+        set_gemm(o, s.d->pl[0], s.d->pl[0], s.d->pl[0], w.layer(3, 0, s.d->nbl), s.d->pl[0], OP_N,
+                 w.layer(1, 0, s.d->nbl), s.d->pl[0], OP_C, w.slot(7), s.d->pl[0], one, zero);
+        PT_EMIT(s);
+        set_gemm(o, s.d->pl[0], s.d->pl[0], s.d->pl[0], w.layer(1, 0, s.d->nbl), s.d->pl[0], OP_N, w.slot(7),
+                 s.d->pl[0], OP_N, w.layer(4 + s.par, 0, s.d->nbl), s.d->pl[0], one, zero);
+        PT_EMIT(s);
+        // downward sweep; E2 slot 9, Gn(i+1,i) slot 10
+        for (s.i = 0; s.i + 1 < s.d->nbl; ++s.i) {
+          op_esh_lo(o, s.d, s.i, s.ec, w.slot(9));
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i + 1], w.layer(3, s.i + 1, s.d->nbl),
+                   s.d->pl[s.i + 1], OP_N, w.layer(2, s.i, s.d->nbl), s.d->pl[s.i], OP_C, w.slot(7), s.d->pl[s.i + 1],
+                   one, zero);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i], w.slot(9), s.d->pl[s.i + 1], OP_N,
+                   w.layer(4 + s.par, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i + 1], mone, one);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i + 1], w.layer(0, s.i + 1, s.d->nbl),
+                   s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i + 1], OP_N, w.slot(10), s.d->pl[s.i + 1], one, zero);
+          PT_EMIT(s);
+          o.kind = K_DAGGER; o.m = s.d->pl[s.i]; o.n = s.d->pl[s.i + 1]; o.A = w.slot(10);
+          o.C = w.layer(6 + s.par, s.i, s.d->nbl);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.layer(3, s.i + 1, s.d->nbl),
+                   s.d->pl[s.i + 1], OP_N, w.layer(1, s.i + 1, s.d->nbl), s.d->pl[s.i + 1], OP_C, w.slot(7),
+                   s.d->pl[s.i + 1], one, zero);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i + 1], s.d->pl[s.i], w.slot(9), s.d->pl[s.i + 1], OP_N,
+                   w.layer(6 + s.par, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i + 1], mone, one);
+          PT_EMIT(s);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.layer(0, s.i + 1, s.d->nbl),
+                   s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i + 1], OP_N, w.layer(4 + s.par, s.i + 1, s.d->nbl),
+                   s.d->pl[s.i + 1], one, zero);
+          PT_EMIT(s);
+        }
+        // set_Gn (sigma_n = D diag(Gn)) and the SCBA error on the S pattern
+        if (threadIdx.x == 0) sm.res[1] = 0.0;
+        __syncthreads();
+        for (s.i = 0; s.i < s.d->nbl; ++s.i) {
+          if (s.have_old) {
+            if (!s.d->has_s) {
+              o.kind = K_ERRDIAG; o.m = s.d->pl[s.i]; o.A = w.layer(4 + s.par, s.i, s.d->nbl);
+              o.B = w.layer(4 + (s.par ^ 1), s.i, s.d->nbl); o.slot = 1;
+              PT_EMIT(s);
+            } else {
+              o.kind = K_ERRPAT; o.m = s.d->pl[s.i]; o.n = s.d->pl[s.i]; o.A = w.layer(4 + s.par, s.i, s.d->nbl);
+              o.B = w.layer(4 + (s.par ^ 1), s.i, s.d->nbl); o.X = s.d->sd + s.d->od[s.i]; o.Y = nullptr; o.slot = 1;
+              PT_EMIT(s);
+              if (s.i + 1 < s.d->nbl) {
+                o.kind = K_ERRPAT; o.m = s.d->pl[s.i]; o.n = s.d->pl[s.i + 1];
+                o.A = w.layer(6 + s.par, s.i, s.d->nbl); o.B = w.layer(6 + (s.par ^ 1), s.i, s.d->nbl);
+                o.X = s.d->su + s.d->oo[s.i]; o.Y = s.d->sl + s.d->oo[s.i]; o.slot = 1;
+                PT_EMIT(s);
+              }
+            }
+          }
+          if (a.coupling) {
+            set_simple(o, K_SIGDIAG, s.d->pl[s.i], w.layer(4 + s.par, s.i, s.d->nbl),
+                       s.vec + s.d->norb + s.d->pstart[s.i]);
+            o.cpl = a.coupling + s.d->pstart[s.i];
+            PT_EMIT(s);
+          }
+        }
+        if (s.have_old) {
+          s.err = sm.res[1];
+          s.conv = s.err < a.scba_tol;
+        }
+        s.have_old = 1;
+        s.par ^= 1;
+        ++s.sit;
+      }
+      s.par ^= 1;   // parity of the last computed Gn
+      // ------------------------------------ Meir-Wingreen (iterative.F90:382-414); Gam slot 7, A slot 8
+      if (a.curr)
+        for (s.c = 0; s.c < s.d->ncont; ++s.c) {
+          set_simple(o, K_SPECTRAL, s.d->pl[s.d->cblk[s.c] - 1], w.sig(s.c), w.slot(7));
+          PT_EMIT(s);
+          set_simple(o, K_SPECTRAL, s.d->pl[s.d->cblk[s.c] - 1], w.layer(1, s.d->cblk[s.c] - 1, s.d->nbl), w.slot(8));
+          PT_EMIT(s);
+          o.kind = K_TRACE; o.m = s.d->pl[s.d->cblk[s.c] - 1]; o.A = w.slot(7);
+          o.B = w.layer(4 + s.par, s.d->cblk[s.c] - 1, s.d->nbl); o.opb = OP_N; o.slot = 2;
+          PT_EMIT(s);
+          o.kind = K_TRACE; o.m = s.d->pl[s.d->cblk[s.c] - 1]; o.A = w.slot(7); o.B = w.slot(8); o.opb = OP_N;
+          o.slot = 3;
+          PT_EMIT(s);
+          if (threadIdx.x == 0)
+            a.curr[(int64_t)s.p * a.curr_stride + s.c] =
+                -(sm.res[2] - a.frm[(int64_t)s.p * a.frm_stride + s.c] * sm.res[3]);
+          __syncthreads();
+        }
+      // ------------------------------------ layer currents / densities (iterative.F90:427-461)
+      if (a.lcurr || a.ldens)
+        for (s.i = 0; s.i < s.d->nbl; ++s.i) {
+          if (a.ldens) {
+            o.kind = K_TRDIAG; o.m = s.d->pl[s.i]; o.A = w.layer(4 + s.par, s.i, s.d->nbl); o.slot = 2;
+            PT_EMIT(s);
+            if (threadIdx.x == 0) a.ldens[(int64_t)s.p * a.ldens_stride + s.i] = sm.res[2];
+            __syncthreads();
+          }
+          if (a.lcurr && s.i + 1 < s.d->nbl) {
+            op_esh_up(o, s.d, s.i, s.ec, w.slot(8));
+            PT_EMIT(s);
+            op_esh_lo(o, s.d, s.i, s.ec, w.slot(9));
+            PT_EMIT(s);
+            o.kind = K_TRACEC; o.m = s.d->pl[s.i]; o.n = s.d->pl[s.i + 1]; o.A = w.slot(8);
+            o.B = w.layer(6 + s.par, s.i, s.d->nbl); o.opb = OP_C; o.slot = 2;   // Tr(ESH(i,i+1) Gn(i+1,i))
+            PT_EMIT(s);
+            o.kind = K_TRACEC; o.m = s.d->pl[s.i]; o.n = s.d->pl[s.i + 1]; o.A = w.layer(6 + s.par, s.i, s.d->nbl);
+            o.B = w.slot(9); o.opb = OP_N; o.slot = 4;                           // Tr(Gn(i,i+1) ESH(i+1,i))
+            PT_EMIT(s);
+            if (threadIdx.x == 0) a.lcurr[(int64_t)s.p * a.lcurr_stride + s.i] = -(sm.res[3] - sm.res[5]);
+            __syncthreads();
+          }
+        }
+      if (threadIdx.x == 0) {
+        if (a.scba_iter) a.scba_iter[s.p] = s.sit;
+        if (a.scba_err) a.scba_err[s.p] = s.err;
+      }
+      goto point_done;
+
+    trans2:
+      // |Re Tr[Gam1 i(G - G^dag) - Gam1 G Gam1 G^dag]|; G in s.gsv, order s.lo.
+      // Gam slot 7, W1 slot 8, W2 slot 2, A slot 3
+      set_simple(o, K_SPECTRAL, s.lo, w.sig(s.ct1), w.slot(7));
+      PT_EMIT(s);
+      set_simple(o, K_SPECTRAL, s.lo, s.gsv, w.slot(3));
+      PT_EMIT(s);
+      set_gemm(o, s.lo, s.lo, s.lo, w.slot(7), s.lo, OP_N, s.gsv, s.lo, OP_N, w.slot(8), s.lo, one, zero);
+      PT_EMIT(s);
+      set_gemm(o, s.lo, s.lo, s.lo, w.slot(8), s.lo, OP_N, w.slot(7), s.lo, OP_N, w.slot(2), s.lo, one, zero);
+      PT_EMIT(s);
+      o.kind = K_TRACE; o.m = s.lo; o.A = w.slot(2); o.B = s.gsv; o.opb = OP_C; o.slot = 0;   // Tr(Gam G Gam G^dag)
+      PT_EMIT(s);
+      o.kind = K_TRACE; o.m = s.lo; o.A = w.slot(7); o.B = w.slot(3); o.opb = OP_N; o.slot = 1;   // Tr(Gam A)
+      PT_EMIT(s);
+      s.T = fabs(sm.res[1] - sm.res[0]);
+
+    point_done:
+      if (a.mode != MODE_GN && !isfinite(s.T)) put_status(s.st, ST_NONFINITE);
+      if (threadIdx.x == 0) {
+        if (a.T) a.T[s.p] = s.T;
+        if (a.ncyc) a.ncyc[s.p] = s.ncyc;
+        if (a.status) a.status[s.p] = s.st;
+      }
+      __syncthreads();
+    }
+  }
+  s.pc = -1;
+  return false;
+}
+
+#undef PT_EMIT
+
+}  // namespace negf
