@@ -10,7 +10,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libnegf_b200.so")
-SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "capi.cu", "noalloc.cu")]
+SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "program.cu", "capi.cu", "noalloc.cu", "gemm_dev.cu", "leaf_dev.cu")]
 DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cta_ops.cuh", "engine.cuh", "program.cuh")] + [
     os.path.join(ROOT, "include", "negf_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -27,7 +27,11 @@ def build(force=False, verbose=False):
     if (not force and os.path.exists(LIB)
             and os.path.getmtime(LIB) >= max(os.path.getmtime(p) for p in DEPS)):
         return LIB
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-shared", "-Xcompiler", "-fPIC",
+    # relocatable device code: the engine kernel with its inlined product
+    # loop, the control code (program.cu) and the inversion leaves
+    # (leaf_dev.cu) are register-allocated apart from one another
+    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-rdc=true", "-Xptxas=--device-function-maxrregcount=128",
+           "-shared", "-Xcompiler", "-fPIC",
            "-I" + os.path.join(ROOT, "include"), *SOURCES, "-o", LIB]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")

@@ -42,7 +42,7 @@ __device__ __forceinline__ void gemm(int M, int N, int K, Operand A, Operand B, 
 }
 
 __device__ __forceinline__ int zinv(int n, const double2* A, double2* out, double2* ws, SmemMap& sm) {
-  return cta_zinv(n, A, out, ws, sm.main, kSmemMain, sm.inv);
+  return cta_zinv(n, A, out, ws, sm.main, sm.inv);
 }
 
 // Sancho-Rubio decimation (src/contselfenergy.F90:271-340), CTA-cooperative.
@@ -96,20 +96,12 @@ __device__ __noinline__ int cta_decimation(int L, const Ws& w, double tol, int m
 }
 
 // ---------------------------------------------------------------- engine kernel
-// Persistent: each CTA pulls points from the queue inside next_op() and
-// executes the block operations it emits.
-// The loop keeps no per-CTA bookkeeping in registers: the shared-memory map
-// lives in shared memory and the workspace descriptor is rebuilt from the
-// kernel arguments per op, so an op (a GEMM above all) runs with the whole
-// register budget, as in a kernel of its own.
-__device__ __noinline__ bool next_op_entry(const EngineArgs& a, Prog& prog, SmemMap& sm, Op& op) {
-  Ws w;
-  w.base = a.ws + (int64_t)blockIdx.x * a.ws_per_cta;
-  w.Q = a.Q;
-  w.ncont = a.ncont_max;
-  return next_op(a, prog, sm, w, op);
-}
-
+// Persistent: each CTA pulls points from the queue inside engine_step() and
+// runs the heavy steps it returns.  The product loop is inlined here and the
+// kernel keeps nothing in registers across engine_step() (its state is in
+// local memory, the shared-memory map in shared memory), so the loop is
+// register-allocated as in a kernel of its own.  The inversion leaves are
+// separately compiled routines (leaf_dev.cu).
 __global__ void __launch_bounds__(kThreads, 2) k_engine(EngineArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   __shared__ SmemMap smap;
@@ -122,11 +114,23 @@ __global__ void __launch_bounds__(kThreads, 2) k_engine(EngineArgs a) {
   if (a.trace && threadIdx.x < TR_NPHASE) smap.tr.acc[threadIdx.x] = 0;
   __syncthreads();
   const long long t_all = a.trace ? clock64() : 0;
-  Prog prog;
-  prog.pc = 0;
-  Op op;
-  while (next_op_entry(a, prog, smap, op))
-    exec_op(op, smap, a.ws + (int64_t)blockIdx.x * a.ws_per_cta + (int64_t)S_INV * a.Q);
+  EngineCtl c;
+  c.prog.pc = 0;
+  c.in_inv = 0;
+  c.open = -1;
+  for (;;) {
+    const int st = engine_step(a, c, smap);
+    if (st == STEP_DONE) break;
+    if (st == STEP_GEMM) {
+      cta_gemm_body<OP_RT, OP_RT, EPI_RT>(reinterpret_cast<const GemmDesc*>(smap.main + kGemmDescOffset), smap.main);
+    } else if (c.ip.rpt == 1) {
+      leaf_run_r1(c.ip.X, c.ip.n, c.ip.c0, c.ip.w, smap.main, smap.inv);
+    } else if (c.ip.rpt == 2) {
+      leaf_run_r2(c.ip.X, c.ip.n, c.ip.c0, c.ip.w, smap.main, smap.inv);
+    } else {
+      leaf_run_r4(c.ip.X, c.ip.n, c.ip.c0, c.ip.w, smap.main, smap.inv);
+    }
+  }
   if (a.trace) {
     if (threadIdx.x == 0) smap.tr.acc[TR_TOTAL] += clock64() - t_all;
     __syncthreads();
@@ -166,7 +170,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int b = blockIdx.x;
   Operand Ao = (dagger == 1) ? opC(A + b * sA, k) : opN(A + b * sA, m);
   Operand Bo = (dagger == 2) ? opC(B + b * sB, n) : opN(B + b * sB, k);
-  gemm(m, n, k, Ao, Bo, C + b * sC, m, alpha, beta, sm);
+  const GemmDesc* d = gemm_desc_publish(m, n, k, Ao, Bo, epi_store(C + b * sC, m, alpha, beta), sm.main);
+  cta_gemm_body<OP_RT, OP_RT, EPI_RT>(d, sm.main);
 }
 
 cudaError_t launch_zgemm_batched(int batch, int m, int n, int k, double2 alpha, const double2* A, int64_t sA,

@@ -144,27 +144,12 @@ __device__ __forceinline__ void set_simple(Op& o, int kind, int m, const double2
 }
 
 // ---------------------------------------------------------------- executor
-__device__ __forceinline__ void exec_op(const Op& o, SmemMap& sm, double2* invws) {
+// The light operations (everything but products and inversions), executed
+// inside engine_step.
+__device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
   const int tid = threadIdx.x;
   long long t0 = sm.tr.start();
   switch (o.kind) {
-    case K_GEMM: {
-      Epilogue e = epi_store(o.C, o.ldc, o.alpha, o.beta);
-      if (o.flag) {
-        if (tid == 0) *sm.maxv = 0.0;
-        __syncthreads();
-        e.maxabs = sm.maxv;
-      }
-      cta_gemm(o.m, o.n, o.k, Operand{o.A, o.lda, o.opa, nullptr}, Operand{o.B, o.ldb, o.opb, nullptr}, e, sm.main);
-      sm.tr.stop(TR_GEMM, t0);
-      return;
-    }
-    case K_ZINV: {
-      const int info = cta_zinv(o.m, o.A, o.C, invws, sm.main, kSmemMain, sm.inv);
-      if (tid == 0) sm.ires[0] = info;
-      __syncthreads();
-      return;
-    }
     case K_ESH:
       cta_esh(o.C, o.m, o.n, o.A, o.X, o.alpha, o.flag != 0, o.Y, o.V, o.opa);
       break;
@@ -811,5 +796,26 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
 }
 
 #undef PT_EMIT
+
+// ---------------------------------------------------------------- stepping
+// State of a CTA between two heavy steps (local memory of the kernel).
+struct EngineCtl {
+  Prog prog;
+  Op op;
+  InvProg ip;
+  int in_inv;       // an inversion is in progress (ip)
+  int open;         // phase of the heavy step just run (TR_GEMM, TR_INV_PANEL) or -1
+  long long t0;
+};
+
+enum StepKind : int { STEP_DONE = 0, STEP_GEMM = 1, STEP_LEAF = 2 };
+
+// Runs the point program (generator, inversion driver, light operations)
+// up to the next heavy step and returns it: STEP_GEMM (descriptor published
+// at sm.main + kGemmDescOffset), STEP_LEAF (leaf of c.ip) or STEP_DONE.
+// The kernel runs the heavy step itself.  Compiled in program.cu, apart
+// from the kernel, so that the product loop in the kernel is register-
+// allocated without the control code around it.
+__device__ int engine_step(const EngineArgs& a, EngineCtl& c, SmemMap& sm);
 
 }  // namespace negf
