@@ -77,23 +77,37 @@ def point_list(wl, seed=11):
 
 
 def flops_per_point(wl, ncyc_total, ncont=2):
-    """Algorithmic FP64 flops of one point, as the engine computes it
-    (uniform PL size n = lead PL size): complex GEMM m*n*k = 8mnk flops,
-    Gauss-Jordan inverse = 8 n^3 flops.
-      decimation, per contact with c iterations: c inverses, 6(c-1)+2 GEMMs,
-        one final inverse  -> 8 n^3 (7c - 3)
-      self-energy: 2 GEMMs per contact
-      gsmr sweep + Gr(1,1): N inverses, 2(N-1) GEMMs
-      diagonal retarded sweep (DOS): 4 GEMMs per layer 2..N
-      2-contact trace: 2 GEMMs"""
+    """Algorithmic FP64 flops of one point under the reference's operation
+    sequence (uniform PL size n = lead PL size; complex GEMM m*n*k = 8mnk,
+    dense inverse = zgetrf + zgetrs with n right-hand sides = 32/3 n^3):
+      decimation, per lead: ncyc (32/3 + 48) n^3 + 32/3 n^3
+        (src/contselfenergy.F90:271-340; ncyc summed over the leads)
+      self-energy: 16 n^3 per lead (:552-566)
+      gsmr sweep + Gr(1,1): (80/3) N n^3 (src/iterative_cpu.F90:51-124)
+      retarded sweep for the DOS: 40 (N-1) n^3 (:134-224)
+      2-contact trace: 32 n^3 (:399-470)
+    This is the unit of the roofline figure."""
+    n, N = wl["n"], wl["nbl"]
+    n3 = float(n) ** 3
+    dec = (176.0 / 3.0) * n3 * ncyc_total + (32.0 / 3.0) * n3 * ncont
+    sig = 16.0 * n3 * ncont
+    sweep = (80.0 / 3.0) * N * n3
+    dos = 40.0 * (N - 1) * n3 if wl["dos"] else 0.0
+    return dec + sig + sweep + dos + 32.0 * n3
+
+
+def executed_flops_per_point(wl, ncyc_total, ncont=2):
+    """Flops the engine itself executes for the same point: Gauss-Jordan
+    inverse = 8 n^3; the last decimation iteration stops after C1 (2 of its 6
+    products); 4 products per layer in the DOS sweep (the diagonal block
+    only); 2 products for the 2-contact trace."""
     n, N = wl["n"], wl["nbl"]
     u = 8.0 * n ** 3
     dec = u * (7.0 * ncyc_total - 3.0 * ncont)
     sig = u * 2 * ncont
     sweep = u * (N + 2 * (N - 1))
     dos = u * 4 * (N - 1) if wl["dos"] else 0.0
-    tr = u * 2
-    return dec + sig + sweep + dos + tr
+    return dec + sig + sweep + dos + u * 2
 
 
 class ClockSampler:
@@ -314,6 +328,7 @@ def main():
     Tgpu = d_T.cpu().numpy()
     timed = slice(args.warmup * P, nsteps * P)
     flops = float(sum(flops_per_point(wl, int(c)) for c in nc[timed]))
+    flops_exec = float(sum(executed_flops_per_point(wl, int(c)) for c in nc[timed]))
     points_total = args.steps * P * world
     value = points_total / (ms * 1e-3)
 
@@ -351,7 +366,10 @@ def main():
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured in-run: cuBLAS ZGEMM 4096^3 complex128 (FP64 DMMA pipe)",
-                         "flops_per_step": flops / args.steps},
+                         "flop_model": "reference operation sequence, inverse = zgetrf+zgetrs 32/3 n^3",
+                         "flops_per_step": flops / args.steps,
+                         "executed_tflops": flops_exec / (ms * 1e-3) / 1e12,
+                         "executed_frac": flops_exec / (ms * 1e-3) / 1e12 / peak},
             "clocks": clk.summary(),
             "status_counts": {str(k): int(v) for k, v in zip(*np.unique(st[timed], return_counts=True))},
             "ncyc_mean": float(nc[timed].mean()),

@@ -189,6 +189,39 @@ int negf_b200_meir_wingreen(negf_b200_ctx* ctx, int32_t npts,
                             int32_t* scba_iter, double* scba_err,
                             int32_t* ncyc, int32_t* status);
 
+/* ---- projections and contact pairs ----------------------------------------
+ * tun_proj of libNEGF (negf%tun_proj): the transmission trace runs over the
+ * listed orbitals only (1-based global orbital indices; the mask of
+ * get_tun_mask, src/iterative_cpu.F90:586-618, used by both transmission
+ * formulas, :466 and :578).  nidx = 0 clears it (whole trace).  Indices
+ * outside the device are ignored.  Kept with the device description. */
+int negf_b200_set_tun_proj(negf_b200_ctx* ctx, int32_t device_id, int32_t nidx,
+                           const int32_t* idx);
+
+/* dos_proj of libNEGF (negf%dos_proj): nsets LDOS index sets, set k =
+ * set_idx[set_ptr[k] .. set_ptr[k+1]) (1-based orbital indices, summed in
+ * that order; indices past the device skipped), as the LDOS loop of
+ * calculate_transmissions_and_dos (src/iterative.F90:1931-1945).  nsets = 0
+ * clears it.  Kept with the device description. */
+int negf_b200_set_dos_proj(negf_b200_ctx* ctx, int32_t device_id, int32_t nsets,
+                           const int32_t* set_ptr, const int32_t* set_idx);
+
+/* Transmissions between the contact pairs ni[q] -> nf[q], q < npairs (T:
+ * npts x npairs, row-major by point), as calculate_transmissions
+ * (src/iterative.F90:1669-1780): the 2-contact fast path iff the device has
+ * 2 contacts, npairs == 1 and min(cblk) == 1, otherwise gsmr is kept and
+ * every pair takes the N-contact formula.  The reference frees gsmr inside
+ * its pair loop after the first pair (:1766-1767); here it stays valid for
+ * every pair.  With ledos != NULL this is calculate_transmissions_and_dos
+ * (:1821-1952) at E + i*dos_delta instead, and ledos (npts x nsets, nsets =
+ * the largest dos_proj set count over the points' devices) gets the LDOS of
+ * the sets given by negf_b200_set_dos_proj.  Both honour tun_proj. */
+int negf_b200_transmissions(negf_b200_ctx* ctx, int32_t npts,
+                            const int32_t* device_id, const double* energy,
+                            double eta, double dos_delta, int32_t npairs,
+                            const int32_t* ni, const int32_t* nf, double* T,
+                            double* ledos, int32_t* ncyc, int32_t* status);
+
 /* ---- batched solves on device buffers ------------------------------------
  * Same as negf_b200_transmission / _transmission_dos with every per-point
  * array already resident in HBM (device pointers) and no host

@@ -29,7 +29,20 @@ struct DeviceRec {
   int nbl = 0, ncont = 0, norb = 0, nmax = 0;
   int cblk[negf::kMaxCont] = {0};
   bool has_s = false;
+  void* proj_tun = nullptr;    // device copies of the projections (owned)
+  void* proj_dos = nullptr;
+  int nldos = 0;
 };
+
+void free_projections(DeviceRec& r) {
+  if (r.proj_tun) cudaFree(r.proj_tun);
+  if (r.proj_dos) cudaFree(r.proj_dos);
+  r.proj_tun = r.proj_dos = nullptr;
+  r.desc.tun_mask = nullptr;
+  r.desc.ldos_ptr = r.desc.ldos_idx = nullptr;
+  r.desc.nldos = 0;
+  r.nldos = 0;
+}
 
 }  // namespace
 
@@ -228,8 +241,10 @@ int negf_b200_ctx_destroy(negf_b200_ctx* ctx) {
   if (!ctx) return NEGF_B200_ERR_BAD_ARG;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (auto& r : ctx->devs)
+  for (auto& r : ctx->devs) {
     if (r.blob) cudaFree(r.blob);
+    free_projections(r);
+  }
   if (ctx->d_descs) cudaFree(ctx->d_descs);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->io) cudaFree(ctx->io);
@@ -365,6 +380,7 @@ int negf_b200_release_device(negf_b200_ctx* ctx, int32_t id) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->devs[id].blob);
+  free_projections(ctx->devs[id]);
   ctx->devs[id] = DeviceRec();
   ctx->descs_dirty = true;
   return NEGF_B200_OK;
@@ -374,6 +390,73 @@ int negf_b200_device_bytes(const negf_b200_ctx* ctx, int32_t id, size_t* bytes) 
   if (!ctx || !bytes || id < 0 || id >= (int)ctx->devs.size() || !ctx->devs[id].live)
     return NEGF_B200_ERR_BAD_ARG;
   *bytes = ctx->devs[id].bytes;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_set_tun_proj(negf_b200_ctx* ctx, int32_t id, int32_t nidx, const int32_t* idx) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (id < 0 || id >= (int)ctx->devs.size() || !ctx->devs[id].live)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+  if (nidx < 0 || (nidx > 0 && !idx)) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad tun_proj index array");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  cudaStreamSynchronize(ctx->stream);
+  DeviceRec& r = ctx->devs[id];
+  if (r.proj_tun) cudaFree(r.proj_tun);
+  r.proj_tun = nullptr;
+  r.desc.tun_mask = nullptr;
+  ctx->descs_dirty = true;
+  if (nidx == 0) return NEGF_B200_OK;
+  // get_tun_mask (src/iterative_cpu.F90:586-618): indices outside the device are ignored
+  std::vector<unsigned char> mask(r.norb, 0);
+  for (int q = 0; q < nidx; ++q)
+    if (idx[q] >= 1 && idx[q] <= r.norb) mask[idx[q] - 1] = 1;
+  if (cudaMalloc(&r.proj_tun, r.norb) != cudaSuccess) {
+    cudaGetLastError();
+    r.proj_tun = nullptr;
+    return fail(ctx, NEGF_B200_ERR_NOMEM, "device allocation of the tun_proj mask failed");
+  }
+  CK(cudaMemcpy(r.proj_tun, mask.data(), r.norb, cudaMemcpyHostToDevice));
+  r.desc.tun_mask = reinterpret_cast<const unsigned char*>(r.proj_tun);
+  return NEGF_B200_OK;
+}
+
+int negf_b200_set_dos_proj(negf_b200_ctx* ctx, int32_t id, int32_t nsets, const int32_t* set_ptr,
+                           const int32_t* set_idx) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (id < 0 || id >= (int)ctx->devs.size() || !ctx->devs[id].live)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+  if (nsets < 0 || (nsets > 0 && !set_ptr)) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad dos_proj arrays");
+  const int nidx = nsets > 0 ? set_ptr[nsets] : 0;
+  if (nsets > 0) {
+    if (set_ptr[0] != 0 || (nidx > 0 && !set_idx)) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad dos_proj arrays");
+    for (int k = 0; k < nsets; ++k)
+      if (set_ptr[k + 1] < set_ptr[k]) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "dos_proj set_ptr must not decrease");
+  }
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  cudaStreamSynchronize(ctx->stream);
+  DeviceRec& r = ctx->devs[id];
+  if (r.proj_dos) cudaFree(r.proj_dos);
+  r.proj_dos = nullptr;
+  r.desc.ldos_ptr = r.desc.ldos_idx = nullptr;
+  r.desc.nldos = 0;
+  r.nldos = 0;
+  ctx->descs_dirty = true;
+  if (nsets == 0) return NEGF_B200_OK;
+  const size_t bytes = (size_t)(nsets + 1 + std::max(1, nidx)) * 4;
+  if (cudaMalloc(&r.proj_dos, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    r.proj_dos = nullptr;
+    return fail(ctx, NEGF_B200_ERR_NOMEM, "device allocation of the dos_proj sets failed");
+  }
+  int* d = reinterpret_cast<int*>(r.proj_dos);
+  CK(cudaMemcpy(d, set_ptr, (size_t)(nsets + 1) * 4, cudaMemcpyHostToDevice));
+  if (nidx > 0) CK(cudaMemcpy(d + nsets + 1, set_idx, (size_t)nidx * 4, cudaMemcpyHostToDevice));
+  r.desc.ldos_ptr = d;
+  r.desc.ldos_idx = d + nsets + 1;
+  r.desc.nldos = nsets;
+  r.nldos = nsets;
   return NEGF_B200_OK;
 }
 
@@ -387,10 +470,20 @@ static int check_pair(negf_b200_ctx* ctx, int npts, const int32_t* ids, int ni, 
   return NEGF_B200_OK;
 }
 
+static int check_pairs(negf_b200_ctx* ctx, int npts, const int32_t* ids, int npairs, const int32_t* ni,
+                       const int32_t* nf) {
+  for (int q = 0; q < npairs; ++q) {
+    int st = check_pair(ctx, npts, ids, ni[q], nf[q]);
+    if (st) return st;
+  }
+  return NEGF_B200_OK;
+}
+
 static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t* ids, const double* E,
                       double eta, double dos_delta, int32_t ni, int32_t nf, double* T, double* dos, int32_t* ncyc,
                       int32_t* status, const double* frm, const double* coupling, double* curr, double* lcurr,
-                      double* ldens, int32_t* scba_iter, double* scba_err) {
+                      double* ldens, int32_t* scba_iter, double* scba_err, int32_t npairs = 1,
+                      const int32_t* pni = nullptr, const int32_t* pnf = nullptr, double* ledos = nullptr) {
   if (!ctx) return NEGF_B200_ERR_BAD_ARG;
   if (npts < 0 || (npts > 0 && (!ids || !E))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
   if (npts == 0) return NEGF_B200_OK;
@@ -399,15 +492,19 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   LaunchShape sh;
   int st = shape_of(ctx, npts, ids, sh);
   if (st) return st;
-  int ncont_pts = 0, nbl_pts = 0, norb_pts = 0;
+  int ncont_pts = 0, nbl_pts = 0, norb_pts = 0, nldos_pts = 0;
   for (int p = 0; p < npts; ++p) {
     const DeviceRec& r = ctx->devs[ids[p]];
     ncont_pts = std::max(ncont_pts, r.ncont);
     nbl_pts = std::max(nbl_pts, r.nbl);
     norb_pts = std::max(norb_pts, r.norb);
+    nldos_pts = std::max(nldos_pts, r.nldos);
   }
+  if (npairs < 1 || (npairs > 1 && (!pni || !pnf)))
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "npairs must be >= 1 with ni/nf arrays");
+  if (ledos && mode != negf::MODE_DOS) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "ledos needs the DOS solve");
   if (mode != negf::MODE_GN) {
-    st = check_pair(ctx, npts, ids, ni, nf);
+    st = (npairs > 1) ? check_pairs(ctx, npts, ids, npairs, pni, pnf) : check_pair(ctx, npts, ids, ni, nf);
     if (st) return st;
   } else {
     for (int p = 0; p < npts; ++p)
@@ -418,9 +515,11 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   size_t need = 0;
   {
     Carve c{nullptr};
-    c.take<int32_t>(npts); c.take<double>(npts); c.take<double>(npts); c.take<int32_t>(npts);
+    c.take<int32_t>(npts); c.take<double>(npts); c.take<double>((size_t)npts * npairs); c.take<int32_t>(npts);
     c.take<int32_t>(npts);
-    if (dos) c.take<double>((size_t)npts * norb_pts);
+    if (dos || ledos) c.take<double>((size_t)npts * norb_pts);
+    if (ledos) c.take<double>((size_t)npts * std::max(1, nldos_pts));
+    if (npairs > 1) { c.take<int32_t>(npairs); c.take<int32_t>(npairs); }
     if (frm) c.take<double>((size_t)npts * ncont_pts);
     if (coupling) c.take<double>((size_t)norb_pts);
     if (curr) c.take<double>((size_t)npts * ncont_pts);
@@ -434,10 +533,13 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   Carve c{reinterpret_cast<char*>(ctx->io)};
   int32_t* d_ids = c.take<int32_t>(npts);
   double* d_E = c.take<double>(npts);
-  double* d_T = c.take<double>(npts);
+  double* d_T = c.take<double>((size_t)npts * npairs);
   int32_t* d_ncyc = c.take<int32_t>(npts);
   int32_t* d_st = c.take<int32_t>(npts);
-  double* d_dos = dos ? c.take<double>((size_t)npts * norb_pts) : nullptr;
+  double* d_dos = (dos || ledos) ? c.take<double>((size_t)npts * norb_pts) : nullptr;
+  double* d_ldos = ledos ? c.take<double>((size_t)npts * std::max(1, nldos_pts)) : nullptr;
+  int32_t* d_pni = (npairs > 1) ? c.take<int32_t>(npairs) : nullptr;
+  int32_t* d_pnf = (npairs > 1) ? c.take<int32_t>(npairs) : nullptr;
   double* d_frm = frm ? c.take<double>((size_t)npts * ncont_pts) : nullptr;
   double* d_cpl = coupling ? c.take<double>((size_t)norb_pts) : nullptr;
   double* d_curr = curr ? c.take<double>((size_t)npts * ncont_pts) : nullptr;
@@ -450,10 +552,14 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   CK(cudaMemcpyAsync(d_E, E, npts * 8, cudaMemcpyHostToDevice, s));
   if (d_frm) CK(cudaMemcpyAsync(d_frm, frm, (size_t)npts * ncont_pts * 8, cudaMemcpyHostToDevice, s));
   if (d_cpl) CK(cudaMemcpyAsync(d_cpl, coupling, (size_t)norb_pts * 8, cudaMemcpyHostToDevice, s));
+  if (d_pni) CK(cudaMemcpyAsync(d_pni, pni, (size_t)npairs * 4, cudaMemcpyHostToDevice, s));
+  if (d_pnf) CK(cudaMemcpyAsync(d_pnf, pnf, (size_t)npairs * 4, cudaMemcpyHostToDevice, s));
   negf::EngineArgs a = base_args(ctx, mode, npts);
   a.dev_id = d_ids; a.energy = d_E; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
   a.T = d_T; a.ncyc = d_ncyc; a.status = d_st;
+  a.npairs = npairs; a.pair_ni = d_pni; a.pair_nf = d_pnf;
   a.dos = d_dos; a.dos_stride = norb_pts;
+  a.ldos = d_ldos; a.ldos_stride = std::max(1, nldos_pts);
   a.frm = d_frm; a.frm_stride = ncont_pts; a.coupling = d_cpl;
   a.curr = d_curr; a.curr_stride = ncont_pts;
   a.lcurr = d_lcurr; a.lcurr_stride = std::max(1, nbl_pts - 1);
@@ -462,7 +568,9 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   st = run_device(ctx, a, sh, s);
   if (st) return st;
   std::vector<int32_t> hst(npts);
-  if (T) CK(cudaMemcpyAsync(T, d_T, npts * 8, cudaMemcpyDeviceToHost, s));
+  if (T) CK(cudaMemcpyAsync(T, d_T, (size_t)npts * npairs * 8, cudaMemcpyDeviceToHost, s));
+  if (ledos && nldos_pts > 0)
+    CK(cudaMemcpyAsync(ledos, d_ldos, (size_t)npts * nldos_pts * 8, cudaMemcpyDeviceToHost, s));
   if (ncyc) CK(cudaMemcpyAsync(ncyc, d_ncyc, npts * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
   if (dos) CK(cudaMemcpyAsync(dos, d_dos, (size_t)npts * norb_pts * 8, cudaMemcpyDeviceToHost, s));
@@ -496,6 +604,15 @@ int negf_b200_meir_wingreen(negf_b200_ctx* ctx, int32_t npts, const int32_t* dev
                             int32_t* ncyc, int32_t* status) {
   return solve_host(ctx, negf::MODE_GN, npts, device_id, energy, eta, 0.0, 1, 2, nullptr, nullptr, ncyc, status,
                     frm, coupling, curr, layer_curr, layer_dens, scba_iter, scba_err);
+}
+
+int negf_b200_transmissions(negf_b200_ctx* ctx, int32_t npts, const int32_t* device_id, const double* energy,
+                            double eta, double dos_delta, int32_t npairs, const int32_t* ni, const int32_t* nf,
+                            double* T, double* ledos, int32_t* ncyc, int32_t* status) {
+  if (!ctx || npairs < 1 || !ni || !nf) return NEGF_B200_ERR_BAD_ARG;
+  return solve_host(ctx, ledos ? negf::MODE_DOS : negf::MODE_T, npts, device_id, energy, eta, ledos ? dos_delta : 0.0,
+                    ni[0], nf[0], T, nullptr, ncyc, status, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                    nullptr, npairs, ni, nf, ledos);
 }
 
 // ---- device-pointer solve (inputs already resident in HBM) ------------------

@@ -557,10 +557,12 @@ __device__ __forceinline__ double cta_max(double v, double* red) {
 }
 
 // Re Tr(X Y) = sum_{i,j} Re(X(i,j) Y(j,i)); op applies to Y (OP_C: Y = Z^dag)
-__device__ __forceinline__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red) {
+__device__ __forceinline__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red,
+                                                   const unsigned char* mask = nullptr) {
   double acc = 0.0;
   for (int idx = threadIdx.x; idx < n * n; idx += blockDim.x) {
     const int i = idx % n, j = idx / n;
+    if (mask && !mask[i]) continue;
     double2 x = X[idx];
     double2 y = (opY == OP_C) ? cconj(Y[(size_t)i + (size_t)j * n]) : Y[(size_t)j + (size_t)i * n];
     acc += x.x * y.x - x.y * y.y;

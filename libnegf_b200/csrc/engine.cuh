@@ -35,6 +35,11 @@ struct DevDesc {
   int64_t omc[kMaxCont];    // offset of hmc/smc blocks (n_cb x L)
   const double2* h00; const double2* h01; const double2* s00; const double2* s01;
   const double2* hmc; const double2* smc;
+  // projections (negf_b200_set_tun_proj / negf_b200_set_dos_proj)
+  const unsigned char* tun_mask;   // [norb], 1 = orbital inside the transmission trace; null = all
+  const int* ldos_ptr;             // [nldos+1] LDOS set k = ldos_idx[ldos_ptr[k] .. ldos_ptr[k+1])
+  const int* ldos_idx;             // 1-based orbital indices
+  int nldos, pad2;
 };
 
 struct EngineArgs {
@@ -44,13 +49,17 @@ struct EngineArgs {
   const double* energy;
   const DevDesc* devs;
   double eta, dos_delta;
-  int ni, nf;
+  int ni, nf;                    // the contact pair when npairs <= 1 (1-based)
+  int npairs;                    // >= 1: T is npts x npairs
+  const int* pair_ni;            // [npairs] (device) when npairs > 1
+  const int* pair_nf;
   double sgf_tol;
   int sgf_max_iter;
   double eps;
   // outputs
   double* T;
   double* dos; int64_t dos_stride;
+  double* ldos; int ldos_stride;  // LDOS over the device's index sets (MODE_DOS; needs dos)
   int* ncyc;
   int* status;
   // non-equilibrium (MODE_GN)

@@ -16,6 +16,7 @@ __device__ int engine_step(const EngineArgs& a, EngineCtl& c, SmemMap& sm) {
   w.base = a.ws + (int64_t)blockIdx.x * a.ws_per_cta;
   w.Q = a.Q;
   w.ncont = a.ncont_max;
+  w.nbl_max = a.nbl_max;
   for (;;) {
     if (c.in_inv) {
       const int st = inv_next(c.ip, sm.main, sm.inv);

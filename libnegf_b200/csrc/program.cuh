@@ -77,10 +77,13 @@ struct Ws {
   double2* base;
   int64_t Q;
   int ncont;
+  int nbl_max;
   __device__ double2* slot(int k) const { return base + (int64_t)k * Q; }
   __device__ double2* inv() const { return slot(S_INV); }
   __device__ double2* sig(int c) const { return slot(S_SIG + c); }
   __device__ double2* layer(int arr, int i, int nbl) const { return slot(S_SIG + ncont + arr * nbl + i); }
+  // T / DOS: Gr(cb,cb) kept at the block of contact c during the forward sweep
+  __device__ double2* keep(int c) const { return slot(S_SIG + ncont + nbl_max + c); }
 };
 
 // ---------------------------------------------------------------- ops
@@ -93,9 +96,9 @@ enum OpKind : int {
   K_SUB,       // C -= A, m elements
   K_DECUPD,    // C -= A and D -= A, m elements (decimation Ao_s, Ao update)
   K_SPECTRAL,  // C = i (A - A^dag), order m
-  K_TRACE,     // res[slot] = Re Tr(A op(B)), order m
+  K_TRACE,     // res[slot] = Re Tr(A op(B)), order m (diagonal entries k with mask[k], if mask)
   K_TRACEC,    // res[slot], res[slot+1] = Tr(A op(B)), A m x n
-  K_TRACEN,    // res[slot] = Re Tr(A B^dag), A and B m x n
+  K_TRACEN,    // res[slot] = Re Tr(A B^dag), A and B m x n (rows k with mask[k], if mask)
   K_DOS,       // out[k] = -Im A_kk / pi, k < m
   K_SIGDIAG,   // C[k] = cpl[k]^2 A_kk, k < m
   K_SNINIT,    // C (m x m) = diag(A) or 0
@@ -106,6 +109,7 @@ enum OpKind : int {
                //   Y (n x m) adds the pattern of Y at transposed positions
   K_MAXABS,    // res[slot] = max |A(q)|, m elements
   K_TRDIAG,    // res[slot] = Re Tr A, order m
+  K_LDOS,      // out[k] = sum over LDOS set k of dos[i-1] (A = dos row as doubles, device sets)
 };
 
 struct Op {
@@ -122,6 +126,8 @@ struct Op {
   const double2* V;
   const double* cpl;
   double* out;
+  const unsigned char* mask;   // K_TRACE / K_TRACEN projection, or null
+  const DevDesc* dd;           // K_LDOS
   double2 alpha, beta;
   double scal;
 };
@@ -170,7 +176,7 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       cta_spectral(o.C, o.A, o.m);
       break;
     case K_TRACE: {
-      const double r = cta_re_trace_prod(o.A, o.B, o.m, o.opb, sm.red);
+      const double r = cta_re_trace_prod(o.A, o.B, o.m, o.opb, sm.red, o.mask);
       if (tid == 0) sm.res[o.slot] = r;
       break;
     }
@@ -193,6 +199,7 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       const int n2 = o.m, n1 = o.n;
       double acc = 0.0;
       for (int idx = tid; idx < n2 * n1; idx += blockDim.x) {
+        if (o.mask && !o.mask[idx % n2]) continue;
         const double2 x = o.A[idx], y = o.B[idx];   // W2(r,c) * conj(G21(r,c))
         acc += x.x * y.x + x.y * y.y;
       }
@@ -269,6 +276,20 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       if (tid == 0) sm.res[o.slot] = tr;
       break;
     }
+    case K_LDOS: {
+      // set k summed in its index order, as the reference's accumulation
+      // loop (src/iterative.F90:1931-1945); indices past the device skipped
+      const double* dos = reinterpret_cast<const double*>(o.A);
+      for (int k = tid; k < o.dd->nldos; k += blockDim.x) {
+        double acc = 0.0;
+        for (int q = o.dd->ldos_ptr[k]; q < o.dd->ldos_ptr[k + 1]; ++q) {
+          const int i2 = o.dd->ldos_idx[q];
+          if (i2 >= 1 && i2 <= o.dd->norb) acc += dos[i2 - 1];
+        }
+        o.out[k] = acc;
+      }
+      break;
+    }
     default:
       break;
   }
@@ -292,8 +313,8 @@ struct Prog {
   double2* gsv;         // target of gr_first
   int keep;
   const double2* sr;    // dephasing sigma_r in effect (or null)
-  // transmission bookkeeping
-  int fast, ct1, ct2, bl1, bl2;
+  // transmission bookkeeping (contact pair q of npairs)
+  int fast, ct1, ct2, bl1, bl2, q, npairs;
   double T;
   // SCBA
   int sit, conv, have_old, par;
@@ -327,6 +348,21 @@ __device__ __forceinline__ void op_esh_lo(Op& o, const DevDesc* d, int i, double
 }
 
 __device__ __forceinline__ void put_status(int& st, int s) { if (st == ST_OK) st = s; }
+
+// Contact pair q (0-based) of the call: ct1 is the contact on the smaller
+// block (src/iterative_cpu.F90:421-427), ct2 the other; bl1/bl2 their blocks.
+__device__ __forceinline__ void pair_of(const EngineArgs& a, Prog& s, int q) {
+  const int ni = (a.npairs > 1 ? a.pair_ni[q] : a.ni) - 1, nf = (a.npairs > 1 ? a.pair_nf[q] : a.nf) - 1;
+  const int cbi = s.d->cblk[ni < s.d->ncont ? ni : 0], cbf = s.d->cblk[nf < s.d->ncont ? nf : 0];
+  s.ct1 = (cbi < cbf) ? ni : nf;
+  s.ct2 = (cbi < cbf) ? nf : ni;
+  s.bl1 = s.d->cblk[s.ct1 < s.d->ncont ? s.ct1 : 0];
+  s.bl2 = s.d->cblk[s.ct2 < s.d->ncont ? s.ct2 : 0];
+}
+
+__device__ __forceinline__ const unsigned char* tun_mask_of(const DevDesc* d, int bl) {
+  return d->tun_mask ? d->tun_mask + d->pstart[bl - 1] : nullptr;
+}
 
 // Fills `o` with the next block operation of this CTA and returns true, or
 // returns false when the work queue is exhausted.
@@ -415,16 +451,23 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
       }
 
       // ------------------------------------------------ transmission bookkeeping
-      {
-        const int ni = a.ni - 1, nf = a.nf - 1;
-        const int cbi = s.d->cblk[ni < s.d->ncont ? ni : 0], cbf = s.d->cblk[nf < s.d->ncont ? nf : 0];
-        s.ct1 = (cbi < cbf) ? ni : nf;
-        s.ct2 = (cbi < cbf) ? nf : ni;
-        s.bl1 = s.d->cblk[s.ct1 < s.d->ncont ? s.ct1 : 0];
-        s.bl2 = s.d->cblk[s.ct2 < s.d->ncont ? s.ct2 : 0];
-        s.fast = (a.mode == MODE_T) && s.d->ncont == 2 && min(cbi, cbf) == 1;
+      // calculate_transmissions (src/iterative.F90:1669-1780): the 2-contact
+      // fast path iff 2 contacts, one pair and that pair's smaller block is 1;
+      // otherwise gsmr is kept and every pair takes the N-contact formula.
+      // The forward sweep runs to the largest ct1 block over the pairs.
+      s.npairs = a.npairs > 1 ? a.npairs : 1;
+      s.last = 0;
+      for (s.q = s.npairs - 1; s.q >= 0; --s.q) {
+        pair_of(a, s, s.q);
+        s.last = max(s.last, s.bl1 - 1);
       }
-      if (a.mode == MODE_T && s.d->ncont == 1) goto point_done;
+      s.q = 0;                              // pair_of(0) is in effect
+      s.fast = (a.mode == MODE_T) && s.d->ncont == 2 && s.npairs == 1 && s.bl1 == 1;
+      if (a.mode == MODE_T && s.d->ncont == 1) {
+        if (threadIdx.x == 0 && a.T)
+          for (int q = 0; q < s.npairs; ++q) a.T[(int64_t)s.p * s.npairs + q] = 0.0;
+        goto point_done;
+      }
 
       // ------------------------------------------------ SCBA loop (once for T / DOS)
       s.sit = 0; s.conv = 0; s.have_old = 0; s.err = 0.0; s.par = 0;
@@ -500,13 +543,14 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         if (s.fast) {
           // ------------------------------------ 2-contact trace (iterative_cpu.F90:399-470)
           s.lo = s.d->pl[0];
+          s.q = 0;
           goto trans2;
         }
         // -------------------------------------- forward retarded sweep
         // T / DOS: Gr(i,i) ping-pongs in slots 11/10, Gr(bl1,bl1) kept in slot 9.
         // GN: Gr(i,i) -> layer 1, Gr(i-1,i) -> layer 2.
         s.cur = 0;
-        s.last = (a.mode == MODE_T) ? s.bl1 - 1 : s.d->nbl - 1;
+        if (a.mode != MODE_T) s.last = s.d->nbl - 1;
         for (s.i = 0; s.i <= s.last; ++s.i) {
           if (s.i > 0) {
             // gr_step(i): E1 = ESH(i-1,i) slot 0, E2 = ESH(i,i-1) slot 1, X slot 2, W2 slot 3, GL slot 6
@@ -545,54 +589,90 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
             o.out = a.dos + (int64_t)s.p * a.dos_stride + s.d->pstart[s.i];
             PT_EMIT(s);
           }
-          if (a.mode != MODE_GN && s.i == s.bl1 - 1) {
-            set_simple(o, K_COPY, s.d->pl[s.i] * s.d->pl[s.i], w.slot(11 - s.cur), w.slot(9));
-            PT_EMIT(s);
-          }
+          if (a.mode != MODE_GN)
+            for (s.j = 0; s.j < s.d->ncont; ++s.j)
+              if (s.d->cblk[s.j] == s.i + 1) {
+                set_simple(o, K_COPY, s.d->pl[s.i] * s.d->pl[s.i], w.slot(11 - s.cur), w.keep(s.j));
+                PT_EMIT(s);
+              }
         }
         if (a.mode != MODE_GN) {
-          if (s.d->ncont == 1) { s.T = 0.0; goto point_done; }
-          if (a.mode == MODE_DOS && s.d->ncont == 2) {
-            s.lo = s.d->pl[s.bl1 - 1];
-            s.gsv = w.slot(9);
-            goto trans2;
+          if (a.mode == MODE_DOS && a.ldos && a.dos && s.d->nldos > 0) {
+            o.kind = K_LDOS; o.A = reinterpret_cast<const double2*>(a.dos + (int64_t)s.p * a.dos_stride);
+            o.out = a.ldos + (int64_t)s.p * a.ldos_stride; o.dd = s.d;
+            PT_EMIT(s);
           }
-          // ------------------------------------ column sweep Gr(i,bl1) (iterative_cpu.F90:507-538)
-          s.cc = 0;
-          s.tiny = 0;
-          for (s.i = s.bl1; s.i <= s.bl2 - 1; ++s.i) {
-            set_simple(o, K_MAXABS, s.d->pl[s.i - 1] * s.d->pl[s.bl1 - 1], s.cc ? w.slot(6) : w.slot(9), nullptr);
-            o.slot = 0;
+          for (s.q = 0; s.q < s.npairs; ++s.q) {
+            pair_of(a, s, s.q);
+            if (s.d->ncont == 1) { s.T = 0.0; goto pair_done; }
+            if (a.mode == MODE_DOS && s.d->ncont == 2) {
+              s.lo = s.d->pl[s.bl1 - 1];
+              s.gsv = w.keep(s.ct1);
+              goto trans2;
+            }
+            // ---------------------------------- column sweep Gr(i,bl1) (iterative_cpu.F90:507-538)
+            set_simple(o, K_COPY, s.d->pl[s.bl1 - 1] * s.d->pl[s.bl1 - 1], w.keep(s.ct1), w.slot(9));
             PT_EMIT(s);
-            if (sm.res[0] < a.eps) { s.tiny = 1; break; }
-            op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(0));
+            s.cc = 0;
+            s.tiny = 0;
+            for (s.i = s.bl1; s.i <= s.bl2 - 1; ++s.i) {
+              set_simple(o, K_MAXABS, s.d->pl[s.i - 1] * s.d->pl[s.bl1 - 1], s.cc ? w.slot(6) : w.slot(9), nullptr);
+              o.slot = 0;
+              PT_EMIT(s);
+              if (sm.res[0] < a.eps) { s.tiny = 1; break; }
+              op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(0));
+              PT_EMIT(s);
+              set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i],
+                       OP_N, w.slot(0), s.d->pl[s.i], OP_N, w.slot(1), s.d->pl[s.i], mone, zero);
+              PT_EMIT(s);
+              set_gemm(o, s.d->pl[s.i], s.d->pl[s.bl1 - 1], s.d->pl[s.i - 1], w.slot(1), s.d->pl[s.i], OP_N,
+                       s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.i - 1], OP_N, s.cc ? w.slot(9) : w.slot(6),
+                       s.d->pl[s.i], one, zero);
+              PT_EMIT(s);
+              s.cc ^= 1;
+            }
+            if (s.tiny) { s.T = a.eps * a.eps; goto pair_done; }
+            // ---------------------------------- N-contact trace |Re Tr[Gam2 G21 Gam1 G21^dag]|
+            // Gam1 slot 7, Gam2 slot 8, W1 slot 2, W2 slot 3; G21 in slot 9 or 6
+            set_simple(o, K_SPECTRAL, s.d->pl[s.bl1 - 1], w.sig(s.ct1), w.slot(7));
             PT_EMIT(s);
-            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
-                     w.slot(0), s.d->pl[s.i], OP_N, w.slot(1), s.d->pl[s.i], mone, zero);
+            set_simple(o, K_SPECTRAL, s.d->pl[s.bl2 - 1], w.sig(s.ct2), w.slot(8));
             PT_EMIT(s);
-            set_gemm(o, s.d->pl[s.i], s.d->pl[s.bl1 - 1], s.d->pl[s.i - 1], w.slot(1), s.d->pl[s.i], OP_N,
-                     s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.i - 1], OP_N, s.cc ? w.slot(9) : w.slot(6), s.d->pl[s.i],
-                     one, zero);
+            set_gemm(o, s.d->pl[s.bl2 - 1], s.d->pl[s.bl1 - 1], s.d->pl[s.bl2 - 1], w.slot(8), s.d->pl[s.bl2 - 1],
+                     OP_N, s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.bl2 - 1], OP_N, w.slot(2), s.d->pl[s.bl2 - 1], one,
+                     zero);
             PT_EMIT(s);
-            s.cc ^= 1;
+            set_gemm(o, s.d->pl[s.bl2 - 1], s.d->pl[s.bl1 - 1], s.d->pl[s.bl1 - 1], w.slot(2), s.d->pl[s.bl2 - 1],
+                     OP_N, w.slot(7), s.d->pl[s.bl1 - 1], OP_N, w.slot(3), s.d->pl[s.bl2 - 1], one, zero);
+            PT_EMIT(s);
+            o.kind = K_TRACEN; o.m = s.d->pl[s.bl2 - 1]; o.n = s.d->pl[s.bl1 - 1]; o.A = w.slot(3);
+            o.B = s.cc ? w.slot(6) : w.slot(9); o.slot = 0; o.mask = tun_mask_of(s.d, s.bl2);
+            PT_EMIT(s);
+            s.T = fabs(sm.res[0]);
+            goto pair_done;
+          trans2:
+            // |Re Tr[Gam1 i(G - G^dag) - Gam1 G Gam1 G^dag]| over the tun_proj rows of block bl1;
+            // G in s.gsv, order s.lo.  Gam slot 7, W1 slot 8, W2 slot 2, A slot 3
+            set_simple(o, K_SPECTRAL, s.lo, w.sig(s.ct1), w.slot(7));
+            PT_EMIT(s);
+            set_simple(o, K_SPECTRAL, s.lo, s.gsv, w.slot(3));
+            PT_EMIT(s);
+            set_gemm(o, s.lo, s.lo, s.lo, w.slot(7), s.lo, OP_N, s.gsv, s.lo, OP_N, w.slot(8), s.lo, one, zero);
+            PT_EMIT(s);
+            set_gemm(o, s.lo, s.lo, s.lo, w.slot(8), s.lo, OP_N, w.slot(7), s.lo, OP_N, w.slot(2), s.lo, one, zero);
+            PT_EMIT(s);
+            o.kind = K_TRACE; o.m = s.lo; o.A = w.slot(2); o.B = s.gsv; o.opb = OP_C; o.slot = 0;  // Tr(Gam G Gam G^dag)
+            o.mask = tun_mask_of(s.d, s.bl1);
+            PT_EMIT(s);
+            o.kind = K_TRACE; o.m = s.lo; o.A = w.slot(7); o.B = w.slot(3); o.opb = OP_N; o.slot = 1;  // Tr(Gam A)
+            o.mask = tun_mask_of(s.d, s.bl1);
+            PT_EMIT(s);
+            s.T = fabs(sm.res[1] - sm.res[0]);
+          pair_done:
+            if (!isfinite(s.T)) put_status(s.st, ST_NONFINITE);
+            if (threadIdx.x == 0 && a.T) a.T[(int64_t)s.p * s.npairs + s.q] = s.T;
+            __syncthreads();
           }
-          if (s.tiny) { s.T = a.eps * a.eps; goto point_done; }
-          // ------------------------------------ N-contact trace |Re Tr[Gam2 G21 Gam1 G21^dag]|
-          // Gam1 slot 7, Gam2 slot 8, W1 slot 2, W2 slot 3; G21 in slot 9 or 6
-          set_simple(o, K_SPECTRAL, s.d->pl[s.bl1 - 1], w.sig(s.ct1), w.slot(7));
-          PT_EMIT(s);
-          set_simple(o, K_SPECTRAL, s.d->pl[s.bl2 - 1], w.sig(s.ct2), w.slot(8));
-          PT_EMIT(s);
-          set_gemm(o, s.d->pl[s.bl2 - 1], s.d->pl[s.bl1 - 1], s.d->pl[s.bl2 - 1], w.slot(8), s.d->pl[s.bl2 - 1], OP_N,
-                   s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.bl2 - 1], OP_N, w.slot(2), s.d->pl[s.bl2 - 1], one, zero);
-          PT_EMIT(s);
-          set_gemm(o, s.d->pl[s.bl2 - 1], s.d->pl[s.bl1 - 1], s.d->pl[s.bl1 - 1], w.slot(2), s.d->pl[s.bl2 - 1],
-                   OP_N, w.slot(7), s.d->pl[s.bl1 - 1], OP_N, w.slot(3), s.d->pl[s.bl2 - 1], one, zero);
-          PT_EMIT(s);
-          o.kind = K_TRACEN; o.m = s.d->pl[s.bl2 - 1]; o.n = s.d->pl[s.bl1 - 1]; o.A = w.slot(3);
-          o.B = s.cc ? w.slot(6) : w.slot(9); o.slot = 0;
-          PT_EMIT(s);
-          s.T = fabs(sm.res[0]);
           goto point_done;
         }
         // ================================== elastic SCBA: lesser sweep (GN)
@@ -724,10 +804,10 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           set_simple(o, K_SPECTRAL, s.d->pl[s.d->cblk[s.c] - 1], w.layer(1, s.d->cblk[s.c] - 1, s.d->nbl), w.slot(8));
           PT_EMIT(s);
           o.kind = K_TRACE; o.m = s.d->pl[s.d->cblk[s.c] - 1]; o.A = w.slot(7);
-          o.B = w.layer(4 + s.par, s.d->cblk[s.c] - 1, s.d->nbl); o.opb = OP_N; o.slot = 2;
+          o.B = w.layer(4 + s.par, s.d->cblk[s.c] - 1, s.d->nbl); o.opb = OP_N; o.slot = 2; o.mask = nullptr;
           PT_EMIT(s);
           o.kind = K_TRACE; o.m = s.d->pl[s.d->cblk[s.c] - 1]; o.A = w.slot(7); o.B = w.slot(8); o.opb = OP_N;
-          o.slot = 3;
+          o.slot = 3; o.mask = nullptr;
           PT_EMIT(s);
           if (threadIdx.x == 0)
             a.curr[(int64_t)s.p * a.curr_stride + s.c] =
@@ -764,27 +844,8 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
       }
       goto point_done;
 
-    trans2:
-      // |Re Tr[Gam1 i(G - G^dag) - Gam1 G Gam1 G^dag]|; G in s.gsv, order s.lo.
-      // Gam slot 7, W1 slot 8, W2 slot 2, A slot 3
-      set_simple(o, K_SPECTRAL, s.lo, w.sig(s.ct1), w.slot(7));
-      PT_EMIT(s);
-      set_simple(o, K_SPECTRAL, s.lo, s.gsv, w.slot(3));
-      PT_EMIT(s);
-      set_gemm(o, s.lo, s.lo, s.lo, w.slot(7), s.lo, OP_N, s.gsv, s.lo, OP_N, w.slot(8), s.lo, one, zero);
-      PT_EMIT(s);
-      set_gemm(o, s.lo, s.lo, s.lo, w.slot(8), s.lo, OP_N, w.slot(7), s.lo, OP_N, w.slot(2), s.lo, one, zero);
-      PT_EMIT(s);
-      o.kind = K_TRACE; o.m = s.lo; o.A = w.slot(2); o.B = s.gsv; o.opb = OP_C; o.slot = 0;   // Tr(Gam G Gam G^dag)
-      PT_EMIT(s);
-      o.kind = K_TRACE; o.m = s.lo; o.A = w.slot(7); o.B = w.slot(3); o.opb = OP_N; o.slot = 1;   // Tr(Gam A)
-      PT_EMIT(s);
-      s.T = fabs(sm.res[1] - sm.res[0]);
-
     point_done:
-      if (a.mode != MODE_GN && !isfinite(s.T)) put_status(s.st, ST_NONFINITE);
       if (threadIdx.x == 0) {
-        if (a.T) a.T[s.p] = s.T;
         if (a.ncyc) a.ncyc[s.p] = s.ncyc;
         if (a.status) a.status[s.p] = s.st;
       }

@@ -13,6 +13,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from .device import Device
+from .projections import dos_sets, tun_indices
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libnegf_b200.so")
@@ -30,7 +31,8 @@ EXPORTED = [
     "negf_b200_meir_wingreen", "negf_b200_transmission_dev", "negf_b200_transmission_dos_dev",
     "negf_b200_zgemm_batched", "negf_b200_zinv_work_bytes", "negf_b200_zinv_batched",
     "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
-    "negf_b200_get_trace", "negf_b200_decimation_noalloc",
+    "negf_b200_get_trace", "negf_b200_decimation_noalloc", "negf_b200_set_tun_proj", "negf_b200_set_dos_proj",
+    "negf_b200_transmissions",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -89,6 +91,9 @@ def load():
     L.negf_b200_set_tracing.argtypes = [vp, i32]
     L.negf_b200_get_trace.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
     L.negf_b200_decimation_noalloc.argtypes = [i32, i32, vp, vp, vp, vp, vp, f64, i32, vp]
+    L.negf_b200_set_tun_proj.argtypes = [vp, i32, i32, ip]
+    L.negf_b200_set_dos_proj.argtypes = [vp, i32, i32, ip, ip]
+    L.negf_b200_transmissions.argtypes = [vp, i32, ip, dp, f64, f64, i32, ip, ip, dp, dp, ip, ip]
     _lib = L
     return L
 
@@ -114,6 +119,7 @@ class Context:
         self._h = h
         self._L = L
         self.devices = {}
+        self._nldos = {}
         if options:
             self.set_options(**options)
 
@@ -170,6 +176,42 @@ class Context:
         self._check(self._L.negf_b200_upload_device(self._h, ctypes.byref(st), ctypes.byref(did)), "upload")
         self.devices[did.value] = dev
         return did.value
+
+    def set_tun_proj(self, device_id, tun_proj):
+        """tun_proj (1-based orbital indices) of the device; None or [] = whole trace."""
+        idx = tun_indices(tun_proj if tun_proj is not None else [])
+        self._check(self._L.negf_b200_set_tun_proj(self._h, device_id, idx.size, _i(idx) if idx.size else None),
+                    "set_tun_proj")
+
+    def set_dos_proj(self, device_id, dos_proj):
+        """dos_proj (list of 1-based orbital index sets) of the device; None or [] = none."""
+        if not dos_proj:
+            self._check(self._L.negf_b200_set_dos_proj(self._h, device_id, 0, None, None), "set_dos_proj")
+            self._nldos[device_id] = 0
+            return
+        ptr, idx = dos_sets(dos_proj)
+        self._check(self._L.negf_b200_set_dos_proj(self._h, device_id, ptr.size - 1, _i(ptr), _i(idx)),
+                    "set_dos_proj")
+        self._nldos[device_id] = ptr.size - 1
+
+    def transmissions(self, device_id, energies, pairs, eta=1e-4, ldos=False, dos_delta=1e-4, check=True):
+        """T over contact pairs [(ni, nf), ...] (npts x npairs); with ldos=True
+        also the LDOS of the device's dos_proj sets (npts x nsets)."""
+        E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
+        n = E.size
+        ids = self._ids(device_id, n)
+        ni = np.ascontiguousarray([p[0] for p in pairs], dtype=np.int32)
+        nf = np.ascontiguousarray([p[1] for p in pairs], dtype=np.int32)
+        T = np.zeros((n, ni.size))
+        nsets = max(self._nldos.get(int(i), 0) for i in set(ids.tolist())) if ldos else 0
+        led = np.zeros((n, max(nsets, 1))) if ldos else None
+        ncyc = np.zeros(n, dtype=np.int32)
+        st = np.zeros(n, dtype=np.int32)
+        rc = self._L.negf_b200_transmissions(self._h, n, _i(ids), _d(E), eta, dos_delta, ni.size, _i(ni), _i(nf),
+                                             _d(T), _d(led) if ldos else None, _i(ncyc), _i(st))
+        if check and rc not in (OK, NOT_CONVERGED):
+            raise NegfError(rc, "transmissions: " + self.last_error())
+        return T, (led[:, :nsets] if ldos else None), ncyc, st
 
     def release(self, device_id: int):
         self._check(self._L.negf_b200_release_device(self._h, device_id), "release")

@@ -27,6 +27,7 @@
 //   src/iterative_cpu.F90:230-372         calculate_Gn_tridiag_blocks
 //   src/iterative_cpu.F90:399-470         calculate_single_transmission_2_contacts
 //   src/iterative_cpu.F90:477-583         calculate_single_transmission_N_contacts
+//   src/iterative_cpu.F90:586-618         get_tun_mask (tun_proj)
 //   src/iterative.F90:1669-1780           calculate_transmissions
 //   src/iterative.F90:1821-1952           calculate_transmissions_and_dos
 //   src/iterative.F90:174-279, 289-363    calculate_Gn_neq_components, elastic SCBA
@@ -129,6 +130,17 @@ void spectral(const Dns& G, Dns& A) {
 cplx trace(const Dns& M) {
   cplx t(0.0, 0.0);
   for (int i = 0; i < M.nr; ++i) t += M.at(i, i);
+  return t;
+}
+
+// trace(M, mask) with the tun_proj mask of get_tun_mask
+// (src/iterative_cpu.F90:586-618): mask[k] != 0 selects diagonal entry k;
+// no mask = the whole diagonal.
+cplx trace_mask(const Dns& M, const unsigned char* mask) {
+  if (!mask) return trace(M);
+  cplx t(0.0, 0.0);
+  for (int i = 0; i < M.nr; ++i)
+    if (mask[i]) t += M.at(i, i);
   return t;
 }
 
@@ -391,7 +403,8 @@ void Gr_sweep(const Trid& ESH, const std::vector<Dns>& gsmr, GrBlocks& Gr,
 
 // calculate_single_transmission_2_contacts (src/iterative_cpu.F90:399-470)
 double transmission_2(int ni, int nf, const std::vector<Dns>& Sig,
-                      const std::vector<int>& cblk, const GrBlocks& Gr) {
+                      const std::vector<int>& cblk, const GrBlocks& Gr,
+                      const unsigned char* tmask = nullptr, const std::vector<int>* start = nullptr) {
   int ct1 = (cblk[ni - 1] < cblk[nf - 1]) ? ni : nf;
   int bl1 = cblk[ct1 - 1];
   const Dns& G = Gr.d[bl1 - 1];
@@ -408,13 +421,14 @@ double transmission_2(int ni, int nf, const std::vector<Dns>& Sig,
   mult(GAM1, AA, work2);
   TRS.create(work1.nr, work1.nc);
   for (size_t q = 0; q < TRS.v.size(); ++q) TRS.v[q] = work2.v[q] - work1.v[q];
-  return std::abs(std::real(trace(TRS)));
+  return std::abs(std::real(trace_mask(TRS, tmask ? tmask + (*start)[bl1 - 1] : nullptr)));
 }
 
 // calculate_single_transmission_N_contacts (src/iterative_cpu.F90:477-583)
 double transmission_N(int ni, int nf, const Trid& ESH, const std::vector<Dns>& Sig,
                       const std::vector<int>& cblk, const std::vector<Dns>& gsmr,
-                      GrBlocks& Gr, double eps) {
+                      GrBlocks& Gr, double eps, const unsigned char* tmask = nullptr,
+                      const std::vector<int>* start = nullptr) {
   int ct1, ct2;
   if (cblk[ni - 1] < cblk[nf - 1]) { ct1 = ni; ct2 = nf; } else { ct1 = nf; ct2 = ni; }
   int bl1 = cblk[ct1 - 1], bl2 = cblk[ct2 - 1];
@@ -442,7 +456,7 @@ double transmission_N(int ni, int nf, const Trid& ESH, const std::vector<Dns>& S
   mult(work1, GAM1, work2);
   dagger(G21, GA);
   mult(work2, GA, TRS);
-  return std::abs(std::real(trace(TRS)));
+  return std::abs(std::real(trace_mask(TRS, tmask ? tmask + (*start)[bl2 - 1] : nullptr)));
 }
 
 struct Opts {
@@ -501,6 +515,87 @@ double point_transmission_dos(const DeviceBlocks& D, double E, double eta,
     for (int k = 0; k < D.n[i]; ++k)
       dos[D.start[i] + k] = -(1.0 / pi) * std::imag(Gr.d[i].at(k, k));
   return tun;
+}
+
+// calculate_transmissions (src/iterative.F90:1669-1780) for the contact
+// pairs ni(:), nf(:) with the tun_proj mask.  The reference frees gsmr
+// inside its pair loop after the first pair (:1766-1767), so a later pair
+// whose contacts are more than one block apart would read freed blocks; here
+// gsmr stays valid for every pair, which is the result the loop is meant to
+// give (identical wherever the reference's loop is well defined).
+void point_transmissions(const DeviceBlocks& D, double E, double eta, int npairs,
+                         const int* ni, const int* nf, const unsigned char* tmask,
+                         const Opts& o, double* T, int& ncyc, Err& err) {
+  std::vector<Dns> Sig;
+  compute_contacts(cplx(E, eta), D, Sig, ncyc, o.sgf_acc, o.max_iter, err);
+  if (D.ncont == 1) {
+    for (int q = 0; q < npairs; ++q) T[q] = 0.0;
+    return;
+  }
+  Trid ESH;
+  build_ESH(cplx(E, 0.0), D, &Sig, ESH);
+  int nbl = D.nbl;
+  int nt = std::min(D.cblk[ni[0] - 1], D.cblk[nf[0] - 1]);
+  std::vector<Dns> gsmr(nbl);
+  GrBlocks Gr(nbl);
+  if (D.ncont == 2 && npairs == 1 && nt == 1) {
+    gsmr_blocks(ESH, nbl, 2, gsmr, false, err);
+    Gr_first(ESH, gsmr, Gr, 1, err);
+    T[0] = transmission_2(ni[0], nf[0], Sig, D.cblk, Gr, tmask, &D.start);
+    return;
+  }
+  gsmr_blocks(ESH, nbl, 2, gsmr, true, err);
+  for (int q = 0; q < npairs; ++q) {
+    int nt1 = std::max(D.cblk[ni[q] - 1], D.cblk[nf[q] - 1]);
+    if (q == 0) {
+      nt = nt1;
+      Gr_first(ESH, gsmr, Gr, 1, err);
+      if (nt > 1) Gr_sweep(ESH, gsmr, Gr, 2, nt);
+    } else if (nt1 > nt) {
+      Gr_sweep(ESH, gsmr, Gr, nt + 1, nt1);
+      nt = nt1;
+    }
+    T[q] = transmission_N(ni[q], nf[q], ESH, Sig, D.cblk, gsmr, Gr, o.eps, tmask, &D.start);
+  }
+}
+
+// calculate_transmissions_and_dos (src/iterative.F90:1821-1952) for the
+// pairs and the LDOS index sets (dos_proj, 1-based orbital indices; set k
+// holds idx[ptr[k]..ptr[k+1])); ledos[k] = sum over its indices of
+// -Im Gr_ii / pi (indices past the device are skipped, :1936-1939).
+void point_transmissions_ldos(const DeviceBlocks& D, double E, double eta, double dos_delta,
+                              int npairs, const int* ni, const int* nf,
+                              const unsigned char* tmask, int nsets, const int* ptr,
+                              const int* idx, const Opts& o, double* T, double* ledos,
+                              int& ncyc, Err& err) {
+  std::vector<Dns> Sig;
+  compute_contacts(cplx(E, eta), D, Sig, ncyc, o.sgf_acc, o.max_iter, err);
+  Trid ESH;
+  build_ESH(cplx(E, dos_delta), D, &Sig, ESH);
+  int nbl = D.nbl;
+  std::vector<Dns> gsmr(nbl);
+  GrBlocks Gr(nbl);
+  gsmr_blocks(ESH, nbl, 2, gsmr, true, err);
+  Gr_first(ESH, gsmr, Gr, 1, err);
+  if (nbl > 1) Gr_sweep(ESH, gsmr, Gr, 2, nbl);
+  for (int q = 0; q < npairs; ++q) {
+    if (D.ncont == 1) T[q] = 0.0;
+    else if (D.ncont == 2) T[q] = transmission_2(ni[q], nf[q], Sig, D.cblk, Gr, tmask, &D.start);
+    else T[q] = transmission_N(ni[q], nf[q], ESH, Sig, D.cblk, gsmr, Gr, o.eps, tmask, &D.start);
+  }
+  const double pi = 3.14159265358979323846;
+  std::vector<double> diag(D.norb);
+  for (int i = 0; i < nbl; ++i)
+    for (int k = 0; k < D.n[i]; ++k)
+      diag[D.start[i] + k] = -(1.0 / pi) * std::imag(Gr.d[i].at(k, k));
+  for (int k = 0; k < nsets; ++k) {
+    double acc = 0.0;
+    for (int j = ptr[k]; j < ptr[k + 1]; ++j) {
+      int i2 = idx[j];
+      if (i2 >= 1 && i2 <= D.norb) acc += diag[i2 - 1];
+    }
+    ledos[k] = acc;
+  }
 }
 
 // calculate_Gn_tridiag_blocks (src/iterative_cpu.F90:230-372).
@@ -764,6 +859,38 @@ int oracle_transmission_dos(const negf_b200_device* dev, int npts,
     int nc = 0;
     T[p] = point_transmission_dos(D, energy[p], eta, dos_delta, ni, nf, o,
                                   dos + (size_t)p * D.norb, nc, err);
+    if (ncyc) ncyc[p] = nc;
+    if (status) status[p] = err.code;
+  }
+  int first = 0;
+  if (status)
+    for (int p = 0; p < npts; ++p) if (status[p] && !first) first = status[p];
+  return first;
+}
+
+// calculate_transmissions / calculate_transmissions_and_dos over contact
+// pairs, with the tun_proj mask (tun_mask: one byte per device orbital, or
+// NULL) and, when ledos != NULL, the LDOS sets (dos_proj) of the DOS path.
+// T is npts x npairs and ledos npts x nsets, point-major.
+int oracle_transmissions(const negf_b200_device* dev, int npts, const double* energy,
+                         double eta, double dos_delta, int npairs, const int* ni,
+                         const int* nf, const unsigned char* tun_mask, int nsets,
+                         const int* set_ptr, const int* set_idx, double sgf_tol,
+                         int sgf_max_iter, double eps, double* T, double* ledos,
+                         int* ncyc, int* status, int nthreads) {
+  set_threads(nthreads);
+  DeviceBlocks D = unpack(dev);
+  Opts o;
+  o.sgf_acc = sgf_tol; o.max_iter = sgf_max_iter; o.eps = eps;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < npts; ++p) {
+    Err err;
+    int nc = 0;
+    if (ledos)
+      point_transmissions_ldos(D, energy[p], eta, dos_delta, npairs, ni, nf, tun_mask, nsets, set_ptr,
+                               set_idx, o, T + (size_t)p * npairs, ledos + (size_t)p * nsets, nc, err);
+    else
+      point_transmissions(D, energy[p], eta, npairs, ni, nf, tun_mask, o, T + (size_t)p * npairs, nc, err);
     if (ncyc) ncyc[p] = nc;
     if (status) status[p] = err.code;
   }

@@ -41,6 +41,9 @@ def lib():
         L.oracle_meir_wingreen.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, dp, dp, ctypes.c_int,
                                            ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                            dp, dp, dp, ip, dp, ip, ip, ctypes.c_int]
+        L.oracle_transmissions.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                           ip, ip, vp, ctypes.c_int, ip, ip, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_double, dp, dp, ip, ip, ctypes.c_int]
         L.oracle_fermi.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.oracle_fermi.restype = ctypes.c_double
         L.oracle_integrate_el.argtypes = [dp, ctypes.c_int] + [ctypes.c_double] * 8
@@ -104,6 +107,39 @@ def transmission_dos(dev: Device, energies, eta=1e-4, dos_delta=1e-4, ni=1, nf=2
     lib().oracle_transmission_dos(ctypes.addressof(st), npts, _d(E), eta, dos_delta, ni, nf, sgf_tol,
                                   sgf_max_iter, eps, _d(T), _d(dos), _i(ncyc), _i(status), nthreads)
     return T, dos, ncyc, status
+
+
+def transmissions(dev: Device, energies, pairs, eta=1e-4, tun_proj=None, dos_proj=None, dos_delta=0.0,
+                  sgf_tol=1e-9, sgf_max_iter=300, eps=0.0, nthreads=0):
+    """calculate_transmissions (dos_proj None) or calculate_transmissions_and_dos
+    over contact pairs [(ni, nf), ...]; tun_proj: 1-based orbital indices;
+    dos_proj: list of 1-based index lists.  Returns T (npts x npairs), ledos
+    (npts x nsets or None), ncyc, status."""
+    from libnegf_b200.projections import tun_mask, dos_sets
+    E = np.ascontiguousarray(energies, dtype=np.float64)
+    npts = E.size
+    ni = np.ascontiguousarray([p[0] for p in pairs], dtype=np.int32)
+    nf = np.ascontiguousarray([p[1] for p in pairs], dtype=np.int32)
+    npairs = ni.size
+    T = np.zeros((npts, npairs))
+    mask = tun_mask(dev.norb, tun_proj)
+    mask_p = mask.ctypes.data if mask is not None else None
+    if dos_proj is not None:
+        ptr, idx = dos_sets(dos_proj)
+        nsets = ptr.size - 1
+        ledos = np.zeros((npts, max(nsets, 1)))
+    else:
+        ptr = np.zeros(1, dtype=np.int32)
+        idx = np.zeros(1, dtype=np.int32)
+        nsets = 0
+        ledos = None
+    ncyc = np.zeros(npts, dtype=np.int32)
+    status = np.zeros(npts, dtype=np.int32)
+    st = dev.to_struct()
+    lib().oracle_transmissions(ctypes.addressof(st), npts, _d(E), eta, dos_delta, npairs, _i(ni), _i(nf), mask_p,
+                               nsets, _i(ptr), _i(idx), sgf_tol, sgf_max_iter, eps, _d(T),
+                               _d(ledos) if ledos is not None else None, _i(ncyc), _i(status), nthreads)
+    return T, (ledos[:, :nsets] if ledos is not None else None), ncyc, status
 
 
 def meir_wingreen(dev: Device, energies, frm, coupling=None, eta=1e-4, scba_niter=5, scba_tol=1e-7,
