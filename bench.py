@@ -256,7 +256,8 @@ def main():
     peak = fp64_peak_tflops(torch, "cuda:%d" % local)
     devs, ks = devices_for(wl)
     ids_all, E_all = point_list(wl)
-    shard = np.arange(rank, ids_all.size, world)     # round-robin, as tunneling_int_def
+    from libnegf_b200.shard import shard_points, max_over_ranks
+    shard = shard_points(ids_all.size, rank, world)     # round-robin, as tunneling_int_def
     ids_r, E_r = ids_all[shard], E_all[shard]
 
     ctx = native.Context(local)
@@ -307,9 +308,7 @@ def main():
     per_step = [ev[j].elapsed_time(ev[j + 1]) for j in range(args.steps)]
     ms = ev[0].elapsed_time(ev[-1])
     if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist)
         dist.barrier()
     trace = None
     if args.trace:
@@ -347,9 +346,7 @@ def main():
             ctx.transmission(h_ids[o:o + P], E_run[o:o + P], eta=wl["eta"], check=False)
     e2e_s = time.perf_counter() - t0
     if dist:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+        e2e_s = max_over_ranks(e2e_s, dist)
     e2e = e2e_steps * P * world / e2e_s
     h2d = P * (4 + 8)
     d2h = P * (8 + 4 + 4 + (8 * norb if wl["dos"] else 0))

@@ -1,0 +1,144 @@
+"""Device description from a global sparse H (and S), as libNEGF builds it.
+
+libNEGF takes the whole Hamiltonian in CSR (negf_set_h / negf_set_s,
+src/api/libnegf_api.f90) plus the block structure of negf_init_structure
+(:146-185, create_TStruct src/ln_structure.F90:77-145):
+
+- plend(1..npl): last orbital of every principal layer (PL) of the device;
+- per contact: surfstart, surfend (a surface block, empty when
+  surfend = surfstart - 1), contend (last orbital of the contact's two PLs);
+- cblk: the device PL each contact couples to.
+
+The per-energy solve then reads dense blocks: the tridiagonal device blocks
+of ES - H (zcsr2blk_sod, src/sparsekit_drv.F90:3409-3436), and per contact
+HC/SC over the contact's two PLs and HMC/SMC between the cblk PL and the
+contact's first PL (extract_cont, src/ln_extract.F90:37-75).  This module
+does that extraction once per k on the host and returns the Device the
+C-ABI uploads; E enters on the device.
+"""
+from __future__ import annotations
+
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .device import Device
+
+
+def _dense(M, r0, r1, c0, c1):
+    """M[r0:r1, c0:c1] (0-based, end exclusive) as a dense complex128 block."""
+    blk = M[r0:r1, c0:c1]
+    if hasattr(blk, "toarray"):
+        blk = blk.toarray()
+    return np.ascontiguousarray(np.asarray(blk, dtype=np.complex128))
+
+
+def device_from_csr(H, S, plend: Sequence[int], cblk: Sequence[int], surfstart: Sequence[int],
+                    surfend: Sequence[int], contend: Sequence[int]) -> Device:
+    """Blocks of H (and S; None = identity, as negf_set_s_id) for the
+    structure of negf_init_structure (1-based indices).  H and S may be
+    scipy.sparse matrices or dense arrays over device + contact orbitals.
+    Surface blocks (surfend >= surfstart) are rejected: the bound-surface
+    correction of surface_green (src/contselfenergy.F90:226-243) is not
+    built."""
+    plend = [int(x) for x in plend]
+    npl = len(plend)
+    if npl < 1:
+        raise ValueError("need at least one principal layer")
+    starts = [0] + plend[:-1]                      # 0-based first orbital of each PL
+    if any(plend[i] <= starts[i] for i in range(npl)):
+        raise ValueError("plend must increase")
+    ncont = len(cblk)
+    if not (len(surfstart) == len(surfend) == len(contend) == ncont):
+        raise ValueError("surfstart, surfend, contend and cblk need one entry per contact")
+    hd = [_dense(H, starts[i], plend[i], starts[i], plend[i]) for i in range(npl)]
+    hu = [_dense(H, starts[i], plend[i], starts[i + 1], plend[i + 1]) for i in range(npl - 1)]
+    hl = [_dense(H, starts[i + 1], plend[i + 1], starts[i], plend[i]) for i in range(npl - 1)]
+    if S is not None:
+        sd = [_dense(S, starts[i], plend[i], starts[i], plend[i]) for i in range(npl)]
+        su = [_dense(S, starts[i], plend[i], starts[i + 1], plend[i + 1]) for i in range(npl - 1)]
+        sl = [_dense(S, starts[i + 1], plend[i + 1], starts[i], plend[i]) for i in range(npl - 1)]
+    else:
+        sd = su = sl = None
+    lh00, lh01, hmc = [], [], []
+    ls00, ls01, smc = [], [], []
+    for c in range(ncont):
+        b0, c_start, c_end = int(surfstart[c]), int(surfend[c]) + 1, int(contend[c])
+        surfdim = c_start - b0
+        if surfdim != 0:
+            raise NotImplementedError("contact %d: surface blocks (surfdim = %d > 0) are not supported"
+                                      % (c + 1, surfdim))
+        ncdim = c_end - b0 + 1
+        if ncdim < 2 or ncdim % 2:
+            raise ValueError("contact %d: its two PLs must have equal size (dimension %d)" % (c + 1, ncdim))
+        L = ncdim // 2
+        j0 = b0 - 1                                 # 0-based first orbital of the contact
+        lh00.append(_dense(H, j0, j0 + L, j0, j0 + L))
+        lh01.append(_dense(H, j0, j0 + L, j0 + L, j0 + 2 * L))
+        cb = int(cblk[c])
+        if not 1 <= cb <= npl:
+            raise ValueError("cblk[%d] = %d outside 1..%d" % (c, cb, npl))
+        hmc.append(_dense(H, starts[cb - 1], plend[cb - 1], j0, j0 + L))
+        if S is not None:
+            ls00.append(_dense(S, j0, j0 + L, j0, j0 + L))
+            ls01.append(_dense(S, j0, j0 + L, j0 + L, j0 + 2 * L))
+            smc.append(_dense(S, starts[cb - 1], plend[cb - 1], j0, j0 + L))
+    dev = Device(hd, hu, hl, [int(x) for x in cblk], lh00, lh01, hmc,
+                 s_diag=sd, s_upper=su, s_lower=sl,
+                 lead_s00=ls00 if S is not None else None, lead_s01=ls01 if S is not None else None,
+                 smc=smc if S is not None else None)
+    dev.validate()
+    return dev
+
+
+def csr_from_device(dev: Device):
+    """The inverse layout (for tests and examples): the global sparse H (and
+    S, or None) of a Device with its contacts appended after the device
+    orbitals, two PLs each, and the negf_init_structure arrays.  Returns
+    (H, S, plend, cblk, surfstart, surfend, contend)."""
+    import scipy.sparse as sp
+    n = dev.pl_size
+    norb = dev.norb
+    plend = list(np.cumsum(n))
+    starts = [0] + plend[:-1]
+    L = dev.lead_size
+    ntot = norb + 2 * sum(L)
+    H = sp.lil_matrix((ntot, ntot), dtype=np.complex128)
+    S = sp.lil_matrix((ntot, ntot), dtype=np.complex128) if dev.s_diag is not None else None
+    for i in range(dev.nbl):
+        H[starts[i]:plend[i], starts[i]:plend[i]] = dev.h_diag[i]
+        if S is not None:
+            S[starts[i]:plend[i], starts[i]:plend[i]] = dev.s_diag[i]
+    for i in range(dev.nbl - 1):
+        H[starts[i]:plend[i], starts[i + 1]:plend[i + 1]] = dev.h_upper[i]
+        H[starts[i + 1]:plend[i + 1], starts[i]:plend[i]] = dev.h_lower[i]
+        if S is not None:
+            S[starts[i]:plend[i], starts[i + 1]:plend[i + 1]] = dev.s_upper[i]
+            S[starts[i + 1]:plend[i + 1], starts[i]:plend[i]] = dev.s_lower[i]
+    surfstart, surfend, contend = [], [], []
+    off = norb
+    for c in range(dev.ncont):
+        l = L[c]
+        j0 = off
+        surfstart.append(j0 + 1)
+        surfend.append(j0)
+        contend.append(j0 + 2 * l)
+        H[j0:j0 + l, j0:j0 + l] = dev.lead_h00[c]
+        H[j0 + l:j0 + 2 * l, j0 + l:j0 + 2 * l] = dev.lead_h00[c]
+        H[j0:j0 + l, j0 + l:j0 + 2 * l] = dev.lead_h01[c]
+        H[j0 + l:j0 + 2 * l, j0:j0 + l] = dev.lead_h01[c].conj().T
+        cb = dev.cblk[c]
+        H[starts[cb - 1]:plend[cb - 1], j0:j0 + l] = dev.hmc[c]
+        H[j0:j0 + l, starts[cb - 1]:plend[cb - 1]] = dev.hmc[c].conj().T
+        if S is not None:
+            s00 = dev.lead_s00[c] if dev.lead_s00 is not None else np.eye(l)
+            s01 = dev.lead_s01[c] if dev.lead_s01 is not None else np.zeros((l, l))
+            smc = dev.smc[c] if dev.smc is not None else np.zeros((n[cb - 1], l))
+            S[j0:j0 + l, j0:j0 + l] = s00
+            S[j0 + l:j0 + 2 * l, j0 + l:j0 + 2 * l] = s00
+            S[j0:j0 + l, j0 + l:j0 + 2 * l] = s01
+            S[j0 + l:j0 + 2 * l, j0:j0 + l] = s01.conj().T
+            S[starts[cb - 1]:plend[cb - 1], j0:j0 + l] = smc
+            S[j0:j0 + l, starts[cb - 1]:plend[cb - 1]] = smc.conj().T
+        off += 2 * l
+    return (H.tocsr(), S.tocsr() if S is not None else None, plend, list(dev.cblk), surfstart, surfend, contend)

@@ -1,0 +1,87 @@
+"""Host side of the path: CSR -> blocks (extract_cont / zcsr2blk_sod), the
+energy grid, fermi_f, integrate_el and the energy loop, checked against the
+oracle's restatements (CPU) and, for the loop, the GPU engine (gpu)."""
+import numpy as np
+import pytest
+
+from libnegf_b200 import energy as En
+from libnegf_b200 import generators as G
+from libnegf_b200 import structure as St
+from oracle import oracle as O
+
+
+def test_energy_grid_is_tunneling_int_def():
+    E = En.energy_grid(-1.0, 1.0, 0.1)
+    assert E.size == 21 and E[0] == -1.0 and abs(E[-1] - 1.0) < 1e-15
+    assert En.energy_grid(0.0, 1.0, 0.3).size == 4          # nint(3.33) + 1
+    assert En.local_points(10, 1, 3).tolist() == [1, 4, 7]
+
+
+def test_fermi_matches_oracle():
+    x = np.linspace(-2, 2, 101)
+    for ef, kt in [(0.1, 0.02), (-0.3, 1e-3), (0.0, 0.0)]:
+        ours = En.fermi_f(x, ef, kt)
+        ref = np.array([O.fermi(v, ef, kt) for v in x])
+        assert np.allclose(ours, ref, rtol=1e-15, atol=0)   # numpy's exp vs libm: 1 ulp
+
+
+@pytest.mark.parametrize("mu1,mu2,kt1,kt2", [(-0.1, 0.1, 1e-3, 2e-3), (0.1, -0.05, 0.0, 3e-3), (0.0, 0.0, 1e-3, 1e-3)])
+def test_integrate_el_matches_oracle(mu1, mu2, kt1, kt2):
+    rng = np.random.default_rng(1)
+    emin, emax, estep = -0.5, 0.5, 0.01
+    T = rng.random(En.energy_grid(emin, emax, estep).size)
+    a = En.integrate_el(T, mu1, mu2, kt1, kt2, emin, emax, estep)
+    b = O.integrate_el(T, mu1, mu2, kt1, kt2, emin, emax, estep)
+    assert abs(a - b) <= 1e-14 * max(1.0, abs(b))
+
+
+def test_perfect_chain_current_is_window_times_gspin():
+    """f90elph_deph-style known answer: T = 1 in the band, so the current is
+    g_spin * (mu2 - mu1) for a bias window well inside the band."""
+    emin, emax, estep = -1.0, 1.0, 0.01
+    E = En.energy_grid(emin, emax, estep)
+    T = np.ones((E.size, 1))
+    I = En.electron_current(T, [(1, 2)], mu=[-0.2, 0.2], kT=[1e-4, 1e-4], emin=emin, emax=emax, estep=estep)
+    assert abs(I[0] - 2.0 * 0.4) < 1e-6
+
+
+@pytest.mark.parametrize("with_s", [False, True])
+def test_csr_extraction_round_trip(with_s):
+    dev = G.transport_c1(nbl=4, n=6, seed=2, density=0.5) if with_s else G.transport_c0(nbl=5, n=4, seed=3)
+    H, S, plend, cblk, ss, se, ce = St.csr_from_device(dev)
+    d2 = St.device_from_csr(H, S, plend, cblk, ss, se, ce)
+    for name in ("h_diag", "h_upper", "h_lower", "lead_h00", "lead_h01", "hmc"):
+        for a, b in zip(getattr(dev, name), getattr(d2, name)):
+            assert np.array_equal(a, b)
+    E = np.linspace(-1, 1, 7)
+    t1, _, _ = O.transmission(dev, E, eta=1e-6)
+    t2, _, _ = O.transmission(d2, E, eta=1e-6)
+    assert np.array_equal(t1, t2)
+
+
+def test_csr_extraction_rejects_surface_blocks():
+    dev = G.transport_c0(nbl=3, n=4, seed=3)
+    H, S, plend, cblk, ss, se, ce = St.csr_from_device(dev)
+    se = [s + 1 for s in ss]            # a one-orbital surface block
+    with pytest.raises(NotImplementedError):
+        St.device_from_csr(H, S, plend, cblk, ss, se, ce)
+
+
+@pytest.mark.gpu
+def test_tunneling_and_dos_loop_matches_oracle(gpu_ctx):
+    """tunn_mat over two k-points with weights, and the Landauer current."""
+    devs = [G.transport_c0(nbl=5, n=6, seed=s) for s in (0, 1)]
+    w = [0.25, 0.75]
+    ids = [gpu_ctx.upload(d) for d in devs]
+    try:
+        emin, emax, estep = -2.0, 2.0, 0.05
+        E, tunn, _, st = En.tunneling_and_dos(gpu_ctx, ids, w, emin, emax, estep, [(1, 2)], eta=1e-4)
+        ref = sum(O.transmission(d, E, eta=1e-4)[0] * wk for d, wk in zip(devs, w))
+        assert np.all(st == 0)
+        assert np.abs(tunn[:, 0] - ref).max() <= 1e-9 * max(1.0, np.abs(ref).max())
+        I = En.electron_current(tunn, [(1, 2)], mu=[-0.1, 0.1], kT=[1e-3, 1e-3], emin=emin, emax=emax, estep=estep)
+        Iref = O.integrate_el(ref, -0.1, 0.1, 1e-3, 1e-3, emin, emax, estep) * 2.0
+        assert abs(I[0] - Iref) <= 1e-9 * max(1.0, abs(Iref))
+    finally:
+        for i in ids:
+            gpu_ctx.release(i)
