@@ -222,6 +222,30 @@ int negf_b200_transmissions(negf_b200_ctx* ctx, int32_t npts,
                             const int32_t* ni, const int32_t* nf, double* T,
                             double* ledos, int32_t* ncyc, int32_t* status);
 
+/* Caps the engine workspace of this context at `bytes` (0 = no cap): a launch
+ * whose resident CTAs would need more runs with fewer CTAs, and one whose
+ * single CTA does not fit returns NEGF_B200_ERR_ADMISSION.  A serving loop
+ * admits requests against this budget. */
+int negf_b200_set_workspace_limit(negf_b200_ctx* ctx, size_t bytes);
+
+/* ---- surface Green's function cache ----------------------------------------
+ * The counterpart of libNEGF's surface_green_cache (src/ln_cache.F90, used
+ * by surface_green, src/contselfenergy.F90:146-167, 251-264): the surface
+ * Green's function of every contact at every solved point is kept in a
+ * device arena of `bytes`, and a later host-buffer solve at the same
+ * (device, contact, E, eta, SGF tolerance, iteration cap) reads it instead
+ * of running the decimation (ncyc then counts 0 for that contact, as the
+ * reference's load path).
+ *   mode 0: off (frees the arena); 1: load if cached, else compute and store
+ *   (ReadOldSGF = 0); 2: compute and overwrite (ReadOldSGF = 2).
+ * When the misses of a call do not fit, they are computed without being
+ * stored and the next call that finds the arena full starts afresh.
+ * Releasing a device drops its entries.  The _dev solves do not use it. */
+int negf_b200_set_sgf_cache(negf_b200_ctx* ctx, int32_t mode, size_t bytes);
+int negf_b200_sgf_cache_stats(const negf_b200_ctx* ctx, int64_t* hits,
+                              int64_t* misses, int64_t* entries,
+                              size_t* bytes_used);
+
 /* ---- batched solves on device buffers ------------------------------------
  * Same as negf_b200_transmission / _transmission_dos with every per-point
  * array already resident in HBM (device pointers) and no host

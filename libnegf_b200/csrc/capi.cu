@@ -12,6 +12,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/negf_b200.h"
@@ -46,6 +47,40 @@ void free_projections(DeviceRec& r) {
 
 }  // namespace
 
+// Surface Green's function cache, the counterpart of libNEGF's
+// surface_green_cache (src/ln_cache.F90; used by surface_green,
+// src/contselfenergy.F90:146-167, 251-264).  The reference labels an entry
+// by (k-point, energy point index, spin, contact); the batched calls here
+// take energies, so an entry is labelled by (device, contact, E, eta, SGF
+// tolerance, iteration cap).  Entries live in one device arena and are
+// bump-allocated; when a launch's misses do not fit, they are computed
+// without being stored, and the next launch that finds the arena full
+// starts a new generation (all entries dropped).  Mode 1 loads what is
+// cached and stores what is computed (ReadOldSGF = 0); mode 2 recomputes
+// everything and overwrites (ReadOldSGF = 2).
+struct SgfKey {
+  int32_t dev, cont;
+  uint64_t e, eta, tol;
+  int32_t maxit;
+  bool operator==(const SgfKey& o) const {
+    return dev == o.dev && cont == o.cont && e == o.e && eta == o.eta && tol == o.tol && maxit == o.maxit;
+  }
+};
+struct SgfKeyHash {
+  size_t operator()(const SgfKey& k) const {
+    uint64_t h = k.e * 0x9E3779B97F4A7C15ull ^ (k.eta + 0x632BE59BD9B4E019ull + ((uint64_t)k.dev << 32 | (uint32_t)k.cont));
+    h ^= k.tol * 0xC2B2AE3D27D4EB4Full ^ (uint64_t)k.maxit;
+    return (size_t)(h ^ (h >> 29));
+  }
+};
+struct SgfCache {
+  int mode = 0;
+  double2* arena = nullptr;
+  int64_t cap = 0, used = 0;   // complex elements
+  std::unordered_map<SgfKey, int64_t, SgfKeyHash> map;
+  int64_t hits = 0, misses = 0;
+};
+
 struct negf_b200_ctx {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -62,6 +97,8 @@ struct negf_b200_ctx {
   int sms = 0;
   bool trace = false;
   unsigned long long* d_trace = nullptr;
+  SgfCache sgf;
+  size_t ws_limit = 0;   // 0 = none
   std::mutex mu;
 };
 
@@ -121,9 +158,15 @@ int shape_of(negf_b200_ctx* ctx, int npts, const int32_t* ids, LaunchShape& sh) 
       return fail(ctx, NEGF_B200_ERR_BAD_ARG, "point " + std::to_string(p) + ": unknown device id " +
                                                    std::to_string(id));
   }
+  // host ids: the launch's own devices; device ids (the _dev calls): every live device
+  std::vector<char> used;
+  if (ids) {
+    used.assign(ctx->devs.size(), 0);
+    for (int p = 0; p < npts; ++p) used[ids[p]] = 1;
+  }
   for (size_t i = 0; i < ctx->devs.size(); ++i) {
     const DeviceRec& r = ctx->devs[i];
-    if (!r.live) continue;
+    if (!r.live || (ids && !used[i])) continue;
     sh.nmax = std::max(sh.nmax, r.nmax);
     sh.nbl_max = std::max(sh.nbl_max, r.nbl);
     sh.ncont_max = std::max(sh.ncont_max, r.ncont);
@@ -144,8 +187,18 @@ int run_device(negf_b200_ctx* ctx, negf::EngineArgs a, const LaunchShape& sh, cu
                                                 std::to_string(negf::kMaxOrder));
   int st = sync_descs(ctx);
   if (st) return st;
-  const int grid = grid_for(ctx, a.npts);
+  int grid = grid_for(ctx, a.npts);
   const int64_t per = negf::engine_ws_elems(a.mode, sh.nbl_max, sh.ncont_max, sh.nmax);
+  if (ctx->ws_limit > 0) {
+    // fewer resident CTAs when the workspace would exceed the limit (the persistent
+    // kernel still runs every point); not even one CTA: refuse
+    const size_t per_bytes = (size_t)per * sizeof(double2);
+    const size_t fit = ctx->ws_limit > 256 ? (ctx->ws_limit - 256) / per_bytes : 0;
+    if (fit < 1)
+      return fail(ctx, NEGF_B200_ERR_ADMISSION, "one CTA's workspace (" + std::to_string(per_bytes) +
+                                                    " bytes) exceeds the workspace limit");
+    grid = (int)std::min<size_t>(grid, fit);
+  }
   // counter lives at the start of the workspace allocation
   const size_t need = 256 + (size_t)grid * per * sizeof(double2);
   st = grow(ctx, &ctx->ws, &ctx->ws_bytes, need);
@@ -196,6 +249,75 @@ struct Carve {
     return p;
   }
 };
+
+uint64_t bits_of(double x) {
+  uint64_t u;
+  std::memcpy(&u, &x, 8);
+  return u;
+}
+
+// Per point and contact: where to read gs from (hit) and where to store the
+// computed one (miss with room), as arena offsets or -1.
+void plan_sgf(negf_b200_ctx* ctx, int npts, const int32_t* ids, const double* E, double eta, int ncont_max,
+              std::vector<int64_t>& in, std::vector<int64_t>& out) {
+  SgfCache& c = ctx->sgf;
+  in.assign((size_t)npts * ncont_max, -1);
+  out.assign((size_t)npts * ncont_max, -1);
+  // a new generation when the arena is full
+  int64_t need = 0;
+  for (int p = 0; p < npts; ++p) {
+    const DeviceRec& r = ctx->devs[ids[p]];
+    for (int k = 0; k < r.ncont; ++k) need += (int64_t)r.desc.L[k] * r.desc.L[k];
+  }
+  if (c.used > 0 && c.used + need > c.cap) {
+    bool all_hit = true;
+    for (int p = 0; p < npts && all_hit; ++p) {
+      const DeviceRec& r = ctx->devs[ids[p]];
+      for (int k = 0; k < r.ncont; ++k) {
+        SgfKey key{ids[p], k, bits_of(E[p]), bits_of(eta), bits_of(ctx->opt.sgf_tol), ctx->opt.sgf_max_iter};
+        if (!c.map.count(key)) { all_hit = false; break; }
+      }
+    }
+    if (!all_hit) {
+      c.map.clear();
+      c.used = 0;
+    }
+  }
+  std::unordered_map<SgfKey, int64_t, SgfKeyHash> fresh;   // stored by this launch: not readable in it
+  for (int p = 0; p < npts; ++p) {
+    const DeviceRec& r = ctx->devs[ids[p]];
+    for (int k = 0; k < r.ncont; ++k) {
+      const int64_t L2 = (int64_t)r.desc.L[k] * r.desc.L[k];
+      SgfKey key{ids[p], k, bits_of(E[p]), bits_of(eta), bits_of(ctx->opt.sgf_tol), ctx->opt.sgf_max_iter};
+      const size_t q = (size_t)p * ncont_max + k;
+      auto it = c.map.find(key);
+      if (c.mode == 1 && it != c.map.end() && !fresh.count(key)) {
+        in[q] = it->second;
+        ++c.hits;
+        continue;
+      }
+      ++c.misses;
+      if (fresh.count(key)) continue;                       // twice in one launch: compute, store once
+      int64_t off = -1;
+      if (it != c.map.end()) {
+        off = it->second;                                   // refresh in place
+      } else if (c.used + L2 <= c.cap) {
+        off = c.used;
+        c.used += (L2 + 15) & ~int64_t(15);
+        c.map[key] = off;
+      }
+      if (off >= 0) {
+        out[q] = off;
+        fresh[key] = off;
+      }
+    }
+  }
+}
+
+void drop_sgf_of(negf_b200_ctx* ctx, int dev) {
+  for (auto it = ctx->sgf.map.begin(); it != ctx->sgf.map.end();)
+    it = (it->first.dev == dev) ? ctx->sgf.map.erase(it) : std::next(it);
+}
 
 }  // namespace
 
@@ -249,6 +371,7 @@ int negf_b200_ctx_destroy(negf_b200_ctx* ctx) {
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->io) cudaFree(ctx->io);
   if (ctx->d_trace) cudaFree(ctx->d_trace);
+  if (ctx->sgf.arena) cudaFree(ctx->sgf.arena);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return NEGF_B200_OK;
@@ -322,10 +445,16 @@ int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int3
   }
   char* b = reinterpret_cast<char*>(blob);
   size_t off = 0;
+  cudaError_t perr = cudaSuccess;
+  // synchronous copies on the legacy stream: no device-wide synchronisation, so an
+  // upload does not wait for launches running on other (non-blocking) streams
   auto put = [&](const void* src, size_t nbytes) -> void* {
     void* dst = b + off;
     off += (nbytes + 15) & ~size_t(15);
-    if (src && nbytes) cudaMemcpy(dst, src, nbytes, cudaMemcpyHostToDevice);
+    if (src && nbytes) {
+      cudaError_t ce = cudaMemcpy(dst, src, nbytes, cudaMemcpyHostToDevice);
+      if (ce != cudaSuccess) perr = ce;
+    }
     return dst;
   };
   DevDesc d{};
@@ -353,8 +482,8 @@ int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int3
     d.olead[c] = olead[c];
     d.omc[c] = omc[c];
   }
-  cudaError_t e = cudaDeviceSynchronize();
-  if (e != cudaSuccess || off > bytes) {
+  if (perr != cudaSuccess || off > bytes) {
+    cudaGetLastError();
     cudaFree(blob);
     return fail(ctx, NEGF_B200_ERR_CUDA, "upload of the device description failed");
   }
@@ -381,6 +510,7 @@ int negf_b200_release_device(negf_b200_ctx* ctx, int32_t id) {
   cudaStreamSynchronize(ctx->stream);
   cudaFree(ctx->devs[id].blob);
   free_projections(ctx->devs[id]);
+  drop_sgf_of(ctx, id);
   ctx->devs[id] = DeviceRec();
   ctx->descs_dirty = true;
   return NEGF_B200_OK;
@@ -460,6 +590,59 @@ int negf_b200_set_dos_proj(negf_b200_ctx* ctx, int32_t id, int32_t nsets, const 
   return NEGF_B200_OK;
 }
 
+int negf_b200_set_sgf_cache(negf_b200_ctx* ctx, int32_t mode, size_t bytes) {
+  if (!ctx || mode < 0 || mode > 2) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  cudaStreamSynchronize(ctx->stream);
+  SgfCache& c = ctx->sgf;
+  const int64_t cap = (int64_t)(bytes / sizeof(double2));
+  if (mode == 0 || cap != c.cap) {
+    if (c.arena) cudaFree(c.arena);
+    c.arena = nullptr;
+    c.cap = c.used = 0;
+    c.map.clear();
+  }
+  c.mode = 0;
+  if (mode == 0) return NEGF_B200_OK;
+  if (cap < 1) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the SGF cache needs a positive size");
+  if (!c.arena) {
+    if (cudaMalloc(&c.arena, (size_t)cap * sizeof(double2)) != cudaSuccess) {
+      cudaGetLastError();
+      c.arena = nullptr;
+      c.cap = 0;
+      return fail(ctx, NEGF_B200_ERR_NOMEM, "device allocation of the SGF cache failed");
+    }
+    c.cap = cap;
+  }
+  c.mode = mode;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_set_workspace_limit(negf_b200_ctx* ctx, size_t bytes) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  ctx->ws_limit = bytes;
+  if (bytes > 0 && ctx->ws_bytes > bytes) {   // give back a larger arena now
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+    cudaStreamSynchronize(ctx->stream);
+    cudaFree(ctx->ws);
+    ctx->ws = nullptr;
+    ctx->ws_bytes = 0;
+  }
+  return NEGF_B200_OK;
+}
+
+int negf_b200_sgf_cache_stats(const negf_b200_ctx* ctx, int64_t* hits, int64_t* misses, int64_t* entries,
+                              size_t* bytes_used) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  if (hits) *hits = ctx->sgf.hits;
+  if (misses) *misses = ctx->sgf.misses;
+  if (entries) *entries = (int64_t)ctx->sgf.map.size();
+  if (bytes_used) *bytes_used = (size_t)ctx->sgf.used * sizeof(double2);
+  return NEGF_B200_OK;
+}
+
 // ---- host-buffer solves ----------------------------------------------------
 static int check_pair(negf_b200_ctx* ctx, int npts, const int32_t* ids, int ni, int nf) {
   for (int p = 0; p < npts; ++p) {
@@ -520,6 +703,7 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
     if (dos || ledos) c.take<double>((size_t)npts * norb_pts);
     if (ledos) c.take<double>((size_t)npts * std::max(1, nldos_pts));
     if (npairs > 1) { c.take<int32_t>(npairs); c.take<int32_t>(npairs); }
+    if (ctx->sgf.mode) { c.take<int64_t>((size_t)npts * sh.ncont_max); c.take<int64_t>((size_t)npts * sh.ncont_max); }
     if (frm) c.take<double>((size_t)npts * ncont_pts);
     if (coupling) c.take<double>((size_t)norb_pts);
     if (curr) c.take<double>((size_t)npts * ncont_pts);
@@ -540,6 +724,9 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   double* d_ldos = ledos ? c.take<double>((size_t)npts * std::max(1, nldos_pts)) : nullptr;
   int32_t* d_pni = (npairs > 1) ? c.take<int32_t>(npairs) : nullptr;
   int32_t* d_pnf = (npairs > 1) ? c.take<int32_t>(npairs) : nullptr;
+  // indexed by point * ncont_max of the launch (run_device sets a.ncont_max = sh.ncont_max)
+  int64_t* d_sgf_in = ctx->sgf.mode ? c.take<int64_t>((size_t)npts * sh.ncont_max) : nullptr;
+  int64_t* d_sgf_out = ctx->sgf.mode ? c.take<int64_t>((size_t)npts * sh.ncont_max) : nullptr;
   double* d_frm = frm ? c.take<double>((size_t)npts * ncont_pts) : nullptr;
   double* d_cpl = coupling ? c.take<double>((size_t)norb_pts) : nullptr;
   double* d_curr = curr ? c.take<double>((size_t)npts * ncont_pts) : nullptr;
@@ -554,12 +741,19 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   if (d_cpl) CK(cudaMemcpyAsync(d_cpl, coupling, (size_t)norb_pts * 8, cudaMemcpyHostToDevice, s));
   if (d_pni) CK(cudaMemcpyAsync(d_pni, pni, (size_t)npairs * 4, cudaMemcpyHostToDevice, s));
   if (d_pnf) CK(cudaMemcpyAsync(d_pnf, pnf, (size_t)npairs * 4, cudaMemcpyHostToDevice, s));
+  std::vector<int64_t> sgf_in, sgf_out;
+  if (ctx->sgf.mode) {
+    plan_sgf(ctx, npts, ids, E, eta, sh.ncont_max, sgf_in, sgf_out);
+    CK(cudaMemcpyAsync(d_sgf_in, sgf_in.data(), sgf_in.size() * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_sgf_out, sgf_out.data(), sgf_out.size() * 8, cudaMemcpyHostToDevice, s));
+  }
   negf::EngineArgs a = base_args(ctx, mode, npts);
   a.dev_id = d_ids; a.energy = d_E; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
   a.T = d_T; a.ncyc = d_ncyc; a.status = d_st;
   a.npairs = npairs; a.pair_ni = d_pni; a.pair_nf = d_pnf;
   a.dos = d_dos; a.dos_stride = norb_pts;
   a.ldos = d_ldos; a.ldos_stride = std::max(1, nldos_pts);
+  a.sgf_in = d_sgf_in; a.sgf_out = d_sgf_out; a.sgf_arena = ctx->sgf.arena;
   a.frm = d_frm; a.frm_stride = ncont_pts; a.coupling = d_cpl;
   a.curr = d_curr; a.curr_stride = ncont_pts;
   a.lcurr = d_lcurr; a.lcurr_stride = std::max(1, nbl_pts - 1);

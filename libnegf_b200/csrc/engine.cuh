@@ -60,6 +60,11 @@ struct EngineArgs {
   double* T;
   double* dos; int64_t dos_stride;
   double* ldos; int ldos_stride;  // LDOS over the device's index sets (MODE_DOS; needs dos)
+  // surface Green's function cache (npts x ncont_max offsets into sgf_arena in
+  // complex elements, -1 = none): read gs instead of the decimation / store it
+  const int64_t* sgf_in;
+  const int64_t* sgf_out;
+  double2* sgf_arena;
   int* ncyc;
   int* status;
   // non-equilibrium (MODE_GN)

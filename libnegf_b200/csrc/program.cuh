@@ -391,6 +391,12 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
       for (s.c = 0; s.c < s.d->ncont; ++s.c) {
         s.L = s.d->L[s.c];
         s.ncb = s.d->pl[s.d->cblk[s.c] - 1];
+        if (a.sgf_in && a.sgf_in[(int64_t)s.p * a.ncont_max + s.c] >= 0) {
+          // cached surface GF (surface_green's retrieve, src/contselfenergy.F90:262-264): no decimation
+          set_simple(o, K_COPY, s.L * s.L, a.sgf_arena + a.sgf_in[(int64_t)s.p * a.ncont_max + s.c], w.slot(4));
+          PT_EMIT(s);
+          goto sgf_ready;
+        }
         set_esh(o, w.slot(0), s.L, s.L, s.d->h00 + s.d->olead[s.c], s.d->has_s00 ? s.d->s00 + s.d->olead[s.c] : nullptr,
                 s.ecs, 1, nullptr, nullptr, OP_N);                                          // Ao
         PT_EMIT(s);
@@ -437,6 +443,12 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         o.kind = K_ZINV; o.m = s.L; o.A = w.slot(1); o.C = w.slot(4);
         PT_EMIT(s);                                                                      // gs = Ao_s^-1
         if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+        if (a.sgf_out && a.sgf_out[(int64_t)s.p * a.ncont_max + s.c] >= 0) {
+          // surface_green's add (:251-256)
+          set_simple(o, K_COPY, s.L * s.L, w.slot(4), a.sgf_arena + a.sgf_out[(int64_t)s.p * a.ncont_max + s.c]);
+          PT_EMIT(s);
+        }
+      sgf_ready:
         // ---- self-energy: Tlc = E SMC - HMC, Tcl = (E^* SMC - HMC)^dag, Sigma = Tlc gs Tcl
         set_esh(o, w.slot(0), s.ncb, s.L, s.d->hmc + s.d->omc[s.c], s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr,
                 s.ecs, 0, nullptr, nullptr, OP_N);

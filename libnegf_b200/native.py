@@ -32,7 +32,8 @@ EXPORTED = [
     "negf_b200_zgemm_batched", "negf_b200_zinv_work_bytes", "negf_b200_zinv_batched",
     "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
     "negf_b200_get_trace", "negf_b200_decimation_noalloc", "negf_b200_set_tun_proj", "negf_b200_set_dos_proj",
-    "negf_b200_transmissions",
+    "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
+    "negf_b200_set_workspace_limit",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -94,6 +95,10 @@ def load():
     L.negf_b200_set_tun_proj.argtypes = [vp, i32, i32, ip]
     L.negf_b200_set_dos_proj.argtypes = [vp, i32, i32, ip, ip]
     L.negf_b200_transmissions.argtypes = [vp, i32, ip, dp, f64, f64, i32, ip, ip, dp, dp, ip, ip]
+    L.negf_b200_set_sgf_cache.argtypes = [vp, i32, ctypes.c_size_t]
+    L.negf_b200_set_workspace_limit.argtypes = [vp, ctypes.c_size_t]
+    i64p = ctypes.POINTER(ctypes.c_int64)
+    L.negf_b200_sgf_cache_stats.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_size_t)]
     _lib = L
     return L
 
@@ -212,6 +217,21 @@ class Context:
         if check and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "transmissions: " + self.last_error())
         return T, (led[:, :nsets] if ldos else None), ncyc, st
+
+    def set_sgf_cache(self, mode: int, nbytes: int = 0):
+        """Surface Green's function cache: 0 off, 1 reuse, 2 refresh."""
+        self._check(self._L.negf_b200_set_sgf_cache(self._h, mode, nbytes), "set_sgf_cache")
+
+    def set_workspace_limit(self, nbytes: int):
+        """Caps the engine workspace (0 = none); see negf_b200_set_workspace_limit."""
+        self._check(self._L.negf_b200_set_workspace_limit(self._h, nbytes), "set_workspace_limit")
+
+    def sgf_cache_stats(self) -> dict:
+        h, m, e = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        b = ctypes.c_size_t()
+        self._check(self._L.negf_b200_sgf_cache_stats(self._h, ctypes.byref(h), ctypes.byref(m), ctypes.byref(e),
+                                                      ctypes.byref(b)), "sgf_cache_stats")
+        return {"hits": h.value, "misses": m.value, "entries": e.value, "bytes": b.value}
 
     def release(self, device_id: int):
         self._check(self._L.negf_b200_release_device(self._h, device_id), "release")

@@ -1,0 +1,130 @@
+"""Serving: the surface Green's function cache, the workspace cap and the
+continuous-batching request loop (results the same alone and in the mix)."""
+import time
+
+import numpy as np
+import pytest
+
+from conftest import assert_T_close, oracle_spread
+from libnegf_b200 import generators as G
+from oracle import oracle as O
+
+
+@pytest.mark.gpu
+def test_sgf_cache_reuses_surface_gf(gpu_ctx):
+    dev = G.transport_c0(nbl=6, n=8, seed=0)
+    E = np.linspace(-2.5, 2.5, 21)
+    did = gpu_ctx.upload(dev)
+    try:
+        T0, nc0, st0 = gpu_ctx.transmission(did, E, eta=1e-6)
+        gpu_ctx.set_sgf_cache(1, 64 << 20)
+        T1, nc1, _ = gpu_ctx.transmission(did, E, eta=1e-6)      # fills the cache
+        s1 = gpu_ctx.sgf_cache_stats()
+        T2, nc2, _ = gpu_ctx.transmission(did, E, eta=1e-6)      # all hits
+        s2 = gpu_ctx.sgf_cache_stats()
+        assert s1["entries"] == 2 * E.size and s2["hits"] - s1["hits"] == 2 * E.size
+        assert np.array_equal(T0, T1) and np.array_equal(T1, T2)
+        assert np.array_equal(nc1, nc0) and np.all(nc2 == 0)     # loaded: no decimation (reference: ncyc = 0)
+        # the DOS solve at the same E + i*eta reuses them too
+        Td, dos, ncd, _ = gpu_ctx.transmission_dos(did, E, eta=1e-6, dos_delta=1e-4)
+        assert np.all(ncd == 0)
+        ref = O.transmission_dos(dev, E, eta=1e-6, dos_delta=1e-4)
+        assert_T_close(Td, ref[0], rtol=1e-9)
+        # another eta is another label
+        _, nc3, _ = gpu_ctx.transmission(did, E, eta=1e-5)
+        assert np.all(nc3 > 0)
+        # refresh mode recomputes
+        gpu_ctx.set_sgf_cache(2, 64 << 20)
+        T4, nc4, _ = gpu_ctx.transmission(did, E, eta=1e-6)
+        assert np.all(nc4 > 0) and np.array_equal(T4, T0)
+    finally:
+        gpu_ctx.set_sgf_cache(0)
+        gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+def test_workspace_limit_runs_fewer_ctas(gpu_ctx):
+    from libnegf_b200 import native
+    dev = G.transport_c0(nbl=8, n=32, seed=3)
+    E = np.linspace(-2, 2, 64)
+    did = gpu_ctx.upload(dev)
+    try:
+        T0, _, _ = gpu_ctx.transmission(did, E, eta=1e-6)
+        slot = 32 * 32 * 16
+        gpu_ctx.set_workspace_limit(256 + 3 * 40 * slot)         # about three CTAs
+        T1, _, _ = gpu_ctx.transmission(did, E, eta=1e-6)
+        assert np.array_equal(T0, T1)
+        gpu_ctx.set_workspace_limit(1024)                         # not one CTA
+        with pytest.raises(native.NegfError) as ei:
+            gpu_ctx.transmission(did, E, eta=1e-6)
+        assert ei.value.code == native.ADMISSION
+    finally:
+        gpu_ctx.set_workspace_limit(0)
+        gpu_ctx.release(did)
+
+
+def _requests():
+    from libnegf_b200.serve import Request
+    a = Request(G.transport_c0(nbl=12, n=16, seed=1), np.linspace(-2.8, 2.8, 97), eta=1e-6)
+    b = Request(G.transport_c0(nbl=6, n=64, seed=2), np.linspace(-2, 2, 41), eta=1e-6, pairs=[(2, 1)])
+    c = Request(G.transport_c0(nbl=5, n=32, seed=3, cblk=[1, 5, 3]), np.linspace(-2, 2, 33), eta=1e-6,
+                pairs=[(1, 2), (1, 3)], ldos=True, dos_delta=1e-4, dos_proj=[[1, 2, 3], list(range(33, 65))])
+    d = Request(G.uneven([5, 9, 4, 7], seed=4), np.linspace(-2, 2, 29), eta=1e-4)
+    return [a, b, c, d]
+
+
+@pytest.mark.gpu
+def test_same_alone_and_in_the_mix():
+    """Each request alone on the server, then all of them with staggered
+    arrivals (later ones join while earlier launches run): identical
+    results, and each matches the oracle."""
+    from libnegf_b200.serve import Server
+    alone = {}
+    srv = Server(lanes=2, points_per_launch=24, hbm_budget=8 << 30, sgf_cache_bytes=64 << 20)
+    try:
+        for i, r in enumerate(_requests()):
+            srv.submit(r)
+            assert r.wait(120)
+            assert r.error is None
+            alone[i] = (r.T.copy(), None if r.ledos is None else r.ledos.copy())
+    finally:
+        srv.close()
+    srv = Server(lanes=2, points_per_launch=24, hbm_budget=8 << 30, sgf_cache_bytes=64 << 20)
+    try:
+        reqs = _requests()
+        for r in reqs[:2]:
+            srv.submit(r)
+        time.sleep(0.05)
+        for r in reqs[2:]:
+            srv.submit(r)
+        for r in reqs:
+            assert r.wait(120)
+        for i, r in enumerate(reqs):
+            assert r.error is None and np.all(r.status == 0)
+            assert np.array_equal(r.T, alone[i][0])
+            if r.ldos:
+                assert np.array_equal(r.ledos, alone[i][1])
+            kw = dict(eta=r.eta, dos_proj=r.dos_proj, dos_delta=r.dos_delta) if r.ldos else dict(eta=r.eta)
+            ref, spread = oracle_spread(lambda d: O.transmissions(d, r.energies, r.pairs, **kw)[0], r.device)
+            assert_T_close(r.T, ref, spread=spread)
+        lat = srv.latencies()
+        assert lat.size == 4 and np.all(lat > 0)
+    finally:
+        srv.close()
+
+
+@pytest.mark.gpu
+def test_admission_rejects_a_device_over_budget():
+    from libnegf_b200 import native
+    from libnegf_b200.serve import Request, Server
+    srv = Server(lanes=1, hbm_budget=64 << 20, sgf_cache_bytes=1 << 20)
+    try:
+        big = Request(G.transport_c0(nbl=100, n=128, seed=5), np.linspace(-1, 1, 4))   # ~80 MB of blocks
+        small = Request(G.transport_c0(nbl=4, n=8, seed=6), np.linspace(-1, 1, 4))
+        srv.submit(big)
+        srv.submit(small)
+        assert big.wait(60) and small.wait(60)
+        assert big.error is not None and np.all(big.status == native.ADMISSION)
+        assert small.error is None and np.all(small.status == 0)
+    finally:
+        srv.close()
