@@ -40,6 +40,8 @@ WORKLOADS = {
     "c2": dict(nbl=60, n=512, nE=1024, emin=-2.0, emax=2.0, nk=8, eta=1e-6, dos=False, gen="c1"),
     # small case of the c1 kernel for profiler captures (few GB on the device)
     "prof": dict(nbl=8, n=256, nE=256, emin=-2.0, emax=2.0, nk=1, eta=1e-6, dos=True, gen="c1"),
+    # serving stream (Poisson arrivals of transmission / LDOS requests; see run_serve)
+    "serve": dict(nbl=0, n=0, nE=0, emin=-2.0, emax=2.0, nk=1, eta=1e-4, dos=False, gen="serve"),
 }
 
 
@@ -55,6 +57,13 @@ def parse():
     p.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline points (0 = auto)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--trace", action="store_true", help="one extra untimed step with per-phase cycle tracing")
+    # serving stream
+    p.add_argument("--serve-rate", type=float, default=4.0, help="request arrivals per second")
+    p.add_argument("--serve-seconds", type=float, default=20.0, help="arrival window")
+    p.add_argument("--serve-blocks", default="16,64,128", help="block sizes drawn uniformly")
+    p.add_argument("--serve-layers", default="10,60", help="layer count range (uniform)")
+    p.add_argument("--serve-grid", default="64,1024", help="energy grid size range (log-uniform)")
+    p.add_argument("--serve-lanes", type=int, default=2)
     return p.parse_args()
 
 
@@ -197,6 +206,75 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
     return done / dt, T, dt
 
 
+def run_serve(args):
+    """Serving stream: requests arrive as a Poisson process; each draws a
+    device from the c0 / c1 generators (layer count uniform in a range, block
+    size from a set), an energy grid of log-uniform size and a kind (T, or T
+    plus the LDOS of two orbital sets).  The full stream of the serving config
+    is blocks {16, 64, 128, 256, 512}, layers 10-200 and grids 64-4096; the
+    default command line runs a bounded slice of it so that the run ends in
+    about a minute (the flags widen it).  Reported: served energy-point
+    solves/s over the whole stream, p50 / p99 request latency."""
+    import torch
+    from libnegf_b200 import generators as G
+    from libnegf_b200.serve import Request, Server
+    rng = np.random.default_rng(7)
+    blocks = [int(x) for x in args.serve_blocks.split(",")]
+    lo, hi = (int(x) for x in args.serve_layers.split(","))
+    g0, g1 = (int(x) for x in args.serve_grid.split(","))
+    t = 0.0
+    plan = []
+    while True:
+        t += rng.exponential(1.0 / args.serve_rate)
+        if t > args.serve_seconds:
+            break
+        n = int(rng.choice(blocks))
+        nbl = int(rng.integers(lo, hi + 1))
+        npts = int(np.exp(rng.uniform(np.log(g0), np.log(g1))))
+        kind = "ldos" if rng.random() < 0.3 else "T"
+        gen = "c1" if rng.random() < 0.5 else "c0"
+        plan.append((t, n, nbl, npts, kind, gen, int(rng.integers(1 << 30))))
+    srv = Server(lanes=args.serve_lanes, sgf_cache_bytes=1 << 30)
+    reqs = []
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        for (ta, n, nbl, npts, kind, gen, seed) in plan:
+            dev = (G.transport_c1(nbl=nbl, n=n, seed=seed, density=0.1) if gen == "c1"
+                   else G.transport_c0(nbl=nbl, n=n, seed=seed))
+            E = np.sort(np.random.default_rng(seed).uniform(-2.0, 2.0, npts))
+            r = Request(dev, E, eta=1e-4, ldos=(kind == "ldos"), dos_delta=1e-4,
+                        dos_proj=[list(range(1, n + 1)), list(range(dev.norb - n + 1, dev.norb + 1))]
+                        if kind == "ldos" else None)
+            while time.perf_counter() - t0 < ta:
+                time.sleep(0.001)
+            reqs.append(srv.submit(r))
+        for r in reqs:
+            r.wait()
+        t_end = time.perf_counter()
+    srv.close()
+    ok = [r for r in reqs if r.error is None]
+    lat = np.array([r.latency for r in ok])
+    pts = sum(r.energies.size for r in ok)
+    span = t_end - t0
+    line = {
+        "metric": "served_energy_point_solves_per_s", "value": pts / span, "unit": "solves/s", "n_gpus": 1,
+        "steps": 1, "warmup": 0, "ms_per_step": span * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "serving stream: Poisson arrivals %.1f/s for %.0f s, blocks %s, layers %d-%d, "
+                               "grids %d-%d log-uniform, 30%% LDOS requests, c0/c1 generators"
+                               % (args.serve_rate, args.serve_seconds, blocks, lo, hi, g0, g1),
+                   "lanes": args.serve_lanes, "eta": 1e-4, "precision": "complex FP64 (plain form)"},
+        "latency_s": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
+                      "p99": float(np.percentile(lat, 99)) if lat.size else None,
+                      "max": float(lat.max()) if lat.size else None},
+        "requests": len(reqs), "rejected": len(reqs) - len(ok), "points": pts,
+        "status_counts": {str(k): int(v) for k, v in
+                          zip(*np.unique(np.concatenate([r.status for r in reqs]), return_counts=True))},
+        "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, wl, rank, world):
     if rank != 0:
         return
@@ -241,6 +319,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, wl, rank, world)
+        return
+    if wl["gen"] == "serve":
+        if rank == 0:
+            run_serve(args)
         return
 
     import torch
