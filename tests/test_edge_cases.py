@@ -1,0 +1,80 @@
+"""Edge cases of the per-point solve: empty calls, a single contact, ragged
+layer sizes across the register-leaf shapes (1, 2 and 4 rows per thread),
+and the decimation iteration cap."""
+import numpy as np
+import pytest
+
+from conftest import assert_T_close, oracle_spread
+from libnegf_b200 import generators as G
+from oracle import oracle as O
+
+
+def test_single_contact_oracle_gives_zero():
+    dev = G.transport_c0(nbl=3, n=4, seed=3, cblk=[1])
+    T, _, st = O.transmission(dev, np.linspace(-1, 1, 5), eta=1e-4, ni=1, nf=1)
+    assert np.all(T == 0.0) and np.all(st == 0)
+
+
+@pytest.mark.gpu
+def test_empty_call(gpu_ctx):
+    dev = G.transport_c0(nbl=3, n=4, seed=3)
+    did = gpu_ctx.upload(dev)
+    try:
+        T, nc, st = gpu_ctx.transmission(did, np.zeros(0), eta=1e-4)
+        assert T.size == 0 and nc.size == 0 and st.size == 0
+        T, led, nc, st = gpu_ctx.transmissions(did, np.zeros(0), [(1, 2), (2, 1)], eta=1e-4)
+        assert T.shape == (0, 2)
+    finally:
+        gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+def test_single_contact(gpu_ctx):
+    """ncont = 1: T = 0 (src/iterative.F90:1684-1687); the DOS is still solved."""
+    dev = G.transport_c0(nbl=3, n=4, seed=3, cblk=[1])
+    E = np.linspace(-2, 2, 9)
+    did = gpu_ctx.upload(dev)
+    try:
+        T, nc, st = gpu_ctx.transmission(did, E, eta=1e-4, ni=1, nf=1)
+        assert np.all(T == 0.0) and np.all(st == 0)
+        Td, dos, _, st = gpu_ctx.transmission_dos(did, E, eta=1e-4, dos_delta=1e-4, ni=1, nf=1)
+        ref = O.transmission_dos(dev, E, eta=1e-4, dos_delta=1e-4, ni=1, nf=1)
+        assert np.all(Td == 0.0)
+        assert np.abs(dos - ref[1]).max() <= 1e-10 * max(1.0, np.abs(ref[1]).max())
+    finally:
+        gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+def test_ragged_layers_across_leaf_shapes(gpu_ctx):
+    """PL sizes 300 (2 rows per thread in the leaves), 40 (whole matrix in
+    shared memory) and 520 (4 rows per thread) in one device."""
+    dev = G.uneven([300, 40, 520], seed=8)
+    E = np.array([-0.7, 0.3])
+    did = gpu_ctx.upload(dev)
+    try:
+        T, nc, st = gpu_ctx.transmission(did, E, eta=1e-4)
+        ref, spread = oracle_spread(lambda d: O.transmission(d, E, eta=1e-4)[0], dev, nsamp=2)
+        assert np.all(st == O.transmission(dev, E, eta=1e-4)[2])
+        assert_T_close(T, ref, spread=spread)
+    finally:
+        gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+def test_decimation_iteration_cap(gpu_ctx):
+    """A cap too small to converge: NOT_CONVERGED on the same points as the
+    oracle, with the same (unconverged) result."""
+    dev = G.transport_c0(nbl=4, n=8, seed=0)
+    E = np.linspace(-2.5, 2.5, 9)
+    did = gpu_ctx.upload(dev)
+    try:
+        gpu_ctx.set_options(sgf_max_iter=3)
+        T, nc, st = gpu_ctx.transmission(did, E, eta=1e-4, check=False)
+        ref, spread = oracle_spread(lambda d: O.transmission(d, E, eta=1e-4, sgf_max_iter=3)[0], dev)
+        rst = O.transmission(dev, E, eta=1e-4, sgf_max_iter=3)[2]
+        assert np.array_equal(st, rst) and np.any(st == 2)
+        assert_T_close(T, ref, spread=spread)
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)

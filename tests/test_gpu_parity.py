@@ -54,7 +54,7 @@ def test_zgemm_batched(m, n, k, dagger):
     assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max()) * np.sqrt(k)
 
 
-@pytest.mark.parametrize("n", [1, 2, 5, 16, 33, 64, 65, 100, 128, 200, 256, 512])
+@pytest.mark.parametrize("n", [1, 2, 5, 16, 33, 64, 65, 100, 128, 200, 256, 257, 512, 513, 777, 1024])
 def test_zinv_batched(n):
     rng = np.random.default_rng(n)
     b = 2
