@@ -189,6 +189,25 @@ int negf_b200_meir_wingreen(negf_b200_ctx* ctx, int32_t npts,
                             int32_t* scba_iter, double* scba_err,
                             int32_t* ncyc, int32_t* status);
 
+/* Equilibrium density matrix by contour integration, the loop of contour_int
+ * (src/integrations.F90:844-897) over the points of one device: at every
+ * complex energy z_p = e_re[p] + i e_im[p] the contact self-energies and ES-H
+ * are taken at z_p (compute_Gr, :2287-2340), the whole tridiagonal Gr is
+ * solved (calculate_Gr, src/iterative.F90:90-148) and w_p Gr accumulated;
+ * finally rho = i (T - T^dag) (zspectral, :893).  weight: npts complex
+ * (interleaved re, im) -- the en_grid%wght of contour_int_def (times z_p for
+ * the energy-weighted matrix, DorE = 'E').  rho_diag / rho_upper / rho_lower
+ * receive the blocks in the layout of h_diag / h_upper / h_lower (NULL to
+ * skip); restricting them to the sparsity of S (blk2csr,
+ * src/iterative.F90:1375-1450) is left to the caller.  The outer blocks
+ * between device and contacts (calculate_Gr_outer) and dephasing are not
+ * included. */
+int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts,
+                      const double* e_re, const double* e_im,
+                      const double* weight, double* rho_diag,
+                      double* rho_upper, double* rho_lower, int32_t* ncyc,
+                      int32_t* status);
+
 /* ---- projections and contact pairs ----------------------------------------
  * tun_proj of libNEGF (negf%tun_proj): the transmission trace runs over the
  * listed orbitals only (1-based global orbital indices; the mask of

@@ -809,6 +809,104 @@ int negf_b200_transmissions(negf_b200_ctx* ctx, int32_t npts, const int32_t* dev
                     nullptr, npairs, ni, nf, ledos);
 }
 
+int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const double* e_re, const double* e_im,
+                      const double* weight, double* rho_diag, double* rho_upper, double* rho_lower, int32_t* ncyc,
+                      int32_t* status) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  if (npts < 0 || (npts > 0 && (!e_re || !e_im || !weight))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (device_id < 0 || device_id >= (int)ctx->devs.size() || !ctx->devs[device_id].live)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+  const DeviceRec& r = ctx->devs[device_id];
+  // block element counts of the device layout
+  int64_t nd = 0, no = 0;
+  std::vector<int> pl(r.nbl);
+  CK(cudaMemcpy(pl.data(), r.desc.pl, r.nbl * 4, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < r.nbl; ++i) {
+    nd += (int64_t)pl[i] * pl[i];
+    if (i + 1 < r.nbl) no += (int64_t)pl[i] * pl[i + 1];
+  }
+  std::vector<double2> T((size_t)(nd + 2 * no), make_double2(0.0, 0.0));
+  if (npts > 0) {
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+    std::vector<int32_t> ids(npts, device_id);
+    LaunchShape sh;
+    int st = shape_of(ctx, npts, ids.data(), sh);
+    if (st) return st;
+    size_t need = 0;
+    {
+      Carve c{nullptr};
+      c.take<int32_t>(npts); c.take<double>(npts); c.take<double>(npts); c.take<double2>(npts);
+      c.take<int32_t>(npts); c.take<int32_t>(npts); c.take<double2>((size_t)(nd + 2 * no));
+      need = c.off + 256;
+    }
+    st = grow(ctx, &ctx->io, &ctx->io_bytes, need);
+    if (st) return st;
+    Carve c{reinterpret_cast<char*>(ctx->io)};
+    int32_t* d_ids = c.take<int32_t>(npts);
+    double* d_re = c.take<double>(npts);
+    double* d_im = c.take<double>(npts);
+    double2* d_w = c.take<double2>(npts);
+    int32_t* d_nc = c.take<int32_t>(npts);
+    int32_t* d_st = c.take<int32_t>(npts);
+    double2* d_acc = c.take<double2>((size_t)(nd + 2 * no));
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(d_ids, ids.data(), npts * 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_re, e_re, npts * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_im, e_im, npts * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_w, weight, npts * 16, cudaMemcpyHostToDevice, s));
+    CK(cudaMemsetAsync(d_acc, 0, (size_t)(nd + 2 * no) * 16, s));
+    negf::EngineArgs a = base_args(ctx, negf::MODE_RHO, npts);
+    a.dev_id = d_ids; a.energy = d_re; a.energy_im = d_im; a.weight = d_w;
+    a.acc_d = d_acc; a.acc_u = d_acc + nd; a.acc_l = d_acc + nd + no;
+    a.ncyc = d_nc; a.status = d_st;
+    st = run_device(ctx, a, sh, s);
+    if (st) return st;
+    std::vector<int32_t> hst(npts);
+    CK(cudaMemcpyAsync(T.data(), d_acc, T.size() * 16, cudaMemcpyDeviceToHost, s));
+    if (ncyc) CK(cudaMemcpyAsync(ncyc, d_nc, npts * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (status) std::memcpy(status, hst.data(), npts * 4);
+    st = first_status(hst.data(), npts);
+    if (st && st != NEGF_B200_ERR_NOT_CONVERGED) return st;
+  }
+  // rho = i (T - T^dag) over the tridiagonal blocks (zspectral, src/integrations.F90:893)
+  const double2* Td = T.data();
+  const double2* Tu = Td + nd;
+  const double2* Tl = Tu + no;
+  auto ispec = [](double2 x, double2 y) {   // i (x - conj(y))
+    return make_double2(-(x.y + y.y), x.x - y.x);
+  };
+  int64_t od = 0, oo = 0;
+  for (int i = 0; i < r.nbl; ++i) {
+    const int n = pl[i];
+    if (rho_diag)
+      for (int c = 0; c < n; ++c)
+        for (int q = 0; q < n; ++q) {
+          const double2 v = ispec(Td[od + q + (int64_t)c * n], Td[od + c + (int64_t)q * n]);
+          rho_diag[2 * (od + q + (int64_t)c * n)] = v.x;
+          rho_diag[2 * (od + q + (int64_t)c * n) + 1] = v.y;
+        }
+    if (i + 1 < r.nbl) {
+      const int m = pl[i + 1];   // upper block n x m, lower block m x n
+      for (int c = 0; c < m; ++c)
+        for (int q = 0; q < n; ++q) {
+          const double2 v = ispec(Tu[oo + q + (int64_t)c * n], Tl[oo + c + (int64_t)q * m]);
+          if (rho_upper) { rho_upper[2 * (oo + q + (int64_t)c * n)] = v.x; rho_upper[2 * (oo + q + (int64_t)c * n) + 1] = v.y; }
+        }
+      for (int c = 0; c < n; ++c)
+        for (int q = 0; q < m; ++q) {
+          const double2 v = ispec(Tl[oo + q + (int64_t)c * m], Tu[oo + c + (int64_t)q * n]);
+          if (rho_lower) { rho_lower[2 * (oo + q + (int64_t)c * m)] = v.x; rho_lower[2 * (oo + q + (int64_t)c * m) + 1] = v.y; }
+        }
+      oo += (int64_t)n * m;
+    }
+    od += (int64_t)n * n;
+  }
+  return NEGF_B200_OK;
+}
+
 // ---- device-pointer solve (inputs already resident in HBM) ------------------
 int negf_b200_transmission_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_device_id,
                                const double* d_energy, double eta, int32_t ni, int32_t nf, double* d_T,

@@ -708,12 +708,12 @@ __device__ __forceinline__ void gj_block_perm(int* perm, const int* piv, int n, 
   __syncthreads();
 }
 
-// Shared scratch of gj_leaf_reg, double-buffered by step parity: per warp
-// the best pivot candidate (|Re|+|Im|, row), its row and its reciprocal, and
-// the row at the pivot position before the exchange.
+// Shared scratch of the register leaves, double-buffered by step parity: per
+// warp the best pivot candidate (ordering key of |Re|+|Im|, row), its row and
+// its reciprocal, and the row at the pivot position before the exchange.
 template <int W>
 struct LeafShared {
-  double candv[2][kThreads / 32];
+  unsigned long long candk[2][kThreads / 32];
   int candi[2][kThreads / 32];
   double2 candd[2][kThreads / 32];
   double2 candrow[2][kThreads / 32][W];
@@ -734,24 +734,27 @@ template <int R, int W, int JJ>
 __device__ __forceinline__ void gj_reg_step(double2 (&x)[R][W], int n, int j, LeafShared<W>& L, InvScratch& s) {
   constexpr int b = JJ & 1;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nt = blockDim.x;
-  // local candidate: first row of max |Re|+|Im| among rows j..n-1 (izamax order)
-  double best = -1.0;
+  // local candidate: first row of max |Re|+|Im| among rows j..n-1 (izamax order).
+  // |Re|+|Im| >= 0, so its bit pattern orders like its value: the key is the
+  // bits + 1 (0 = no candidate, NaN never wins) and the warp maximum takes two
+  // integer reductions, the lowest row among ties a third.
+  unsigned long long key = 0ull;
   int bi = n;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = tid + r * nt;
     if (i >= j && i < n) {
       const double v = cabs1(x[r][JJ]);
-      if (v > best) { best = v; bi = i; }
+      const unsigned long long kk = (v >= 0.0) ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+      if (kk > key) { key = kk; bi = i; }
     }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    const double ov = __shfl_xor_sync(0xffffffffu, best, o);
-    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-  }
-  if (lane == 0) { L.candv[b][warp] = best; L.candi[b][warp] = bi; }
+  const unsigned hi = __reduce_max_sync(0xffffffffu, (unsigned)(key >> 32));
+  const unsigned lo = __reduce_max_sync(0xffffffffu, ((unsigned)(key >> 32) == hi) ? (unsigned)key : 0u);
+  const unsigned long long wkey = ((unsigned long long)hi << 32) | lo;
+  const int widx = (int)__reduce_min_sync(0xffffffffu, (key == wkey) ? (unsigned)bi : 0xffffffffu);
+  bi = widx;
+  if (lane == 0) { L.candk[b][warp] = wkey; L.candi[b][warp] = widx; }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = tid + r * nt;
@@ -767,14 +770,15 @@ __device__ __forceinline__ void gj_reg_step(double2 (&x)[R][W], int n, int j, Le
   }
   __syncthreads();
   int wb = 0;
-  best = L.candv[b][0]; bi = L.candi[b][0];
+  unsigned long long best = L.candk[b][0];
+  bi = L.candi[b][0];
 #pragma unroll
   for (int q = 1; q < kThreads / 32; ++q) {
-    const double ov = L.candv[b][q];
+    const unsigned long long ok = L.candk[b][q];
     const int oi = L.candi[b][q];
-    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; wb = q; }
+    if (ok > best || (ok == best && oi < bi)) { best = ok; bi = oi; wb = q; }
   }
-  const int p = bi;   // rows j..n-1 are never empty: some warp holds a candidate
+  const int p = (bi >= n || bi < 0) ? j : bi;   // no candidate only if every entry is NaN
   if (tid == 0) s.piv[j] = p;
   const double2* prow = L.candrow[b][wb];
   const double2 piv = prow[JJ];
@@ -830,7 +834,9 @@ __device__ __forceinline__ void leaf_apply(double2 (&y)[R][W], const double2* Wc
 #pragma unroll
     for (int c = 0; c < W; ++c) acc[c] = make_double2(0.0, 0.0);
     if (i < n) {
-      for (int k = 0; k < kw; ++k) {
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        if (k >= kw) break;
         const double2 wv = Wc[i + (size_t)k * n];
         const double2* trow = T + perm[k0 + k];
 #pragma unroll

@@ -10,7 +10,7 @@ constexpr int kMaxCont = 10;           // MAXNCONT (src/api/lnParams.h:10)
 constexpr int kMaxOrder = 1024;        // largest PL / contact PL size supported
 constexpr int kSmemMain = 100 * 1024;  // GEMM staging ring / inversion panel region
 
-enum Mode : int { MODE_T = 0, MODE_DOS = 1, MODE_GN = 2 };
+enum Mode : int { MODE_T = 0, MODE_DOS = 1, MODE_GN = 2, MODE_RHO = 3 };
 
 // Status codes (identical to include/negf_b200.h)
 enum Status : int {
@@ -60,6 +60,12 @@ struct EngineArgs {
   double* T;
   double* dos; int64_t dos_stride;
   double* ldos; int ldos_stride;  // LDOS over the device's index sets (MODE_DOS; needs dos)
+  // MODE_RHO (contour integration of Gr): complex energies E + i*energy_im and
+  // complex weights; sum_p w_p Gr_p accumulated (atomically) into blocks laid
+  // out like the device's H blocks (od / oo offsets)
+  const double* energy_im;
+  const double2* weight;
+  double2* acc_d; double2* acc_u; double2* acc_l;
   // surface Green's function cache (npts x ncont_max offsets into sgf_arena in
   // complex elements, -1 = none): read gs instead of the decimation / store it
   const int64_t* sgf_in;

@@ -110,6 +110,7 @@ enum OpKind : int {
   K_MAXABS,    // res[slot] = max |A(q)|, m elements
   K_TRDIAG,    // res[slot] = Re Tr A, order m
   K_LDOS,      // out[k] = sum over LDOS set k of dos[i-1] (A = dos row as doubles, device sets)
+  K_ACCUM,     // C[q] += alpha * A[q], q < m (atomic: C is shared by all CTAs)
 };
 
 struct Op {
@@ -290,6 +291,13 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       }
       break;
     }
+    case K_ACCUM:
+      for (int q = tid; q < o.m; q += blockDim.x) {
+        const double2 v = cmul(o.alpha, o.A[q]);
+        atomicAdd(&o.C[q].x, v.x);
+        atomicAdd(&o.C[q].y, v.y);
+      }
+      break;
     default:
       break;
   }
@@ -385,6 +393,10 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
       s.T = 0.0;
       s.ecs = cz(s.E, a.eta);
       s.ec = (a.mode == MODE_DOS) ? cz(s.E, a.dos_delta) : cz(s.E, 0.0);
+      if (a.mode == MODE_RHO) {   // compute_Gr (src/integrations.F90:2287-2340): contacts and ES-H at Ec
+        s.ec = cz(s.E, a.energy_im[s.p]);
+        s.ecs = s.ec;
+      }
       if (threadIdx.x == 0 && sm.tr.acc) sm.tr.acc[TR_POINTS] += 1;
 
       // ------------------------------------------ contacts (compute_contacts_dns)
@@ -586,6 +598,18 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                        s.d->pl[s.i - 1], mone, zero);                                              // Gr(i-1,i)
               PT_EMIT(s);
             }
+            if (a.mode == MODE_RHO) {
+              // Gr(i-1,i) = -Gr(i-1,i-1) ESH(i-1,i) gsmr(i); then w Gr(i,i-1), w Gr(i-1,i) into the sums
+              set_gemm(o, s.d->pl[s.i - 1], s.d->pl[s.i], s.d->pl[s.i - 1], w.slot(11 - s.cur), s.d->pl[s.i - 1],
+                       OP_N, w.slot(3), s.d->pl[s.i - 1], OP_N, w.slot(5), s.d->pl[s.i - 1], mone, zero);
+              PT_EMIT(s);
+              set_simple(o, K_ACCUM, s.d->pl[s.i] * s.d->pl[s.i - 1], w.slot(6), a.acc_l + s.d->oo[s.i - 1]);
+              o.alpha = a.weight[s.p];
+              PT_EMIT(s);
+              set_simple(o, K_ACCUM, s.d->pl[s.i] * s.d->pl[s.i - 1], w.slot(5), a.acc_u + s.d->oo[s.i - 1]);
+              o.alpha = a.weight[s.p];
+              PT_EMIT(s);
+            }
             set_simple(o, K_COPY, s.d->pl[s.i] * s.d->pl[s.i], w.layer(0, s.i, s.d->nbl),
                        (a.mode == MODE_GN) ? w.layer(1, s.i, s.d->nbl) : w.slot(11 - (s.cur ^ 1)));
             PT_EMIT(s);
@@ -595,6 +619,11 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                      one);                                                                         // Gr(i,i)
             PT_EMIT(s);
             s.cur ^= 1;
+          }
+          if (a.mode == MODE_RHO) {
+            set_simple(o, K_ACCUM, s.d->pl[s.i] * s.d->pl[s.i], w.slot(11 - s.cur), a.acc_d + s.d->od[s.i]);
+            o.alpha = a.weight[s.p];
+            PT_EMIT(s);
           }
           if (a.mode == MODE_DOS && a.dos) {
             set_simple(o, K_DOS, s.d->pl[s.i], w.slot(11 - s.cur), nullptr);
@@ -608,6 +637,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                 PT_EMIT(s);
               }
         }
+        if (a.mode == MODE_RHO) goto point_done;
         if (a.mode != MODE_GN) {
           if (a.mode == MODE_DOS && a.ldos && a.dos && s.d->nldos > 0) {
             o.kind = K_LDOS; o.A = reinterpret_cast<const double2*>(a.dos + (int64_t)s.p * a.dos_stride);

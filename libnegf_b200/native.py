@@ -33,7 +33,7 @@ EXPORTED = [
     "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
     "negf_b200_get_trace", "negf_b200_decimation_noalloc", "negf_b200_set_tun_proj", "negf_b200_set_dos_proj",
     "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
-    "negf_b200_set_workspace_limit",
+    "negf_b200_set_workspace_limit", "negf_b200_density",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -97,6 +97,7 @@ def load():
     L.negf_b200_transmissions.argtypes = [vp, i32, ip, dp, f64, f64, i32, ip, ip, dp, dp, ip, ip]
     L.negf_b200_set_sgf_cache.argtypes = [vp, i32, ctypes.c_size_t]
     L.negf_b200_set_workspace_limit.argtypes = [vp, ctypes.c_size_t]
+    L.negf_b200_density.argtypes = [vp, i32, i32, dp, dp, dp, dp, dp, dp, ip, ip]
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.negf_b200_sgf_cache_stats.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_size_t)]
     _lib = L
@@ -232,6 +233,29 @@ class Context:
         self._check(self._L.negf_b200_sgf_cache_stats(self._h, ctypes.byref(h), ctypes.byref(m), ctypes.byref(e),
                                                       ctypes.byref(b)), "sgf_cache_stats")
         return {"hits": h.value, "misses": m.value, "entries": e.value, "bytes": b.value}
+
+    def density(self, device_id, z, w, pl=None, check=True):
+        """Equilibrium density-matrix blocks from the contour points z with
+        weights w (see negf_b200_density): (diag, upper, lower) block lists,
+        ncyc, status."""
+        from .density import split_blocks
+        pl = pl if pl is not None else self.devices[device_id].pl_size
+        z = np.ascontiguousarray(z, dtype=np.complex128).ravel()
+        wt = np.ascontiguousarray(w, dtype=np.complex128).ravel()
+        er, ei = np.ascontiguousarray(z.real), np.ascontiguousarray(z.imag)
+        nd = sum(x * x for x in pl)
+        no = sum(pl[i] * pl[i + 1] for i in range(len(pl) - 1))
+        rd = np.zeros(max(nd, 1), dtype=np.complex128)
+        ru = np.zeros(max(no, 1), dtype=np.complex128)
+        rl = np.zeros(max(no, 1), dtype=np.complex128)
+        nc = np.zeros(z.size, dtype=np.int32)
+        st = np.zeros(z.size, dtype=np.int32)
+        rc = self._L.negf_b200_density(self._h, device_id, z.size, _d(er), _d(ei), _d(wt.view(np.float64)),
+                                       _d(rd.view(np.float64)), _d(ru.view(np.float64)), _d(rl.view(np.float64)),
+                                       _i(nc), _i(st))
+        if check and rc not in (OK, NOT_CONVERGED):
+            raise NegfError(rc, "density: " + self.last_error())
+        return split_blocks(pl, rd, ru, rl), nc, st
 
     def release(self, device_id: int):
         self._check(self._L.negf_b200_release_device(self._h, device_id), "release")

@@ -36,6 +36,7 @@
 //   src/iterative.F90:382-461             meir_wingreen / layer current kernels
 //   src/distributions.F90:27-72           fermi_f
 //   src/integrations.F90:2688-2830        integrate_el, integrate_el_meir_wingreen
+//   src/integrations.F90:844-897, 2287    contour_int, compute_Gr (density matrix)
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -598,6 +599,21 @@ void point_transmissions_ldos(const DeviceBlocks& D, double E, double eta, doubl
   }
 }
 
+// One contour point of contour_int (src/integrations.F90:844-897): Gr at the
+// complex energy Ec (contacts and ES-H at Ec, compute_Gr :2287-2340 /
+// calculate_Gr src/iterative.F90:90-148), all tridiagonal blocks.
+void point_gr_blocks(const DeviceBlocks& D, cplx Ec, const Opts& o, GrBlocks& Gr, int& ncyc, Err& err) {
+  std::vector<Dns> Sig;
+  compute_contacts(Ec, D, Sig, ncyc, o.sgf_acc, o.max_iter, err);
+  Trid ESH;
+  build_ESH(Ec, D, &Sig, ESH);
+  int nbl = D.nbl;
+  std::vector<Dns> gsmr(nbl);
+  gsmr_blocks(ESH, nbl, 2, gsmr, true, err);
+  Gr_first(ESH, gsmr, Gr, 1, err);
+  if (nbl > 1) Gr_sweep(ESH, gsmr, Gr, 2, nbl);
+}
+
 // calculate_Gn_tridiag_blocks (src/iterative_cpu.F90:230-372).
 // Sigma_n holds the tridiagonal lesser self-energy (dephasing already added).
 void Gn_blocks(const Trid& ESH, const std::vector<Dns>& Sig, const double* frm,
@@ -893,6 +909,70 @@ int oracle_transmissions(const negf_b200_device* dev, int npts, const double* en
       point_transmissions(D, energy[p], eta, npairs, ni, nf, tun_mask, o, T + (size_t)p * npairs, nc, err);
     if (ncyc) ncyc[p] = nc;
     if (status) status[p] = err.code;
+  }
+  int first = 0;
+  if (status)
+    for (int p = 0; p < npts; ++p) if (status[p] && !first) first = status[p];
+  return first;
+}
+
+// contour_int: TmpMt = sum_p w_p Gr(z_p) over the tridiagonal blocks (points
+// in order), then rho = i (TmpMt - TmpMt^dag) (zspectral).  rho blocks in the
+// layout of h_diag / h_upper / h_lower.
+int oracle_density(const negf_b200_device* dev, int npts, const double* e_re, const double* e_im,
+                   const double* weight, double sgf_tol, int sgf_max_iter, double* rho_d, double* rho_u,
+                   double* rho_l, int* ncyc, int* status, int nthreads) {
+  set_threads(nthreads);
+  DeviceBlocks D = unpack(dev);
+  Opts o;
+  o.sgf_acc = sgf_tol; o.max_iter = sgf_max_iter;
+  int nbl = D.nbl;
+  std::vector<GrBlocks> G(npts, GrBlocks(nbl));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < npts; ++p) {
+    Err err;
+    int nc = 0;
+    point_gr_blocks(D, cplx(e_re[p], e_im[p]), o, G[p], nc, err);
+    if (ncyc) ncyc[p] = nc;
+    if (status) status[p] = err.code;
+  }
+  size_t od = 0, oo = 0;
+  for (int i = 0; i < nbl; ++i) {
+    int n = D.n[i];
+    std::vector<cplx> T((size_t)n * n, cplx(0.0, 0.0));
+    for (int p = 0; p < npts; ++p) {
+      cplx w(weight[2 * p], weight[2 * p + 1]);
+      for (size_t q = 0; q < T.size(); ++q) T[q] += w * G[p].d[i].v[q];
+    }
+    for (int c = 0; c < n; ++c)
+      for (int r = 0; r < n; ++r) {
+        cplx v = I1 * (T[r + (size_t)c * n] - std::conj(T[c + (size_t)r * n]));
+        rho_d[2 * (od + r + (size_t)c * n)] = v.real();
+        rho_d[2 * (od + r + (size_t)c * n) + 1] = v.imag();
+      }
+    od += (size_t)n * n;
+    if (i + 1 < nbl) {
+      int m = D.n[i + 1];
+      std::vector<cplx> U((size_t)n * m, cplx(0.0, 0.0)), Lw((size_t)m * n, cplx(0.0, 0.0));
+      for (int p = 0; p < npts; ++p) {
+        cplx w(weight[2 * p], weight[2 * p + 1]);
+        for (size_t q = 0; q < U.size(); ++q) U[q] += w * G[p].u[i].v[q];
+        for (size_t q = 0; q < Lw.size(); ++q) Lw[q] += w * G[p].l[i].v[q];
+      }
+      for (int c = 0; c < m; ++c)
+        for (int r = 0; r < n; ++r) {
+          cplx v = I1 * (U[r + (size_t)c * n] - std::conj(Lw[c + (size_t)r * m]));
+          rho_u[2 * (oo + r + (size_t)c * n)] = v.real();
+          rho_u[2 * (oo + r + (size_t)c * n) + 1] = v.imag();
+        }
+      for (int c = 0; c < n; ++c)
+        for (int r = 0; r < m; ++r) {
+          cplx v = I1 * (Lw[r + (size_t)c * m] - std::conj(U[c + (size_t)r * n]));
+          rho_l[2 * (oo + r + (size_t)c * m)] = v.real();
+          rho_l[2 * (oo + r + (size_t)c * m) + 1] = v.imag();
+        }
+      oo += (size_t)n * m;
+    }
   }
   int first = 0;
   if (status)

@@ -44,6 +44,8 @@ def lib():
         L.oracle_transmissions.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                            ip, ip, vp, ctypes.c_int, ip, ip, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double, dp, dp, ip, ip, ctypes.c_int]
+        L.oracle_density.argtypes = [vp, ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp, dp, dp, ip, ip,
+                                     ctypes.c_int]
         L.oracle_fermi.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.oracle_fermi.restype = ctypes.c_double
         L.oracle_integrate_el.argtypes = [dp, ctypes.c_int] + [ctypes.c_double] * 8
@@ -140,6 +142,29 @@ def transmissions(dev: Device, energies, pairs, eta=1e-4, tun_proj=None, dos_pro
                                nsets, _i(ptr), _i(idx), sgf_tol, sgf_max_iter, eps, _d(T),
                                _d(ledos) if ledos is not None else None, _i(ncyc), _i(status), nthreads)
     return T, (ledos[:, :nsets] if ledos is not None else None), ncyc, status
+
+
+def density(dev: Device, z, w, sgf_tol=1e-9, sgf_max_iter=300, nthreads=0):
+    """contour_int over complex points z with complex weights w: the density
+    matrix blocks (lists of diag, upper, lower blocks), ncyc, status."""
+    z = np.ascontiguousarray(z, dtype=np.complex128).ravel()
+    wt = np.ascontiguousarray(w, dtype=np.complex128).ravel()
+    er = np.ascontiguousarray(z.real)
+    ei = np.ascontiguousarray(z.imag)
+    n = dev.pl_size
+    nd = sum(x * x for x in n)
+    no = sum(n[i] * n[i + 1] for i in range(len(n) - 1))
+    rd = np.zeros(max(nd, 1), dtype=np.complex128)
+    ru = np.zeros(max(no, 1), dtype=np.complex128)
+    rl = np.zeros(max(no, 1), dtype=np.complex128)
+    ncyc = np.zeros(z.size, dtype=np.int32)
+    status = np.zeros(z.size, dtype=np.int32)
+    st = dev.to_struct()
+    lib().oracle_density(ctypes.addressof(st), z.size, _d(er), _d(ei), _d(wt.view(np.float64)), sgf_tol,
+                         sgf_max_iter, _d(rd.view(np.float64)), _d(ru.view(np.float64)), _d(rl.view(np.float64)),
+                         _i(ncyc), _i(status), nthreads)
+    from libnegf_b200.density import split_blocks
+    return split_blocks(n, rd, ru, rl), ncyc, status
 
 
 def meir_wingreen(dev: Device, energies, frm, coupling=None, eta=1e-4, scba_niter=5, scba_tol=1e-7,

@@ -1,0 +1,89 @@
+"""Equilibrium density matrix by contour integration (contour_int_def +
+contour_int): the host contour, the oracle's known answer, the blk2csr
+restriction, and the device sum against the oracle (gpu)."""
+import numpy as np
+import pytest
+
+from libnegf_b200 import density as D
+from libnegf_b200 import generators as G
+from libnegf_b200 import structure as St
+from oracle import oracle as O
+
+CONTOUR = dict(elow=-4.0, muref=0.0, kT=0.01, n_kt=10, np1=24, np2=12, n_poles=3)
+
+
+def test_gauleg_matches_reference_convention():
+    x, w = D.gauleg(np.pi, 0.3, 7)
+    assert x[0] > x[-1] and np.all(np.diff(x) < 0)       # from x1 towards x2
+    assert np.all(w < 0) and abs(w.sum() - (0.3 - np.pi)) < 1e-14
+    # exact for polynomials of degree 2n-1
+    x, w = D.gauleg(-1.0, 2.0, 4)
+    assert abs(np.sum(w * x ** 7) - (2.0 ** 8 - 1.0) / 8.0) < 1e-12
+
+
+def test_contour_layout():
+    z, w = D.contour_points(**CONTOUR)
+    assert z.size == 24 + 12 + 3
+    assert np.all(z.imag > 0)                              # upper half plane
+    poles = z[-3:]
+    assert np.allclose(poles.imag, 0.01 * np.pi * np.array([1, 3, 5]))
+    z0, _ = D.contour_points(elow=-4.0, muref=0.0, kT=0.0, n_kt=10, np1=8, np2=8, n_poles=0)
+    assert z0.size == 16
+
+
+def test_oracle_half_filled_chain_has_one_electron_per_site():
+    """Perfect chain at mu = 0 (band centre): occupation g_spin / 2 = 1 per
+    site by particle-hole symmetry."""
+    dev = G.chain(1, 6)
+    z, w = D.contour_points(**CONTOUR)
+    (rd, ru, rl), nc, st = O.density(dev, z, w)
+    assert np.all(st == 0)
+    occ = np.array([b[0, 0].real for b in rd])
+    assert np.allclose(occ, 1.0, atol=1e-10)
+    for b in rd:
+        assert np.abs(b - b.conj().T).max() < 1e-14
+    for u, l in zip(ru, rl):
+        assert np.abs(u - l.conj().T).max() < 1e-14
+
+
+def test_restrict_to_pattern_is_blk2csr():
+    dev = G.transport_c1(nbl=3, n=5, seed=4, density=0.4)
+    H, S, plend, *_ = St.csr_from_device(dev)
+    d = [np.arange(25, dtype=complex).reshape(5, 5) + 100 * i for i in range(3)]
+    u = [np.full((5, 5), 1000.0 + i, dtype=complex) for i in range(2)]
+    l = [np.full((5, 5), 2000.0 + i, dtype=complex) for i in range(2)]
+    R = D.restrict_to_pattern((d, u, l), S, plend).toarray()
+    Sp = (S[:15, :15].toarray() != 0)
+    full = np.zeros((15, 15), dtype=complex)
+    for i in range(3):
+        full[5 * i:5 * i + 5, 5 * i:5 * i + 5] = d[i]
+    for i in range(2):
+        full[5 * i:5 * i + 5, 5 * i + 5:5 * i + 10] = u[i]
+        full[5 * i + 5:5 * i + 10, 5 * i:5 * i + 5] = l[i]
+    assert np.array_equal(R, np.where(Sp, full, 0))
+
+
+def _close(a, b, rel=1e-10):
+    scale = max(max(np.abs(x).max() for x in b), 1.0)
+    return all(np.abs(x - y).max() <= rel * scale for x, y in zip(a, b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["chain", "c0", "uneven", "c1_S", "three"])
+def test_density_parity(gpu_ctx, case):
+    dev = {"chain": lambda: G.chain(1, 6),
+           "c0": lambda: G.transport_c0(nbl=5, n=8, seed=1),
+           "uneven": lambda: G.uneven([5, 9, 4, 7], seed=4),
+           "c1_S": lambda: G.transport_c1(nbl=4, n=12, seed=2, density=0.3),
+           "three": lambda: G.transport_c0(nbl=5, n=8, seed=1, cblk=[1, 5, 3])}[case]()
+    z, w = D.contour_points(**CONTOUR)
+    did = gpu_ctx.upload(dev)
+    try:
+        (gd, gu, gl), nc, st = gpu_ctx.density(did, z, w)
+        (od, ou, ol), onc, ost = O.density(dev, z, w)
+        assert np.all(st == ost)
+        assert _close(gd, od) and _close(gu, ou) and _close(gl, ol)
+        if case == "chain":
+            assert np.allclose([b[0, 0].real for b in gd], 1.0, atol=1e-10)
+    finally:
+        gpu_ctx.release(did)
