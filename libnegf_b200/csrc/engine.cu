@@ -16,6 +16,8 @@
 // DOS src/iterative.F90:1821-1952, elastic SCBA :289-363 with
 // src/elphdd.F90:108-276 and src/scba.F90:120-147, Meir-Wingreen and layer
 // current src/iterative.F90:382-461.
+#include <mutex>
+
 #include "program.cuh"
 
 namespace negf {
@@ -153,9 +155,24 @@ int64_t engine_ws_elems(int mode, int nbl_max, int ncont_max, int nmax) {
 }
 
 cudaError_t launch_engine(const EngineArgs& a, int grid, cudaStream_t s) {
+  // the shared-memory opt-in is raised once per device and size (not per launch), so
+  // a launch is a stream operation only and can be captured into a CUDA graph
+  static std::mutex mu;
+  static int set_bytes[64] = {0};
   const size_t smem = engine_smem_bytes(a.nmax);
-  cudaError_t e = cudaFuncSetAttribute(k_engine, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64 || set_bytes[dev] < (int)smem) {
+      // every size up to the largest block order, so that later launches never need it
+      const int want = (int)engine_smem_bytes(kMaxOrder);
+      e = cudaFuncSetAttribute(k_engine, cudaFuncAttributeMaxDynamicSharedMemorySize, want);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) set_bytes[dev] = want;
+    }
+  }
   k_engine<<<grid, kThreads, smem, s>>>(a);
   return cudaGetLastError();
 }

@@ -1,0 +1,76 @@
+"""Launch schedule: the autotuner's choice never changes results, and a
+device-buffer solve captured into a CUDA graph replays to the same outputs."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from libnegf_b200 import generators as G
+
+
+@pytest.mark.gpu
+def test_autotune_picks_a_schedule_without_changing_results(gpu_ctx, tmp_path):
+    from libnegf_b200 import autotune
+    dev = G.transport_c0(nbl=6, n=16, seed=2)
+    E = np.linspace(-2, 2, 300)
+    did = gpu_ctx.upload(dev)
+    try:
+        T0, _, _ = gpu_ctx.transmission(did, E, eta=1e-4)
+        autotune.forget()
+        rec = autotune.tune(gpu_ctx, did, E[:200], mode="T", cache_file=str(tmp_path / "sched.json"))
+        assert rec["ctas_per_sm"] in (1, 2) and set(rec["timings"]) == {"1", "2"}
+        T1, _, _ = gpu_ctx.transmission(did, E, eta=1e-4)
+        assert np.array_equal(T0, T1)
+        for c in (1, 2):
+            gpu_ctx.set_options(ctas_per_sm=c)
+            assert np.array_equal(gpu_ctx.transmission(did, E, eta=1e-4)[0], T0)
+        autotune.forget()
+        rec2 = autotune.tune(gpu_ctx, did, E[:200], mode="T", cache_file=str(tmp_path / "sched.json"))
+        assert rec2 == rec                                   # read back from the file
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+def test_device_solve_replays_from_a_cuda_graph(gpu_ctx):
+    torch = pytest.importorskip("torch")
+    from libnegf_b200 import native
+    dev = G.transport_c0(nbl=5, n=8, seed=1)
+    E = np.linspace(-2.5, 2.5, 64)
+    did = gpu_ctx.upload(dev)
+    L = native.load()
+    try:
+        n = E.size
+        d_ids = torch.full((n,), did, dtype=torch.int32, device="cuda")
+        d_E = torch.from_numpy(E).cuda()
+        d_T = torch.zeros(n, dtype=torch.float64, device="cuda")
+        d_dos = torch.zeros((n, dev.norb), dtype=torch.float64, device="cuda")
+        d_nc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
+        s = torch.cuda.Stream()
+
+        def call():
+            return L.negf_b200_transmission_dos_dev(gpu_ctx.handle, n, d_ids.data_ptr(), d_E.data_ptr(), 1e-4, 1e-4,
+                                                    1, 2, d_T.data_ptr(), d_dos.data_ptr(), dev.norb,
+                                                    d_nc.data_ptr(), d_st.data_ptr(), ctypes.c_void_p(s.cuda_stream))
+        with torch.cuda.stream(s):
+            assert call() == 0                               # eager (sizes the workspace)
+        torch.cuda.synchronize()
+        T_eager, dos_eager = d_T.cpu().numpy().copy(), d_dos.cpu().numpy().copy()
+        d_T.zero_(); d_dos.zero_()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            rc = call()
+        assert rc == 0
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(d_T.cpu().numpy(), T_eager)
+        assert np.array_equal(d_dos.cpu().numpy(), dos_eager)
+        d_E.copy_(torch.from_numpy(E[::-1].copy()))           # new inputs, same graph
+        g.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(d_T.cpu().numpy(), T_eager[::-1])
+        del g
+    finally:
+        gpu_ctx.release(did)
