@@ -208,6 +208,21 @@ int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts,
                       double* rho_upper, double* rho_lower, int32_t* ncyc,
                       int32_t* status);
 
+/* Non-equilibrium part of the density matrix on the real axis, the loop of
+ * real_axis_int (src/integrations.F90:1093-1176): at every real energy E_p
+ * the Gn blocks (contacts at E_p + i*eta, ES-H at E_p, the elastic-dephasing
+ * SCBA when coupling != NULL, as compute_Gn :2350-2395) are summed with the
+ * complex weights w_p into rho_* (same layout as negf_b200_density; no
+ * spectral combination, the reference adds this sum to rho as it is).
+ * frm: npts x ncont occupations with the reference contact's subtracted
+ * (f_c - f_ref, 0 for ref), the Sigma^n of calculate_Gn_neq_components.
+ * The device needs nbl >= 2. */
+int negf_b200_density_neq(negf_b200_ctx* ctx, int32_t device_id, int32_t npts,
+                          const double* energy, double eta, const double* weight,
+                          const double* frm, const double* coupling,
+                          double* rho_diag, double* rho_upper, double* rho_lower,
+                          int32_t* ncyc, int32_t* status);
+
 /* ---- projections and contact pairs ----------------------------------------
  * tun_proj of libNEGF (negf%tun_proj): the transmission trace runs over the
  * listed orbitals only (1-based global orbital indices; the mask of

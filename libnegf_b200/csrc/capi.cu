@@ -809,68 +809,103 @@ int negf_b200_transmissions(negf_b200_ctx* ctx, int32_t npts, const int32_t* dev
                     nullptr, npairs, ni, nf, ledos);
 }
 
+namespace {
+
+// Sum of w_p * (Gr or Gn blocks) over the points of one device (engine MODE_RHO
+// or MODE_GN with block accumulation), copied back to T (diag | upper | lower).
+int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t npts, const double* e_re,
+                      const double* e_im, double eta, const double* weight, const double* frm,
+                      const double* coupling, std::vector<double2>& T, std::vector<int>& pl, int64_t& nd,
+                      int64_t& no, int32_t* ncyc, int32_t* status) {
+  if (device_id < 0 || device_id >= (int)ctx->devs.size() || !ctx->devs[device_id].live)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+  const DeviceRec& r = ctx->devs[device_id];
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  pl.assign(r.nbl, 0);
+  CK(cudaMemcpy(pl.data(), r.desc.pl, r.nbl * 4, cudaMemcpyDeviceToHost));
+  nd = no = 0;
+  for (int i = 0; i < r.nbl; ++i) {
+    nd += (int64_t)pl[i] * pl[i];
+    if (i + 1 < r.nbl) no += (int64_t)pl[i] * pl[i + 1];
+  }
+  T.assign((size_t)(nd + 2 * no), make_double2(0.0, 0.0));
+  if (npts == 0) return NEGF_B200_OK;
+  if (mode == negf::MODE_GN && r.nbl < 2) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the Gn solve needs nbl >= 2");
+  std::vector<int32_t> ids(npts, device_id);
+  LaunchShape sh;
+  int st = shape_of(ctx, npts, ids.data(), sh);
+  if (st) return st;
+  size_t need = 0;
+  {
+    Carve c{nullptr};
+    c.take<int32_t>(npts); c.take<double>(npts); c.take<double>(npts); c.take<double2>(npts);
+    c.take<int32_t>(npts); c.take<int32_t>(npts); c.take<double2>((size_t)(nd + 2 * no));
+    c.take<double>((size_t)npts * r.ncont); c.take<double>((size_t)r.norb); c.take<int32_t>(npts);
+    c.take<double>(npts);
+    need = c.off + 256;
+  }
+  st = grow(ctx, &ctx->io, &ctx->io_bytes, need);
+  if (st) return st;
+  Carve c{reinterpret_cast<char*>(ctx->io)};
+  int32_t* d_ids = c.take<int32_t>(npts);
+  double* d_re = c.take<double>(npts);
+  double* d_im = c.take<double>(npts);
+  double2* d_w = c.take<double2>(npts);
+  int32_t* d_nc = c.take<int32_t>(npts);
+  int32_t* d_st = c.take<int32_t>(npts);
+  double2* d_acc = c.take<double2>((size_t)(nd + 2 * no));
+  double* d_frm = c.take<double>((size_t)npts * r.ncont);
+  double* d_cpl = c.take<double>((size_t)r.norb);
+  int32_t* d_it = c.take<int32_t>(npts);
+  double* d_err = c.take<double>(npts);
+  cudaStream_t s = ctx->stream;
+  CK(cudaMemcpyAsync(d_ids, ids.data(), npts * 4, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_re, e_re, npts * 8, cudaMemcpyHostToDevice, s));
+  if (e_im) CK(cudaMemcpyAsync(d_im, e_im, npts * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(d_w, weight, npts * 16, cudaMemcpyHostToDevice, s));
+  if (frm) CK(cudaMemcpyAsync(d_frm, frm, (size_t)npts * r.ncont * 8, cudaMemcpyHostToDevice, s));
+  if (coupling) CK(cudaMemcpyAsync(d_cpl, coupling, (size_t)r.norb * 8, cudaMemcpyHostToDevice, s));
+  CK(cudaMemsetAsync(d_acc, 0, (size_t)(nd + 2 * no) * 16, s));
+  negf::EngineArgs a = base_args(ctx, mode, npts);
+  a.dev_id = d_ids; a.energy = d_re; a.energy_im = d_im; a.weight = d_w; a.eta = eta;
+  a.acc_d = d_acc; a.acc_u = d_acc + nd; a.acc_l = d_acc + nd + no;
+  a.ncyc = d_nc; a.status = d_st;
+  if (mode == negf::MODE_GN) {
+    a.frm = d_frm; a.frm_stride = r.ncont; a.coupling = coupling ? d_cpl : nullptr;
+    a.scba_iter = d_it; a.scba_err = d_err;
+  }
+  st = run_device(ctx, a, sh, s);
+  if (st) return st;
+  std::vector<int32_t> hst(npts);
+  CK(cudaMemcpyAsync(T.data(), d_acc, T.size() * 16, cudaMemcpyDeviceToHost, s));
+  if (ncyc) CK(cudaMemcpyAsync(ncyc, d_nc, npts * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (status) std::memcpy(status, hst.data(), npts * 4);
+  st = first_status(hst.data(), npts);
+  if (st && st != NEGF_B200_ERR_NOT_CONVERGED && st != NEGF_B200_ERR_SCBA_NOT_CONVERGED) return st;
+  return NEGF_B200_OK;
+}
+
+void store_blocks(const double2* src, int64_t n, double* dst) {
+  if (dst) std::memcpy(dst, src, (size_t)n * 16);
+}
+
+}  // namespace
+
 int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const double* e_re, const double* e_im,
                       const double* weight, double* rho_diag, double* rho_upper, double* rho_lower, int32_t* ncyc,
                       int32_t* status) {
   if (!ctx) return NEGF_B200_ERR_BAD_ARG;
   if (npts < 0 || (npts > 0 && (!e_re || !e_im || !weight))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
   std::lock_guard<std::mutex> lk(ctx->mu);
-  if (device_id < 0 || device_id >= (int)ctx->devs.size() || !ctx->devs[device_id].live)
-    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
-  const DeviceRec& r = ctx->devs[device_id];
-  // block element counts of the device layout
+  std::vector<double2> T;
+  std::vector<int> pl;
   int64_t nd = 0, no = 0;
-  std::vector<int> pl(r.nbl);
-  CK(cudaMemcpy(pl.data(), r.desc.pl, r.nbl * 4, cudaMemcpyDeviceToHost));
-  for (int i = 0; i < r.nbl; ++i) {
-    nd += (int64_t)pl[i] * pl[i];
-    if (i + 1 < r.nbl) no += (int64_t)pl[i] * pl[i + 1];
-  }
-  std::vector<double2> T((size_t)(nd + 2 * no), make_double2(0.0, 0.0));
-  if (npts > 0) {
-    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
-    std::vector<int32_t> ids(npts, device_id);
-    LaunchShape sh;
-    int st = shape_of(ctx, npts, ids.data(), sh);
-    if (st) return st;
-    size_t need = 0;
-    {
-      Carve c{nullptr};
-      c.take<int32_t>(npts); c.take<double>(npts); c.take<double>(npts); c.take<double2>(npts);
-      c.take<int32_t>(npts); c.take<int32_t>(npts); c.take<double2>((size_t)(nd + 2 * no));
-      need = c.off + 256;
-    }
-    st = grow(ctx, &ctx->io, &ctx->io_bytes, need);
-    if (st) return st;
-    Carve c{reinterpret_cast<char*>(ctx->io)};
-    int32_t* d_ids = c.take<int32_t>(npts);
-    double* d_re = c.take<double>(npts);
-    double* d_im = c.take<double>(npts);
-    double2* d_w = c.take<double2>(npts);
-    int32_t* d_nc = c.take<int32_t>(npts);
-    int32_t* d_st = c.take<int32_t>(npts);
-    double2* d_acc = c.take<double2>((size_t)(nd + 2 * no));
-    cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(d_ids, ids.data(), npts * 4, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(d_re, e_re, npts * 8, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(d_im, e_im, npts * 8, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(d_w, weight, npts * 16, cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(d_acc, 0, (size_t)(nd + 2 * no) * 16, s));
-    negf::EngineArgs a = base_args(ctx, negf::MODE_RHO, npts);
-    a.dev_id = d_ids; a.energy = d_re; a.energy_im = d_im; a.weight = d_w;
-    a.acc_d = d_acc; a.acc_u = d_acc + nd; a.acc_l = d_acc + nd + no;
-    a.ncyc = d_nc; a.status = d_st;
-    st = run_device(ctx, a, sh, s);
-    if (st) return st;
-    std::vector<int32_t> hst(npts);
-    CK(cudaMemcpyAsync(T.data(), d_acc, T.size() * 16, cudaMemcpyDeviceToHost, s));
-    if (ncyc) CK(cudaMemcpyAsync(ncyc, d_nc, npts * 4, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (status) std::memcpy(status, hst.data(), npts * 4);
-    st = first_status(hst.data(), npts);
-    if (st && st != NEGF_B200_ERR_NOT_CONVERGED) return st;
-  }
+  int st = accumulate_blocks(ctx, negf::MODE_RHO, device_id, npts, e_re, e_im, 0.0, weight, nullptr, nullptr, T, pl,
+                             nd, no, ncyc, status);
+  if (st) return st;
+  const int nbl = (int)pl.size();
   // rho = i (T - T^dag) over the tridiagonal blocks (zspectral, src/integrations.F90:893)
   const double2* Td = T.data();
   const double2* Tu = Td + nd;
@@ -879,7 +914,7 @@ int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const
     return make_double2(-(x.y + y.y), x.x - y.x);
   };
   int64_t od = 0, oo = 0;
-  for (int i = 0; i < r.nbl; ++i) {
+  for (int i = 0; i < nbl; ++i) {
     const int n = pl[i];
     if (rho_diag)
       for (int c = 0; c < n; ++c)
@@ -888,7 +923,7 @@ int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const
           rho_diag[2 * (od + q + (int64_t)c * n)] = v.x;
           rho_diag[2 * (od + q + (int64_t)c * n) + 1] = v.y;
         }
-    if (i + 1 < r.nbl) {
+    if (i + 1 < nbl) {
       const int m = pl[i + 1];   // upper block n x m, lower block m x n
       for (int c = 0; c < m; ++c)
         for (int q = 0; q < n; ++q) {
@@ -904,6 +939,25 @@ int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const
     }
     od += (int64_t)n * n;
   }
+  return NEGF_B200_OK;
+}
+
+int negf_b200_density_neq(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const double* energy, double eta,
+                          const double* weight, const double* frm, const double* coupling, double* rho_diag,
+                          double* rho_upper, double* rho_lower, int32_t* ncyc, int32_t* status) {
+  if (!ctx) return NEGF_B200_ERR_BAD_ARG;
+  if (npts < 0 || (npts > 0 && (!energy || !weight || !frm))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  std::vector<double2> T;
+  std::vector<int> pl;
+  int64_t nd = 0, no = 0;
+  int st = accumulate_blocks(ctx, negf::MODE_GN, device_id, npts, energy, nullptr, eta, weight, frm, coupling, T, pl,
+                             nd, no, ncyc, status);
+  if (st) return st;
+  // real_axis_int adds the sum itself to rho (no spectral combination, :1166-1170)
+  store_blocks(T.data(), nd, rho_diag);
+  store_blocks(T.data() + nd, no, rho_upper);
+  store_blocks(T.data() + nd + no, no, rho_lower);
   return NEGF_B200_OK;
 }
 

@@ -838,6 +838,27 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         ++s.sit;
       }
       s.par ^= 1;   // parity of the last computed Gn
+      if (a.acc_d) {
+        // real_axis_int (src/integrations.F90:1093-1176): w_p Gn(E_p) summed over the points
+        for (s.i = 0; s.i < s.d->nbl; ++s.i) {
+          set_simple(o, K_ACCUM, s.d->pl[s.i] * s.d->pl[s.i], w.layer(4 + s.par, s.i, s.d->nbl),
+                     a.acc_d + s.d->od[s.i]);
+          o.alpha = a.weight[s.p];
+          PT_EMIT(s);
+          if (s.i + 1 < s.d->nbl) {
+            set_simple(o, K_ACCUM, s.d->pl[s.i] * s.d->pl[s.i + 1], w.layer(6 + s.par, s.i, s.d->nbl),
+                       a.acc_u + s.d->oo[s.i]);                                     // Gn(i,i+1)
+            o.alpha = a.weight[s.p];
+            PT_EMIT(s);
+            o.kind = K_DAGGER; o.m = s.d->pl[s.i + 1]; o.n = s.d->pl[s.i]; o.A = w.layer(6 + s.par, s.i, s.d->nbl);
+            o.C = w.slot(10);                                                       // Gn(i+1,i)
+            PT_EMIT(s);
+            set_simple(o, K_ACCUM, s.d->pl[s.i] * s.d->pl[s.i + 1], w.slot(10), a.acc_l + s.d->oo[s.i]);
+            o.alpha = a.weight[s.p];
+            PT_EMIT(s);
+          }
+        }
+      }
       // ------------------------------------ Meir-Wingreen (iterative.F90:382-414); Gam slot 7, A slot 8
       if (a.curr)
         for (s.c = 0; s.c < s.d->ncont; ++s.c) {

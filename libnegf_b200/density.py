@@ -76,6 +76,26 @@ def contour_points(elow: float, muref: float, kT: float, n_kt: float, np1: int, 
     return np.concatenate(zs).astype(np.complex128), np.concatenate(ws).astype(np.complex128)
 
 
+def real_axis_points(mu: Sequence[float], kT: Sequence[float], n_kt: float, np_real: int, delta: float,
+                     g_spin: float = 2.0) -> Tuple[np.ndarray, np.ndarray]:
+    """real_axis_int_def (src/integrations.F90:989-1084), elastic case:
+    np_real Gauss-Legendre energies on [min mu - Omega, max mu + Omega],
+    Omega = n_kt * max kT, weights g_spin w / (2 pi).  Returns (E, w); the
+    contacts see E + i*delta."""
+    omega = n_kt * max(kT)
+    x, wg = gauleg(min(mu) - omega, max(mu) + omega, np_real)
+    return x, (g_spin * wg / (2.0 * np.pi)).astype(np.complex128)
+
+
+def neq_occupations(E, mu: Sequence[float], kT: Sequence[float], ref: int) -> np.ndarray:
+    """f_c(E) - f_ref(E) per point and contact (ref is 1-based): the
+    occupations calculate_Gn_neq_components folds into Sigma^n."""
+    from .energy import fermi_f
+    E = np.asarray(E, dtype=np.float64)
+    f = np.stack([fermi_f(E, m, t) for m, t in zip(mu, kT)], axis=1)
+    return np.ascontiguousarray(f - f[:, ref - 1:ref])
+
+
 def split_blocks(pl: Sequence[int], diag, upper, lower):
     """Flat block arrays (the h_diag / h_upper / h_lower layout) -> lists of
     column-major blocks (diag, upper, lower)."""

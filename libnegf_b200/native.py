@@ -33,7 +33,7 @@ EXPORTED = [
     "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
     "negf_b200_get_trace", "negf_b200_decimation_noalloc", "negf_b200_set_tun_proj", "negf_b200_set_dos_proj",
     "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
-    "negf_b200_set_workspace_limit", "negf_b200_density",
+    "negf_b200_set_workspace_limit", "negf_b200_density", "negf_b200_density_neq",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -98,6 +98,7 @@ def load():
     L.negf_b200_set_sgf_cache.argtypes = [vp, i32, ctypes.c_size_t]
     L.negf_b200_set_workspace_limit.argtypes = [vp, ctypes.c_size_t]
     L.negf_b200_density.argtypes = [vp, i32, i32, dp, dp, dp, dp, dp, dp, ip, ip]
+    L.negf_b200_density_neq.argtypes = [vp, i32, i32, dp, f64, dp, dp, dp, dp, dp, dp, ip, ip]
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.negf_b200_sgf_cache_stats.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_size_t)]
     _lib = L
@@ -255,6 +256,29 @@ class Context:
                                        _i(nc), _i(st))
         if check and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "density: " + self.last_error())
+        return split_blocks(pl, rd, ru, rl), nc, st
+
+    def density_neq(self, device_id, energies, w, frm, eta=1e-4, coupling=None, check=True):
+        """Real-axis non-equilibrium density blocks sum_p w_p Gn(E_p) (see
+        negf_b200_density_neq); frm: npts x ncont, reference contact subtracted."""
+        from .density import split_blocks
+        pl = self.devices[device_id].pl_size
+        E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
+        wt = np.ascontiguousarray(w, dtype=np.complex128).ravel()
+        f = np.ascontiguousarray(frm, dtype=np.float64)
+        cp = None if coupling is None else np.ascontiguousarray(coupling, dtype=np.float64)
+        nd = sum(x * x for x in pl)
+        no = sum(pl[i] * pl[i + 1] for i in range(len(pl) - 1))
+        rd = np.zeros(max(nd, 1), dtype=np.complex128)
+        ru = np.zeros(max(no, 1), dtype=np.complex128)
+        rl = np.zeros(max(no, 1), dtype=np.complex128)
+        nc = np.zeros(E.size, dtype=np.int32)
+        st = np.zeros(E.size, dtype=np.int32)
+        rc = self._L.negf_b200_density_neq(self._h, device_id, E.size, _d(E), eta, _d(wt.view(np.float64)), _d(f),
+                                           _d(cp) if cp is not None else None, _d(rd.view(np.float64)),
+                                           _d(ru.view(np.float64)), _d(rl.view(np.float64)), _i(nc), _i(st))
+        if check and rc not in (OK, NOT_CONVERGED, SCBA_NOT_CONVERGED):
+            raise NegfError(rc, "density_neq: " + self.last_error())
         return split_blocks(pl, rd, ru, rl), nc, st
 
     def release(self, device_id: int):

@@ -707,7 +707,7 @@ struct ScbaOut {
 void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
                 const double* coupling, int niter, double tol, const Opts& o,
                 double* curr, double* lcurr, double* ldens, ScbaOut& so,
-                int& ncyc, Err& err) {
+                int& ncyc, Err& err, Trid* gn_out = nullptr) {
   int nbl = D.nbl, ncont = D.ncont;
   std::vector<Dns> Sig;
   compute_contacts(cplx(E, eta), D, Sig, ncyc, o.sgf_acc, o.max_iter, err);
@@ -776,6 +776,7 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
     ++it;
   }
   so.iters = it;
+  if (gn_out) *gn_out = Gn;
   // iterative_meir_wingreen (src/iterative.F90:382-414)
   if (curr) {
     for (int c = 0; c < ncont; ++c) {
@@ -1006,6 +1007,59 @@ int oracle_meir_wingreen(const negf_b200_device* dev, int npts,
     if (scba_err) scba_err[p] = so.err;
     if (ncyc) ncyc[p] = nc;
     if (status) status[p] = err.code;
+  }
+  int first = 0;
+  if (status)
+    for (int p = 0; p < npts; ++p) if (status[p] && !first) first = status[p];
+  return first;
+}
+
+// real_axis_int (src/integrations.F90:1093-1176): sum_p w_p Gn(E_p), Gn of
+// compute_Gn with the occupations frm (reference contact already
+// subtracted: Sigma^n = sum_c frm_c Gamma_c).  Blocks in the h_* layout.
+int oracle_density_neq(const negf_b200_device* dev, int npts, const double* energy, double eta,
+                       const double* weight, const double* frm, const double* coupling, int scba_niter,
+                       double scba_tol, double sgf_tol, int sgf_max_iter, double* rho_d, double* rho_u,
+                       double* rho_l, int* ncyc, int* status, int nthreads) {
+  set_threads(nthreads);
+  DeviceBlocks D = unpack(dev);
+  Opts o;
+  o.sgf_acc = sgf_tol; o.max_iter = sgf_max_iter;
+  int nbl = D.nbl, ncont = D.ncont;
+  std::vector<Trid> G(npts);
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < npts; ++p) {
+    Err err;
+    ScbaOut so;
+    int nc = 0;
+    point_scba(D, energy[p], eta, frm + (size_t)p * ncont, coupling, scba_niter, scba_tol, o, nullptr, nullptr,
+               nullptr, so, nc, err, &G[p]);
+    if (ncyc) ncyc[p] = nc;
+    if (status) status[p] = err.code;
+  }
+  size_t od = 0, oo = 0;
+  for (int i = 0; i < nbl; ++i) {
+    size_t nn = G.empty() ? 0 : G[0].d[i].v.size();
+    for (size_t q = 0; q < nn; ++q) {
+      cplx t(0.0, 0.0);
+      for (int p = 0; p < npts; ++p) t += cplx(weight[2 * p], weight[2 * p + 1]) * G[p].d[i].v[q];
+      rho_d[2 * (od + q)] = t.real(); rho_d[2 * (od + q) + 1] = t.imag();
+    }
+    od += (size_t)D.n[i] * D.n[i];
+    if (i + 1 < nbl) {
+      size_t nm = (size_t)D.n[i] * D.n[i + 1];
+      for (size_t q = 0; q < nm; ++q) {
+        cplx tu(0.0, 0.0), tl(0.0, 0.0);
+        for (int p = 0; p < npts; ++p) {
+          cplx w(weight[2 * p], weight[2 * p + 1]);
+          tu += w * G[p].u[i].v[q];
+          tl += w * G[p].l[i].v[q];
+        }
+        rho_u[2 * (oo + q)] = tu.real(); rho_u[2 * (oo + q) + 1] = tu.imag();
+        rho_l[2 * (oo + q)] = tl.real(); rho_l[2 * (oo + q) + 1] = tl.imag();
+      }
+      oo += nm;
+    }
   }
   int first = 0;
   if (status)

@@ -87,3 +87,32 @@ def test_density_parity(gpu_ctx, case):
             assert np.allclose([b[0, 0].real for b in gd], 1.0, atol=1e-10)
     finally:
         gpu_ctx.release(did)
+
+
+def test_oracle_real_axis_vanishes_in_equilibrium():
+    dev = G.transport_c0(nbl=4, n=6, seed=1)
+    E, w = D.real_axis_points(mu=[0.0, 0.0], kT=[0.01, 0.01], n_kt=10, np_real=12, delta=1e-4)
+    frm = D.neq_occupations(E, [0.0, 0.0], [0.01, 0.01], ref=1)
+    assert np.all(frm == 0.0)
+    (rd, ru, rl), nc, st = O.density_neq(dev, E, w, frm, eta=1e-4)
+    assert all(np.abs(b).max() == 0.0 for b in rd + ru + rl)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("deph", [False, True])
+def test_density_neq_parity(gpu_ctx, deph):
+    dev = G.transport_c0(nbl=4, n=6, seed=2)
+    mu, kT = [0.1, -0.1], [0.01, 0.01]
+    E, w = D.real_axis_points(mu=mu, kT=kT, n_kt=10, np_real=24, delta=1e-4)
+    frm = D.neq_occupations(E, mu, kT, ref=2)
+    cpl = np.full(dev.norb, 0.05) if deph else None
+    did = gpu_ctx.upload(dev)
+    try:
+        gpu_ctx.set_options(scba_niter=5 if deph else 0)
+        (gd, gu, gl), nc, st = gpu_ctx.density_neq(did, E, w, frm, eta=1e-4, coupling=cpl)
+        (od, ou, ol), onc, ost = O.density_neq(dev, E, w, frm, eta=1e-4, coupling=cpl, scba_niter=5 if deph else 0)
+        assert _close(gd, od, 1e-9) and _close(gu, ou, 1e-9) and _close(gl, ol, 1e-9)
+        assert max(np.abs(b).max() for b in od) > 1e-4          # a bias window: a non-zero density
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
