@@ -199,14 +199,17 @@ int negf_b200_meir_wingreen(negf_b200_ctx* ctx, int32_t npts,
  * the energy-weighted matrix, DorE = 'E').  rho_diag / rho_upper / rho_lower
  * receive the blocks in the layout of h_diag / h_upper / h_lower (NULL to
  * skip); restricting them to the sparsity of S (blk2csr,
- * src/iterative.F90:1375-1450) is left to the caller.  The outer blocks
- * between device and contacts (calculate_Gr_outer) and dephasing are not
+ * src/iterative.F90:1375-1450) is left to the caller.  rho_dc / rho_cd
+ * (NULL to skip) receive the outer blocks of calculate_Gr_outer with
+ * outer_blocks = 2 (src/iterative.F90:1463-1573): device PL cblk[c] ->
+ * contact c (n_cb x L_c, the hmc layout) and contact -> device (L_c x n_cb,
+ * same offsets), kept on the pattern of E SMC - HMC.  Dephasing is not
  * included. */
 int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts,
                       const double* e_re, const double* e_im,
                       const double* weight, double* rho_diag,
-                      double* rho_upper, double* rho_lower, int32_t* ncyc,
-                      int32_t* status);
+                      double* rho_upper, double* rho_lower, double* rho_dc,
+                      double* rho_cd, int32_t* ncyc, int32_t* status);
 
 /* Non-equilibrium part of the density matrix on the real axis, the loop of
  * real_axis_int (src/integrations.F90:1093-1176): at every real energy E_p

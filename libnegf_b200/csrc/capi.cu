@@ -816,7 +816,8 @@ namespace {
 int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t npts, const double* e_re,
                       const double* e_im, double eta, const double* weight, const double* frm,
                       const double* coupling, std::vector<double2>& T, std::vector<int>& pl, int64_t& nd,
-                      int64_t& no, int32_t* ncyc, int32_t* status) {
+                      int64_t& no, int32_t* ncyc, int32_t* status, std::vector<double2>* outer = nullptr,
+                      int64_t* nm_out = nullptr) {
   if (device_id < 0 || device_id >= (int)ctx->devs.size() || !ctx->devs[device_id].live)
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
   const DeviceRec& r = ctx->devs[device_id];
@@ -829,6 +830,10 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
     if (i + 1 < r.nbl) no += (int64_t)pl[i] * pl[i + 1];
   }
   T.assign((size_t)(nd + 2 * no), make_double2(0.0, 0.0));
+  int64_t nm = 0;   // outer blocks: sum over contacts of n_cb x L (the hmc layout)
+  for (int c = 0; c < r.ncont; ++c) nm += (int64_t)pl[r.desc.cblk[c] - 1] * r.desc.L[c];
+  if (nm_out) *nm_out = nm;
+  if (outer) outer->assign((size_t)(2 * nm), make_double2(0.0, 0.0));
   if (npts == 0) return NEGF_B200_OK;
   if (mode == negf::MODE_GN && r.nbl < 2) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the Gn solve needs nbl >= 2");
   std::vector<int32_t> ids(npts, device_id);
@@ -842,6 +847,7 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
     c.take<int32_t>(npts); c.take<int32_t>(npts); c.take<double2>((size_t)(nd + 2 * no));
     c.take<double>((size_t)npts * r.ncont); c.take<double>((size_t)r.norb); c.take<int32_t>(npts);
     c.take<double>(npts);
+    if (outer) c.take<double2>((size_t)(2 * nm));
     need = c.off + 256;
   }
   st = grow(ctx, &ctx->io, &ctx->io_bytes, need);
@@ -858,7 +864,9 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
   double* d_cpl = c.take<double>((size_t)r.norb);
   int32_t* d_it = c.take<int32_t>(npts);
   double* d_err = c.take<double>(npts);
+  double2* d_outer = outer ? c.take<double2>((size_t)(2 * nm)) : nullptr;
   cudaStream_t s = ctx->stream;
+  if (d_outer) CK(cudaMemsetAsync(d_outer, 0, (size_t)(2 * nm) * 16, s));
   CK(cudaMemcpyAsync(d_ids, ids.data(), npts * 4, cudaMemcpyHostToDevice, s));
   CK(cudaMemcpyAsync(d_re, e_re, npts * 8, cudaMemcpyHostToDevice, s));
   if (e_im) CK(cudaMemcpyAsync(d_im, e_im, npts * 8, cudaMemcpyHostToDevice, s));
@@ -869,6 +877,7 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
   negf::EngineArgs a = base_args(ctx, mode, npts);
   a.dev_id = d_ids; a.energy = d_re; a.energy_im = d_im; a.weight = d_w; a.eta = eta;
   a.acc_d = d_acc; a.acc_u = d_acc + nd; a.acc_l = d_acc + nd + no;
+  a.acc_lc = d_outer; a.acc_cl = d_outer ? d_outer + nm : nullptr;
   a.ncyc = d_nc; a.status = d_st;
   if (mode == negf::MODE_GN) {
     a.frm = d_frm; a.frm_stride = r.ncont; a.coupling = coupling ? d_cpl : nullptr;
@@ -878,6 +887,7 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
   if (st) return st;
   std::vector<int32_t> hst(npts);
   CK(cudaMemcpyAsync(T.data(), d_acc, T.size() * 16, cudaMemcpyDeviceToHost, s));
+  if (d_outer) CK(cudaMemcpyAsync(outer->data(), d_outer, outer->size() * 16, cudaMemcpyDeviceToHost, s));
   if (ncyc) CK(cudaMemcpyAsync(ncyc, d_nc, npts * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
@@ -894,17 +904,49 @@ void store_blocks(const double2* src, int64_t n, double* dst) {
 }  // namespace
 
 int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const double* e_re, const double* e_im,
-                      const double* weight, double* rho_diag, double* rho_upper, double* rho_lower, int32_t* ncyc,
-                      int32_t* status) {
+                      const double* weight, double* rho_diag, double* rho_upper, double* rho_lower, double* rho_dc,
+                      double* rho_cd, int32_t* ncyc, int32_t* status) {
   if (!ctx) return NEGF_B200_ERR_BAD_ARG;
   if (npts < 0 || (npts > 0 && (!e_re || !e_im || !weight))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
   std::lock_guard<std::mutex> lk(ctx->mu);
-  std::vector<double2> T;
+  std::vector<double2> T, Tout;
   std::vector<int> pl;
-  int64_t nd = 0, no = 0;
+  int64_t nd = 0, no = 0, nm = 0;
+  const bool want_outer = rho_dc || rho_cd;
   int st = accumulate_blocks(ctx, negf::MODE_RHO, device_id, npts, e_re, e_im, 0.0, weight, nullptr, nullptr, T, pl,
-                             nd, no, ncyc, status);
+                             nd, no, ncyc, status, want_outer ? &Tout : nullptr, &nm);
   if (st) return st;
+  if (want_outer) {
+    // calculate_Gr_outer keeps the entries on the pattern of Tlc = E SMC - HMC (and of
+    // Tcl for the lower block): the nonzeros of HMC or SMC; then zspectral pairs them
+    const DeviceRec& r = ctx->devs[device_id];
+    std::vector<double2> hmc((size_t)std::max<int64_t>(nm, 1)), smc;
+    CK(cudaMemcpy(hmc.data(), r.desc.hmc, (size_t)nm * 16, cudaMemcpyDeviceToHost));
+    if (r.desc.smc) {
+      smc.resize((size_t)nm);
+      CK(cudaMemcpy(smc.data(), r.desc.smc, (size_t)nm * 16, cudaMemcpyDeviceToHost));
+    }
+    auto nz = [&](int64_t q) {
+      return hmc[q].x != 0.0 || hmc[q].y != 0.0 || (!smc.empty() && (smc[q].x != 0.0 || smc[q].y != 0.0));
+    };
+    const double2* Tlc = Tout.data();
+    const double2* Tcl = Tlc + nm;
+    int64_t om = 0;
+    for (int c = 0; c < r.ncont; ++c) {
+      const int n = pl[r.desc.cblk[c] - 1], L = r.desc.L[c];
+      for (int j = 0; j < L; ++j)
+        for (int q = 0; q < n; ++q) {
+          const int64_t idc = om + q + (int64_t)j * n;   // (q, j) of the n x L block
+          const int64_t icd = om + j + (int64_t)q * L;   // (j, q) of the L x n block
+          const bool on = nz(idc);
+          const double2 lc = on ? Tlc[idc] : make_double2(0.0, 0.0);
+          const double2 cl = on ? Tcl[icd] : make_double2(0.0, 0.0);
+          if (rho_dc) { rho_dc[2 * idc] = -(lc.y + cl.y); rho_dc[2 * idc + 1] = lc.x - cl.x; }   // i (lc - conj(cl))
+          if (rho_cd) { rho_cd[2 * icd] = -(cl.y + lc.y); rho_cd[2 * icd + 1] = cl.x - lc.x; }   // i (cl - conj(lc))
+        }
+      om += (int64_t)n * L;
+    }
+  }
   const int nbl = (int)pl.size();
   // rho = i (T - T^dag) over the tridiagonal blocks (zspectral, src/integrations.F90:893)
   const double2* Td = T.data();

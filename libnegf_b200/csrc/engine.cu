@@ -142,7 +142,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_engine(EngineArgs a) {
 
 int64_t engine_slots(int mode, int nbl_max, int ncont_max) {
   int64_t s = S_SIG + ncont_max;
-  if (mode == MODE_T || mode == MODE_DOS || mode == MODE_RHO) s += nbl_max + ncont_max;   // gsmr, Gr(cb,cb)
+  if (mode == MODE_T || mode == MODE_DOS) s += nbl_max + ncont_max;   // gsmr, Gr(cb,cb)
+  else if (mode == MODE_RHO) s += nbl_max + 2 * ncont_max;             // + gs per contact
   else s += 8 * (int64_t)nbl_max;                                 // GN arrays
   return s;
 }

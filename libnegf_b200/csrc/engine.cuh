@@ -66,6 +66,7 @@ struct EngineArgs {
   const double* energy_im;
   const double2* weight;
   double2* acc_d; double2* acc_u; double2* acc_l;
+  double2* acc_lc; double2* acc_cl;   // outer blocks per contact (hmc layout), or null
   // surface Green's function cache (npts x ncont_max offsets into sgf_arena in
   // complex elements, -1 = none): read gs instead of the decimation / store it
   const int64_t* sgf_in;

@@ -84,6 +84,8 @@ struct Ws {
   __device__ double2* layer(int arr, int i, int nbl) const { return slot(S_SIG + ncont + arr * nbl + i); }
   // T / DOS: Gr(cb,cb) kept at the block of contact c during the forward sweep
   __device__ double2* keep(int c) const { return slot(S_SIG + ncont + nbl_max + c); }
+  // density: the surface GF of contact c, kept for the outer blocks
+  __device__ double2* gskeep(int c) const { return slot(S_SIG + 2 * ncont + nbl_max + c); }
 };
 
 // ---------------------------------------------------------------- ops
@@ -461,6 +463,10 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           PT_EMIT(s);
         }
       sgf_ready:
+        if (a.mode == MODE_RHO && a.acc_lc) {
+          set_simple(o, K_COPY, s.L * s.L, w.slot(4), w.gskeep(s.c));
+          PT_EMIT(s);
+        }
         // ---- self-energy: Tlc = E SMC - HMC, Tcl = (E^* SMC - HMC)^dag, Sigma = Tlc gs Tcl
         set_esh(o, w.slot(0), s.ncb, s.L, s.d->hmc + s.d->omc[s.c], s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr,
                 s.ecs, 0, nullptr, nullptr, OP_N);
@@ -637,7 +643,40 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                 PT_EMIT(s);
               }
         }
-        if (a.mode == MODE_RHO) goto point_done;
+        if (a.mode == MODE_RHO) {
+          if (a.acc_lc)
+            // calculate_Gr_outer, outer_blocks = 2 (src/iterative.F90:1463-1573): for every contact
+            // -Gr(cb,cb) Tlc gs and -gs Tcl Gr(cb,cb), summed with the weight (masked on the host)
+            for (s.c = 0; s.c < s.d->ncont; ++s.c) {
+              s.L = s.d->L[s.c];
+              s.ncb = s.d->pl[s.d->cblk[s.c] - 1];
+              set_esh(o, w.slot(0), s.ncb, s.L, s.d->hmc + s.d->omc[s.c],
+                      s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr, s.ecs, 0, nullptr, nullptr, OP_N);   // Tlc
+              PT_EMIT(s);
+              set_gemm(o, s.ncb, s.L, s.ncb, w.keep(s.c), s.ncb, OP_N, w.slot(0), s.ncb, OP_N, w.slot(2), s.ncb,
+                       mone, zero);
+              PT_EMIT(s);
+              set_gemm(o, s.ncb, s.L, s.L, w.slot(2), s.ncb, OP_N, w.gskeep(s.c), s.L, OP_N, w.slot(3), s.ncb, one,
+                       zero);
+              PT_EMIT(s);
+              set_simple(o, K_ACCUM, s.ncb * s.L, w.slot(3), a.acc_lc + s.d->omc[s.c]);
+              o.alpha = a.weight[s.p];
+              PT_EMIT(s);
+              set_esh(o, w.slot(1), s.L, s.ncb, s.d->hmc + s.d->omc[s.c],
+                      s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr, cconj(s.ecs), 0, nullptr, nullptr, OP_C);  // Tcl
+              PT_EMIT(s);
+              set_gemm(o, s.L, s.ncb, s.L, w.gskeep(s.c), s.L, OP_N, w.slot(1), s.L, OP_N, w.slot(2), s.L, mone,
+                       zero);
+              PT_EMIT(s);
+              set_gemm(o, s.L, s.ncb, s.ncb, w.slot(2), s.L, OP_N, w.keep(s.c), s.ncb, OP_N, w.slot(3), s.L, one,
+                       zero);
+              PT_EMIT(s);
+              set_simple(o, K_ACCUM, s.ncb * s.L, w.slot(3), a.acc_cl + s.d->omc[s.c]);
+              o.alpha = a.weight[s.p];
+              PT_EMIT(s);
+            }
+          goto point_done;
+        }
         if (a.mode != MODE_GN) {
           if (a.mode == MODE_DOS && a.ldos && a.dos && s.d->nldos > 0) {
             o.kind = K_LDOS; o.A = reinterpret_cast<const double2*>(a.dos + (int64_t)s.p * a.dos_stride);

@@ -114,6 +114,19 @@ def split_blocks(pl: Sequence[int], diag, upper, lower):
     return d, u, l
 
 
+def split_outer(dev, dc, cd):
+    """Flat outer blocks (hmc layout) -> per contact (device->contact n_cb x L,
+    contact->device L x n_cb)."""
+    out_dc, out_cd = [], []
+    o = 0
+    for cb, L in zip(dev.cblk, dev.lead_size):
+        n = dev.pl_size[cb - 1]
+        out_dc.append(np.asarray(dc[o:o + n * L]).reshape((n, L), order="F"))
+        out_cd.append(np.asarray(cd[o:o + n * L]).reshape((L, n), order="F"))
+        o += n * L
+    return out_dc, out_cd
+
+
 def restrict_to_pattern(blocks, pattern, plend: Sequence[int]):
     """blk2csr: the entries of the tridiagonal blocks on the sparsity of
     `pattern` (a scipy.sparse matrix over at least the device orbitals);

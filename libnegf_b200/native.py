@@ -97,7 +97,7 @@ def load():
     L.negf_b200_transmissions.argtypes = [vp, i32, ip, dp, f64, f64, i32, ip, ip, dp, dp, ip, ip]
     L.negf_b200_set_sgf_cache.argtypes = [vp, i32, ctypes.c_size_t]
     L.negf_b200_set_workspace_limit.argtypes = [vp, ctypes.c_size_t]
-    L.negf_b200_density.argtypes = [vp, i32, i32, dp, dp, dp, dp, dp, dp, ip, ip]
+    L.negf_b200_density.argtypes = [vp, i32, i32, dp, dp, dp, dp, dp, dp, dp, dp, ip, ip]
     L.negf_b200_density_neq.argtypes = [vp, i32, i32, dp, f64, dp, dp, dp, dp, dp, dp, ip, ip]
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.negf_b200_sgf_cache_stats.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_size_t)]
@@ -238,9 +238,14 @@ class Context:
     def density(self, device_id, z, w, pl=None, check=True):
         """Equilibrium density-matrix blocks from the contour points z with
         weights w (see negf_b200_density): (diag, upper, lower) block lists,
+        the outer (device->contact, contact->device) blocks per contact,
         ncyc, status."""
-        from .density import split_blocks
-        pl = pl if pl is not None else self.devices[device_id].pl_size
+        from .density import split_blocks, split_outer
+        dev = self.devices[device_id]
+        pl = pl if pl is not None else dev.pl_size
+        nm = sum(dev.pl_size[cb - 1] * L for cb, L in zip(dev.cblk, dev.lead_size))
+        rdc = np.zeros(max(nm, 1), dtype=np.complex128)
+        rcd = np.zeros(max(nm, 1), dtype=np.complex128)
         z = np.ascontiguousarray(z, dtype=np.complex128).ravel()
         wt = np.ascontiguousarray(w, dtype=np.complex128).ravel()
         er, ei = np.ascontiguousarray(z.real), np.ascontiguousarray(z.imag)
@@ -253,10 +258,10 @@ class Context:
         st = np.zeros(z.size, dtype=np.int32)
         rc = self._L.negf_b200_density(self._h, device_id, z.size, _d(er), _d(ei), _d(wt.view(np.float64)),
                                        _d(rd.view(np.float64)), _d(ru.view(np.float64)), _d(rl.view(np.float64)),
-                                       _i(nc), _i(st))
+                                       _d(rdc.view(np.float64)), _d(rcd.view(np.float64)), _i(nc), _i(st))
         if check and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "density: " + self.last_error())
-        return split_blocks(pl, rd, ru, rl), nc, st
+        return split_blocks(pl, rd, ru, rl), split_outer(dev, rdc, rcd), nc, st
 
     def density_neq(self, device_id, energies, w, frm, eta=1e-4, coupling=None, check=True):
         """Real-axis non-equilibrium density blocks sum_p w_p Gn(E_p) (see

@@ -274,10 +274,20 @@ void surface_green(cplx E, const DeviceBlocks& D, int c, Dns& GS, int& ncyc,
 }
 
 // compute_contacts_dns (src/contselfenergy.F90:445-491) + SelfEnergy_dns
+struct ContactParts {   // GS, Tlc, Tcl per contact (for calculate_Gr_outer)
+  std::vector<Dns> GS, Tlc, Tcl;
+};
+
 void compute_contacts(cplx Ec, const DeviceBlocks& D, std::vector<Dns>& Sig,
-                      int& ncyc_max, double sgf_acc, int max_iter, Err& err) {
+                      int& ncyc_max, double sgf_acc, int max_iter, Err& err,
+                      ContactParts* parts = nullptr) {
   Sig.assign(D.ncont, Dns());
   ncyc_max = 0;
+  if (parts) {
+    parts->GS.assign(D.ncont, Dns());
+    parts->Tlc.assign(D.ncont, Dns());
+    parts->Tcl.assign(D.ncont, Dns());
+  }
   for (int c = 0; c < D.ncont; ++c) {
     Dns GS;
     int ncyc = 0;
@@ -296,6 +306,11 @@ void compute_contacts(cplx Ec, const DeviceBlocks& D, std::vector<Dns>& Sig,
     Dns TG;
     mult(Tlc, GS, TG);
     mult(TG, Tcl, Sig[c]);
+    if (parts) {
+      parts->GS[c] = GS;
+      parts->Tlc[c] = Tlc;
+      parts->Tcl[c] = Tcl;
+    }
   }
 }
 
@@ -602,9 +617,10 @@ void point_transmissions_ldos(const DeviceBlocks& D, double E, double eta, doubl
 // One contour point of contour_int (src/integrations.F90:844-897): Gr at the
 // complex energy Ec (contacts and ES-H at Ec, compute_Gr :2287-2340 /
 // calculate_Gr src/iterative.F90:90-148), all tridiagonal blocks.
-void point_gr_blocks(const DeviceBlocks& D, cplx Ec, const Opts& o, GrBlocks& Gr, int& ncyc, Err& err) {
+void point_gr_blocks(const DeviceBlocks& D, cplx Ec, const Opts& o, GrBlocks& Gr, int& ncyc, Err& err,
+                     ContactParts* parts = nullptr) {
   std::vector<Dns> Sig;
-  compute_contacts(Ec, D, Sig, ncyc, o.sgf_acc, o.max_iter, err);
+  compute_contacts(Ec, D, Sig, ncyc, o.sgf_acc, o.max_iter, err, parts);
   Trid ESH;
   build_ESH(Ec, D, &Sig, ESH);
   int nbl = D.nbl;
@@ -922,20 +938,53 @@ int oracle_transmissions(const negf_b200_device* dev, int npts, const double* en
 // layout of h_diag / h_upper / h_lower.
 int oracle_density(const negf_b200_device* dev, int npts, const double* e_re, const double* e_im,
                    const double* weight, double sgf_tol, int sgf_max_iter, double* rho_d, double* rho_u,
-                   double* rho_l, int* ncyc, int* status, int nthreads) {
+                   double* rho_l, double* rho_dc, double* rho_cd, int* ncyc, int* status, int nthreads) {
   set_threads(nthreads);
   DeviceBlocks D = unpack(dev);
   Opts o;
   o.sgf_acc = sgf_tol; o.max_iter = sgf_max_iter;
-  int nbl = D.nbl;
+  int nbl = D.nbl, ncont = D.ncont;
   std::vector<GrBlocks> G(npts, GrBlocks(nbl));
+  std::vector<ContactParts> parts(npts);
 #pragma omp parallel for schedule(dynamic, 1)
   for (int p = 0; p < npts; ++p) {
     Err err;
     int nc = 0;
-    point_gr_blocks(D, cplx(e_re[p], e_im[p]), o, G[p], nc, err);
+    point_gr_blocks(D, cplx(e_re[p], e_im[p]), o, G[p], nc, err, &parts[p]);
     if (ncyc) ncyc[p] = nc;
     if (status) status[p] = err.code;
+  }
+  // calculate_Gr_outer, outer_blocks = 2 (src/iterative.F90:1463-1573):
+  // Grlc = -Gr(cb,cb) Tlc gs on Tlc's pattern, Grcl = -gs Tcl Gr(cb,cb) on
+  // Tcl's pattern, summed with the weights; then rho = i (T - T^dag) pairs
+  // the device->contact block with the contact->device one.
+  if (rho_dc || rho_cd) {
+    size_t om = 0;
+    for (int c = 0; c < ncont; ++c) {
+      const int cb = D.cblk[c] - 1, n = D.n[cb], L = D.L[c];
+      std::vector<cplx> Tlcs((size_t)n * L, cplx(0.0, 0.0)), Tcls((size_t)L * n, cplx(0.0, 0.0));
+      for (int p = 0; p < npts; ++p) {
+        const cplx w(weight[2 * p], weight[2 * p + 1]);
+        const ContactParts& cp = parts[p];
+        Dns work1, Grlc, work2, Grcl;
+        mult(G[p].d[cb], cp.Tlc[c], work1, cplx(-1.0, 0.0));
+        mult(work1, cp.GS[c], Grlc);
+        mult(cp.GS[c], cp.Tcl[c], work2, cplx(-1.0, 0.0));
+        mult(work2, G[p].d[cb], Grcl);
+        for (size_t q = 0; q < Tlcs.size(); ++q)
+          if (cp.Tlc[c].v[q] != cplx(0.0, 0.0)) Tlcs[q] += w * Grlc.v[q];
+        for (size_t q = 0; q < Tcls.size(); ++q)
+          if (cp.Tcl[c].v[q] != cplx(0.0, 0.0)) Tcls[q] += w * Grcl.v[q];
+      }
+      for (int j = 0; j < L; ++j)
+        for (int r = 0; r < n; ++r) {
+          const cplx v = I1 * (Tlcs[r + (size_t)j * n] - std::conj(Tcls[j + (size_t)r * L]));
+          if (rho_dc) { rho_dc[2 * (om + r + (size_t)j * n)] = v.real(); rho_dc[2 * (om + r + (size_t)j * n) + 1] = v.imag(); }
+          const cplx u = I1 * (Tcls[j + (size_t)r * L] - std::conj(Tlcs[r + (size_t)j * n]));
+          if (rho_cd) { rho_cd[2 * (om + j + (size_t)r * L)] = u.real(); rho_cd[2 * (om + j + (size_t)r * L) + 1] = u.imag(); }
+        }
+      om += (size_t)n * L;
+    }
   }
   size_t od = 0, oo = 0;
   for (int i = 0; i < nbl; ++i) {

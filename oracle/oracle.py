@@ -44,8 +44,8 @@ def lib():
         L.oracle_transmissions.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                            ip, ip, vp, ctypes.c_int, ip, ip, ctypes.c_double, ctypes.c_int,
                                            ctypes.c_double, dp, dp, ip, ip, ctypes.c_int]
-        L.oracle_density.argtypes = [vp, ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp, dp, dp, ip, ip,
-                                     ctypes.c_int]
+        L.oracle_density.argtypes = [vp, ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp,
+                                     ip, ip, ctypes.c_int]
         L.oracle_density_neq.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, dp, dp, dp, ctypes.c_int,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp, ip, ip,
                                          ctypes.c_int]
@@ -160,14 +160,17 @@ def density(dev: Device, z, w, sgf_tol=1e-9, sgf_max_iter=300, nthreads=0):
     rd = np.zeros(max(nd, 1), dtype=np.complex128)
     ru = np.zeros(max(no, 1), dtype=np.complex128)
     rl = np.zeros(max(no, 1), dtype=np.complex128)
+    nm = sum(n[cb - 1] * L for cb, L in zip(dev.cblk, dev.lead_size))
+    rdc = np.zeros(max(nm, 1), dtype=np.complex128)
+    rcd = np.zeros(max(nm, 1), dtype=np.complex128)
     ncyc = np.zeros(z.size, dtype=np.int32)
     status = np.zeros(z.size, dtype=np.int32)
     st = dev.to_struct()
     lib().oracle_density(ctypes.addressof(st), z.size, _d(er), _d(ei), _d(wt.view(np.float64)), sgf_tol,
                          sgf_max_iter, _d(rd.view(np.float64)), _d(ru.view(np.float64)), _d(rl.view(np.float64)),
-                         _i(ncyc), _i(status), nthreads)
-    from libnegf_b200.density import split_blocks
-    return split_blocks(n, rd, ru, rl), ncyc, status
+                         _d(rdc.view(np.float64)), _d(rcd.view(np.float64)), _i(ncyc), _i(status), nthreads)
+    from libnegf_b200.density import split_blocks, split_outer
+    return split_blocks(n, rd, ru, rl), split_outer(dev, rdc, rcd), ncyc, status
 
 
 def density_neq(dev: Device, energies, w, frm, eta=1e-4, coupling=None, scba_niter=5, scba_tol=1e-7,

@@ -36,7 +36,7 @@ def test_oracle_half_filled_chain_has_one_electron_per_site():
     site by particle-hole symmetry."""
     dev = G.chain(1, 6)
     z, w = D.contour_points(**CONTOUR)
-    (rd, ru, rl), nc, st = O.density(dev, z, w)
+    (rd, ru, rl), (odc, ocd), nc, st = O.density(dev, z, w)
     assert np.all(st == 0)
     occ = np.array([b[0, 0].real for b in rd])
     assert np.allclose(occ, 1.0, atol=1e-10)
@@ -79,10 +79,13 @@ def test_density_parity(gpu_ctx, case):
     z, w = D.contour_points(**CONTOUR)
     did = gpu_ctx.upload(dev)
     try:
-        (gd, gu, gl), nc, st = gpu_ctx.density(did, z, w)
-        (od, ou, ol), onc, ost = O.density(dev, z, w)
+        (gd, gu, gl), (gdc, gcd), nc, st = gpu_ctx.density(did, z, w)
+        (od, ou, ol), (odc, ocd), onc, ost = O.density(dev, z, w)
         assert np.all(st == ost)
         assert _close(gd, od) and _close(gu, ou) and _close(gl, ol)
+        assert _close(gdc, odc) and _close(gcd, ocd)
+        for a, b in zip(odc, ocd):                               # rho is Hermitian across the outer blocks
+            assert np.abs(a - b.conj().T).max() <= 1e-12 * max(1.0, np.abs(a).max())
         if case == "chain":
             assert np.allclose([b[0, 0].real for b in gd], 1.0, atol=1e-10)
     finally:
