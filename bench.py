@@ -85,6 +85,11 @@ def point_list(wl, seed=11):
     return ids[perm], en[perm]
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_engine
+# launch, from an ncu capture of the default c1 command (592 points per step)
+DRAM_BYTES_PER_LAUNCH = {("c1", 592): 8.4577e12}
+
+
 def flops_per_point(wl, ncyc_total, ncont=2):
     """Algorithmic FP64 flops of one point under the reference's operation
     sequence (uniform PL size n = lead PL size; complex GEMM m*n*k = 8mnk,
@@ -443,7 +448,9 @@ def main():
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak,
+                         "traffic": DRAM_BYTES_PER_LAUNCH.get((args.workload, P)),
+                         "traffic_unit": "bytes per launch (one step)",
                          "peak_source": "measured in-run: cuBLAS ZGEMM 4096^3 complex128 (FP64 DMMA pipe)",
                          "flop_model": "reference operation sequence, inverse = zgetrf+zgetrs 32/3 n^3",
                          "flops_per_step": flops / args.steps,
