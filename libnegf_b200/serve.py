@@ -73,6 +73,7 @@ class Request:
 class _Resident:
     ids: List[int]                        # device id in every lane
     nbytes: int
+    device: object = None                 # held, so that an id()-based key is never reused while resident
     users: int = 0
     last_use: float = 0.0
 
@@ -81,14 +82,23 @@ class Server:
     """Continuous-batching request loop on one GPU (see the module docstring)."""
 
     def __init__(self, cuda_device: int = 0, lanes: int = 2, points_per_launch: int = 0,
-                 hbm_budget: int = 0, sgf_cache_bytes: int = 1 << 30, options: Optional[dict] = None):
-        self.lanes = [native.Context(cuda_device) for _ in range(lanes)]
-        import torch
-        props = torch.cuda.get_device_properties(cuda_device)
-        self.sms = props.multi_processor_count
-        if not hbm_budget:
-            free, _ = torch.cuda.mem_get_info(cuda_device)
-            hbm_budget = int(free * 0.8)
+                 hbm_budget: int = 0, sgf_cache_bytes: int = 1 << 30, options: Optional[dict] = None,
+                 contexts: Optional[list] = None, sms: int = 0):
+        """`contexts` (one per lane) and `sms` replace the engine contexts and
+        the device query, for driving the loop with stand-ins."""
+        if contexts is not None:
+            self.lanes = list(contexts)
+            lanes = len(self.lanes)
+        else:
+            self.lanes = [native.Context(cuda_device) for _ in range(lanes)]
+        if not sms or not hbm_budget:
+            import torch
+            if not sms:
+                sms = torch.cuda.get_device_properties(cuda_device).multi_processor_count
+            if not hbm_budget:
+                free, _ = torch.cuda.mem_get_info(cuda_device)
+                hbm_budget = int(free * 0.8)
+        self.sms = sms
         self.budget = hbm_budget
         # the budget is split: resident devices, then per-lane workspace + cache
         self.ws_share = int(self.budget * 0.6) // lanes
@@ -109,7 +119,6 @@ class Server:
         self._active: List[Request] = []
         self._pending: List[Tuple[Request, int]] = []   # (request, point index)
         self._resident: Dict[object, _Resident] = {}
-        self._busy = [False] * lanes
         self._stop = False
         self._threads = [threading.Thread(target=self._lane_loop, args=(i,), daemon=True) for i in range(lanes)]
         self._sched = threading.Thread(target=self._admit_loop, daemon=True)
@@ -178,7 +187,7 @@ class Server:
                 ctx.set_tun_proj(did, req.tun_proj)
                 ctx.set_dos_proj(did, req.dos_proj)
                 ids.append(did)
-            r = _Resident(ids=ids, nbytes=nbytes)
+            r = _Resident(ids=ids, nbytes=nbytes, device=req.device)
             self._resident[k] = r
         r.users += 1
         r.last_use = time.perf_counter()

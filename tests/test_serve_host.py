@@ -1,0 +1,115 @@
+"""The request loop's host logic on CPU, with stand-in engine contexts: every
+point of every request is solved once, batches mix requests of one solve
+kind, later arrivals join running work, idle devices are evicted to admit new
+ones, and an oversize device is rejected."""
+import threading
+import time
+
+import numpy as np
+
+from libnegf_b200 import generators as G
+from libnegf_b200.serve import Request, Server
+
+
+class FakeContext:
+    """Records launches; T(E) = E * (device id + 1) per pair index + pair number."""
+
+    def __init__(self):
+        self.devices = {}
+        self.next_id = 0
+        self.launches = []
+        self.released = []
+        self.lock = threading.Lock()
+
+    def set_options(self, **kw): pass
+    def set_workspace_limit(self, n): pass
+    def set_sgf_cache(self, mode, n=0): pass
+    def set_tun_proj(self, did, p): pass
+    def set_dos_proj(self, did, p): pass
+    def close(self): pass
+
+    def upload(self, dev):
+        with self.lock:
+            did = self.next_id
+            self.next_id += 1
+            self.devices[did] = dev
+            return did
+
+    def release(self, did):
+        with self.lock:
+            self.devices.pop(did)
+            self.released.append(did)
+
+    def transmissions(self, ids, E, pairs, eta=1e-4, ldos=False, dos_delta=1e-4, check=True):
+        ids = np.asarray(ids)
+        with self.lock:
+            self.launches.append((tuple(sorted(set(ids.tolist()))), len(E), ldos))
+        time.sleep(0.01)
+        T = np.stack([E * (ids + 1) + q for q in range(len(pairs))], axis=1)
+        led = np.stack([E, -E], axis=1) if ldos else None
+        return T, led, np.zeros(len(E), np.int32), np.zeros(len(E), np.int32)
+
+
+def _expected(r, srv, lane=0):
+    did = srv._resident[srv._key(r)].ids[lane] if srv._key(r) in srv._resident else None
+    return did
+
+
+def test_every_point_once_and_batches_mix_requests():
+    ctxs = [FakeContext(), FakeContext()]
+    srv = Server(contexts=ctxs, sms=4, points_per_launch=16, hbm_budget=1 << 34, sgf_cache_bytes=0)
+    try:
+        devs = [G.transport_c0(nbl=3, n=4, seed=s) for s in range(3)]
+        reqs = [srv.submit(Request(devs[i], np.linspace(-1, 1, 10 + 7 * i), pairs=[(1, 2), (2, 1)])) for i in range(3)]
+        time.sleep(0.02)
+        late = srv.submit(Request(devs[0], np.linspace(0, 1, 9), pairs=[(1, 2), (2, 1)]))
+        for r in reqs + [late]:
+            assert r.wait(30) and r.error is None
+        # device ids are the same in both lanes (uploaded in the same order)
+        for r in reqs + [late]:
+            did = srv._resident[srv._key(r)].ids[0]
+            exp = np.stack([r.energies * (did + 1) + q for q in range(2)], axis=1)
+            assert np.array_equal(r.T, exp)
+        launches = ctxs[0].launches + ctxs[1].launches
+        assert sum(n for _, n, _ in launches) == sum(r.energies.size for r in reqs + [late])
+        assert all(n <= 16 for _, n, _ in launches)
+        assert any(len(ids) > 1 for ids, _, _ in launches)          # points of several devices in one launch
+        assert len(srv.latencies()) == 4
+    finally:
+        srv.close()
+
+
+def test_kinds_are_not_mixed_in_a_launch():
+    ctxs = [FakeContext()]
+    srv = Server(contexts=ctxs, sms=4, points_per_launch=64, hbm_budget=1 << 34, sgf_cache_bytes=0)
+    try:
+        d = G.transport_c0(nbl=3, n=4, seed=0)
+        a = srv.submit(Request(d, np.linspace(-1, 1, 20)))
+        b = srv.submit(Request(d, np.linspace(-1, 1, 20), ldos=True, dos_proj=[[1], [2]]))
+        assert a.wait(30) and b.wait(30)
+        assert a.ledos is None and b.ledos.shape == (20, 2)
+        assert np.array_equal(b.ledos[:, 0], b.energies)
+        kinds = {(n, l) for _, n, l in ctxs[0].launches}
+        assert all(isinstance(l, bool) for _, l in kinds)
+    finally:
+        srv.close()
+
+
+def test_eviction_and_rejection():
+    ctxs = [FakeContext()]
+    one = G.transport_c0(nbl=3, n=4, seed=0)
+    budget_dev = one.nbytes() + 100                     # room for one such device at a time
+    srv = Server(contexts=ctxs, sms=4, points_per_launch=8, hbm_budget=budget_dev * 3, sgf_cache_bytes=0)
+    srv.dev_budget = budget_dev                          # pin the device share for the test
+    try:
+        r1 = srv.submit(Request(one, np.linspace(-1, 1, 8)))
+        assert r1.wait(30) and r1.error is None
+        other = G.transport_c0(nbl=3, n=4, seed=1)
+        r2 = srv.submit(Request(other, np.linspace(-1, 1, 8)))
+        assert r2.wait(30) and r2.error is None
+        assert ctxs[0].released == [0]                   # the idle first device made room
+        big = G.transport_c0(nbl=12, n=8, seed=2)
+        r3 = srv.submit(Request(big, np.linspace(-1, 1, 4)))
+        assert r3.wait(30) and r3.error is not None and np.all(r3.status == 8)
+    finally:
+        srv.close()
