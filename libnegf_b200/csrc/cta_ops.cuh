@@ -23,11 +23,18 @@
 
 namespace negf {
 
+#ifndef NEGF_GEMM_TK
+#define NEGF_GEMM_TK 16
+#endif
+#ifndef NEGF_GEMM_STAGES
+#define NEGF_GEMM_STAGES 2
+#endif
 constexpr int kThreads = 256;          // threads per CTA (8 warps)
-constexpr int TM = 64, TN = 64, TK = 16;
+constexpr int TM = 64, TN = 64, TK = NEGF_GEMM_TK;
 constexpr int A_LD = TM + 2;           // sA[k][m], padded: conflict-free fragment loads
 constexpr int B_LD = TK + 4;           // sB[n][k], padded: conflict-free fragment loads
-constexpr int kStages = 2;             // cp.async double buffer
+constexpr int kStages = NEGF_GEMM_STAGES;   // cp.async ring depth
+static_assert(TK == 8 || TK == 16, "K tile of 8 or 16");
 constexpr int kStageElems = TK * A_LD + TN * B_LD;
 constexpr int kGemmSmemBytes = kStages * kStageElems * 16;
 constexpr int kSmallInvMax = 64;       // n <= 64: whole matrix in shared memory
@@ -307,10 +314,20 @@ __device__ __forceinline__ void cta_gemm_body(const GemmDesc* d, double2* smem) 
   const int total = d->total;
   double lmax = 0.0;
   double accR[2][2][4], accI[2][2][4];
-  int ld_tile = 0, ld_kt = 0;   // (tile, K-tile) of the next step to load
+  int ld_tile = 0, ld_kt = 0, ld_step = 0;   // (tile, K-tile) and index of the next step to load
 
-  gemm_issue<AM, BM>(d, ld_tile, ld_kt, smem);
-  if (++ld_kt == d->nk) { ld_kt = 0; ++ld_tile; }
+  // the first kStages - 1 steps in flight (an empty group keeps the count when
+  // there are fewer steps)
+#pragma unroll
+  for (int q = 0; q < kStages - 1; ++q) {
+    if (ld_step < total) {
+      gemm_issue<AM, BM>(d, ld_tile, ld_kt, smem + q * kStageElems);
+      if (++ld_kt == d->nk) { ld_kt = 0; ++ld_tile; }
+      ++ld_step;
+    } else {
+      cp_async_commit();
+    }
+  }
   int tile = 0, kt = 0;
   for (int step = 0; step < total; ++step) {
     if (kt == 0) {
@@ -321,15 +338,17 @@ __device__ __forceinline__ void cta_gemm_body(const GemmDesc* d, double2* smem) 
 #pragma unroll
           for (int q = 0; q < 4; ++q) { accR[i][j][q] = 0.0; accI[i][j][q] = 0.0; }
     }
-    if (step + 1 < total) {
-      gemm_issue<AM, BM>(d, ld_tile, ld_kt, smem + ((step + 1) & 1) * kStageElems);
+    cp_async_wait<kStages - 2>();   // this step's group has landed (groups complete in order)
+    __syncthreads();                // ... for every thread, and every thread is done with step - 1
+    // refill the buffer of step - 1 with step + kStages - 1
+    if (ld_step < total) {
+      gemm_issue<AM, BM>(d, ld_tile, ld_kt, smem + (ld_step % kStages) * kStageElems);
       if (++ld_kt == d->nk) { ld_kt = 0; ++ld_tile; }
-      cp_async_wait<1>();
+      ++ld_step;
     } else {
-      cp_async_wait<0>();
+      cp_async_commit();
     }
-    __syncthreads();
-    const double2* sA = smem + (step & 1) * kStageElems;
+    const double2* sA = smem + (step % kStages) * kStageElems;
     const double2* sB = sA + TK * A_LD;
     // warps whose 32 x 16 block lies outside M x N, and the K steps past K,
     // skip their products (narrow Gauss-Jordan updates: N, K = 16 or 32)
@@ -367,7 +386,6 @@ __device__ __forceinline__ void cta_gemm_body(const GemmDesc* d, double2* smem) 
         for (int j = 0; j < 2; ++j) dmma_16x8x4(accI[i][j], ai0, ai1, bre[j]);
       }
     }
-    __syncthreads();
     if (kt == d->nk - 1) {
       const int tilesM = d->tilesM;
       const int m0 = (tile % tilesM) * TM, n0 = (tile / tilesM) * TN;
