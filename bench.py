@@ -465,17 +465,30 @@ def main():
             line["trace_phase_share"] = trace
         if world == 1 and not args.no_cpu_baseline:
             cores = os.cpu_count() or 1
-            nsamp = args.cpu_sample or (cores if wl["n"] >= 256 else 8 * cores)
+            nsamp = args.cpu_sample or (max(64, cores) if wl["n"] >= 256 else 8 * max(64, cores))
             o = args.warmup * P
-            # points of the timed batches at one k-point (all k share structure and cost), so that
-            # OpenMP spreads the sample over every host core
-            k0 = ids_run[o]
-            sel = o + np.nonzero(ids_run[o:] == k0)[0][:nsamp]
+            # points of the timed batches, grouped by k-point so that OpenMP spreads each call over
+            # every host core: up to `cores` points of each of the first k-points met, energies
+            # spread over the grid by the batch order
+            tids, tE = ids_run[o:], E_run[o:]
+            order = list(dict.fromkeys(tids.tolist()))
+            picks = []
+            for k in order:
+                picks.extend((o + np.nonzero(tids == k)[0][:cores]).tolist())
+                if len(picks) >= nsamp:
+                    break
+            sel = np.sort(np.asarray(picks[:nsamp], dtype=np.int64))
             nsamp = sel.size
             v, Tc, dt = cpu_baseline(wl, devs, ids_run[sel], E_run[sel], nsamp, cores)
+            # one host core: two of the same points, single-threaded
+            v1, _, dt1 = cpu_baseline(wl, devs, ids_run[sel[:2]], E_run[sel[:2]], 2, 1)
             err = np.abs(Tgpu[sel] - Tc)
+            grid = wl["nE"] * wl["nk"]
             line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                                    "sample": "%d points of the timed batches, %.1f s" % (nsamp, dt)}
+                                    "sample": "%d points of the timed batches over %d k-points, %.1f s"
+                                              % (nsamp, len(set(ids_run[sel].tolist())), dt),
+                                    "one_core": {"value": v1, "unit": "solves/s", "sample": "2 points, %.1f s" % dt1},
+                                    "full_grid_s": grid / v, "full_grid_points": grid}
             line["parity_sample"] = {"points": int(nsamp), "max_abs_dT": float(err.max()),
                                      "max_rel_dT_T_gt_1e-6": float((err / np.maximum(np.abs(Tc), 1e-300))[
                                          np.abs(Tc) > 1e-6].max()) if (np.abs(Tc) > 1e-6).any() else 0.0}
