@@ -211,6 +211,49 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
     return done / dt, T, dt
 
 
+def parity_summary(wl, devs, ids, E, Tg, Tc, cores, nworst=32):
+    """GPU vs oracle on the CPU-baseline sample, with the parity bound of the
+    tests: |dT| <= max(1e-10 |T|, 1e-13, 10 * spread), spread being the
+    oracle's own change under 1e-15 relative perturbations of the device
+    blocks, computed for the worst points (the eta = 1e-6 solve is
+    ill-conditioned at lead band edges)."""
+    import copy
+    from oracle import oracle as O
+    err = np.abs(Tg - Tc)
+    plain = np.maximum(1e-10 * np.abs(Tc), 1e-13)
+    out = {"points": int(E.size), "max_abs_dT": float(err.max()),
+           "within_1e-10_rel_or_1e-13_abs": int((err <= plain).sum())}
+    worst = [int(q) for q in np.argsort(-(err / plain))[:nworst] if err[q] > plain[q]]
+    if worst:
+        rng = np.random.default_rng(0)
+        spread = np.zeros(len(worst))
+        wq = np.asarray(worst)
+        for _ in range(2):
+            for k in sorted(set(ids[wq].tolist())):          # one call per k-point, OpenMP over its points
+                j = np.nonzero(ids[wq] == k)[0]
+                d = copy.deepcopy(devs[k])
+                for name in ("h_diag", "h_upper", "h_lower", "s_diag", "s_upper", "s_lower", "lead_h00", "lead_h01",
+                             "lead_s00", "lead_s01", "hmc", "smc"):
+                    lst = getattr(d, name)
+                    if lst is None:
+                        continue
+                    for i in range(len(lst)):
+                        lst[i] = lst[i] * (1.0 + 1e-15 * rng.standard_normal(lst[i].shape))
+                if wl["dos"]:
+                    t = O.transmission_dos(d, E[wq[j]], eta=wl["eta"], dos_delta=0.0, nthreads=cores)[0]
+                else:
+                    t = O.transmission(d, E[wq[j]], eta=wl["eta"], nthreads=cores)[0]
+                spread[j] = np.maximum(spread[j], np.abs(t - Tc[wq[j]]))
+        ok = [bool(err[q] <= max(plain[q], 10 * spread[j])) for j, q in enumerate(worst)]
+        out["beyond_1e-10"] = [{"E": float(E[q]), "T": float(Tc[q]), "abs_dT": float(err[q]),
+                                "oracle_spread": float(spread[j]), "within_spread_bound": ok[j]}
+                               for j, q in enumerate(worst)]
+        out["all_within_test_bound"] = bool(all(ok)) and len(worst) == int((err > plain).sum())
+    else:
+        out["all_within_test_bound"] = True
+    return out
+
+
 def run_serve(args):
     """Serving stream: requests arrive as a Poisson process; each draws a
     device from the c0 / c1 generators (layer count uniform in a range, block
@@ -489,9 +532,7 @@ def main():
                                               % (nsamp, len(set(ids_run[sel].tolist())), dt),
                                     "one_core": {"value": v1, "unit": "solves/s", "sample": "2 points, %.1f s" % dt1},
                                     "full_grid_s": grid / v, "full_grid_points": grid}
-            line["parity_sample"] = {"points": int(nsamp), "max_abs_dT": float(err.max()),
-                                     "max_rel_dT_T_gt_1e-6": float((err / np.maximum(np.abs(Tc), 1e-300))[
-                                         np.abs(Tc) > 1e-6].max()) if (np.abs(Tc) > 1e-6).any() else 0.0}
+            line["parity_sample"] = parity_summary(wl, devs, ids_run[sel], E_run[sel], Tgpu[sel], Tc, cores)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
