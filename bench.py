@@ -211,7 +211,7 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
     return done / dt, T, dt
 
 
-def parity_summary(wl, devs, ids, E, Tg, Tc, cores, nworst=32):
+def parity_summary(wl, devs, ids, E, Tg, Tc, cores, nworst=64):
     """GPU vs oracle on the CPU-baseline sample, with the parity bound of the
     tests: |dT| <= max(1e-10 |T|, 1e-13, 10 * spread), spread being the
     oracle's own change under 1e-15 relative perturbations of the device
@@ -245,9 +245,10 @@ def parity_summary(wl, devs, ids, E, Tg, Tc, cores, nworst=32):
                     t = O.transmission(d, E[wq[j]], eta=wl["eta"], nthreads=cores)[0]
                 spread[j] = np.maximum(spread[j], np.abs(t - Tc[wq[j]]))
         ok = [bool(err[q] <= max(plain[q], 10 * spread[j])) for j, q in enumerate(worst)]
-        out["beyond_1e-10"] = [{"E": float(E[q]), "T": float(Tc[q]), "abs_dT": float(err[q]),
-                                "oracle_spread": float(spread[j]), "within_spread_bound": ok[j]}
-                               for j, q in enumerate(worst)]
+        out["beyond_1e-10"] = int((err > plain).sum())
+        out["beyond_1e-10_within_10x_oracle_spread"] = int(sum(ok))
+        out["worst"] = [{"E": float(E[q]), "T": float(Tc[q]), "abs_dT": float(err[q]),
+                         "oracle_spread": float(spread[j])} for j, q in enumerate(worst[:4])]
         out["all_within_test_bound"] = bool(all(ok)) and len(worst) == int((err > plain).sum())
     else:
         out["all_within_test_bound"] = True
@@ -515,9 +516,10 @@ def main():
             # spread over the grid by the batch order
             tids, tE = ids_run[o:], E_run[o:]
             order = list(dict.fromkeys(tids.tolist()))
+            per_k = max(cores, nsamp // min(4, len(order)))
             picks = []
             for k in order:
-                picks.extend((o + np.nonzero(tids == k)[0][:cores]).tolist())
+                picks.extend((o + np.nonzero(tids == k)[0][:per_k]).tolist())
                 if len(picks) >= nsamp:
                     break
             sel = np.sort(np.asarray(picks[:nsamp], dtype=np.int64))
