@@ -38,6 +38,11 @@ WORKLOADS = {
     "c1": dict(nbl=100, n=256, nE=2048, emin=-2.0, emax=2.0, nk=16, eta=1e-6, dos=True, gen="c1"),
     "c0": dict(nbl=20, n=32, nE=512, emin=-3.0, emax=3.0, nk=1, eta=1e-6, dos=False, gen="c0"),
     "c2": dict(nbl=60, n=512, nE=1024, emin=-2.0, emax=2.0, nk=8, eta=1e-6, dos=False, gen="c1"),
+    # elastic-dephasing SCBA: dephasing coupling 0.1 eV (D = 0.01 eV^2) on every orbital, bias 0.2 eV
+    # symmetric, 300 K leads; linear mixing 0.5 until the contact-1 current changes by < 1e-8, at most
+    # 100 sweeps; one step = the whole 1024-point grid
+    "c3": dict(nbl=40, n=128, nE=1024, emin=-1.0, emax=1.0, nk=1, eta=1e-4, dos=False, gen="c0", pps=1024,
+               scba=dict(coupling=0.1, bias=0.2, temp_k=300.0, niter=100, tol=1e-8, mix=0.5, rule=1)),
     # small case of the c1 kernel for profiler captures (few GB on the device)
     "prof": dict(nbl=8, n=256, nE=256, emin=-2.0, emax=2.0, nk=1, eta=1e-6, dos=True, gen="c1"),
     # serving stream (Poisson arrivals of transmission / LDOS requests; see run_serve)
@@ -108,6 +113,39 @@ def flops_per_point(wl, ncyc_total, ncont=2):
     sweep = (80.0 / 3.0) * N * n3
     dos = 40.0 * (N - 1) * n3 if wl["dos"] else 0.0
     return dec + sig + sweep + dos + 32.0 * n3
+
+
+def scba_flops_per_point(wl, ncyc_total, sweeps, ncont=2):
+    """Algorithmic flops of one SCBA point (reference model): decimation and
+    self-energies once, then per SCBA sweep the gsmr sweep + Gr(1,1)
+    (80/3 N n^3), the retarded sweep (40 N n^3) and the lesser fold and
+    sweep (128 N n^3) (src/iterative.F90:289-363)."""
+    n, N = wl["n"], wl["nbl"]
+    n3 = float(n) ** 3
+    dec = (176.0 / 3.0) * n3 * ncyc_total + (32.0 / 3.0) * n3 * ncont
+    return dec + 16.0 * n3 * ncont + sweeps * (80.0 / 3.0 + 40.0 + 128.0) * N * n3
+
+
+def scba_executed_flops_per_point(wl, ncyc_total, sweeps, ncont=2):
+    """Flops the engine executes for one SCBA point, in units of one n x n x n
+    complex product or Gauss-Jordan inverse (8 n^3): per sweep 3N-2 for gsmr
+    and Gr(1,1), 5(N-1) for the retarded sweep, 4N-2 for the Sigma_n fold,
+    2 for Gn(1,1), 6(N-1) for the lesser sweep; then the currents."""
+    n, N = wl["n"], wl["nbl"]
+    u = 8.0 * n ** 3
+    per_sweep = (3 * N - 2) + 5 * (N - 1) + (4 * N - 2) + 2 + 6 * (N - 1)
+    return u * ((7.0 * ncyc_total - 3.0 * ncont) + 2 * ncont + sweeps * per_sweep + 2 * ncont + 2 * (N - 1))
+
+
+def scba_occupations(wl, E):
+    """Contact occupations of the SCBA workload, as meir_wingreen sets them
+    (src/integrations.F90:1883-1887): f_c = fermi(E, mu_c, kT), reference
+    occupation 0; mu = +-bias/2."""
+    from libnegf_b200.energy import fermi_f
+    sc = wl["scba"]
+    kT = 8.617333262e-5 * sc["temp_k"]          # eV
+    mu = (0.5 * sc["bias"], -0.5 * sc["bias"])
+    return np.ascontiguousarray(np.stack([fermi_f(E, mu[0], kT), fermi_f(E, mu[1], kT)], axis=1))
 
 
 def executed_flops_per_point(wl, ncyc_total, ncont=2):
@@ -197,10 +235,23 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
     from oracle import oracle as O
     O.lib()
     T = np.zeros(nsamp)
+    sc = wl.get("scba")
+    if sc:
+        out = {"curr": np.zeros((nsamp, 2)), "layer_dens": np.zeros((nsamp, wl["nbl"])),
+               "scba_iter": np.zeros(nsamp, dtype=np.int32)}
     t0 = time.perf_counter()
     done = 0
     for k in sorted(set(ids[:nsamp].tolist())):
         sel = np.nonzero(ids[:nsamp] == k)[0]
+        if sc:
+            r = O.meir_wingreen(devs[k], E[sel], scba_occupations(wl, E[sel]),
+                                coupling=np.full(devs[k].norb, sc["coupling"]), eta=wl["eta"],
+                                scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"],
+                                scba_rule=sc["rule"], nthreads=nthreads)
+            for key in out:
+                out[key][sel] = r[key]
+            done += sel.size
+            continue
         if wl["dos"]:
             t, _, _, _ = O.transmission_dos(devs[k], E[sel], eta=wl["eta"], dos_delta=0.0, nthreads=nthreads)
         else:
@@ -208,7 +259,49 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
         T[sel] = t
         done += sel.size
     dt = time.perf_counter() - t0
-    return done / dt, T, dt
+    return done / dt, (out if sc else T), dt
+
+
+def scba_parity_summary(wl, devs, ids, E, got, ref, cores):
+    """GPU vs oracle SCBA outputs on the CPU-baseline sample, with the bound
+    of the tests: |d| <= max(1e-10 max(1, max|ref|), 10 * spread), spread
+    being the oracle's own change under 1e-15 relative perturbations of the
+    device blocks (computed only when some point exceeds 1e-10)."""
+    import copy
+    from oracle import oracle as O
+    out = {"points": int(E.size),
+           "scba_sweeps_equal_or_off_by_one": int((np.abs(got["scba_iter"] - ref["scba_iter"]) <= 1).sum())}
+    spread = None
+    ok = True
+    for key in ("curr", "layer_dens"):
+        err = np.abs(got[key] - ref[key])
+        scale = max(1.0, float(np.abs(ref[key]).max()))
+        out[key] = {"max_abs_diff": float(err.max()), "scale": scale,
+                    "within_1e-10_of_scale": bool(err.max() <= 1e-10 * scale)}
+        if err.max() > 1e-10 * scale:
+            if spread is None:
+                sc = wl["scba"]
+                rng = np.random.default_rng(0)
+                spread = {k2: np.zeros_like(ref[k2]) for k2 in ("curr", "layer_dens")}
+                for k in sorted(set(ids.tolist())):
+                    j = np.nonzero(ids == k)[0]
+                    d = copy.deepcopy(devs[k])
+                    for name in ("h_diag", "h_upper", "h_lower", "lead_h00", "lead_h01", "hmc"):
+                        lst = getattr(d, name)
+                        for i in range(len(lst)):
+                            lst[i] = lst[i] * (1.0 + 1e-15 * rng.standard_normal(lst[i].shape))
+                    r = O.meir_wingreen(d, E[j], scba_occupations(wl, E[j]),
+                                        coupling=np.full(d.norb, sc["coupling"]), eta=wl["eta"],
+                                        scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"],
+                                        scba_rule=sc["rule"], nthreads=cores)
+                    for k2 in spread:
+                        spread[k2][j] = np.abs(r[k2] - ref[k2][j])
+            okk = bool(np.all(err <= np.maximum(1e-10 * scale, 10 * spread[key])))
+            out[key]["within_10x_oracle_spread"] = okk
+            out[key]["max_oracle_spread"] = float(spread[key].max())
+            ok = ok and okk
+    out["all_within_test_bound"] = ok
+    return out
 
 
 def parity_summary(wl, devs, ids, E, Tg, Tc, cores, nworst=64):
@@ -330,7 +423,7 @@ def run_reference(args, wl, rank, world):
     devs, _ = devices_for(wl)
     ids, E = point_list(wl)
     cores = os.cpu_count() or 1
-    nsamp = args.cpu_sample or max(cores, 8) * (1 if wl["n"] >= 256 else 8)
+    nsamp = args.cpu_sample or max(cores, 8) * (1 if wl["n"] >= 256 or wl.get("scba") else 8)
     vals = []
     for s in range(args.warmup + args.steps):
         k0 = ids[s % ids.size]
@@ -354,6 +447,18 @@ def run_reference(args, wl, rank, world):
 
 
 def config_of(args, wl, pts):
+    sc = wl.get("scba")
+    if sc:
+        return {"workload": "transport_%s: elastic-dephasing SCBA, N=%d PLs x n=%d (c0 generator), complex128, "
+                            "%d energies on [%g, %g] eV, dephasing coupling %g eV (D = %g eV^2) on every orbital, "
+                            "bias %g eV, %g K; Meir-Wingreen currents, layer currents and densities"
+                            % (args.workload, wl["nbl"], wl["n"], wl["nE"], wl["emin"], wl["emax"], sc["coupling"],
+                               sc["coupling"] ** 2, sc["bias"], sc["temp_k"]),
+                "points_per_step": pts, "eta": wl["eta"], "sgf_tol": 1e-9,
+                "scba_rule": ("linear mixing %g, stop when the contact-1 current changes by < %g, at most %d sweeps"
+                              % (sc["mix"], sc["tol"], sc["niter"])) if sc["rule"] == 1 else
+                             ("mixing %g, max|dGn| < %g, at most %d sweeps" % (sc["mix"], sc["tol"], sc["niter"])),
+                "l2": "inputs and workspace larger than L2 (126 MB)", "parallelism": "dp%d (E shards)" % args.gpus}
     return {"workload": "transport_%s: N=%d PLs x n=%d, complex128, %d energies x %d k-points%s" % (
         args.workload, wl["nbl"], wl["n"], wl["nE"], wl["nk"], ", T(E,k) + diagonal DOS" if wl["dos"] else
         ", T(E,k)"), "points_per_step": pts, "eta": wl["eta"], "sgf_tol": 1e-9,
@@ -395,7 +500,7 @@ def main():
     dids = [ctx.upload(d) for d in devs]
     norb = devs[0].norb
     sms = torch.cuda.get_device_properties(local).multi_processor_count
-    P = args.points_per_step or 4 * sms
+    P = args.points_per_step or wl.get("pps") or 4 * sms
     nsteps = args.warmup + args.steps
     need = P * nsteps
     reps = int(np.ceil(need / ids_r.size))
@@ -409,10 +514,29 @@ def main():
     d_st = torch.zeros(need, dtype=torch.int32, device="cuda")
     stream = torch.cuda.Stream()          # a real stream: NULL would mean the context's own stream
     sh = ctypes.c_void_p(stream.cuda_stream)
+    sc = wl.get("scba")
+    nbl = devs[0].nbl
+    if sc:
+        ctx.set_options(scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"], scba_rule=sc["rule"])
+        frm_run = scba_occupations(wl, E_run)
+        cpl = np.full(norb, sc["coupling"])
+        d_frm = torch.from_numpy(frm_run).cuda()
+        d_cpl = torch.from_numpy(cpl).cuda()
+        d_curr = torch.zeros((need, 2), dtype=torch.float64, device="cuda")
+        d_lcurr = torch.zeros((need, nbl), dtype=torch.float64, device="cuda")
+        d_ldens = torch.zeros((need, nbl), dtype=torch.float64, device="cuda")
+        d_it = torch.zeros(need, dtype=torch.int32, device="cuda")
+        d_err = torch.zeros(need, dtype=torch.float64, device="cuda")
 
     def step(s):
         o = s * P
-        if wl["dos"]:
+        if sc:
+            rc = L.negf_b200_meir_wingreen_dev(
+                ctx.handle, P, d_ids.data_ptr() + 4 * o, d_E.data_ptr() + 8 * o, wl["eta"],
+                d_frm.data_ptr() + 16 * o, d_cpl.data_ptr(), d_curr.data_ptr() + 16 * o,
+                d_lcurr.data_ptr() + 8 * nbl * o, d_ldens.data_ptr() + 8 * nbl * o, d_it.data_ptr() + 4 * o,
+                d_err.data_ptr() + 8 * o, d_nc.data_ptr() + 4 * o, d_st.data_ptr() + 4 * o, 2, nbl, sh)
+        elif wl["dos"]:
             rc = L.negf_b200_transmission_dos_dev(
                 ctx.handle, P, d_ids.data_ptr() + 4 * o, d_E.data_ptr() + 8 * o, wl["eta"], 0.0, 1, 2,
                 d_T.data_ptr() + 8 * o, d_dos.data_ptr(), norb, d_nc.data_ptr() + 4 * o, d_st.data_ptr() + 4 * o, sh)
@@ -457,8 +581,16 @@ def main():
     nc = d_nc.cpu().numpy()
     Tgpu = d_T.cpu().numpy()
     timed = slice(args.warmup * P, nsteps * P)
-    flops = float(sum(flops_per_point(wl, int(c)) for c in nc[timed]))
-    flops_exec = float(sum(executed_flops_per_point(wl, int(c)) for c in nc[timed]))
+    if sc:
+        sweeps = d_it.cpu().numpy()
+        curr_g = d_curr.cpu().numpy()
+        ldens_g = d_ldens.cpu().numpy()
+        flops = float(sum(scba_flops_per_point(wl, int(c), int(k)) for c, k in zip(nc[timed], sweeps[timed])))
+        flops_exec = float(sum(scba_executed_flops_per_point(wl, int(c), int(k))
+                               for c, k in zip(nc[timed], sweeps[timed])))
+    else:
+        flops = float(sum(flops_per_point(wl, int(c)) for c in nc[timed]))
+        flops_exec = float(sum(executed_flops_per_point(wl, int(c)) for c in nc[timed]))
     points_total = args.steps * P * world
     value = points_total / (ms * 1e-3)
 
@@ -471,7 +603,10 @@ def main():
     t0 = time.perf_counter()
     for j in range(e2e_steps):
         o = (args.warmup + j % args.steps) * P
-        if wl["dos"]:
+        if sc:
+            ctx.meir_wingreen(h_ids[o:o + P], E_run[o:o + P], frm_run[o:o + P], coupling=cpl, eta=wl["eta"],
+                              check=False)
+        elif wl["dos"]:
             ctx.transmission_dos(h_ids[o:o + P], E_run[o:o + P], eta=wl["eta"], dos_delta=0.0, check=False)
         else:
             ctx.transmission(h_ids[o:o + P], E_run[o:o + P], eta=wl["eta"], check=False)
@@ -479,8 +614,12 @@ def main():
     if dist:
         e2e_s = max_over_ranks(e2e_s, dist)
     e2e = e2e_steps * P * world / e2e_s
-    h2d = P * (4 + 8)
-    d2h = P * (8 + 4 + 4 + (8 * norb if wl["dos"] else 0))
+    if sc:
+        h2d = P * (4 + 8 + 16) + 8 * norb
+        d2h = P * (16 + 8 * (nbl - 1) + 8 * nbl + 4 + 8 + 4 + 4)
+    else:
+        h2d = P * (4 + 8)
+        d2h = P * (8 + 4 + 4 + (8 * norb if wl["dos"] else 0))
 
     if rank == 0:
         achieved = flops / (ms * 1e-3) / 1e12 / 1.0
@@ -505,11 +644,14 @@ def main():
             "ncyc_mean": float(nc[timed].mean()),
             "step_ms": per_step,
         }
+        if sc:
+            line["scba_sweeps_mean"] = float(sweeps[timed].mean())
+            line["scba_sweeps_max"] = int(sweeps[timed].max())
         if trace:
             line["trace_phase_share"] = trace
         if world == 1 and not args.no_cpu_baseline:
             cores = os.cpu_count() or 1
-            nsamp = args.cpu_sample or (max(64, cores) if wl["n"] >= 256 else 8 * max(64, cores))
+            nsamp = args.cpu_sample or (cores if sc else max(64, cores) if wl["n"] >= 256 else 8 * max(64, cores))
             o = args.warmup * P
             # points of the timed batches, grouped by k-point so that OpenMP spreads each call over
             # every host core: up to `cores` points of each of the first k-points met, energies
@@ -525,16 +667,21 @@ def main():
             sel = np.sort(np.asarray(picks[:nsamp], dtype=np.int64))
             nsamp = sel.size
             v, Tc, dt = cpu_baseline(wl, devs, ids_run[sel], E_run[sel], nsamp, cores)
-            # one host core: two of the same points, single-threaded
-            v1, _, dt1 = cpu_baseline(wl, devs, ids_run[sel[:2]], E_run[sel[:2]], 2, 1)
-            err = np.abs(Tgpu[sel] - Tc)
+            # one host core: one or two of the same points, single-threaded
+            n1 = 1 if sc else 2
+            v1, _, dt1 = cpu_baseline(wl, devs, ids_run[sel[:n1]], E_run[sel[:n1]], n1, 1)
             grid = wl["nE"] * wl["nk"]
             line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
                                     "sample": "%d points of the timed batches over %d k-points, %.1f s"
                                               % (nsamp, len(set(ids_run[sel].tolist())), dt),
-                                    "one_core": {"value": v1, "unit": "solves/s", "sample": "2 points, %.1f s" % dt1},
+                                    "one_core": {"value": v1, "unit": "solves/s",
+                                                 "sample": "%d points, %.1f s" % (n1, dt1)},
                                     "full_grid_s": grid / v, "full_grid_points": grid}
-            line["parity_sample"] = parity_summary(wl, devs, ids_run[sel], E_run[sel], Tgpu[sel], Tc, cores)
+            if sc:
+                got = {"curr": curr_g[sel], "layer_dens": ldens_g[sel], "scba_iter": sweeps[sel]}
+                line["parity_sample"] = scba_parity_summary(wl, devs, ids_run[sel], E_run[sel], got, Tc, cores)
+            else:
+                line["parity_sample"] = parity_summary(wl, devs, ids_run[sel], E_run[sel], Tgpu[sel], Tc, cores)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

@@ -97,6 +97,7 @@ typedef struct negf_b200_device {
  *   sgf_max_iter = 300               src/contselfenergy.F90:289
  *   eps_drop = 0 (EPS is never set inside libNEGF, src/ln_precision.F90:36)
  *   scba_tol = 1e-7                  src/lib_param.F90:653
+ *   scba_mix = 1, scba_rule = 0      (no mixing, the Gn convergence check)
  */
 typedef struct negf_b200_options {
   double sgf_tol;
@@ -108,6 +109,16 @@ typedef struct negf_b200_options {
   int32_t precision;
   /* Resident CTAs per SM for the persistent point engine (0 = auto). */
   int32_t ctas_per_sm;
+  /* Elastic SCBA mixing and stopping rule.  scba_mix = 1 (default) is the
+   * reference: the dephasing self-energies are overwritten by D diag(G)
+   * each sweep (src/elphdd.F90:108-156, 227-276).  0 < scba_mix < 1 is
+   * linear mixing from Sigma = 0: Sigma <- mix D diag(G) + (1-mix) Sigma.
+   * scba_rule = 0 (default) stops when max |Gn - Gn_old| on the S pattern
+   * is below scba_tol (src/scba.F90:120-147); scba_rule = 1 stops when the
+   * Meir-Wingreen current of contact 1 changes by less than scba_tol
+   * between sweeps.  Neither alternative exists in the reference. */
+  double scba_mix;
+  int32_t scba_rule;
 } negf_b200_options;
 
 typedef struct negf_b200_ctx negf_b200_ctx;
@@ -301,6 +312,23 @@ int negf_b200_transmission_dos_dev(negf_b200_ctx* ctx, int32_t npts,
                                    double* d_T, double* d_dos,
                                    int64_t dos_stride, int32_t* d_ncyc,
                                    int32_t* d_status, void* stream);
+/* negf_b200_meir_wingreen on device buffers (the SCBA energy loop of
+ * meir_wingreen, src/integrations.F90:1855-1930, with every per-point array
+ * in HBM).  Row strides: d_frm and d_curr rows hold cont_stride doubles,
+ * d_layer_curr and d_layer_dens rows hold layer_stride doubles (at least
+ * the largest ncont / nbl over the uploaded devices; every uploaded device
+ * needs nbl >= 2).  d_device_id, d_energy, d_frm, d_scba_iter, d_scba_err
+ * and d_status are required; d_coupling (no dephasing), d_curr,
+ * d_layer_curr, d_layer_dens and d_ncyc may be NULL. */
+int negf_b200_meir_wingreen_dev(negf_b200_ctx* ctx, int32_t npts,
+                                const int32_t* d_device_id,
+                                const double* d_energy, double eta,
+                                const double* d_frm, const double* d_coupling,
+                                double* d_curr, double* d_layer_curr,
+                                double* d_layer_dens, int32_t* d_scba_iter,
+                                double* d_scba_err, int32_t* d_ncyc,
+                                int32_t* d_status, int32_t cont_stride,
+                                int32_t layer_stride, void* stream);
 
 /* ---- tracing ---------------------------------------------------------------
  * libNEGF times phases with a stack of host wall clocks (src/clock.F90:35-93,

@@ -228,6 +228,8 @@ negf::EngineArgs base_args(negf_b200_ctx* ctx, int mode, int npts) {
   a.eps = ctx->opt.eps_drop;
   a.scba_niter = ctx->opt.scba_niter;
   a.scba_tol = ctx->opt.scba_tol;
+  a.scba_mix = ctx->opt.scba_mix;
+  a.scba_rule = ctx->opt.scba_rule;
   return a;
 }
 
@@ -332,6 +334,8 @@ void negf_b200_default_options(negf_b200_options* o) {
   o->scba_niter = 0;
   o->precision = 0;
   o->ctas_per_sm = 0;
+  o->scba_mix = 1.0;
+  o->scba_rule = 0;
 }
 
 const char* negf_b200_version(void) { return "negf_b200 0.1 (sm_100a, complex FP64)"; }
@@ -383,6 +387,8 @@ int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* o) {
       o->ctas_per_sm > 2)
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "invalid options");
   if (o->precision != 0) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "only precision 0 (complex FP64) is built");
+  if (!(o->scba_mix > 0.0 && o->scba_mix <= 1.0) || (o->scba_rule != 0 && o->scba_rule != 1))
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "scba_mix must be in (0, 1] and scba_rule 0 or 1");
   ctx->opt = *o;
   return NEGF_B200_OK;
 }
@@ -1034,6 +1040,35 @@ int negf_b200_transmission_dos_dev(negf_b200_ctx* ctx, int32_t npts, const int32
   negf::EngineArgs a = base_args(ctx, negf::MODE_DOS, npts);
   a.dev_id = d_device_id; a.energy = d_energy; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
   a.T = d_T; a.dos = d_dos; a.dos_stride = dos_stride; a.ncyc = d_ncyc; a.status = d_status;
+  return run_device(ctx, a, sh, stream ? (cudaStream_t)stream : ctx->stream);
+}
+
+int negf_b200_meir_wingreen_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_device_id,
+                                const double* d_energy, double eta, const double* d_frm,
+                                const double* d_coupling, double* d_curr, double* d_layer_curr,
+                                double* d_layer_dens, int32_t* d_scba_iter, double* d_scba_err, int32_t* d_ncyc,
+                                int32_t* d_status, int32_t cont_stride, int32_t layer_stride, void* stream) {
+  if (!ctx || npts < 0) return NEGF_B200_ERR_BAD_ARG;
+  if (npts == 0) return NEGF_B200_OK;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  if (!d_device_id || !d_energy || !d_frm || !d_scba_iter || !d_scba_err || !d_status)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "device_id, energy, frm, scba_iter, scba_err and status are required");
+  LaunchShape sh;
+  int st = shape_of(ctx, npts, nullptr, sh);
+  if (st) return st;
+  for (const DeviceRec& r : ctx->devs)
+    if (r.live && r.nbl < 2) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the Gn solve needs nbl >= 2 on every device");
+  if (cont_stride < sh.ncont_max || layer_stride < sh.nbl_max)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "cont_stride / layer_stride below the largest ncont / nbl");
+  negf::EngineArgs a = base_args(ctx, negf::MODE_GN, npts);
+  a.dev_id = d_device_id; a.energy = d_energy; a.eta = eta; a.ni = 1; a.nf = 2;
+  a.ncyc = d_ncyc; a.status = d_status;
+  a.frm = d_frm; a.frm_stride = cont_stride; a.coupling = d_coupling;
+  a.curr = d_curr; a.curr_stride = cont_stride;
+  a.lcurr = d_layer_curr; a.lcurr_stride = layer_stride;
+  a.ldens = d_layer_dens; a.ldens_stride = layer_stride;
+  a.scba_iter = d_scba_iter; a.scba_err = d_scba_err;
   return run_device(ctx, a, sh, stream ? (cudaStream_t)stream : ctx->stream);
 }
 

@@ -78,6 +78,7 @@ struct EngineArgs {
   const double* frm; int frm_stride;
   const double* coupling;       // norb (unsquared) or null
   int scba_niter; double scba_tol;
+  double scba_mix; int scba_rule;  // linear mixing factor (1 = overwrite), stopping rule (0 Gn, 1 current)
   double* curr; int curr_stride;
   double* lcurr; int lcurr_stride;
   double* ldens; int ldens_stride;

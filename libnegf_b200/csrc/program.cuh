@@ -102,7 +102,7 @@ enum OpKind : int {
   K_TRACEC,    // res[slot], res[slot+1] = Tr(A op(B)), A m x n
   K_TRACEN,    // res[slot] = Re Tr(A B^dag), A and B m x n (rows k with mask[k], if mask)
   K_DOS,       // out[k] = -Im A_kk / pi, k < m
-  K_SIGDIAG,   // C[k] = cpl[k]^2 A_kk, k < m
+  K_SIGDIAG,   // C[k] = cpl[k]^2 A_kk, k < m; flag 1: scal cpl^2 A_kk + (1-scal) C[k]; flag 2: scal cpl^2 A_kk
   K_SNINIT,    // C (m x m) = diag(A) or 0
   K_SNGAMMA,   // C += scal * i (A - A^dag), order m
   K_DAGGER,    // C (m x n) = A^dag, A is n x m
@@ -218,7 +218,10 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
     case K_SIGDIAG:
       for (int k = tid; k < o.m; k += blockDim.x) {
         const double c = o.cpl[k];
-        o.C[k] = cscale(c * c, o.A[(size_t)k * (o.m + 1)]);
+        const double2 v = cscale(c * c, o.A[(size_t)k * (o.m + 1)]);
+        if (o.flag == 0) o.C[k] = v;
+        else if (o.flag == 1) o.C[k] = cadd(cscale(o.scal, v), cscale(1.0 - o.scal, o.C[k]));
+        else o.C[k] = cscale(o.scal, v);
       }
       break;
     case K_SNINIT:
@@ -328,7 +331,7 @@ struct Prog {
   double T;
   // SCBA
   int sit, conv, have_old, par;
-  double err;
+  double err, iold;     // SCBA error; contact-1 current of the previous sweep (scba_rule 1)
   double2* vec;
 };
 
@@ -762,6 +765,8 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           for (s.i = 0; s.i < s.d->nbl; ++s.i) {
             set_simple(o, K_SIGDIAG, s.d->pl[s.i], w.layer(1, s.i, s.d->nbl), s.vec + s.d->pstart[s.i]);
             o.cpl = a.coupling + s.d->pstart[s.i];
+            o.scal = a.scba_mix;
+            o.flag = (a.scba_mix == 1.0) ? 0 : (s.sit > 0 ? 1 : 2);   // linear mixing from sigma = 0
             PT_EMIT(s);
           }
         // Sigma_n(i,i) = dephasing (it > 0) + contacts (f_c - f_ref) Gam_c, f_ref = 0
@@ -844,7 +849,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         if (threadIdx.x == 0) sm.res[1] = 0.0;
         __syncthreads();
         for (s.i = 0; s.i < s.d->nbl; ++s.i) {
-          if (s.have_old) {
+          if (s.have_old && a.scba_rule == 0) {
             if (!s.d->has_s) {
               o.kind = K_ERRDIAG; o.m = s.d->pl[s.i]; o.A = w.layer(4 + s.par, s.i, s.d->nbl);
               o.B = w.layer(4 + (s.par ^ 1), s.i, s.d->nbl); o.slot = 1;
@@ -865,10 +870,34 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
             set_simple(o, K_SIGDIAG, s.d->pl[s.i], w.layer(4 + s.par, s.i, s.d->nbl),
                        s.vec + s.d->norb + s.d->pstart[s.i]);
             o.cpl = a.coupling + s.d->pstart[s.i];
+            o.scal = a.scba_mix;
+            o.flag = (a.scba_mix == 1.0) ? 0 : (s.sit > 0 ? 1 : 2);
             PT_EMIT(s);
           }
         }
-        if (s.have_old) {
+        if (a.scba_rule == 1) {
+          // stopping rule 1: change of the contact-1 Meir-Wingreen current between sweeps
+          // (the formula of the final currents below; Gam slot 7, A slot 8)
+          set_simple(o, K_SPECTRAL, s.d->pl[s.d->cblk[0] - 1], w.sig(0), w.slot(7));
+          PT_EMIT(s);
+          set_simple(o, K_SPECTRAL, s.d->pl[s.d->cblk[0] - 1], w.layer(1, s.d->cblk[0] - 1, s.d->nbl), w.slot(8));
+          PT_EMIT(s);
+          o.kind = K_TRACE; o.m = s.d->pl[s.d->cblk[0] - 1]; o.A = w.slot(7);
+          o.B = w.layer(4 + s.par, s.d->cblk[0] - 1, s.d->nbl); o.opb = OP_N; o.slot = 2; o.mask = nullptr;
+          PT_EMIT(s);
+          o.kind = K_TRACE; o.m = s.d->pl[s.d->cblk[0] - 1]; o.A = w.slot(7); o.B = w.slot(8); o.opb = OP_N;
+          o.slot = 3; o.mask = nullptr;
+          PT_EMIT(s);
+          {
+            const double icur = -(sm.res[2] - a.frm[(int64_t)s.p * a.frm_stride] * sm.res[3]);
+            if (s.have_old) {
+              s.err = fabs(icur - s.iold);
+              s.conv = s.err < a.scba_tol;
+            }
+            s.iold = icur;
+          }
+          __syncthreads();
+        } else if (s.have_old) {
           s.err = sm.res[1];
           s.conv = s.err < a.scba_tol;
         }

@@ -33,7 +33,7 @@ EXPORTED = [
     "negf_b200_decimation_work_bytes", "negf_b200_decimation_batched", "negf_b200_set_tracing",
     "negf_b200_get_trace", "negf_b200_decimation_noalloc", "negf_b200_set_tun_proj", "negf_b200_set_dos_proj",
     "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
-    "negf_b200_set_workspace_limit", "negf_b200_density", "negf_b200_density_neq",
+    "negf_b200_set_workspace_limit", "negf_b200_density", "negf_b200_density_neq", "negf_b200_meir_wingreen_dev",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -48,7 +48,7 @@ class Options(ctypes.Structure):
     """Mirror of negf_b200_options."""
     _fields_ = [("sgf_tol", ctypes.c_double), ("sgf_max_iter", ctypes.c_int32), ("eps_drop", ctypes.c_double),
                 ("scba_tol", ctypes.c_double), ("scba_niter", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32)]
+                ("ctas_per_sm", ctypes.c_int32), ("scba_mix", ctypes.c_double), ("scba_rule", ctypes.c_int32)]
 
 
 _lib = None
@@ -81,6 +81,7 @@ def load():
     L.negf_b200_transmission_dev.argtypes = [vp, i32, vp, vp, f64, i32, i32, vp, vp, vp, vp]
     L.negf_b200_transmission_dos_dev.argtypes = [vp, i32, vp, vp, f64, f64, i32, i32, vp, vp, ctypes.c_int64,
                                                  vp, vp, vp]
+    L.negf_b200_meir_wingreen_dev.argtypes = [vp, i32, vp, vp, f64, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp]
     L.negf_b200_zgemm_batched.argtypes = [i32, i32, i32, i32, dp, vp, ctypes.c_int64, vp, ctypes.c_int64, dp, vp,
                                           ctypes.c_int64, i32, vp]
     L.negf_b200_zinv_work_bytes.restype = ctypes.c_size_t

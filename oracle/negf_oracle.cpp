@@ -479,6 +479,11 @@ struct Opts {
   double sgf_acc = 1e-9;
   int max_iter = 300;
   double eps = 0.0;
+  // SCBA variants of the engine (not in the reference): linear mixing factor of the
+  // dephasing self-energies (1 = overwrite, the reference) and stopping rule
+  // (0 = max |dGn| on the S pattern, the reference; 1 = change of the contact-1 current)
+  double scba_mix = 1.0;
+  int scba_rule = 0;
 };
 
 // calculate_transmissions (src/iterative.F90:1669-1780) after
@@ -735,6 +740,23 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
   if (coupling)
     for (int q = 0; q < D.norb; ++q) D2[q] = coupling[q] * coupling[q];
   std::vector<cplx> sigma_r(D.norb, cplx(0.0, 0.0)), sigma_n(D.norb, cplx(0.0, 0.0));
+  const double mix = o.scba_mix;
+  // sigma <- D diag(G), or linear mixing from sigma = 0
+  auto update = [&](cplx& sig, cplx g, double d2) {
+    const cplx v = g * d2;
+    sig = (mix == 1.0) ? v : mix * v + (1.0 - mix) * sig;
+  };
+  // iterative_meir_wingreen (src/iterative.F90:382-414) for contact c
+  auto mw_current = [&](int c, const GrBlocks& Gr, const Trid& Gn) {
+    int cb = D.cblk[c] - 1;
+    Dns Gam, A, work1;
+    spectral(Sig[c], Gam);
+    mult(Gam, Gn.d[cb], work1);
+    spectral(Gr.d[cb], A);
+    mult(Gam, A, work1, cplx(-frm_ext[c], 0.0));
+    return -std::real(trace(work1));
+  };
+  double iold = 0.0;
   // Mat_old pattern: S nonzeros inside the tridiagonal device blocks
   std::vector<cplx> old;
   bool have_old = false, converged = false;
@@ -755,7 +777,7 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
     if (coupling && it <= niter)
       for (int i = 0; i < nbl; ++i)
         for (int k = 0; k < D.n[i]; ++k)
-          sigma_r[D.start[i] + k] = Gr.d[i].at(k, k) * D2[D.start[i] + k];
+          update(sigma_r[D.start[i] + k], Gr.d[i].at(k, k), D2[D.start[i] + k]);
     Trid Sn;
     init_trid_zero(Sn, ESH);
     if (it > 0 && coupling)
@@ -766,7 +788,7 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
     if (coupling && it <= niter)
       for (int i = 0; i < nbl; ++i)
         for (int k = 0; k < D.n[i]; ++k)
-          sigma_n[D.start[i] + k] = Gn.d[i].at(k, k) * D2[D.start[i] + k];
+          update(sigma_n[D.start[i] + k], Gn.d[i].at(k, k), D2[D.start[i] + k]);
     // blk2csr(Gn) on the S pattern + check_Mat_convergence
     std::vector<cplx> cur;
     for (int i = 0; i < nbl; ++i) {
@@ -781,7 +803,14 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
           if (D.Sl[i].v[q] != cplx(0.0, 0.0)) cur.push_back(Gn.l[i].v[q]);
       }
     }
-    if (have_old) {
+    if (o.scba_rule == 1) {
+      const double icur = mw_current(0, Gr, Gn);
+      if (have_old) {
+        so.err = std::abs(icur - iold);
+        converged = so.err < tol;
+      }
+      iold = icur;
+    } else if (have_old) {
       double e = 0.0;
       for (size_t q = 0; q < cur.size(); ++q) e = std::max(e, std::abs(cur[q] - old[q]));
       so.err = e;
@@ -794,17 +823,8 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
   so.iters = it;
   if (gn_out) *gn_out = Gn;
   // iterative_meir_wingreen (src/iterative.F90:382-414)
-  if (curr) {
-    for (int c = 0; c < ncont; ++c) {
-      int cb = D.cblk[c] - 1;
-      Dns Gam, A, work1;
-      spectral(Sig[c], Gam);
-      mult(Gam, Gn.d[cb], work1);
-      spectral(Gr.d[cb], A);
-      mult(Gam, A, work1, cplx(-frm_ext[c], 0.0));
-      curr[c] = -std::real(trace(work1));
-    }
-  }
+  if (curr)
+    for (int c = 0; c < ncont; ++c) curr[c] = mw_current(c, Gr, Gn);
   // iterative_layer_current (src/iterative.F90:427-461): ES-H without Sigma
   if (lcurr || ldens) {
     Trid E0;
@@ -1033,7 +1053,7 @@ int oracle_density(const negf_b200_device* dev, int npts, const double* e_re, co
 int oracle_meir_wingreen(const negf_b200_device* dev, int npts,
                          const double* energy, double eta, const double* frm,
                          const double* coupling, int scba_niter,
-                         double scba_tol, double sgf_tol, int sgf_max_iter,
+                         double scba_tol, double scba_mix, int scba_rule, double sgf_tol, int sgf_max_iter,
                          double eps, double* curr, double* lcurr,
                          double* ldens, int* scba_iter, double* scba_err,
                          int* ncyc, int* status, int nthreads) {
@@ -1041,6 +1061,7 @@ int oracle_meir_wingreen(const negf_b200_device* dev, int npts,
   DeviceBlocks D = unpack(dev);
   Opts o;
   o.sgf_acc = sgf_tol; o.max_iter = sgf_max_iter; o.eps = eps;
+  o.scba_mix = scba_mix; o.scba_rule = scba_rule;
   int nbl = D.nbl, ncont = D.ncont;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int p = 0; p < npts; ++p) {

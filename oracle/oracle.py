@@ -39,7 +39,8 @@ def lib():
                                               ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                               ctypes.c_double, dp, dp, ip, ip, ctypes.c_int]
         L.oracle_meir_wingreen.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, dp, dp, ctypes.c_int,
-                                           ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_double, ctypes.c_int, ctypes.c_double,
                                            dp, dp, dp, ip, dp, ip, ip, ctypes.c_int]
         L.oracle_transmissions.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                            ip, ip, vp, ctypes.c_int, ip, ip, ctypes.c_double, ctypes.c_int,
@@ -198,7 +199,11 @@ def density_neq(dev: Device, energies, w, frm, eta=1e-4, coupling=None, scba_nit
 
 
 def meir_wingreen(dev: Device, energies, frm, coupling=None, eta=1e-4, scba_niter=5, scba_tol=1e-7,
-                  sgf_tol=1e-9, sgf_max_iter=300, eps=0.0, nthreads=0):
+                  sgf_tol=1e-9, sgf_max_iter=300, eps=0.0, nthreads=0, scba_mix=1.0, scba_rule=0):
+    """meir_wingreen + layer_current with the elastic SCBA per point.  The
+    defaults are the reference rule (no mixing, max |dGn| < scba_tol);
+    scba_mix < 1 mixes the dephasing self-energies linearly from zero and
+    scba_rule = 1 stops on the change of the contact-1 current instead."""
     E = np.ascontiguousarray(energies, dtype=np.float64)
     npts = E.size
     frm = np.ascontiguousarray(np.broadcast_to(frm, (npts, dev.ncont)), dtype=np.float64)
@@ -214,7 +219,7 @@ def meir_wingreen(dev: Device, energies, frm, coupling=None, eta=1e-4, scba_nite
     st = dev.to_struct()
     lib().oracle_meir_wingreen(ctypes.addressof(st), npts, _d(E), eta, _d(frm),
                                _d(cp) if cp is not None else ctypes.POINTER(ctypes.c_double)(),
-                               scba_niter, scba_tol, sgf_tol, sgf_max_iter, eps,
+                               scba_niter, scba_tol, scba_mix, scba_rule, sgf_tol, sgf_max_iter, eps,
                                _d(curr), _d(lcurr), _d(ldens), _i(it), _d(err), _i(ncyc), _i(status), nthreads)
     return dict(curr=curr, layer_curr=lcurr[:, :dev.nbl - 1], layer_dens=ldens, scba_iter=it,
                 scba_err=err, ncyc=ncyc, status=status)

@@ -32,6 +32,7 @@ def test_version_and_defaults():
     o = native.Options()
     native.load().negf_b200_default_options(ctypes.byref(o))
     assert o.sgf_tol == 1e-9 and o.sgf_max_iter == 300 and o.scba_tol == 1e-7 and o.eps_drop == 0.0
+    assert o.scba_mix == 1.0 and o.scba_rule == 0
 
 
 def test_no_gpu_is_an_error_not_a_fallback():

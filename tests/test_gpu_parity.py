@@ -208,8 +208,9 @@ def test_multi_device_batch(gpu_ctx):
         gpu_ctx.release(i2)
 
 
-@pytest.mark.parametrize("case", ["elph", "c0_deph", "c1_S_deph"])
+@pytest.mark.parametrize("case", ["elph", "c0_deph", "c1_S_deph", "c0_mix_current_rule", "c1_S_mix"])
 def test_meir_wingreen_parity(gpu_ctx, case):
+    mix, rule, niter, tol = 1.0, 0, 5, 1e-7
     if case == "elph":
         dev = G.chain(10, 6, cblk=[6, 1])
         E = np.arange(-2.0, 2.0 + 1e-9, 0.1)
@@ -220,22 +221,83 @@ def test_meir_wingreen_parity(gpu_ctx, case):
         E = np.linspace(-1, 1, 7)
         cpl = np.full(dev.norb, 0.1)
         frm = np.stack([[0.9, 0.2]] * len(E))
+    elif case == "c0_mix_current_rule":
+        # the elastic-dephasing workload's rule: mixing 0.5, stop on a current change below 1e-8
+        dev = G.transport_c0(nbl=6, n=8, seed=3)
+        E = np.linspace(-1, 1, 9)
+        cpl = np.full(dev.norb, 0.1)
+        frm = np.stack([[0.9, 0.2]] * len(E))
+        mix, rule, niter, tol = 0.5, 1, 40, 1e-8
+    elif case == "c1_S_mix":
+        dev = G.transport_c1(nbl=4, n=10, seed=4, density=0.3)
+        E = np.linspace(-1, 1, 5)
+        cpl = np.full(dev.norb, 0.1)
+        frm = [1.0, 0.0]
+        mix, niter = 0.3, 8
     else:
         dev = G.transport_c1(nbl=4, n=10, seed=4, density=0.3)
         E = np.linspace(-1, 1, 5)
         cpl = np.full(dev.norb, 0.1)
         frm = [1.0, 0.0]
     did = gpu_ctx.upload(dev)
-    gpu_ctx.set_options(scba_niter=5)
+    gpu_ctx.set_options(scba_niter=niter, scba_tol=tol, scba_mix=mix, scba_rule=rule)
     try:
         r = gpu_ctx.meir_wingreen(did, E, frm, coupling=cpl, eta=1e-4)
-        o, spread = oracle_spread(lambda d: O.meir_wingreen(d, E, frm, coupling=cpl, eta=1e-4, scba_niter=5), dev)
+        o, spread = oracle_spread(lambda d: O.meir_wingreen(d, E, frm, coupling=cpl, eta=1e-4, scba_niter=niter,
+                                                            scba_tol=tol, scba_mix=mix, scba_rule=rule), dev)
         assert np.all(r["status"] == o["status"])
         assert np.all(np.abs(r["scba_iter"] - o["scba_iter"]) <= 1)
         for key in ("curr", "layer_curr", "layer_dens"):
             a, b = r[key], o[key]
             bound = np.maximum(1e-10 * max(1.0, np.abs(b).max()), 10 * spread[key])
             assert np.all(np.abs(a - b) <= bound), key
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
+
+
+def test_meir_wingreen_dev_matches_host_call(gpu_ctx):
+    """negf_b200_meir_wingreen_dev (device buffers, caller's stream) gives the
+    host-buffer call's outputs bit for bit."""
+    dev = G.transport_c0(nbl=5, n=8, seed=3)
+    E = np.linspace(-1, 1, 7)
+    cpl = np.full(dev.norb, 0.1)
+    frm = np.ascontiguousarray(np.stack([[0.9, 0.2]] * len(E)))
+    did = gpu_ctx.upload(dev)
+    gpu_ctx.set_options(scba_niter=6, scba_mix=0.5, scba_rule=1, scba_tol=1e-8)
+    try:
+        r = gpu_ctx.meir_wingreen(did, E, frm, coupling=cpl, eta=1e-4)
+        n, nbl, ncs = len(E), dev.nbl, 3      # strides above the minimum
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+        d_ids, d_E = t(np.full(n, did, dtype=np.int32)), t(E)
+        d_frm = t(np.concatenate([frm, np.zeros((n, 1))], axis=1))
+        d_cpl = t(cpl)
+        d_curr = torch.zeros((n, ncs), dtype=torch.float64, device="cuda")
+        d_lc = torch.zeros((n, nbl + 1), dtype=torch.float64, device="cuda")
+        d_ld = torch.zeros((n, nbl + 1), dtype=torch.float64, device="cuda")
+        d_it = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_err = torch.zeros(n, dtype=torch.float64, device="cuda")
+        d_nc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
+        s = torch.cuda.Stream()
+        L = native.load()
+        rc = L.negf_b200_meir_wingreen_dev(gpu_ctx.handle, n, d_ids.data_ptr(), d_E.data_ptr(), 1e-4,
+                                           d_frm.data_ptr(), d_cpl.data_ptr(), d_curr.data_ptr(), d_lc.data_ptr(),
+                                           d_ld.data_ptr(), d_it.data_ptr(), d_err.data_ptr(), d_nc.data_ptr(),
+                                           d_st.data_ptr(), ncs, nbl + 1, ctypes.c_void_p(s.cuda_stream))
+        assert rc == 0
+        s.synchronize()
+        assert np.array_equal(d_curr.cpu().numpy()[:, :2], r["curr"])
+        assert np.array_equal(d_lc.cpu().numpy()[:, :nbl - 1], r["layer_curr"])
+        assert np.array_equal(d_ld.cpu().numpy()[:, :nbl], r["layer_dens"])
+        assert np.array_equal(d_it.cpu().numpy(), r["scba_iter"])
+        assert np.array_equal(d_st.cpu().numpy(), r["status"])
+        # strides below the largest ncont / nbl are rejected
+        rc = L.negf_b200_meir_wingreen_dev(gpu_ctx.handle, n, d_ids.data_ptr(), d_E.data_ptr(), 1e-4,
+                                           d_frm.data_ptr(), d_cpl.data_ptr(), d_curr.data_ptr(), d_lc.data_ptr(),
+                                           d_ld.data_ptr(), d_it.data_ptr(), d_err.data_ptr(), d_nc.data_ptr(),
+                                           d_st.data_ptr(), 1, nbl, None)
+        assert rc == native.BAD_ARG
     finally:
         gpu_ctx.set_options()
         gpu_ctx.release(did)

@@ -147,3 +147,40 @@ def test_fermi_and_integrate_el():
     cur = O.integrate_el(np.ones_like(E), -0.3, 0.2, 1e-3, 1e-3, -2.0, 2.0, 0.1)
     assert abs(cur - 0.5) < 1e-6
     assert abs(O.integrate_el(np.ones_like(E), 0.2, -0.3, 1e-3, 1e-3, -2.0, 2.0, 0.1) + 0.5) < 1e-6
+
+
+def _scba_case():
+    from libnegf_b200.energy import fermi_f
+    dev = G.transport_c0(nbl=8, n=12, seed=0)
+    E = np.linspace(-1.0, 1.0, 13)
+    kT = 8.617333262e-5 * 300.0
+    frm = np.stack([fermi_f(E, 0.1, kT), fermi_f(E, -0.1, kT)], axis=1)
+    return dev, E, frm, np.full(dev.norb, 0.1)
+
+
+def test_scba_mix_one_is_the_reference_rule():
+    dev, E, frm, cpl = _scba_case()
+    a = O.meir_wingreen(dev, E, frm, coupling=cpl, eta=1e-4, scba_niter=30)
+    b = O.meir_wingreen(dev, E, frm, coupling=cpl, eta=1e-4, scba_niter=30, scba_mix=1.0, scba_rule=0)
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_scba_mixing_and_current_rule_reach_the_same_fixed_point():
+    """Linear mixing changes the path, not the SCBA fixed point.  The current
+    rule stops once the contact-1 current moves by less than the tolerance:
+    the currents agree with the converged ones, the densities need not (where
+    both contacts are filled the current is ~0 from the first sweep on)."""
+    dev, E, frm, cpl = _scba_case()
+    ref = O.meir_wingreen(dev, E, frm, coupling=cpl, eta=1e-4, scba_niter=200, scba_tol=1e-12)
+    mix = O.meir_wingreen(dev, E, frm, coupling=cpl, eta=1e-4, scba_niter=200, scba_tol=1e-12, scba_mix=0.5)
+    ok = (ref["scba_err"] < 1e-12) & (mix["scba_err"] < 1e-12)
+    assert ok.sum() >= 10
+    scale = np.abs(ref["curr"]).max()
+    assert np.abs(mix["curr"][ok] - ref["curr"][ok]).max() <= 1e-8 * scale
+    assert np.abs(mix["layer_dens"][ok] - ref["layer_dens"][ok]).max() <= 1e-8 * np.abs(ref["layer_dens"]).max()
+    cur = O.meir_wingreen(dev, E, frm, coupling=cpl, eta=1e-4, scba_niter=200, scba_tol=1e-11, scba_mix=0.5,
+                          scba_rule=1)
+    ok = (ref["scba_err"] < 1e-12) & (cur["scba_err"] < 1e-11)
+    assert ok.sum() >= 10 and np.all(cur["scba_iter"] >= 2)
+    assert np.abs(cur["curr"][ok] - ref["curr"][ok]).max() <= 1e-8 * scale
