@@ -667,15 +667,19 @@ def main():
             sel = np.sort(np.asarray(picks[:nsamp], dtype=np.int64))
             nsamp = sel.size
             v, Tc, dt = cpu_baseline(wl, devs, ids_run[sel], E_run[sel], nsamp, cores)
-            # one host core: one or two of the same points, single-threaded
+            # one host core: one or two of the same points, single-threaded (SCBA: the point whose sweep
+            # count on the GPU is closest to the sample's mean)
             n1 = 1 if sc else 2
-            v1, _, dt1 = cpu_baseline(wl, devs, ids_run[sel[:n1]], E_run[sel[:n1]], n1, 1)
+            one = sel[:n1] if not sc else sel[[int(np.argmin(np.abs(sweeps[sel] - sweeps[sel].mean())))]]
+            v1, _, dt1 = cpu_baseline(wl, devs, ids_run[one], E_run[one], n1, 1)
             grid = wl["nE"] * wl["nk"]
             line["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
                                     "sample": "%d points of the timed batches over %d k-points, %.1f s"
                                               % (nsamp, len(set(ids_run[sel].tolist())), dt),
                                     "one_core": {"value": v1, "unit": "solves/s",
-                                                 "sample": "%d points, %.1f s" % (n1, dt1)},
+                                                 "sample": "%d points, %.1f s" % (n1, dt1) + (
+                                                     "; %d SCBA sweeps (sample mean %.1f)" % (
+                                                         sweeps[one[0]], sweeps[sel].mean()) if sc else "")},
                                     "full_grid_s": grid / v, "full_grid_points": grid}
             if sc:
                 got = {"curr": curr_g[sel], "layer_dens": ldens_g[sel], "scba_iter": sweeps[sel]}
