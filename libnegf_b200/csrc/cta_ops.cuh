@@ -736,6 +736,7 @@ struct LeafShared {
   double2 candd[2][kThreads / 32];
   double2 candrow[2][kThreads / 32][W];
   double2 rowj[2][W];
+  double2 stage[2][2 * W * W];   // pivot rows of leaf_apply, two pieces (K up to 2W)
 };
 
 // One pivot step of gj_leaf_reg on panel column JJ (global column j).
@@ -835,44 +836,50 @@ __device__ __forceinline__ void gj_reg_steps(double2 (&x)[R][W], int n, int c0, 
   }
 }
 
-// Delayed update of the tree's lowest level done inside a leaf, rows in
+// Delayed update of the tree's lowest levels done inside a leaf, rows in
 // registers: y(i, c) = [i outside the pivot rows [k0, k0+kw)] T(perm[i], c)
-// + sum_k Wc(i, k) T(perm[k0+k], c), c < tw.  Wc (kw columns) and T (tw
-// columns) are n x . column-major with ld n; T must not change while any
-// thread runs this.  The same product as the EPI_GJ GEMM for a node of two
-// leaves (the sum over k first, then the masked gathered row).
-template <int R, int W>
+// + sum_k Wc(i, k) T(perm[k0+k], c), c < tw.  Wc (kw columns, kw <= KW)
+// and T (tw columns) are n x . column-major with ld n.  The kw pivot rows
+// of T, which every thread needs, are first staged in shared memory
+// (`stage`, KW x W elements) by all threads at once, so that the product
+// waits for one memory round trip instead of one per row; each thread's own
+// Wc row and gathered T row are independent loads.  T must not change while
+// any thread runs this, and `stage` not before every thread has finished
+// (the callers' next barrier).  The same product as the EPI_GJ GEMM for a
+// node of the tree.
+template <int R, int W, int KW = W>
 __device__ __forceinline__ void leaf_apply(double2 (&y)[R][W], const double2* Wc, int kw, const double2* T, int tw,
-                                           const int* perm, int k0, int n) {
+                                           const int* perm, int k0, int n, double2* stage) {
   const int tid = threadIdx.x, nt = blockDim.x;
+  for (int q = tid; q < kw * W; q += nt) {
+    const int k = q / W, c = q % W;
+    stage[q] = (c < tw) ? T[perm[k0 + k] + (size_t)c * n] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int i = tid + r * nt;
     double2 acc[W];
+    const bool live = i < n;
+    const bool masked = (i >= k0 && i < k0 + kw);
+    const double2* orow = T + (live ? perm[i] : 0);
 #pragma unroll
-    for (int c = 0; c < W; ++c) acc[c] = make_double2(0.0, 0.0);
-    if (i < n) {
+    for (int c = 0; c < W; ++c)
+      acc[c] = (live && c < tw && !masked) ? orow[(size_t)c * n] : make_double2(0.0, 0.0);
 #pragma unroll
-      for (int k = 0; k < W; ++k) {
-        if (k >= kw) break;
-        const double2 wv = Wc[i + (size_t)k * n];
-        const double2* trow = T + perm[k0 + k];
-#pragma unroll
-        for (int c = 0; c < W; ++c)
-          if (c < tw) {
-            const double2 t = trow[(size_t)c * n];
-            acc[c].x = fma(wv.x, t.x, fma(-wv.y, t.y, acc[c].x));
-            acc[c].y = fma(wv.x, t.y, fma(wv.y, t.x, acc[c].y));
-          }
-      }
-      const bool masked = (i >= k0 && i < k0 + kw);
-      const double2* orow = T + perm[i];
+    for (int k = 0; k < KW; ++k) {
+      if (k >= kw) break;
+      const double2 wv = live ? Wc[i + (size_t)k * n] : make_double2(0.0, 0.0);
+      const double2* srow = stage + k * W;
 #pragma unroll
       for (int c = 0; c < W; ++c) {
-        const double2 o = (c < tw && !masked) ? orow[(size_t)c * n] : make_double2(0.0, 0.0);
-        y[r][c] = make_double2(acc[c].x + o.x, acc[c].y + o.y);
+        const double2 t = srow[c];
+        acc[c].x = fma(wv.x, t.x, fma(-wv.y, t.y, acc[c].x));
+        acc[c].y = fma(wv.x, t.y, fma(wv.y, t.x, acc[c].y));
       }
     }
+#pragma unroll
+    for (int c = 0; c < W; ++c) y[r][c] = acc[c];   // rows i >= n: zeros
   }
 }
 
@@ -916,7 +923,7 @@ __device__ __forceinline__ void gj_leaf2(double2* X, int n, int c0, int w, doubl
   }
   if (wb > 0) {
     gj_block_perm(s.perm, s.piv, n, c0, c0 + wa);      // its barriers also publish a
-    leaf_apply<R, W>(x, A, wa, B, wb, s.perm, c0, n);  // b <- a's elimination applied to b
+    leaf_apply<R, W>(x, A, wa, B, wb, s.perm, c0, n, L.stage[0]);  // b <- a's elimination applied to b
     gj_reg_steps<R, W, 0>(x, n, c0 + wa, wb, L, s);    // every thread is past its reads of b
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -928,7 +935,7 @@ __device__ __forceinline__ void gj_leaf2(double2* X, int n, int c0, int w, doubl
       }
     }
     gj_block_perm(s.perm, s.piv, n, c0 + wa, c0 + w);
-    leaf_apply<R, W>(x, B, wb, A, wa, s.perm, c0 + wa, n);  // a <- b's elimination applied to a
+    leaf_apply<R, W>(x, B, wb, A, wa, s.perm, c0 + wa, n, L.stage[0]);  // a <- b's elimination applied to a
     __syncthreads();                                          // all gathers of a done before a is rewritten
 #pragma unroll
     for (int r = 0; r < R; ++r) {
@@ -943,11 +950,136 @@ __device__ __forceinline__ void gj_leaf2(double2* X, int n, int c0, int w, doubl
   __syncthreads();
 }
 
-// gj_leaf2 for 1, 2 and 4 rows per thread, each compiled out of line in
-// leaf_dev.cu (see gemm_run).
+// Register rows of a W-column piece: store columns [0, tw) of y to T.
+template <int R, int W>
+__device__ __forceinline__ void leaf_store(const double2 (&y)[R][W], double2* T, int tw, int n) {
+  const int tid = threadIdx.x, nt = blockDim.x;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int i = tid + r * nt;
+    if (i < n) {
+#pragma unroll
+      for (int c = 0; c < W; ++c)
+        if (c < tw) T[i + (size_t)c * n] = y[r][c];
+    }
+  }
+}
+
+// A leaf of up to 4W columns: the next node of the tree done inside the leaf
+// as well.  Left half (up to 2W columns) by gj_leaf2; its elimination
+// applied to the right half in registers, two W-column pieces with K up to
+// 2W; right half by gj_leaf2; its elimination applied back to the left half
+// the same way.  This replaces the tree's K = 2W products, whose 64 x 64
+// tiles are mostly empty and whose cost is the fixed latency of a product
+// call (measured: 53 us per update at n = 256, K = 16, against 5 us of
+// arithmetic).
+template <int R, int W>
+__device__ __forceinline__ void gj_leaf4(double2* X, int n, int c0, int w, double2* sh, InvScratch& s) {
+  const int wl = (w + 1) >> 1, wr = w - wl;
+  double2* Lp = X + (size_t)c0 * n;
+  double2* Rp = Lp + (size_t)wl * n;
+  // h = 0: factorise the left half, apply it to the right half; h = 1: the
+  // other way round (one copy of the code: two would spill)
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {
+    const int fc = h ? c0 + wl : c0, fw = h ? wr : wl, tw = h ? wl : wr;
+    double2* F = h ? Rp : Lp;
+    double2* T = h ? Lp : Rp;
+    gj_leaf2<R, W>(X, n, fc, fw, sh, s);   // reads only its own rows first; its barriers publish the rest
+    if (wr <= 0) return;
+    const int p0 = tw < W ? tw : W, p1 = tw - p0;
+    double2 x[R][W], y[R][W];
+    gj_block_perm(s.perm, s.piv, n, fc, fc + fw);
+    LeafShared<W>& L = *reinterpret_cast<LeafShared<W>*>(sh);
+    leaf_apply<R, W, 2 * W>(x, F, fw, T, p0, s.perm, fc, n, L.stage[0]);
+    if (p1 > 0) leaf_apply<R, W, 2 * W>(y, F, fw, T + (size_t)p0 * n, p1, s.perm, fc, n, L.stage[1]);
+    __syncthreads();                        // every gather of T done before it is rewritten
+    leaf_store<R, W>(x, T, p0, n);
+    if (p1 > 0) leaf_store<R, W>(y, T + (size_t)p0 * n, p1, n);
+  }
+  __syncthreads();
+}
+
+// A node update of the delayed-update tree with narrow halves, done by row
+// owners on the FP64 FMA pipe instead of the 64 x 64 product tiles:
+//   Y(:, c) = rowmask(X[perm, c]) + Wm(:, 0:K) X[perm[k0:k0+K], c],  c < N,
+// all n-row column-major with ld n (Y != X).  Each thread owns rows (TPR
+// threads per row, each taking every TPR-th column of a chunk of CWT * TPR
+// columns) and keeps its chunk of the output row in registers; the K pivot
+// rows of the chunk, which every thread needs, are staged in shared memory
+// (`stage`, K x CWT*TPR elements) by all threads at once.  A product call
+// at these shapes pays one memory round trip per mostly-empty tile step; the
+// row owners pay about three per chunk but issue from shared memory at a
+// lower rate.  Measured per update (296 CTAs): K = N = 16 at n = 512, 225
+// -> 90 us; K = N = 32 at n = 256, 76 -> 64 us; K = N = 64 at n = 256,
+// 132 -> 239 us.  So K <= kRowsMax = 32.
+constexpr int kRowsMax = 32;
+
+template <int R, int TPR, int CWT>
+__device__ __forceinline__ void gj_rows_update(const double2* X, double2* Y, const double2* Wm, int n, int N, int k0,
+                                               int K, const int* perm, double2* stage) {
+  constexpr int CW = CWT * TPR;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int rt = tid / TPR, sub = tid - rt * TPR, rstride = nt / TPR;
+  for (int cc = 0; cc < N; cc += CW) {
+    const int cw = (N - cc) < CW ? (N - cc) : CW;
+    for (int q = tid; q < K * CW; q += nt) {
+      const int k = q / CW, c = q - k * CW;
+      stage[q] = (c < cw) ? X[perm[k0 + k] + (size_t)(cc + c) * n] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int i = rt + r * rstride;
+      const bool live = i < n;
+      const bool masked = (i >= k0 && i < k0 + K);
+      const double2* orow = X + (live ? perm[i] : 0) + (size_t)cc * n;
+      double2 acc[CWT];
+#pragma unroll
+      for (int j = 0; j < CWT; ++j) {
+        const int c = sub + j * TPR;
+        acc[j] = (live && c < cw && !masked) ? orow[(size_t)c * n] : make_double2(0.0, 0.0);
+      }
+      const double2* wrow = Wm + (live ? i : 0);
+#pragma unroll 4
+      for (int k = 0; k < K; ++k) {
+        const double2 wv = live ? wrow[(size_t)k * n] : make_double2(0.0, 0.0);
+        const double2* srow = stage + k * CW + sub;
+#pragma unroll
+        for (int j = 0; j < CWT; ++j) {
+          const double2 t = srow[j * TPR];
+          acc[j].x = fma(wv.x, t.x, fma(-wv.y, t.y, acc[j].x));
+          acc[j].y = fma(wv.x, t.y, fma(wv.y, t.x, acc[j].y));
+        }
+      }
+      if (live) {
+        double2* yrow = Y + i + (size_t)cc * n;
+#pragma unroll
+        for (int j = 0; j < CWT; ++j) {
+          const int c = sub + j * TPR;
+          if (c < cw) yrow[(size_t)c * n] = acc[j];
+        }
+      }
+    }
+    __syncthreads();   // every read of the stage done before the next chunk's
+  }
+}
+
+// gj_leaf4 for 1, 2 and 4 rows per thread, each compiled out of line in
+// leaf_dev.cu (see gemm_run); gj_rows_update likewise (rows_run_*: n <= 128
+// two threads per row, n <= 256 one, n <= 512 two rows per thread, n <= 1024
+// four).
 __device__ void leaf_run_r1(double2* X, int n, int c0, int w, double2* sh, InvScratch& s);
 __device__ void leaf_run_r2(double2* X, int n, int c0, int w, double2* sh, InvScratch& s);
 __device__ void leaf_run_r4(double2* X, int n, int c0, int w, double2* sh, InvScratch& s);
+__device__ void rows_run_t2(const double2* X, double2* Y, const double2* Wm, int n, int N, int k0, int K,
+                            const int* perm, double2* stage);
+__device__ void rows_run_r1(const double2* X, double2* Y, const double2* Wm, int n, int N, int k0, int K,
+                            const int* perm, double2* stage);
+__device__ void rows_run_r2(const double2* X, double2* Y, const double2* Wm, int n, int N, int k0, int K,
+                            const int* perm, double2* stage);
+__device__ void rows_run_r4(const double2* X, double2* Y, const double2* Wm, int n, int N, int k0, int K,
+                            const int* perm, double2* stage);
 
 // ---------------------------------------------------------------- inversion driver
 // out = A^-1 (n x n).  A is read only (out may alias A).  `ws` holds
@@ -955,22 +1087,30 @@ __device__ void leaf_run_r4(double2* X, int n, int c0, int w, double2* sh, InvSc
 //
 // n <= kSmallInvMax: Gauss-Jordan with partial pivoting on the whole matrix
 // in shared memory.  Larger n: the same elimination with delayed updates
-// over a perfect binary tree of 2^d column leaves.  A leaf is factorised
-// (gj_leaf_reg, panel in registers) once every earlier pivot has been
-// applied to it; after the left half of a node is done, its pivots are
-// applied to the right half, and after the right half, the right half's
-// pivots to the left half, each as one product
-// X' = rowmask(X[perm,:]) + W * X[perm[J],:] with K equal to the half's
-// width (n/2, n/4, ...).  Every column is rewritten once per tree level, so
-// the matrix makes d ~ log2(n/16) trips through memory instead of n/16.
-// Products are out of place between two buffers (row exchanges then have
-// no hazards); a perfect tree keeps every leaf of a node in the same buffer.
+// over a perfect binary tree of 2^d column leaves.  A leaf (up to 32
+// columns, gj_leaf4, panel in registers, its own two lowest nodes inside)
+// is factorised once every earlier pivot has been applied to it; after the
+// left half of a node is done, its pivots are applied to the right half,
+// and after the right half, the right half's pivots to the left half, each
+// as one product X' = rowmask(X[perm,:]) + W * X[perm[J],:] with K equal to
+// the half's width (n/2, n/4, ...).  Every column is rewritten once per
+// tree level, so the matrix makes d ~ log2(n/32) trips through memory
+// instead of n/32.  Products are out of place between two buffers (row
+// exchanges then have no hazards), the first one reading its target
+// columns from A itself; a perfect tree keeps every leaf of a node in the
+// same place.
 //
 // The elimination is a loop of steps (factorise a leaf, apply a node) whose
 // state lives in an InvProg in local memory: inv_next() advances it and
 // prepares the next step, and the caller runs the step's heavy routine
 // itself, so that the leaf factorisation and the product loop are called
 // with no live state around them.
+// Leaf columns not yet copied out of the input.  They stand for buffer 0
+// (the old code copied A there first): the first update moves them to
+// buffer 1, leaf 0 is copied to buffer 0, so that the leaves of a node stay
+// in one buffer.
+constexpr unsigned char kInA = 2;
+
 struct InvProg {
   const double2* A;
   double2* out;
@@ -980,12 +1120,19 @@ struct InvProg {
   double2* X;               // leaf step: panel base, first column, width
   int c0, w;
   long long t0;
+  // row-owner update step: Y(:, 0:N) from X, Wm, pivot rows [rk0, rk0 + rK)
+  const double2* rX;
+  double2* rY;
+  const double2* rW;
+  int rN, rk0, rK;
 };
 
-enum InvStep : int { INV_DONE = 0, INV_LEAF = 1, INV_APPLY = 2 };
+enum InvStep : int { INV_DONE = 0, INV_LEAF = 1, INV_APPLY = 2, INV_ROWS = 3 };
 
-// Small orders entirely; larger ones: copy A into the first buffer and set
-// up the tree.  Returns 1 when the inversion is already complete.
+// Small orders entirely; larger ones: set up the tree.  No copy of A: a
+// leaf's columns are read from A by the first update that targets them (or,
+// for leaf 0, copied out before its factorisation).  Returns 1 when the
+// inversion is already complete.
 static __device__ __noinline__ int inv_begin(InvProg& ip, int n, const double2* A, double2* out, double2* ws, double2* smem,
                                       InvScratch& s) {
   if (threadIdx.x == 0) *s.flag = 0;
@@ -1018,10 +1165,10 @@ static __device__ __noinline__ int inv_begin(InvProg& ip, int n, const double2* 
     s.tr.stop(TR_INV_OTHER, t0);
     return 1;
   }
-  // leaves are factorised in registers: rpt rows per thread, two sub-leaves
+  // leaves are factorised in registers: rpt rows per thread, four sub-leaves
   // of 8/rpt columns
   const int rpt = (n + (int)blockDim.x - 1) / (int)blockDim.x;
-  const int wmax = rpt <= 1 ? 16 : (rpt <= 2 ? 8 : 4);
+  const int wmax = rpt <= 1 ? 32 : (rpt <= 2 ? 16 : 8);
   int d = 0;
   while ((n + (1 << d) - 1) >> d > wmax) ++d;
   ip.rpt = rpt <= 1 ? 1 : (rpt <= 2 ? 2 : 4);
@@ -1030,12 +1177,10 @@ static __device__ __noinline__ int inv_begin(InvProg& ip, int n, const double2* 
   ip.buf[0] = ws;
   ip.buf[1] = ws + (size_t)n * n;
   ip.k = 0; ip.l = 0; ip.phase = 0; ip.flip_half = 0;
-  unsigned char* par = reinterpret_cast<unsigned char*>(s.cperm);   // per-leaf buffer index (nl <= n)
-  long long t0 = s.tr.start();
-  cta_copy(ip.buf[0], A, n * n);
-  for (int k = threadIdx.x; k < ip.nl; k += blockDim.x) par[k] = 0;
+  // per-leaf location (nl <= n): 0 / 1 = buffer, kInA = still only in A (read in place, never written)
+  unsigned char* par = reinterpret_cast<unsigned char*>(s.cperm);
+  for (int k = threadIdx.x; k < ip.nl; k += blockDim.x) par[k] = kInA;
   __syncthreads();
-  s.tr.stop(TR_INV_OTHER, t0);
   return 0;
 }
 
@@ -1045,7 +1190,10 @@ static __device__ __noinline__ int inv_next(InvProg& ip, double2* smem, InvScrat
   unsigned char* par = reinterpret_cast<unsigned char*>(s.cperm);
   const int n = ip.n, d = ip.d;
   if (ip.flip_half) {   // the update just run moved its target leaves to the other buffer
-    for (int q = threadIdx.x; q < ip.flip_half; q += blockDim.x) par[ip.flip_ta + q] ^= 1;
+    for (int q = threadIdx.x; q < ip.flip_half; q += blockDim.x) {
+      const unsigned char b = par[ip.flip_ta + q];
+      par[ip.flip_ta + q] = (b == kInA) ? 1 : (b ^ 1);
+    }
     ip.flip_half = 0;
     __syncthreads();
     s.tr.stop(TR_INV_UPDATE, ip.t0);
@@ -1056,6 +1204,14 @@ static __device__ __noinline__ int inv_next(InvProg& ip, double2* smem, InvScrat
       const int k = ip.k;
       ip.c0 = (k * n) >> d;
       ip.w = (((k + 1) * n) >> d) - ip.c0;
+      if (par[k] == kInA) {   // only leaf 0: every later leaf is the target of an update first
+        const long long t0 = s.tr.start();
+        cta_copy(ip.buf[0] + (size_t)ip.c0 * n, ip.A + (size_t)ip.c0 * n, n * ip.w);
+        __syncthreads();
+        if (threadIdx.x == 0) par[k] = 0;
+        __syncthreads();
+        s.tr.stop(TR_INV_OTHER, t0);
+      }
       ip.X = ip.buf[par[k]];
       ip.phase = 1;
       ip.l = 1;
@@ -1077,18 +1233,23 @@ static __device__ __noinline__ int inv_next(InvProg& ip, double2* smem, InvScrat
     const int a0 = (ta * n) >> d, a1 = ((ta + half) * n) >> d;
     ip.t0 = s.tr.start();
     gj_block_perm(s.perm, s.piv, n, j0, j1);
-    const int pw = par[fa], pt = par[ta];
+    const int pw = par[fa], pt = par[ta];           // pw is a buffer: factorised leaves never stay in A
     double2* W = ip.buf[pw] + (size_t)j0 * n;
-    const double2* X = ip.buf[pt] + (size_t)a0 * n;
-    double2* Y = ip.buf[pt ^ 1] + (size_t)a0 * n;
+    const double2* X = (pt == kInA ? ip.A : ip.buf[pt]) + (size_t)a0 * n;
+    double2* Y = ip.buf[pt == kInA ? 1 : (pt ^ 1)] + (size_t)a0 * n;
+    ip.flip_ta = ta;
+    ip.flip_half = half;
+    if (j1 - j0 <= kRowsMax) {   // narrow halves: row owners (gj_rows_update), run by the caller
+      ip.rX = X; ip.rY = Y; ip.rW = W; ip.rN = a1 - a0; ip.rk0 = j0; ip.rK = j1 - j0;
+      if (r == half) { ip.phase = 0; ++ip.k; } else { ++ip.l; }
+      return INV_ROWS;
+    }
     Operand Aop = opN(W, n);
     Operand Bop{X, n, OP_GATHER, s.perm + j0};
     Epilogue e;
     e.mode = EPI_GJ; e.C = Y; e.ldc = n; e.alpha = make_double2(1, 0); e.beta = make_double2(0, 0);
     e.xcur = X; e.ldx = n; e.perm = s.perm; e.W = nullptr; e.k0 = j0; e.jb = j1 - j0; e.maxabs = nullptr;
     gemm_desc_publish(n, a1 - a0, j1 - j0, Aop, Bop, e, smem);
-    ip.flip_ta = ta;
-    ip.flip_half = half;
     if (r == half) { ip.phase = 0; ++ip.k; } else { ++ip.l; }
     return INV_APPLY;
   }
@@ -1116,6 +1277,14 @@ static __device__ __noinline__ int inv_end(InvProg& ip, InvScratch& s) {
   return 0;
 }
 
+// The row-owner update step of ip (INV_ROWS), by rows per thread.
+__device__ __forceinline__ void rows_run(const InvProg& ip, double2* smem, const InvScratch& s) {
+  if (2 * ip.n <= (int)blockDim.x) rows_run_t2(ip.rX, ip.rY, ip.rW, ip.n, ip.rN, ip.rk0, ip.rK, s.perm, smem);
+  else if (ip.rpt == 1) rows_run_r1(ip.rX, ip.rY, ip.rW, ip.n, ip.rN, ip.rk0, ip.rK, s.perm, smem);
+  else if (ip.rpt == 2) rows_run_r2(ip.rX, ip.rY, ip.rW, ip.n, ip.rN, ip.rk0, ip.rK, s.perm, smem);
+  else rows_run_r4(ip.rX, ip.rY, ip.rW, ip.n, ip.rN, ip.rk0, ip.rK, s.perm, smem);
+}
+
 // Returns info (0 or the 1-based column of the first exactly-zero pivot) in
 // all threads.  Inlined: the heavy routines are called from the caller's
 // level.
@@ -1132,6 +1301,8 @@ __device__ __forceinline__ int cta_zinv(int n, const double2* A, double2* out, d
         else if (ip.rpt == 2) leaf_run_r2(ip.X, ip.n, ip.c0, ip.w, smem, s);
         else leaf_run_r4(ip.X, ip.n, ip.c0, ip.w, smem, s);
         s.tr.stop(TR_INV_PANEL, t0);
+      } else if (step == INV_ROWS) {
+        rows_run(ip, smem, s);
       } else {
         gemm_run(reinterpret_cast<const GemmDesc*>(smem + kGemmDescOffset), smem);
       }

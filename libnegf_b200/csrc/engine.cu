@@ -125,6 +125,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_engine(EngineArgs a) {
     if (st == STEP_DONE) break;
     if (st == STEP_GEMM) {
       cta_gemm_body<OP_RT, OP_RT, EPI_RT>(reinterpret_cast<const GemmDesc*>(smap.main + kGemmDescOffset), smap.main);
+    } else if (st == STEP_ROWS) {
+      rows_run(c.ip, smap.main, smap.inv);
     } else if (c.ip.rpt == 1) {
       leaf_run_r1(c.ip.X, c.ip.n, c.ip.c0, c.ip.w, smap.main, smap.inv);
     } else if (c.ip.rpt == 2) {

@@ -26,6 +26,7 @@ __device__ int engine_step(const EngineArgs& a, EngineCtl& c, SmemMap& sm) {
         return STEP_LEAF;
       }
       if (st == INV_APPLY) return STEP_GEMM;   // timed by inv_next
+      if (st == INV_ROWS) return STEP_ROWS;    // likewise
       inv_end(c.ip, sm.inv);
       c.in_inv = 0;
       if (tid == 0) sm.ires[0] = *sm.inv.flag;

@@ -1000,11 +1000,12 @@ struct EngineCtl {
   long long t0;
 };
 
-enum StepKind : int { STEP_DONE = 0, STEP_GEMM = 1, STEP_LEAF = 2 };
+enum StepKind : int { STEP_DONE = 0, STEP_GEMM = 1, STEP_LEAF = 2, STEP_ROWS = 3 };
 
 // Runs the point program (generator, inversion driver, light operations)
 // up to the next heavy step and returns it: STEP_GEMM (descriptor published
-// at sm.main + kGemmDescOffset), STEP_LEAF (leaf of c.ip) or STEP_DONE.
+// at sm.main + kGemmDescOffset), STEP_LEAF (leaf of c.ip), STEP_ROWS
+// (row-owner node update of c.ip) or STEP_DONE.
 // The kernel runs the heavy step itself.  Compiled in program.cu, apart
 // from the kernel, so that the product loop in the kernel is register-
 // allocated without the control code around it.

@@ -54,7 +54,9 @@ def test_ragged_layers_across_leaf_shapes(gpu_ctx):
     did = gpu_ctx.upload(dev)
     try:
         T, nc, st = gpu_ctx.transmission(did, E, eta=1e-4)
-        ref, spread = oracle_spread(lambda d: O.transmission(d, E, eta=1e-4)[0], dev, nsamp=2)
+        # ill-conditioned: 1e-15 input perturbations move the oracle's T by up to ~1e-8 here,
+        # so the spread needs a few samples to be representative
+        ref, spread = oracle_spread(lambda d: O.transmission(d, E, eta=1e-4)[0], dev, nsamp=4)
         assert np.all(st == O.transmission(dev, E, eta=1e-4)[2])
         assert_T_close(T, ref, spread=spread)
     finally:
