@@ -230,12 +230,19 @@ int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts,
  * spectral combination, the reference adds this sum to rho as it is).
  * frm: npts x ncont occupations with the reference contact's subtracted
  * (f_c - f_ref, 0 for ref), the Sigma^n of calculate_Gn_neq_components.
+ * rho_dc / rho_cd (NULL to skip) receive the outer blocks of
+ * calculate_Gn_outer with outer_blocks = 2 (src/iterative.F90:1576-1665):
+ * Gn(cb,c) = -Gn(cb,cb) Tlc gs^dag - (f_c - f_ref) Gr(cb,cb) Tlc i(gs - gs^dag)
+ * kept on the pattern of E SMC - HMC, and Gn(c,cb) = Gn(cb,c)^dag, summed
+ * with the weights (layouts as in negf_b200_density).
  * The device needs nbl >= 2. */
 int negf_b200_density_neq(negf_b200_ctx* ctx, int32_t device_id, int32_t npts,
-                          const double* energy, double eta, const double* weight,
-                          const double* frm, const double* coupling,
-                          double* rho_diag, double* rho_upper, double* rho_lower,
-                          int32_t* ncyc, int32_t* status);
+                          const double* energy, double eta,
+                          const double* weight, const double* frm,
+                          const double* coupling, double* rho_diag,
+                          double* rho_upper, double* rho_lower,
+                          double* rho_dc, double* rho_cd, int32_t* ncyc,
+                          int32_t* status);
 
 /* ---- projections and contact pairs ----------------------------------------
  * tun_proj of libNEGF (negf%tun_proj): the transmission trace runs over the

@@ -992,16 +992,45 @@ int negf_b200_density(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const
 
 int negf_b200_density_neq(negf_b200_ctx* ctx, int32_t device_id, int32_t npts, const double* energy, double eta,
                           const double* weight, const double* frm, const double* coupling, double* rho_diag,
-                          double* rho_upper, double* rho_lower, int32_t* ncyc, int32_t* status) {
+                          double* rho_upper, double* rho_lower, double* rho_dc, double* rho_cd, int32_t* ncyc,
+                          int32_t* status) {
   if (!ctx) return NEGF_B200_ERR_BAD_ARG;
   if (npts < 0 || (npts > 0 && (!energy || !weight || !frm))) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad point arrays");
   std::lock_guard<std::mutex> lk(ctx->mu);
-  std::vector<double2> T;
+  std::vector<double2> T, Tout;
   std::vector<int> pl;
-  int64_t nd = 0, no = 0;
+  int64_t nd = 0, no = 0, nm = 0;
+  const bool want_outer = rho_dc || rho_cd;
   int st = accumulate_blocks(ctx, negf::MODE_GN, device_id, npts, energy, nullptr, eta, weight, frm, coupling, T, pl,
-                             nd, no, ncyc, status);
+                             nd, no, ncyc, status, want_outer ? &Tout : nullptr, &nm);
   if (st) return st;
+  if (want_outer) {
+    // calculate_Gn_outer masks Gn(cb,c) with Tlc's pattern (the nonzeros of HMC or SMC) and
+    // takes Gn(c,cb) as the dagger of the masked block; the sums are masked the same way
+    const DeviceRec& r = ctx->devs[device_id];
+    std::vector<double2> hmc((size_t)std::max<int64_t>(nm, 1)), smc;
+    CK(cudaMemcpy(hmc.data(), r.desc.hmc, (size_t)nm * 16, cudaMemcpyDeviceToHost));
+    if (r.desc.smc) {
+      smc.resize((size_t)nm);
+      CK(cudaMemcpy(smc.data(), r.desc.smc, (size_t)nm * 16, cudaMemcpyDeviceToHost));
+    }
+    int64_t om = 0;
+    for (int c = 0; c < r.ncont; ++c) {
+      const int n = pl[r.desc.cblk[c] - 1], L = r.desc.L[c];
+      for (int j = 0; j < L; ++j)
+        for (int q = 0; q < n; ++q) {
+          const int64_t idc = om + q + (int64_t)j * n;   // (q, j) of the n x L block
+          const int64_t icd = om + j + (int64_t)q * L;   // (j, q) of the L x n block
+          const bool on = hmc[idc].x != 0.0 || hmc[idc].y != 0.0 ||
+                          (!smc.empty() && (smc[idc].x != 0.0 || smc[idc].y != 0.0));
+          const double2 lc = on ? Tout[idc] : make_double2(0.0, 0.0);
+          const double2 cl = on ? Tout[nm + icd] : make_double2(0.0, 0.0);
+          if (rho_dc) { rho_dc[2 * idc] = lc.x; rho_dc[2 * idc + 1] = lc.y; }
+          if (rho_cd) { rho_cd[2 * icd] = cl.x; rho_cd[2 * icd + 1] = cl.y; }
+        }
+      om += (int64_t)n * L;
+    }
+  }
   // real_axis_int adds the sum itself to rho (no spectral combination, :1166-1170)
   store_blocks(T.data(), nd, rho_diag);
   store_blocks(T.data() + nd, no, rho_upper);

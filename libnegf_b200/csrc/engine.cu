@@ -146,7 +146,7 @@ int64_t engine_slots(int mode, int nbl_max, int ncont_max) {
   int64_t s = S_SIG + ncont_max;
   if (mode == MODE_T || mode == MODE_DOS) s += nbl_max + ncont_max;   // gsmr, Gr(cb,cb)
   else if (mode == MODE_RHO) s += nbl_max + 2 * ncont_max;             // + gs per contact
-  else s += 8 * (int64_t)nbl_max;                                 // GN arrays
+  else s += 8 * (int64_t)nbl_max + ncont_max;                     // GN arrays, gs per contact
   return s;
 }
 

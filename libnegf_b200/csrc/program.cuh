@@ -86,6 +86,8 @@ struct Ws {
   __device__ double2* keep(int c) const { return slot(S_SIG + ncont + nbl_max + c); }
   // density: the surface GF of contact c, kept for the outer blocks
   __device__ double2* gskeep(int c) const { return slot(S_SIG + 2 * ncont + nbl_max + c); }
+  // GN: the same, after the eight layer arrays
+  __device__ double2* gnkeep(int c) const { return slot(S_SIG + ncont + 8 * nbl_max + c); }
 };
 
 // ---------------------------------------------------------------- ops
@@ -466,8 +468,8 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           PT_EMIT(s);
         }
       sgf_ready:
-        if (a.mode == MODE_RHO && a.acc_lc) {
-          set_simple(o, K_COPY, s.L * s.L, w.slot(4), w.gskeep(s.c));
+        if (a.acc_lc && (a.mode == MODE_RHO || a.mode == MODE_GN)) {
+          set_simple(o, K_COPY, s.L * s.L, w.slot(4), a.mode == MODE_RHO ? w.gskeep(s.c) : w.gnkeep(s.c));
           PT_EMIT(s);
         }
         // ---- self-energy: Tlc = E SMC - HMC, Tcl = (E^* SMC - HMC)^dag, Sigma = Tlc gs Tcl
@@ -504,7 +506,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
 
       // ------------------------------------------------ SCBA loop (once for T / DOS)
       s.sit = 0; s.conv = 0; s.have_old = 0; s.err = 0.0; s.par = 0;
-      s.vec = w.slot(S_SIG + a.ncont_max + 8 * a.nbl_max);
+      s.vec = w.slot(S_SIG + 2 * a.ncont_max + 8 * a.nbl_max);   // after the layers and gnkeep
       for (;;) {
         if (a.mode == MODE_GN && (s.conv || s.sit > a.scba_niter)) break;
         s.sr = (a.mode == MODE_GN && s.sit > 0 && a.coupling) ? s.vec : nullptr;
@@ -926,6 +928,40 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
             PT_EMIT(s);
           }
         }
+        if (a.acc_lc)
+          // calculate_Gn_outer, outer_blocks = 2 (src/iterative.F90:1576-1665): per contact
+          // Gn(cb,c) = -Gn(cb,cb) Tlc gs^dag - (f_c - f_ref) Gr(cb,cb) Tlc i(gs - gs^dag), and
+          // Gn(c,cb) = Gn(cb,c)^dag, summed with the weight (masked on the host)
+          for (s.c = 0; s.c < s.d->ncont; ++s.c) {
+            s.L = s.d->L[s.c];
+            s.ncb = s.d->pl[s.d->cblk[s.c] - 1];
+            set_esh(o, w.slot(0), s.ncb, s.L, s.d->hmc + s.d->omc[s.c],
+                    s.d->has_smc ? s.d->smc + s.d->omc[s.c] : nullptr, s.ecs, 0, nullptr, nullptr, OP_N);   // Tlc
+            PT_EMIT(s);
+            set_gemm(o, s.ncb, s.L, s.L, w.slot(0), s.ncb, OP_N, w.gnkeep(s.c), s.L, OP_C, w.slot(2), s.ncb, one,
+                     zero);                                                                                 // Tlc gA
+            PT_EMIT(s);
+            set_gemm(o, s.ncb, s.L, s.ncb, w.layer(4 + s.par, s.d->cblk[s.c] - 1, s.d->nbl), s.ncb, OP_N, w.slot(2),
+                     s.ncb, OP_N, w.slot(3), s.ncb, mone, zero);
+            PT_EMIT(s);
+            if (fabs(a.frm[(int64_t)s.p * a.frm_stride + s.c]) > a.eps) {
+              set_simple(o, K_SPECTRAL, s.L, w.gnkeep(s.c), w.slot(1));                 // i (gs - gs^dag)
+              PT_EMIT(s);
+              set_gemm(o, s.ncb, s.L, s.L, w.slot(0), s.ncb, OP_N, w.slot(1), s.L, OP_N, w.slot(2), s.ncb, one, zero);
+              PT_EMIT(s);
+              set_gemm(o, s.ncb, s.L, s.ncb, w.layer(1, s.d->cblk[s.c] - 1, s.d->nbl), s.ncb, OP_N, w.slot(2),
+                       s.ncb, OP_N, w.slot(3), s.ncb, cz(-a.frm[(int64_t)s.p * a.frm_stride + s.c], 0.0), one);
+              PT_EMIT(s);
+            }
+            set_simple(o, K_ACCUM, s.ncb * s.L, w.slot(3), a.acc_lc + s.d->omc[s.c]);
+            o.alpha = a.weight[s.p];
+            PT_EMIT(s);
+            o.kind = K_DAGGER; o.m = s.L; o.n = s.ncb; o.A = w.slot(3); o.C = w.slot(2);      // L x ncb
+            PT_EMIT(s);
+            set_simple(o, K_ACCUM, s.ncb * s.L, w.slot(2), a.acc_cl + s.d->omc[s.c]);
+            o.alpha = a.weight[s.p];
+            PT_EMIT(s);
+          }
       }
       // ------------------------------------ Meir-Wingreen (iterative.F90:382-414); Gam slot 7, A slot 8
       if (a.curr)

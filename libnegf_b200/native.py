@@ -99,7 +99,7 @@ def load():
     L.negf_b200_set_sgf_cache.argtypes = [vp, i32, ctypes.c_size_t]
     L.negf_b200_set_workspace_limit.argtypes = [vp, ctypes.c_size_t]
     L.negf_b200_density.argtypes = [vp, i32, i32, dp, dp, dp, dp, dp, dp, dp, dp, ip, ip]
-    L.negf_b200_density_neq.argtypes = [vp, i32, i32, dp, f64, dp, dp, dp, dp, dp, dp, ip, ip]
+    L.negf_b200_density_neq.argtypes = [vp, i32, i32, dp, f64, dp, dp, dp, dp, dp, dp, dp, dp, ip, ip]
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.negf_b200_sgf_cache_stats.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_size_t)]
     _lib = L
@@ -266,9 +266,15 @@ class Context:
 
     def density_neq(self, device_id, energies, w, frm, eta=1e-4, coupling=None, check=True):
         """Real-axis non-equilibrium density blocks sum_p w_p Gn(E_p) (see
-        negf_b200_density_neq); frm: npts x ncont, reference contact subtracted."""
-        from .density import split_blocks
-        pl = self.devices[device_id].pl_size
+        negf_b200_density_neq); frm: npts x ncont, reference contact
+        subtracted.  Returns (diag, upper, lower) block lists, the outer
+        (device->contact, contact->device) blocks per contact, ncyc, status."""
+        from .density import split_blocks, split_outer
+        dev = self.devices[device_id]
+        pl = dev.pl_size
+        nm = sum(dev.pl_size[cb - 1] * L for cb, L in zip(dev.cblk, dev.lead_size))
+        rdc = np.zeros(max(nm, 1), dtype=np.complex128)
+        rcd = np.zeros(max(nm, 1), dtype=np.complex128)
         E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
         wt = np.ascontiguousarray(w, dtype=np.complex128).ravel()
         f = np.ascontiguousarray(frm, dtype=np.float64)
@@ -282,10 +288,11 @@ class Context:
         st = np.zeros(E.size, dtype=np.int32)
         rc = self._L.negf_b200_density_neq(self._h, device_id, E.size, _d(E), eta, _d(wt.view(np.float64)), _d(f),
                                            _d(cp) if cp is not None else None, _d(rd.view(np.float64)),
-                                           _d(ru.view(np.float64)), _d(rl.view(np.float64)), _i(nc), _i(st))
+                                           _d(ru.view(np.float64)), _d(rl.view(np.float64)),
+                                           _d(rdc.view(np.float64)), _d(rcd.view(np.float64)), _i(nc), _i(st))
         if check and rc not in (OK, NOT_CONVERGED, SCBA_NOT_CONVERGED):
             raise NegfError(rc, "density_neq: " + self.last_error())
-        return split_blocks(pl, rd, ru, rl), nc, st
+        return split_blocks(pl, rd, ru, rl), split_outer(dev, rdc, rcd), nc, st
 
     def release(self, device_id: int):
         self._check(self._L.negf_b200_release_device(self._h, device_id), "release")

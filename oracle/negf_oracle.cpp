@@ -728,10 +728,11 @@ struct ScbaOut {
 void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
                 const double* coupling, int niter, double tol, const Opts& o,
                 double* curr, double* lcurr, double* ldens, ScbaOut& so,
-                int& ncyc, Err& err, Trid* gn_out = nullptr) {
+                int& ncyc, Err& err, Trid* gn_out = nullptr, ContactParts* parts = nullptr,
+                std::vector<Dns>* grd_out = nullptr) {
   int nbl = D.nbl, ncont = D.ncont;
   std::vector<Dns> Sig;
-  compute_contacts(cplx(E, eta), D, Sig, ncyc, o.sgf_acc, o.max_iter, err);
+  compute_contacts(cplx(E, eta), D, Sig, ncyc, o.sgf_acc, o.max_iter, err, parts);
   // meir_wingreen: ref = ncont+1 with f(ref) = 0 (src/integrations.F90:1833-1837)
   std::vector<double> frm_ext(frm, frm + ncont);
   frm_ext.push_back(0.0);
@@ -822,6 +823,7 @@ void point_scba(const DeviceBlocks& D, double E, double eta, const double* frm,
   }
   so.iters = it;
   if (gn_out) *gn_out = Gn;
+  if (grd_out) *grd_out = Gr.d;
   // iterative_meir_wingreen (src/iterative.F90:382-414)
   if (curr)
     for (int c = 0; c < ncont; ++c) curr[c] = mw_current(c, Gr, Gn);
@@ -1087,25 +1089,64 @@ int oracle_meir_wingreen(const negf_b200_device* dev, int npts,
 // real_axis_int (src/integrations.F90:1093-1176): sum_p w_p Gn(E_p), Gn of
 // compute_Gn with the occupations frm (reference contact already
 // subtracted: Sigma^n = sum_c frm_c Gamma_c).  Blocks in the h_* layout.
+// rho_dc / rho_cd (optional): calculate_Gn_outer with outer_blocks = 2
+// (src/iterative.F90:1576-1665), summed with the weights.
 int oracle_density_neq(const negf_b200_device* dev, int npts, const double* energy, double eta,
                        const double* weight, const double* frm, const double* coupling, int scba_niter,
                        double scba_tol, double sgf_tol, int sgf_max_iter, double* rho_d, double* rho_u,
-                       double* rho_l, int* ncyc, int* status, int nthreads) {
+                       double* rho_l, double* rho_dc, double* rho_cd, int* ncyc, int* status, int nthreads) {
   set_threads(nthreads);
   DeviceBlocks D = unpack(dev);
   Opts o;
   o.sgf_acc = sgf_tol; o.max_iter = sgf_max_iter;
   int nbl = D.nbl, ncont = D.ncont;
   std::vector<Trid> G(npts);
+  std::vector<ContactParts> parts(npts);
+  std::vector<std::vector<Dns>> grd(npts);
+  const bool outer = rho_dc || rho_cd;
 #pragma omp parallel for schedule(dynamic, 1)
   for (int p = 0; p < npts; ++p) {
     Err err;
     ScbaOut so;
     int nc = 0;
     point_scba(D, energy[p], eta, frm + (size_t)p * ncont, coupling, scba_niter, scba_tol, o, nullptr, nullptr,
-               nullptr, so, nc, err, &G[p]);
+               nullptr, so, nc, err, &G[p], outer ? &parts[p] : nullptr, outer ? &grd[p] : nullptr);
     if (ncyc) ncyc[p] = nc;
     if (status) status[p] = err.code;
+  }
+  if (outer) {
+    size_t om = 0;
+    for (int c = 0; c < ncont; ++c) {
+      const int cb = D.cblk[c] - 1, n = D.n[cb], L = D.L[c];
+      std::vector<cplx> lc((size_t)n * L, cplx(0.0, 0.0)), cl((size_t)L * n, cplx(0.0, 0.0));
+      for (int p = 0; p < npts; ++p) {
+        const cplx w(weight[2 * p], weight[2 * p + 1]);
+        const ContactParts& cp = parts[p];
+        Dns gA, work1, work2, work3;
+        dagger(cp.GS[c], gA);
+        mult(cp.Tlc[c], gA, work2);
+        mult(G[p].d[cb], work2, work3, cplx(-1.0, 0.0));          // -Gn(cb,cb) Tlc gA
+        const double f = frm[(size_t)p * ncont + c];
+        if (std::abs(f) > o.eps) {
+          Dns A, w2;
+          spectral(cp.GS[c], A);
+          mult(cp.Tlc[c], A, w2);
+          mult(grd[p][cb], w2, work3, cplx(-f, 0.0));             // += (f_ref - f_c) Gr(cb,cb) Tlc A, accumulated
+        }
+        for (int j = 0; j < L; ++j)
+          for (int r = 0; r < n; ++r) {
+            const size_t q = r + (size_t)j * n;
+            if (cp.Tlc[c].v[q] == cplx(0.0, 0.0)) continue;           // mask(Gn_lc, Tlc)
+            lc[q] += w * work3.v[q];
+            cl[j + (size_t)r * L] += w * std::conj(work3.v[q]);        // Gn(c,cb) = Gn(cb,c)^dag
+          }
+      }
+      for (size_t q = 0; q < lc.size(); ++q) {
+        if (rho_dc) { rho_dc[2 * (om + q)] = lc[q].real(); rho_dc[2 * (om + q) + 1] = lc[q].imag(); }
+        if (rho_cd) { rho_cd[2 * (om + q)] = cl[q].real(); rho_cd[2 * (om + q) + 1] = cl[q].imag(); }
+      }
+      om += (size_t)n * L;
+    }
   }
   size_t od = 0, oo = 0;
   for (int i = 0; i < nbl; ++i) {

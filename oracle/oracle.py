@@ -48,7 +48,7 @@ def lib():
         L.oracle_density.argtypes = [vp, ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp,
                                      ip, ip, ctypes.c_int]
         L.oracle_density_neq.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, dp, dp, dp, ctypes.c_int,
-                                         ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp, ip, ip,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp, ip, ip,
                                          ctypes.c_int]
         L.oracle_fermi.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.oracle_fermi.restype = ctypes.c_double
@@ -176,7 +176,8 @@ def density(dev: Device, z, w, sgf_tol=1e-9, sgf_max_iter=300, nthreads=0):
 
 def density_neq(dev: Device, energies, w, frm, eta=1e-4, coupling=None, scba_niter=5, scba_tol=1e-7,
                 sgf_tol=1e-9, sgf_max_iter=300, nthreads=0):
-    """real_axis_int: sum_p w_p Gn(E_p) blocks, ncyc, status."""
+    """real_axis_int: sum_p w_p Gn(E_p) blocks, the calculate_Gn_outer
+    blocks per contact (device->contact, contact->device), ncyc, status."""
     E = np.ascontiguousarray(energies, dtype=np.float64).ravel()
     wt = np.ascontiguousarray(w, dtype=np.complex128).ravel()
     f = np.ascontiguousarray(frm, dtype=np.float64)
@@ -187,15 +188,18 @@ def density_neq(dev: Device, energies, w, frm, eta=1e-4, coupling=None, scba_nit
     rd = np.zeros(max(nd, 1), dtype=np.complex128)
     ru = np.zeros(max(no, 1), dtype=np.complex128)
     rl = np.zeros(max(no, 1), dtype=np.complex128)
+    nm = sum(n[cb - 1] * L for cb, L in zip(dev.cblk, dev.lead_size))
+    rdc = np.zeros(max(nm, 1), dtype=np.complex128)
+    rcd = np.zeros(max(nm, 1), dtype=np.complex128)
     ncyc = np.zeros(E.size, dtype=np.int32)
     status = np.zeros(E.size, dtype=np.int32)
     st = dev.to_struct()
     lib().oracle_density_neq(ctypes.addressof(st), E.size, _d(E), eta, _d(wt.view(np.float64)), _d(f),
                              _d(cp) if cp is not None else None, scba_niter, scba_tol, sgf_tol, sgf_max_iter,
                              _d(rd.view(np.float64)), _d(ru.view(np.float64)), _d(rl.view(np.float64)),
-                             _i(ncyc), _i(status), nthreads)
-    from libnegf_b200.density import split_blocks
-    return split_blocks(n, rd, ru, rl), ncyc, status
+                             _d(rdc.view(np.float64)), _d(rcd.view(np.float64)), _i(ncyc), _i(status), nthreads)
+    from libnegf_b200.density import split_blocks, split_outer
+    return split_blocks(n, rd, ru, rl), split_outer(dev, rdc, rcd), ncyc, status
 
 
 def meir_wingreen(dev: Device, energies, frm, coupling=None, eta=1e-4, scba_niter=5, scba_tol=1e-7,

@@ -97,25 +97,35 @@ def test_oracle_real_axis_vanishes_in_equilibrium():
     E, w = D.real_axis_points(mu=[0.0, 0.0], kT=[0.01, 0.01], n_kt=10, np_real=12, delta=1e-4)
     frm = D.neq_occupations(E, [0.0, 0.0], [0.01, 0.01], ref=1)
     assert np.all(frm == 0.0)
-    (rd, ru, rl), nc, st = O.density_neq(dev, E, w, frm, eta=1e-4)
-    assert all(np.abs(b).max() == 0.0 for b in rd + ru + rl)
+    (rd, ru, rl), (rdc, rcd), nc, st = O.density_neq(dev, E, w, frm, eta=1e-4)
+    assert all(np.abs(b).max() == 0.0 for b in rd + ru + rl + rdc + rcd)
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("deph", [False, True])
-def test_density_neq_parity(gpu_ctx, deph):
-    dev = G.transport_c0(nbl=4, n=6, seed=2)
+@pytest.mark.parametrize("deph,three", [(False, False), (True, False), (False, True)])
+def test_density_neq_parity(gpu_ctx, deph, three):
+    """Tridiagonal blocks and the outer blocks of calculate_Gn_outer."""
+    dev = G.transport_c0(nbl=4, n=6, seed=2, cblk=[1, 4, 2] if three else None)
     mu, kT = [0.1, -0.1], [0.01, 0.01]
     E, w = D.real_axis_points(mu=mu, kT=kT, n_kt=10, np_real=24, delta=1e-4)
+    if three:
+        mu, kT = mu + [0.05], kT + [0.01]
+        E, w = D.real_axis_points(mu=mu, kT=kT, n_kt=10, np_real=24, delta=1e-4)
     frm = D.neq_occupations(E, mu, kT, ref=2)
     cpl = np.full(dev.norb, 0.05) if deph else None
     did = gpu_ctx.upload(dev)
     try:
         gpu_ctx.set_options(scba_niter=5 if deph else 0)
-        (gd, gu, gl), nc, st = gpu_ctx.density_neq(did, E, w, frm, eta=1e-4, coupling=cpl)
-        (od, ou, ol), onc, ost = O.density_neq(dev, E, w, frm, eta=1e-4, coupling=cpl, scba_niter=5 if deph else 0)
+        (gd, gu, gl), (gdc, gcd), nc, st = gpu_ctx.density_neq(did, E, w, frm, eta=1e-4, coupling=cpl)
+        (od, ou, ol), (odc, ocd), onc, ost = O.density_neq(dev, E, w, frm, eta=1e-4, coupling=cpl,
+                                                           scba_niter=5 if deph else 0)
+        assert np.all(st == ost)
         assert _close(gd, od, 1e-9) and _close(gu, ou, 1e-9) and _close(gl, ol, 1e-9)
+        assert _close(gdc, odc, 1e-9) and _close(gcd, ocd, 1e-9)
         assert max(np.abs(b).max() for b in od) > 1e-4          # a bias window: a non-zero density
+        assert max(np.abs(b).max() for b in odc) > 1e-6          # and non-zero outer blocks
+        for a, b in zip(odc, ocd):                               # Gn(c,cb) = Gn(cb,c)^dag (real weights)
+            assert np.abs(a - b.conj().T).max() <= 1e-12 * max(1.0, np.abs(a).max())
     finally:
         gpu_ctx.set_options()
         gpu_ctx.release(did)
