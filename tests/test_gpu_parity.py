@@ -160,6 +160,25 @@ def test_transmission_parity(gpu_ctx, case):
         gpu_ctx.release(did)
 
 
+@pytest.mark.parametrize("gen", ["c0", "c1_S"])
+def test_transmission_parity_band_edges(gpu_ctx, gen):
+    """64 energies within 1e-3 eV of the band edges of lead 1 (the cluster of
+    the 512-orbital mixed-precision config), eta = 1e-6, where the solve is
+    least well conditioned."""
+    dev = (G.transport_c0(nbl=6, n=16, seed=5) if gen == "c0"
+           else G.transport_c1(nbl=5, n=24, seed=3, density=0.2))
+    E = G.band_edge_energies(dev, contact=0, nk=64, n_edges=64, window=1e-3)
+    did = gpu_ctx.upload(dev)
+    try:
+        T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6, check=False)
+        ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev)
+        assert np.all(st == ref["status"])
+        assert np.all(np.abs(ncyc - ref["ncyc"]) <= 4)
+        assert_T_close(T, ref["T"], spread=spread["T"])
+    finally:
+        gpu_ctx.release(did)
+
+
 @pytest.mark.parametrize("case", ["chain1", "c0_small", "c0_n32"])
 def test_transmission_parity_default_eta(gpu_ctx, case):
     """At libNEGF's default broadening delta = 1e-4 (lib_param.F90:628)."""
