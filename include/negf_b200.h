@@ -143,6 +143,24 @@ const char* negf_b200_last_error(const negf_b200_ctx* ctx);
  * arrays may be freed after the call. */
 int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dev,
                             int32_t* device_id);
+/* The same from libNEGF's own input: the global H (and S; s_vals = NULL is
+ * S = I, set_S_id) over device + contact orbitals as a 1-based z_CSR
+ * (rowptr nrow+1, colind and values nnz, complex interleaved) and the
+ * negf_init_structure arrays (src/api/libnegf_api.f90:146-185: plend per
+ * PL, cblk / surfstart / surfend / contend per contact, 1-based).  The
+ * dense blocks that zcsr2blk_sod (src/sparsekit_drv.F90:3409-3436) and
+ * extract_cont (src/ln_extract.F90:37-75) take from the CSR on the host are
+ * scattered from it on the GPU: the device's tridiagonal blocks, per
+ * contact its first-PL block, the PL1 -> PL2 coupling and the coupling of
+ * device PL cblk to PL1.  Surface blocks (surfend >= surfstart) are
+ * rejected.  Temporary device memory: the CSR plus the dense blocks. */
+int negf_b200_upload_csr(negf_b200_ctx* ctx, int32_t nrow, int32_t nnz,
+                         const int32_t* rowptr, const int32_t* colind,
+                         const double* h_vals, const double* s_vals,
+                         int32_t npl, const int32_t* plend, int32_t ncont,
+                         const int32_t* cblk, const int32_t* surfstart,
+                         const int32_t* surfend, const int32_t* contend,
+                         int32_t* device_id);
 int negf_b200_release_device(negf_b200_ctx* ctx, int32_t device_id);
 /* Bytes of HBM the device description holds. */
 int negf_b200_device_bytes(const negf_b200_ctx* ctx, int32_t device_id,
@@ -297,6 +315,20 @@ int negf_b200_set_workspace_limit(negf_b200_ctx* ctx, size_t bytes);
  * stored and the next call that finds the arena full starts afresh.
  * Releasing a device drops its entries.  The _dev solves do not use it. */
 int negf_b200_set_sgf_cache(negf_b200_ctx* ctx, int32_t mode, size_t bytes);
+/* Disk copy of the cache, for reuse across runs: the counterpart of
+ * TMatrixCacheDisk (src/ln_cache.F90:154-511), which writes each surface GF
+ * to its own file and reads it back when ReadOldSGF = 0
+ * (src/contselfenergy.F90:161-167).  _save writes every cached gs with a
+ * fingerprint of its lead (L and the H00, H01, S00, S01 blocks), the energy,
+ * broadening, tolerance and iteration cap to one file; *entries = number
+ * written.  _load (cache enabled) adds the file's entries for every
+ * uploaded device whose contact has a lead with that fingerprint, as far as
+ * the arena has room; *entries = number of file entries used.  Device ids
+ * need not match between runs. */
+int negf_b200_sgf_cache_save(negf_b200_ctx* ctx, const char* path,
+                             int64_t* entries);
+int negf_b200_sgf_cache_load(negf_b200_ctx* ctx, const char* path,
+                             int64_t* entries);
 int negf_b200_sgf_cache_stats(const negf_b200_ctx* ctx, int64_t* hits,
                               int64_t* misses, int64_t* entries,
                               size_t* bytes_used);

@@ -33,7 +33,21 @@ struct DeviceRec {
   void* proj_tun = nullptr;    // device copies of the projections (owned)
   void* proj_dos = nullptr;
   int nldos = 0;
+  // fingerprint of each contact's lead blocks (L, H00, H01, S00, S01): the surface
+  // Green's function depends on nothing else, so a saved one is reused by any
+  // device whose contact has the same lead
+  uint64_t lead_hash[negf::kMaxCont] = {0};
 };
+
+// FNV-1a over a byte range, chained
+uint64_t fnv1a(uint64_t h, const void* p, size_t n) {
+  const unsigned char* b = static_cast<const unsigned char*>(p);
+  for (size_t i = 0; i < n; ++i) {
+    h ^= b[i];
+    h *= 0x100000001B3ull;
+  }
+  return h;
+}
 
 void free_projections(DeviceRec& r) {
   if (r.proj_tun) cudaFree(r.proj_tun);
@@ -395,9 +409,10 @@ int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* o) {
 
 const char* negf_b200_last_error(const negf_b200_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
 
-int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_id) {
-  if (!ctx || !dv || !device_id) return NEGF_B200_ERR_BAD_ARG;
-  std::lock_guard<std::mutex> lk(ctx->mu);
+namespace {
+// The block arrays of `dv` may be host or device memory (copies with
+// cudaMemcpyDefault); pl_size, cblk and lead_size are host arrays.
+int upload_impl(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_id) {
   const int nbl = dv->nbl, ncont = dv->ncont;
   if (nbl < 1 || !dv->pl_size || !dv->h_diag || (nbl > 1 && (!dv->h_upper || !dv->h_lower)))
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "device needs nbl >= 1 and H blocks");
@@ -458,7 +473,7 @@ int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int3
     void* dst = b + off;
     off += (nbytes + 15) & ~size_t(15);
     if (src && nbytes) {
-      cudaError_t ce = cudaMemcpy(dst, src, nbytes, cudaMemcpyHostToDevice);
+      cudaError_t ce = cudaMemcpy(dst, src, nbytes, cudaMemcpyDefault);
       if (ce != cudaSuccess) perr = ce;
     }
     return dst;
@@ -496,7 +511,30 @@ int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int3
   DeviceRec r;
   r.live = true; r.blob = blob; r.bytes = bytes; r.desc = d;
   r.nbl = nbl; r.ncont = ncont; r.norb = norb; r.nmax = nmax; r.has_s = has_s;
-  for (int c = 0; c < ncont; ++c) r.cblk[c] = dv->cblk[c];
+  for (int c = 0; c < ncont; ++c) {
+    r.cblk[c] = dv->cblk[c];
+    const int L = dv->lead_size[c];
+    const size_t nb = (size_t)L * L * 16;
+    std::vector<char> tmp(nb);
+    auto blk = [&](const double2* p) {   // the uploaded copy: host and device sources alike
+      if (cudaMemcpy(tmp.data(), p + olead[c], nb, cudaMemcpyDeviceToHost) != cudaSuccess) perr = cudaErrorUnknown;
+      return tmp.data();
+    };
+    uint64_t h = fnv1a(0xCBF29CE484222325ull, &L, sizeof(L));
+    h = fnv1a(h, blk(d.h00), nb);
+    h = fnv1a(h, blk(d.h01), nb);
+    const int32_t f00 = has00 ? 1 : 0, f01 = has01 ? 1 : 0;
+    h = fnv1a(h, &f00, 4);
+    if (has00) h = fnv1a(h, blk(d.s00), nb);
+    h = fnv1a(h, &f01, 4);
+    if (has01) h = fnv1a(h, blk(d.s01), nb);
+    r.lead_hash[c] = h;
+  }
+  if (perr != cudaSuccess) {
+    cudaGetLastError();
+    cudaFree(blob);
+    return fail(ctx, NEGF_B200_ERR_CUDA, "upload of the device description failed");
+  }
   int id = -1;
   for (size_t i = 0; i < ctx->devs.size(); ++i)
     if (!ctx->devs[i].live) { id = (int)i; break; }
@@ -505,6 +543,119 @@ int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int3
   *device_id = id;
   (void)st;
   return NEGF_B200_OK;
+}
+}  // namespace
+
+int negf_b200_upload_device(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_id) {
+  if (!ctx || !dv || !device_id) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  return upload_impl(ctx, dv, device_id);
+}
+
+int negf_b200_upload_csr(negf_b200_ctx* ctx, int32_t nrow, int32_t nnz, const int32_t* rowptr, const int32_t* colind,
+                         const double* h_vals, const double* s_vals, int32_t npl, const int32_t* plend,
+                         int32_t ncont, const int32_t* cblk, const int32_t* surfstart, const int32_t* surfend,
+                         const int32_t* contend, int32_t* device_id) {
+  if (!ctx || !device_id) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (nrow < 1 || nnz < 0 || !rowptr || (nnz > 0 && (!colind || !h_vals)) || npl < 1 || !plend || ncont < 1 ||
+      ncont > negf::kMaxCont || !cblk || !surfstart || !surfend || !contend)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "bad CSR or structure arrays");
+  if (rowptr[0] != 1 || rowptr[nrow] != nnz + 1)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "rowptr must be 1-based with rowptr(nrow+1) = nnz + 1");
+  // create_TStruct: PLs from plend, contacts from surfstart / surfend / contend
+  std::vector<int32_t> pl(npl), plstart(npl + 1, 0), L(ncont);
+  std::vector<int64_t> od(npl), oo(std::max(1, npl - 1));
+  int64_t nd = 0, no = 0, nl = 0, nm = 0;
+  for (int i = 0; i < npl; ++i) {
+    plstart[i + 1] = plend[i];
+    pl[i] = plend[i] - plstart[i];
+    if (pl[i] < 1) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "plend must increase");
+    od[i] = nd;
+    nd += (int64_t)pl[i] * pl[i];
+  }
+  for (int i = 0; i + 1 < npl; ++i) {
+    oo[i] = no;
+    no += (int64_t)pl[i] * pl[i + 1];
+  }
+  negf::CsrScatter a{};
+  a.nrow = nrow; a.nnz = nnz; a.ndev = plend[npl - 1]; a.npl = npl; a.ncont = ncont;
+  for (int c = 0; c < ncont; ++c) {
+    const int ncdim = contend[c] - surfstart[c] + 1;
+    if (surfend[c] != surfstart[c] - 1)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "contact " + std::to_string(c + 1) +
+                                                  ": surface blocks (surfdim > 0) are not supported");
+    if (ncdim < 2 || ncdim % 2 || contend[c] > nrow || surfstart[c] <= a.ndev || cblk[c] < 1 || cblk[c] > npl)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "contact " + std::to_string(c + 1) + ": bad extent or cblk");
+    L[c] = ncdim / 2;
+    a.j0[c] = surfstart[c] - 1; a.L[c] = L[c]; a.cb[c] = cblk[c];
+    a.olead[c] = nl; nl += (int64_t)L[c] * L[c];
+    a.omc[c] = nm; nm += (int64_t)pl[cblk[c] - 1] * L[c];
+  }
+  const bool has_s = s_vals != nullptr;
+  const int64_t ns = has_s ? 2 : 1;
+  // one scratch allocation: staging blocks, then the CSR and index copies
+  const int64_t blk_elems = ns * (nd + 2 * no + 2 * nl + nm);
+  size_t off = 0;
+  auto carve = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~size_t(255); return o; };
+  const size_t o_blk = carve((size_t)blk_elems * 16), o_rp = carve((size_t)(nrow + 1) * 4),
+               o_ci = carve((size_t)std::max(nnz, 1) * 4), o_hv = carve((size_t)std::max(nnz, 1) * 16),
+               o_sv = carve(has_s ? (size_t)std::max(nnz, 1) * 16 : 0), o_ps = carve((size_t)(npl + 1) * 4),
+               o_od = carve((size_t)npl * 8), o_oo = carve(oo.size() * 8), o_bad = carve(4);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  char* tmp = nullptr;
+  if (cudaMalloc(&tmp, off) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, NEGF_B200_ERR_NOMEM, "device allocation of the CSR staging failed");
+  }
+  cudaStream_t s = ctx->stream;
+  double2* blk = reinterpret_cast<double2*>(tmp + o_blk);
+  double2* p = blk;
+  auto take = [&](int64_t n) { double2* q = p; p += n; return q; };
+  a.hd = take(nd); a.hu = take(no); a.hl = take(no); a.h00 = take(nl); a.h01 = take(nl); a.hmc = take(nm);
+  if (has_s) { a.sd = take(nd); a.su = take(no); a.sl = take(no); a.s00 = take(nl); a.s01 = take(nl); a.smc = take(nm); }
+  a.rowptr = reinterpret_cast<const int*>(tmp + o_rp);
+  a.colind = reinterpret_cast<const int*>(tmp + o_ci);
+  a.hv = reinterpret_cast<const double2*>(tmp + o_hv);
+  a.sv = has_s ? reinterpret_cast<const double2*>(tmp + o_sv) : nullptr;
+  a.plstart = reinterpret_cast<const int*>(tmp + o_ps);
+  a.od = reinterpret_cast<const int64_t*>(tmp + o_od);
+  a.oo = reinterpret_cast<const int64_t*>(tmp + o_oo);
+  a.bad = reinterpret_cast<int*>(tmp + o_bad);
+  cudaError_t e = cudaMemsetAsync(blk, 0, (size_t)blk_elems * 16, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(a.bad, 0, 4, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + o_rp, rowptr, (size_t)(nrow + 1) * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nnz > 0) e = cudaMemcpyAsync(tmp + o_ci, colind, (size_t)nnz * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && nnz > 0) e = cudaMemcpyAsync(tmp + o_hv, h_vals, (size_t)nnz * 16, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && has_s && nnz > 0)
+    e = cudaMemcpyAsync(tmp + o_sv, s_vals, (size_t)nnz * 16, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + o_ps, plstart.data(), (size_t)(npl + 1) * 4, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + o_od, od.data(), (size_t)npl * 8, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(tmp + o_oo, oo.data(), oo.size() * 8, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = negf::launch_csr_scatter(a, s);
+  int bad = 0;
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&bad, a.bad, 4, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    cudaFree(tmp);
+    return cuda_fail(ctx, e, "CSR extraction");
+  }
+  if (bad) {
+    cudaFree(tmp);
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "CSR index outside the matrix or rowptr not monotone");
+  }
+  negf_b200_device dv{};
+  dv.nbl = npl; dv.pl_size = pl.data(); dv.ncont = ncont; dv.cblk = cblk; dv.lead_size = L.data();
+  auto dp = [](const double2* q) { return reinterpret_cast<const double*>(q); };
+  dv.h_diag = dp(a.hd); dv.h_upper = dp(a.hu); dv.h_lower = dp(a.hl);
+  dv.lead_h00 = dp(a.h00); dv.lead_h01 = dp(a.h01); dv.hmc = dp(a.hmc);
+  if (has_s) {
+    dv.s_diag = dp(a.sd); dv.s_upper = dp(a.su); dv.s_lower = dp(a.sl);
+    dv.lead_s00 = dp(a.s00); dv.lead_s01 = dp(a.s01); dv.smc = dp(a.smc);
+  }
+  const int st = upload_impl(ctx, &dv, device_id);
+  cudaFree(tmp);
+  return st;
 }
 
 int negf_b200_release_device(negf_b200_ctx* ctx, int32_t id) {
@@ -636,6 +787,105 @@ int negf_b200_set_workspace_limit(negf_b200_ctx* ctx, size_t bytes) {
     ctx->ws = nullptr;
     ctx->ws_bytes = 0;
   }
+  return NEGF_B200_OK;
+}
+
+// File layout (little-endian): "NEGFSGF1", int64 count, then per entry
+// uint64 lead fingerprint, int32 L, int32 maxit, uint64 bits of E, eta, tol,
+// L*L complex128 (column-major) values.
+namespace {
+const char kSgfMagic[8] = {'N', 'E', 'G', 'F', 'S', 'G', 'F', '1'};
+struct SgfFileEntry {
+  uint64_t hash;
+  int32_t L, maxit;
+  uint64_t e, eta, tol;
+};
+}  // namespace
+
+int negf_b200_sgf_cache_save(negf_b200_ctx* ctx, const char* path, int64_t* entries) {
+  if (!ctx || !path) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream));
+  const SgfCache& c = ctx->sgf;
+  std::vector<double2> host((size_t)std::max<int64_t>(c.used, 1));
+  if (c.used > 0) CK(cudaMemcpy(host.data(), c.arena, (size_t)c.used * 16, cudaMemcpyDeviceToHost));
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(ctx, NEGF_B200_ERR_BAD_ARG, std::string("cannot write ") + path);
+  // one entry per (lead, energy, broadening, tolerance): devices sharing a lead share it
+  std::vector<std::pair<SgfFileEntry, int64_t>> out;
+  std::unordered_map<uint64_t, int> seen;
+  for (const auto& kv : c.map) {
+    const DeviceRec& r = ctx->devs[kv.first.dev];
+    SgfFileEntry e{r.lead_hash[kv.first.cont], r.desc.L[kv.first.cont], kv.first.maxit, kv.first.e, kv.first.eta,
+                   kv.first.tol};
+    const uint64_t k = fnv1a(fnv1a(fnv1a(e.hash, &e.e, 8), &e.eta, 8), &e.tol, 8);
+    if (seen.count(k)) continue;
+    seen[k] = 1;
+    out.push_back({e, kv.second});
+  }
+  const int64_t n = (int64_t)out.size();
+  bool ok = std::fwrite(kSgfMagic, 1, 8, f) == 8 && std::fwrite(&n, 8, 1, f) == 1;
+  for (const auto& e : out) {
+    ok = ok && std::fwrite(&e.first, sizeof(SgfFileEntry), 1, f) == 1;
+    ok = ok && std::fwrite(host.data() + e.second, 16, (size_t)e.first.L * e.first.L, f) ==
+                   (size_t)e.first.L * e.first.L;
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) return fail(ctx, NEGF_B200_ERR_BAD_ARG, std::string("write error on ") + path);
+  if (entries) *entries = n;
+  return NEGF_B200_OK;
+}
+
+int negf_b200_sgf_cache_load(negf_b200_ctx* ctx, const char* path, int64_t* entries) {
+  if (!ctx || !path) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  SgfCache& c = ctx->sgf;
+  if (c.mode == 0 || !c.arena) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "enable the SGF cache before loading into it");
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  CK(cudaStreamSynchronize(ctx->stream));
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(ctx, NEGF_B200_ERR_BAD_ARG, std::string("cannot read ") + path);
+  char magic[8];
+  int64_t n = 0, loaded = 0;
+  bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kSgfMagic, 8) == 0 && std::fread(&n, 8, 1, f) == 1 &&
+            n >= 0;
+  std::vector<SgfFileEntry> ents;
+  std::vector<std::vector<double2>> vals;
+  for (int64_t q = 0; ok && q < n; ++q) {
+    SgfFileEntry e;
+    ok = std::fread(&e, sizeof(e), 1, f) == 1 && e.L >= 1 && e.L <= negf::kMaxOrder;
+    if (!ok) break;
+    std::vector<double2> v((size_t)e.L * e.L);
+    ok = std::fread(v.data(), 16, v.size(), f) == v.size();
+    ents.push_back(e);
+    vals.push_back(std::move(v));
+  }
+  std::fclose(f);
+  if (!ok) return fail(ctx, NEGF_B200_ERR_BAD_ARG, std::string("not an SGF cache file or truncated: ") + path);
+  for (size_t q = 0; q < ents.size(); ++q) {
+    const SgfFileEntry& e = ents[q];
+    const int64_t L2 = (int64_t)e.L * e.L;
+    const std::vector<double2>& buf = vals[q];
+    bool used_once = false;
+    for (size_t d = 0; d < ctx->devs.size(); ++d) {
+      const DeviceRec& r = ctx->devs[d];
+      if (!r.live) continue;
+      for (int k = 0; k < r.ncont; ++k) {
+        if (r.lead_hash[k] != e.hash || r.desc.L[k] != e.L) continue;
+        SgfKey key{(int32_t)d, k, e.e, e.eta, e.tol, e.maxit};
+        if (c.map.count(key)) continue;
+        if (c.used + L2 > c.cap) continue;                 // no room: computed when needed
+        const int64_t off = c.used;
+        CK(cudaMemcpy(c.arena + off, buf.data(), (size_t)L2 * 16, cudaMemcpyHostToDevice));
+        c.used += (L2 + 15) & ~int64_t(15);
+        c.map[key] = off;
+        used_once = true;
+      }
+    }
+    loaded += used_once ? 1 : 0;
+  }
+  if (entries) *entries = loaded;
   return NEGF_B200_OK;
 }
 

@@ -98,6 +98,24 @@ int64_t engine_ws_elems(int mode, int nbl_max, int ncont_max, int nmax);
 size_t engine_smem_bytes(int nmax);
 
 cudaError_t launch_engine(const EngineArgs& a, int grid, cudaStream_t s);
+
+// CSR -> dense blocks (csr.cu).  Indices 1-based as libNEGF's z_CSR; the
+// outputs are zero-filled staging arrays in the negf_b200_device layout.
+struct CsrScatter {
+  int nrow, nnz, ndev, npl, ncont;
+  const int* rowptr;            // nrow + 1
+  const int* colind;            // nnz
+  const double2* hv;            // nnz
+  const double2* sv;            // nnz or null (S = I)
+  const int* plstart;           // npl + 1, 0-based first orbital of each PL, plstart[npl] = ndev
+  const int64_t* od;            // npl, offsets of H(i,i) in hd
+  const int64_t* oo;            // npl - 1, offsets of H(i,i+1) / H(i+1,i)
+  int j0[kMaxCont], L[kMaxCont], cb[kMaxCont];   // 0-based first contact orbital, PL size, cblk
+  int64_t olead[kMaxCont], omc[kMaxCont];
+  double2 *hd, *hu, *hl, *sd, *su, *sl, *h00, *h01, *s00, *s01, *hmc, *smc;
+  int* bad;                     // set on an index outside the matrix
+};
+cudaError_t launch_csr_scatter(const CsrScatter& a, cudaStream_t s);
 cudaError_t launch_zgemm_batched(int batch, int m, int n, int k, double2 alpha, const double2* A,
                                  int64_t sA, const double2* B, int64_t sB, double2 beta, double2* C,
                                  int64_t sC, int dagger, cudaStream_t s);

@@ -34,8 +34,23 @@ EXPORTED = [
     "negf_b200_get_trace", "negf_b200_decimation_noalloc", "negf_b200_set_tun_proj", "negf_b200_set_dos_proj",
     "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
     "negf_b200_set_workspace_limit", "negf_b200_density", "negf_b200_density_neq", "negf_b200_meir_wingreen_dev",
+    "negf_b200_sgf_cache_save", "negf_b200_sgf_cache_load", "negf_b200_upload_csr",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
+
+
+class DeviceShape:
+    """Structure of a device uploaded from CSR (its blocks live only on the
+    GPU): what the solve wrappers need to size their outputs."""
+
+    def __init__(self, pl_size, cblk, lead_size):
+        self.pl_size = list(pl_size)
+        self.cblk = list(cblk)
+        self.lead_size = list(lead_size)
+
+    nbl = property(lambda self: len(self.pl_size))
+    norb = property(lambda self: int(sum(self.pl_size)))
+    ncont = property(lambda self: len(self.cblk))
 
 
 class NegfError(RuntimeError):
@@ -73,6 +88,7 @@ def load():
     L.negf_b200_ctx_destroy.argtypes = [vp]
     L.negf_b200_set_options.argtypes = [vp, ctypes.POINTER(Options)]
     L.negf_b200_upload_device.argtypes = [vp, vp, ip]
+    L.negf_b200_upload_csr.argtypes = [vp, i32, i32, ip, ip, dp, dp, i32, ip, i32, ip, ip, ip, ip, ip]
     L.negf_b200_release_device.argtypes = [vp, i32]
     L.negf_b200_device_bytes.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_size_t)]
     L.negf_b200_transmission.argtypes = [vp, i32, ip, dp, f64, i32, i32, dp, ip, ip]
@@ -102,6 +118,8 @@ def load():
     L.negf_b200_density_neq.argtypes = [vp, i32, i32, dp, f64, dp, dp, dp, dp, dp, dp, dp, dp, ip, ip]
     i64p = ctypes.POINTER(ctypes.c_int64)
     L.negf_b200_sgf_cache_stats.argtypes = [vp, i64p, i64p, i64p, ctypes.POINTER(ctypes.c_size_t)]
+    L.negf_b200_sgf_cache_save.argtypes = [vp, ctypes.c_char_p, i64p]
+    L.negf_b200_sgf_cache_load.argtypes = [vp, ctypes.c_char_p, i64p]
     _lib = L
     return L
 
@@ -185,6 +203,25 @@ class Context:
         self.devices[did.value] = dev
         return did.value
 
+    def upload_csr(self, H, S, plend, cblk, surfstart, surfend, contend) -> int:
+        """Uploads a device from the global sparse H (and S, or None for
+        S = I) and the negf_init_structure arrays (1-based), the blocks
+        being extracted on the GPU (negf_b200_upload_csr).  H and S go to
+        the C-ABI on their union pattern."""
+        from .structure import csr_arrays
+        rp, ci, hv, sv = csr_arrays(H, S)
+        a = lambda x: np.ascontiguousarray(x, dtype=np.int32)
+        pe, cb, ss, se, ce = a(plend), a(cblk), a(surfstart), a(surfend), a(contend)
+        did = ctypes.c_int32()
+        self._check(self._L.negf_b200_upload_csr(
+            self._h, rp.size - 1, int(ci.size), _i(rp), _i(ci), _d(hv.view(np.float64)),
+            _d(sv.view(np.float64)) if sv is not None else None, pe.size, _i(pe), cb.size, _i(cb), _i(ss), _i(se),
+            _i(ce), ctypes.byref(did)), "upload_csr")
+        starts = np.concatenate([[0], pe[:-1]])
+        self.devices[did.value] = DeviceShape(pl_size=[int(x) for x in pe - starts], cblk=[int(x) for x in cb],
+                                              lead_size=[int(x) for x in (ce - ss + 1) // 2])
+        return did.value
+
     def set_tun_proj(self, device_id, tun_proj):
         """tun_proj (1-based orbital indices) of the device; None or [] = whole trace."""
         idx = tun_indices(tun_proj if tun_proj is not None else [])
@@ -228,6 +265,19 @@ class Context:
     def set_workspace_limit(self, nbytes: int):
         """Caps the engine workspace (0 = none); see negf_b200_set_workspace_limit."""
         self._check(self._L.negf_b200_set_workspace_limit(self._h, nbytes), "set_workspace_limit")
+
+    def sgf_cache_save(self, path) -> int:
+        """Writes the cached surface GFs to `path`; returns the entry count."""
+        n = ctypes.c_int64()
+        self._check(self._L.negf_b200_sgf_cache_save(self._h, os.fsencode(path), ctypes.byref(n)), "sgf_cache_save")
+        return n.value
+
+    def sgf_cache_load(self, path) -> int:
+        """Adds the entries of `path` for the uploaded devices' leads; returns
+        the number of file entries used."""
+        n = ctypes.c_int64()
+        self._check(self._L.negf_b200_sgf_cache_load(self._h, os.fsencode(path), ctypes.byref(n)), "sgf_cache_load")
+        return n.value
 
     def sgf_cache_stats(self) -> dict:
         h, m, e = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

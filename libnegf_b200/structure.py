@@ -91,6 +91,31 @@ def device_from_csr(H, S, plend: Sequence[int], cblk: Sequence[int], surfstart: 
     return dev
 
 
+def csr_arrays(H, S=None):
+    """The arrays negf_b200_upload_csr takes: 1-based rowptr / colind (int32)
+    of one pattern, and the complex values of H and of S (or None) on it.
+    With S, the pattern is the union of both sparsity patterns, each matrix
+    holding zeros where only the other has an entry."""
+    import scipy.sparse as sp
+    H = sp.csr_matrix(H, dtype=np.complex128)
+    if S is None:
+        H = H.copy()
+        H.sum_duplicates()
+        return (np.ascontiguousarray(H.indptr + 1, dtype=np.int32), np.ascontiguousarray(H.indices + 1, dtype=np.int32),
+                np.ascontiguousarray(H.data), None)
+    S = sp.csr_matrix(S, dtype=np.complex128)
+    if S.shape != H.shape:
+        raise ValueError("H and S differ in shape")
+    pattern = (abs(H) + abs(S)).tocsr()
+    pattern.sum_duplicates()
+    pattern.sort_indices()
+    rows = np.repeat(np.arange(pattern.shape[0]), np.diff(pattern.indptr))
+    hv = np.ascontiguousarray(np.asarray(H[rows, pattern.indices]).ravel(), dtype=np.complex128)
+    sv = np.ascontiguousarray(np.asarray(S[rows, pattern.indices]).ravel(), dtype=np.complex128)
+    return (np.ascontiguousarray(pattern.indptr + 1, dtype=np.int32),
+            np.ascontiguousarray(pattern.indices + 1, dtype=np.int32), hv, sv)
+
+
 def csr_from_device(dev: Device):
     """The inverse layout (for tests and examples): the global sparse H (and
     S, or None) of a Device with its contacts appended after the device

@@ -1,10 +1,13 @@
 """Host side of the path: CSR -> blocks (extract_cont / zcsr2blk_sod), the
 energy grid, fermi_f, integrate_el and the energy loop, checked against the
 oracle's restatements (CPU) and, for the loop, the GPU engine (gpu)."""
+import ctypes
+
 import numpy as np
 import pytest
 
 from libnegf_b200 import energy as En
+from libnegf_b200 import native
 from libnegf_b200 import generators as G
 from libnegf_b200 import structure as St
 from oracle import oracle as O
@@ -57,6 +60,62 @@ def test_csr_extraction_round_trip(with_s):
     t1, _, _ = O.transmission(dev, E, eta=1e-6)
     t2, _, _ = O.transmission(d2, E, eta=1e-6)
     assert np.array_equal(t1, t2)
+
+
+@pytest.mark.parametrize("with_s", [False, True])
+def test_csr_arrays_hold_h_and_s_on_one_pattern(with_s):
+    """The 1-based arrays of negf_b200_upload_csr rebuild H and S exactly."""
+    import scipy.sparse as sp
+    dev = G.transport_c1(nbl=4, n=6, seed=2, density=0.5) if with_s else G.transport_c0(nbl=5, n=4, seed=3)
+    H, S, *_ = St.csr_from_device(dev)
+    rp, ci, hv, sv = St.csr_arrays(H, S)
+    assert rp.dtype == np.int32 and ci.dtype == np.int32 and rp[0] == 1 and rp[-1] == ci.size + 1
+    n = rp.size - 1
+    H2 = sp.csr_matrix((hv, ci - 1, rp - 1), shape=(n, n))
+    assert abs(H2 - sp.csr_matrix(H)).max() == 0
+    if with_s:
+        S2 = sp.csr_matrix((sv, ci - 1, rp - 1), shape=(n, n))
+        assert abs(S2 - sp.csr_matrix(S)).max() == 0
+    else:
+        assert sv is None
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", ["c0", "c1_S", "three"])
+def test_upload_csr_matches_block_upload(gpu_ctx, case):
+    """Blocks extracted from the CSR on the GPU give the same T and DOS, bit
+    for bit, as the host-extracted blocks."""
+    dev = {"c0": lambda: G.transport_c0(nbl=5, n=12, seed=3),
+           "c1_S": lambda: G.transport_c1(nbl=4, n=20, seed=2, density=0.3),
+           "three": lambda: G.transport_c0(nbl=5, n=8, seed=1, cblk=[1, 5, 3])}[case]()
+    H, S, plend, cblk, ss, se, ce = St.csr_from_device(dev)
+    E = np.linspace(-2, 2, 9)
+    d1 = gpu_ctx.upload(dev)
+    d2 = gpu_ctx.upload_csr(H, S, plend, cblk, ss, se, ce)
+    try:
+        pairs = [(1, 2), (1, 3), (2, 3)] if case == "three" else [(1, 2)]
+        T1, l1, _, _ = gpu_ctx.transmissions(d1, E, pairs, eta=1e-4)
+        T2, l2, _, _ = gpu_ctx.transmissions(d2, E, pairs, eta=1e-4)
+        assert np.array_equal(T1, T2)
+        if case != "three":
+            _, dos1, _, _ = gpu_ctx.transmission_dos(d1, E, eta=1e-4)
+            _, dos2, _, _ = gpu_ctx.transmission_dos(d2, E, eta=1e-4)
+            assert np.array_equal(dos1, dos2)
+        # a column index outside the matrix is an argument error, not a fault
+        rp, ci, hv, sv = St.csr_arrays(H, S)
+        ci[3] = rp.size + 5
+        L = native.load()
+        a = lambda x: np.ascontiguousarray(x, dtype=np.int32)
+        dp = lambda x: x.view(np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double)) if x is not None else None
+        ip = lambda x: x.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+        did = ctypes.c_int32()
+        pe, cb, s1, s2, c2 = a(plend), a(cblk), a(ss), a(se), a(ce)
+        rc = L.negf_b200_upload_csr(gpu_ctx.handle, rp.size - 1, ci.size, ip(rp), ip(ci), dp(hv), dp(sv), pe.size,
+                                    ip(pe), cb.size, ip(cb), ip(s1), ip(s2), ip(c2), ctypes.byref(did))
+        assert rc == native.BAD_ARG
+    finally:
+        gpu_ctx.release(d1)
+        gpu_ctx.release(d2)
 
 
 def test_csr_extraction_rejects_surface_blocks():

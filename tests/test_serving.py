@@ -43,6 +43,41 @@ def test_sgf_cache_reuses_surface_gf(gpu_ctx):
 
 
 @pytest.mark.gpu
+def test_sgf_cache_file_round_trip(tmp_path):
+    """Saved surface GFs are read back in another context (other device ids)
+    and by a device that only shares the leads: all hits, the same T."""
+    import copy
+    from libnegf_b200 import native
+    dev = G.transport_c0(nbl=5, n=16, seed=2)
+    other = copy.deepcopy(dev)
+    other.h_diag[2] = other.h_diag[2] + 0.1 * np.eye(16)        # same leads, another interior
+    E = np.linspace(-2.5, 2.5, 13)
+    path = str(tmp_path / "sgf.bin")
+    with native.Context(0) as c1:
+        c1.set_sgf_cache(1, 64 << 20)
+        d1 = c1.upload(dev)
+        T1, nc1, _ = c1.transmission(d1, E, eta=1e-6)
+        assert c1.sgf_cache_save(path) == 2 * E.size
+    with native.Context(0) as c2:
+        c2.set_sgf_cache(1, 64 << 20)
+        c2.upload(G.transport_c0(nbl=3, n=8, seed=9))              # shifts the device ids
+        d2 = c2.upload(dev)
+        d3 = c2.upload(other)
+        assert c2.sgf_cache_load(path) == 2 * E.size
+        s0 = c2.sgf_cache_stats()
+        T2, nc2, _ = c2.transmission(d2, E, eta=1e-6)
+        T3, nc3, _ = c2.transmission(d3, E, eta=1e-6)
+        s1 = c2.sgf_cache_stats()
+        assert s1["hits"] - s0["hits"] == 4 * E.size and s1["misses"] == s0["misses"]
+        assert np.array_equal(T2, T1) and np.all(nc2 == 0) and np.all(nc3 == 0)
+        ref, spread = oracle_spread(lambda d: O.transmission(d, E, eta=1e-6)[0], other)
+        assert_T_close(T3, ref, spread=spread)
+        # another broadening is not in the file
+        _, nc4, _ = c2.transmission(d2, E, eta=1e-5)
+        assert np.all(nc4 > 0)
+
+
+@pytest.mark.gpu
 def test_workspace_limit_runs_fewer_ctas(gpu_ctx):
     from libnegf_b200 import native
     dev = G.transport_c0(nbl=8, n=32, seed=3)
