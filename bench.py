@@ -92,7 +92,7 @@ def point_list(wl, seed=11):
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_engine
 # launch, from an ncu capture of the default c1 command (592 points per step)
-DRAM_BYTES_PER_LAUNCH = {("c1", 592): 8.4577e12}
+DRAM_BYTES_PER_LAUNCH = {("c1", 592): 8.028e12}
 
 
 def flops_per_point(wl, ncyc_total, ncont=2):
