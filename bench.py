@@ -413,6 +413,11 @@ def run_serve(args):
         "status_counts": {str(k): int(v) for k, v in
                           zip(*np.unique(np.concatenate([r.status for r in reqs]), return_counts=True))},
         "clocks": clk.summary(),
+        # the served figure is end to end already: host submission to host results
+        "e2e": {"value": pts / span, "unit": "solves/s",
+                "h2d_bytes_per_step": int(sum(r.energies.nbytes + r.device.nbytes() for r in reqs)),
+                "d2h_bytes_per_step": int(sum(r.T.nbytes + (r.ledos.nbytes if r.ledos is not None else 0)
+                                              for r in reqs))},
     }
     print(json.dumps(line), flush=True)
 
