@@ -37,7 +37,10 @@ constexpr int kStages = NEGF_GEMM_STAGES;   // cp.async ring depth
 static_assert(TK == 8 || TK == 16, "K tile of 8 or 16");
 constexpr int kStageElems = TK * A_LD + TN * B_LD;
 constexpr int kGemmSmemBytes = kStages * kStageElems * 16;
-constexpr int kSmallInvMax = 64;       // n <= 64: whole matrix in shared memory
+#ifndef NEGF_SMALL_INV_MAX
+#define NEGF_SMALL_INV_MAX 64
+#endif
+constexpr int kSmallInvMax = NEGF_SMALL_INV_MAX;   // n <= kSmallInvMax: whole matrix in shared memory
 
 // ---------------------------------------------------------------- complex
 __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
@@ -627,7 +630,9 @@ struct InvScratch {
 };
 
 // Pivot search on a column in shared memory: rows [j, n) of col[] -> index
-// of max |Re|+|Im| (first occurrence, as izamax).  All threads call.
+// of max |Re|+|Im| (first occurrence, as izamax).  All threads call; the
+// caller puts a barrier between two calls (s.redv / s.redi are reused):
+// gj_step's capture and update barriers do.
 __device__ __forceinline__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double best = -1.0;
@@ -650,17 +655,28 @@ __device__ __forceinline__ int cta_pivot(const double2* col, int j, int n, InvSc
     int oi = s.redi[w];
     if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
   }
-  __syncthreads();
   return bi;
 }
 
 // One Gauss-Jordan step on a column panel P (n rows x w cols, ld = n) held in
 // shared memory: pivot row j (global row index), panel column jj.
-// f[] (n) and rowj[] (2w) are shared scratch.  Returns the pivot row chosen.
+// f[] (n) and rowj[] (2w + 1) are shared scratch.  Returns the pivot row chosen.
 // Four barriers per step: pivot search (2), exchange + capture (1),
 // scale + rank-1 update (1).
+// Thread layout of gj_step's update: rows spread over threads, columns
+// looped inside (computed once per inversion: integer divides).
+struct GjLayout {
+  int rows_per_pass, cgroups, i0, c0;
+  __device__ __forceinline__ explicit GjLayout(int n) {
+    rows_per_pass = blockDim.x >= (unsigned)n ? n : (int)blockDim.x;
+    cgroups = max(1, (int)blockDim.x / rows_per_pass);
+    i0 = threadIdx.x % rows_per_pass;
+    c0 = threadIdx.x / rows_per_pass;
+  }
+};
+
 __device__ __forceinline__ int gj_step(double2* P, int n, int w, int j, int jj, double2* f, double2* rowj,
-                                    InvScratch& s, int* info) {
+                                    InvScratch& s, int* info, const GjLayout& lay) {
   const double2* colj = P + (size_t)jj * n;
   int p = cta_pivot(colj, j, n, s);
   if (p >= n) p = j;
@@ -675,14 +691,14 @@ __device__ __forceinline__ int gj_step(double2* P, int n, int w, int j, int jj, 
     rowj[c] = P[p + (size_t)c * n];
     rowo[c] = P[j + (size_t)c * n];
   }
+  // one thread forms the reciprocal of the pivot (three divides), published
+  // by the capture barrier: computed by every thread it was most of a step
+  if (threadIdx.x == 0) rowj[2 * w] = crecip(colj[p]);
   __syncthreads();
   const double2 piv = f[j];
   if (piv.x == 0.0 && piv.y == 0.0 && threadIdx.x == 0 && *info == 0) *info = j + 1;
-  const double2 d = crecip(piv);
-  // rows are spread over threads, columns looped inside: no integer divide
-  const int rows_per_pass = blockDim.x >= (unsigned)n ? n : (int)blockDim.x;
-  const int cgroups = max(1, (int)blockDim.x / rows_per_pass);
-  const int i0 = threadIdx.x % rows_per_pass, c0 = threadIdx.x / rows_per_pass;
+  const double2 d = rowj[2 * w];
+  const int rows_per_pass = lay.rows_per_pass, cgroups = lay.cgroups, i0 = lay.i0, c0 = lay.c0;
   if (c0 < cgroups)
     for (int i = i0; i < n; i += rows_per_pass) {
       const double2 fi = f[i];
@@ -1145,8 +1161,9 @@ static __device__ __noinline__ int inv_begin(InvProg& ip, int n, const double2* 
     long long t0 = s.tr.start();
     cta_copy(P, A, n * n);
     __syncthreads();
+    const GjLayout lay(n);
     for (int j = 0; j < n; ++j) {
-      int p = gj_step(P, n, n, j, j, f, rowj, s, s.flag);
+      int p = gj_step(P, n, n, j, j, f, rowj, s, s.flag, lay);
       if (threadIdx.x == 0) s.piv[j] = p;
     }
     __syncthreads();

@@ -24,7 +24,7 @@ namespace negf {
 
 static_assert(kGemmSmemBytes + (int)sizeof(GemmDesc) <= kSmemMain,
               "GEMM staging ring and descriptor must fit the main shared-memory region");
-static_assert((kSmallInvMax * kSmallInvMax + 3 * kSmallInvMax) * 16 <= kSmemMain,
+static_assert((kSmallInvMax * kSmallInvMax + 3 * kSmallInvMax + 1) * 16 <= kSmemMain,
               "small inversion must fit the main shared-memory region");
 
 size_t engine_smem_bytes(int nmax) { return smem_bytes_for(nmax); }
