@@ -633,28 +633,36 @@ struct InvScratch {
 // of max |Re|+|Im| (first occurrence, as izamax).  All threads call; the
 // caller puts a barrier between two calls (s.redv / s.redi are reused):
 // gj_step's capture and update barriers do.
+// (key, row) of the warp's best candidate: the largest key, the lowest row
+// among equal keys.  Keys are the bits of |Re|+|Im| plus one (that value is
+// >= 0, so its bit pattern orders like it; 0 = no candidate, NaN never
+// wins); three integer warp reductions instead of five rounds of shuffles.
+__device__ __forceinline__ void warp_argmax_key(unsigned long long& key, int& bi) {
+  const unsigned hi = __reduce_max_sync(0xffffffffu, (unsigned)(key >> 32));
+  const unsigned lo = __reduce_max_sync(0xffffffffu, ((unsigned)(key >> 32) == hi) ? (unsigned)key : 0u);
+  const unsigned long long wkey = ((unsigned long long)hi << 32) | lo;
+  bi = (int)__reduce_min_sync(0xffffffffu, (key == wkey) ? (unsigned)bi : 0xffffffffu);
+  key = wkey;
+}
+
 __device__ __forceinline__ int cta_pivot(const double2* col, int j, int n, InvScratch& s) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  double best = -1.0;
+  unsigned long long key = 0ull;
   int bi = n;
   for (int i = j + threadIdx.x; i < n; i += blockDim.x) {
-    double v = cabs1(col[i]);
-    if (v > best) { best = v; bi = i; }
+    const double v = cabs1(col[i]);
+    const unsigned long long kk = (v >= 0.0) ? (unsigned long long)__double_as_longlong(v) + 1ull : 0ull;
+    if (kk > key) { key = kk; bi = i; }
   }
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    double ov = __shfl_xor_sync(0xffffffffu, best, o);
-    int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-  }
-  if (lane == 0) { s.redv[warp] = best; s.redi[warp] = bi; }
+  warp_argmax_key(key, bi);
+  unsigned long long* redk = reinterpret_cast<unsigned long long*>(s.redv);
+  if (lane == 0) { redk[warp] = key; s.redi[warp] = bi; }
   __syncthreads();
-  best = s.redv[0]; bi = s.redi[0];
-  for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
-    double ov = s.redv[w];
-    int oi = s.redi[w];
-    if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-  }
+  // every warp reduces the per-warp candidates itself (no second barrier)
+  const int nw = (int)(blockDim.x >> 5);
+  key = (lane < nw) ? redk[lane] : 0ull;
+  bi = (lane < nw) ? s.redi[lane] : n;
+  warp_argmax_key(key, bi);
   return bi;
 }
 
@@ -804,16 +812,14 @@ __device__ __forceinline__ void gj_reg_step(double2 (&x)[R][W], int n, int j, Le
     }
   }
   __syncthreads();
-  int wb = 0;
-  unsigned long long best = L.candk[b][0];
-  bi = L.candi[b][0];
-#pragma unroll
-  for (int q = 1; q < kThreads / 32; ++q) {
-    const unsigned long long ok = L.candk[b][q];
-    const int oi = L.candi[b][q];
-    if (ok > best || (ok == best && oi < bi)) { best = ok; bi = oi; wb = q; }
-  }
-  const int p = (bi >= n || bi < 0) ? j : bi;   // no candidate only if every entry is NaN
+  // every warp reduces the per-warp candidates itself; the winner's warp is
+  // the owner of its row (row i belongs to thread i mod blockDim.x)
+  unsigned long long best = (lane < kThreads / 32) ? L.candk[b][lane] : 0ull;
+  bi = (lane < kThreads / 32) ? L.candi[b][lane] : n;
+  warp_argmax_key(best, bi);
+  const bool none = (best == 0ull || bi >= n || bi < 0);
+  const int wb = none ? 0 : ((bi % nt) >> 5);
+  const int p = none ? j : bi;   // no candidate only if every entry is NaN
   if (tid == 0) s.piv[j] = p;
   const double2* prow = L.candrow[b][wb];
   const double2 piv = prow[JJ];
