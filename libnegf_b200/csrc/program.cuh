@@ -362,6 +362,20 @@ __device__ __forceinline__ void op_esh_lo(Op& o, const DevDesc* d, int i, double
           nullptr, OP_N);
 }
 
+// With S = I the off-diagonal ES-H blocks are E*0 - H = -H: the products
+// take the H block itself and the sign in their alpha (the negation is
+// exact), so no assembly pass is run for them.  With S they take the
+// assembled block in `slot`.
+__device__ __forceinline__ const double2* esh_up_op(const DevDesc* d, int i, const double2* slot) {
+  return d->has_s ? slot : d->hu + d->oo[i];
+}
+__device__ __forceinline__ const double2* esh_lo_op(const DevDesc* d, int i, const double2* slot) {
+  return d->has_s ? slot : d->hl + d->oo[i];
+}
+__device__ __forceinline__ double2 esh_al(const DevDesc* d, double2 a) {
+  return d->has_s ? a : make_double2(-a.x, -a.y);
+}
+
 __device__ __forceinline__ void put_status(int& st, int s) { if (st == ST_OK) st = s; }
 
 // Contact pair q (0-based) of the call: ct1 is the contact on the smaller
@@ -526,10 +540,12 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
           s.pp = 1;
           for (s.i = s.d->nbl - 2; s.i >= 1; --s.i) {
-            op_esh_up(o, s.d, s.i, s.ec, w.slot(1));
-            PT_EMIT(s);
-            op_esh_lo(o, s.d, s.i, s.ec, w.slot(2));
-            PT_EMIT(s);
+            if (s.d->has_s) {
+              op_esh_up(o, s.d, s.i, s.ec, w.slot(1));
+              PT_EMIT(s);
+              op_esh_lo(o, s.d, s.i, s.ec, w.slot(2));
+              PT_EMIT(s);
+            }
             op_esh_diag(o, s.d, s.i, s.ec, w.slot(0), w, s.sr, s.sub_first);
             PT_EMIT(s);
             for (s.j = s.sub_first + 1; s.sub_first >= 0 && s.j < s.d->ncont; ++s.j)
@@ -537,11 +553,13 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                 set_simple(o, K_SUB, s.d->pl[s.i] * s.d->pl[s.i], w.sig(s.j), w.slot(0));
                 PT_EMIT(s);
               }
-            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.slot(1), s.d->pl[s.i], OP_N, s.gnext,
-                     s.d->pl[s.i + 1], OP_N, w.slot(3), s.d->pl[s.i], mone, zero);   // -ESH(i,i+1) gsmr(i+1)
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i + 1], s.d->pl[s.i + 1], esh_up_op(s.d, s.i, w.slot(1)), s.d->pl[s.i],
+                     OP_N, s.gnext, s.d->pl[s.i + 1], OP_N, w.slot(3), s.d->pl[s.i], esh_al(s.d, mone),
+                     zero);                                                          // -ESH(i,i+1) gsmr(i+1)
             PT_EMIT(s);
-            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i + 1], w.slot(3), s.d->pl[s.i], OP_N, w.slot(2),
-                     s.d->pl[s.i + 1], OP_N, w.slot(0), s.d->pl[s.i], one, one);    // ESH(i,i) + W ESH(i+1,i)
+            set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i + 1], w.slot(3), s.d->pl[s.i], OP_N,
+                     esh_lo_op(s.d, s.i, w.slot(2)), s.d->pl[s.i + 1], OP_N, w.slot(0), s.d->pl[s.i],
+                     esh_al(s.d, one), one);                                        // ESH(i,i) + W ESH(i+1,i)
             PT_EMIT(s);
             o.kind = K_ZINV; o.m = s.d->pl[s.i]; o.A = w.slot(0);
             o.C = s.keep ? w.layer(0, s.i, s.d->nbl) : w.slot(4 + s.pp);
@@ -561,15 +579,17 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
             PT_EMIT(s);
           }
         if (s.d->nbl > 1) {
-          op_esh_up(o, s.d, 0, s.ec, w.slot(1));
+          if (s.d->has_s) {
+            op_esh_up(o, s.d, 0, s.ec, w.slot(1));
+            PT_EMIT(s);
+            op_esh_lo(o, s.d, 0, s.ec, w.slot(2));
+            PT_EMIT(s);
+          }
+          set_gemm(o, s.d->pl[0], s.d->pl[1], s.d->pl[1], esh_up_op(s.d, 0, w.slot(1)), s.d->pl[0], OP_N, s.gnext,
+                   s.d->pl[1], OP_N, w.slot(3), s.d->pl[0], esh_al(s.d, one), zero);
           PT_EMIT(s);
-          op_esh_lo(o, s.d, 0, s.ec, w.slot(2));
-          PT_EMIT(s);
-          set_gemm(o, s.d->pl[0], s.d->pl[1], s.d->pl[1], w.slot(1), s.d->pl[0], OP_N, s.gnext, s.d->pl[1], OP_N,
-                   w.slot(3), s.d->pl[0], one, zero);
-          PT_EMIT(s);
-          set_gemm(o, s.d->pl[0], s.d->pl[0], s.d->pl[1], w.slot(3), s.d->pl[0], OP_N, w.slot(2), s.d->pl[1], OP_N,
-                   w.slot(0), s.d->pl[0], mone, one);
+          set_gemm(o, s.d->pl[0], s.d->pl[0], s.d->pl[1], w.slot(3), s.d->pl[0], OP_N, esh_lo_op(s.d, 0, w.slot(2)),
+                   s.d->pl[1], OP_N, w.slot(0), s.d->pl[0], esh_al(s.d, mone), one);
           PT_EMIT(s);
         }
         o.kind = K_ZINV; o.m = s.d->pl[0]; o.A = w.slot(0); o.C = s.gsv;
@@ -589,19 +609,23 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         for (s.i = 0; s.i <= s.last; ++s.i) {
           if (s.i > 0) {
             // gr_step(i): E1 = ESH(i-1,i) slot 0, E2 = ESH(i,i-1) slot 1, X slot 2, W2 slot 3, GL slot 6
-            op_esh_up(o, s.d, s.i - 1, s.ec, w.slot(0));
-            PT_EMIT(s);
-            op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(1));
-            PT_EMIT(s);
+            if (s.d->has_s) {
+              op_esh_up(o, s.d, s.i - 1, s.ec, w.slot(0));
+              PT_EMIT(s);
+              op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(1));
+              PT_EMIT(s);
+            }
             set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
-                     w.slot(1), s.d->pl[s.i], OP_N, w.slot(2), s.d->pl[s.i], one, zero);          // gsmr(i) ESH(i,i-1)
+                     esh_lo_op(s.d, s.i - 1, w.slot(1)), s.d->pl[s.i], OP_N, w.slot(2), s.d->pl[s.i],
+                     esh_al(s.d, one), zero);                                                     // gsmr(i) ESH(i,i-1)
             PT_EMIT(s);
             set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i - 1], w.slot(2), s.d->pl[s.i], OP_N,
                      (a.mode == MODE_GN) ? w.layer(1, s.i - 1, s.d->nbl) : w.slot(11 - s.cur), s.d->pl[s.i - 1], OP_N,
                      w.slot(6), s.d->pl[s.i], mone, zero);                                         // Gr(i,i-1)
             PT_EMIT(s);
-            set_gemm(o, s.d->pl[s.i - 1], s.d->pl[s.i], s.d->pl[s.i], w.slot(0), s.d->pl[s.i - 1], OP_N,
-                     w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(3), s.d->pl[s.i - 1], one, zero);  // ESH gsmr
+            set_gemm(o, s.d->pl[s.i - 1], s.d->pl[s.i], s.d->pl[s.i], esh_up_op(s.d, s.i - 1, w.slot(0)),
+                     s.d->pl[s.i - 1], OP_N, w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(3),
+                     s.d->pl[s.i - 1], esh_al(s.d, one), zero);                                   // ESH gsmr
             PT_EMIT(s);
             if (a.mode == MODE_GN) {
               set_gemm(o, s.d->pl[s.i - 1], s.d->pl[s.i], s.d->pl[s.i - 1], w.layer(1, s.i - 1, s.d->nbl),
@@ -706,10 +730,13 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
               o.slot = 0;
               PT_EMIT(s);
               if (sm.res[0] < a.eps) { s.tiny = 1; break; }
-              op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(0));
-              PT_EMIT(s);
+              if (s.d->has_s) {
+                op_esh_lo(o, s.d, s.i - 1, s.ec, w.slot(0));
+                PT_EMIT(s);
+              }
               set_gemm(o, s.d->pl[s.i], s.d->pl[s.i - 1], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i],
-                       OP_N, w.slot(0), s.d->pl[s.i], OP_N, w.slot(1), s.d->pl[s.i], mone, zero);
+                       OP_N, esh_lo_op(s.d, s.i - 1, w.slot(0)), s.d->pl[s.i], OP_N, w.slot(1), s.d->pl[s.i],
+                       esh_al(s.d, mone), zero);
               PT_EMIT(s);
               set_gemm(o, s.d->pl[s.i], s.d->pl[s.bl1 - 1], s.d->pl[s.i - 1], w.slot(1), s.d->pl[s.i], OP_N,
                        s.cc ? w.slot(6) : w.slot(9), s.d->pl[s.i - 1], OP_N, s.cc ? w.slot(9) : w.slot(6),
@@ -794,13 +821,16 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                  w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_C, w.slot(6), s.d->pl[s.i], one, zero);
         PT_EMIT(s);
         for (s.i = s.d->nbl - 2; s.i >= 0; --s.i) {
-          op_esh_up(o, s.d, s.i, s.ec, w.slot(8));
+          if (s.d->has_s) {
+            op_esh_up(o, s.d, s.i, s.ec, w.slot(8));
+            PT_EMIT(s);
+          }
+          set_gemm(o, s.d->pl[s.i], s.d->pl[s.i + 1], s.d->pl[s.i + 1], esh_up_op(s.d, s.i, w.slot(8)), s.d->pl[s.i],
+                   OP_N, w.slot(6), s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i], esh_al(s.d, one), zero);
           PT_EMIT(s);
-          set_gemm(o, s.d->pl[s.i], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.slot(8), s.d->pl[s.i], OP_N, w.slot(6),
-                   s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i], one, zero);
-          PT_EMIT(s);
-          set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i + 1], w.slot(7), s.d->pl[s.i], OP_N, w.slot(8),
-                   s.d->pl[s.i], OP_C, w.layer(3, s.i, s.d->nbl), s.d->pl[s.i], one, one);
+          set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i + 1], w.slot(7), s.d->pl[s.i], OP_N,
+                   esh_up_op(s.d, s.i, w.slot(8)), s.d->pl[s.i], OP_C, w.layer(3, s.i, s.d->nbl), s.d->pl[s.i],
+                   esh_al(s.d, one), one);
           PT_EMIT(s);
           if (s.i > 0) {
             set_gemm(o, s.d->pl[s.i], s.d->pl[s.i], s.d->pl[s.i], w.layer(0, s.i, s.d->nbl), s.d->pl[s.i], OP_N,
@@ -820,14 +850,17 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         PT_EMIT(s);
         // downward sweep; E2 slot 9, Gn(i+1,i) slot 10
         for (s.i = 0; s.i + 1 < s.d->nbl; ++s.i) {
-          op_esh_lo(o, s.d, s.i, s.ec, w.slot(9));
-          PT_EMIT(s);
+          if (s.d->has_s) {
+            op_esh_lo(o, s.d, s.i, s.ec, w.slot(9));
+            PT_EMIT(s);
+          }
           set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i + 1], w.layer(3, s.i + 1, s.d->nbl),
                    s.d->pl[s.i + 1], OP_N, w.layer(2, s.i, s.d->nbl), s.d->pl[s.i], OP_C, w.slot(7), s.d->pl[s.i + 1],
                    one, zero);
           PT_EMIT(s);
-          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i], w.slot(9), s.d->pl[s.i + 1], OP_N,
-                   w.layer(4 + s.par, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i + 1], mone, one);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i], esh_lo_op(s.d, s.i, w.slot(9)), s.d->pl[s.i + 1],
+                   OP_N, w.layer(4 + s.par, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i + 1],
+                   esh_al(s.d, mone), one);
           PT_EMIT(s);
           set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i], s.d->pl[s.i + 1], w.layer(0, s.i + 1, s.d->nbl),
                    s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i + 1], OP_N, w.slot(10), s.d->pl[s.i + 1], one, zero);
@@ -839,8 +872,9 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
                    s.d->pl[s.i + 1], OP_N, w.layer(1, s.i + 1, s.d->nbl), s.d->pl[s.i + 1], OP_C, w.slot(7),
                    s.d->pl[s.i + 1], one, zero);
           PT_EMIT(s);
-          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i + 1], s.d->pl[s.i], w.slot(9), s.d->pl[s.i + 1], OP_N,
-                   w.layer(6 + s.par, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7), s.d->pl[s.i + 1], mone, one);
+          set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i + 1], s.d->pl[s.i], esh_lo_op(s.d, s.i, w.slot(9)),
+                   s.d->pl[s.i + 1], OP_N, w.layer(6 + s.par, s.i, s.d->nbl), s.d->pl[s.i], OP_N, w.slot(7),
+                   s.d->pl[s.i + 1], esh_al(s.d, mone), one);
           PT_EMIT(s);
           set_gemm(o, s.d->pl[s.i + 1], s.d->pl[s.i + 1], s.d->pl[s.i + 1], w.layer(0, s.i + 1, s.d->nbl),
                    s.d->pl[s.i + 1], OP_N, w.slot(7), s.d->pl[s.i + 1], OP_N, w.layer(4 + s.par, s.i + 1, s.d->nbl),
