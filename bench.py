@@ -69,6 +69,8 @@ def parse():
     p.add_argument("--serve-layers", default="10,60", help="layer count range (uniform)")
     p.add_argument("--serve-grid", default="64,1024", help="energy grid size range (log-uniform)")
     p.add_argument("--serve-lanes", type=int, default=2)
+    p.add_argument("--serve-policy", default="srpt", choices=["srpt", "fifo"],
+                   help="batching order: least remaining work first, or oldest first")
     return p.parse_args()
 
 
@@ -376,7 +378,7 @@ def run_serve(args):
         kind = "ldos" if rng.random() < 0.3 else "T"
         gen = "c1" if rng.random() < 0.5 else "c0"
         plan.append((t, n, nbl, npts, kind, gen, int(rng.integers(1 << 30))))
-    srv = Server(lanes=args.serve_lanes, sgf_cache_bytes=1 << 30)
+    srv = Server(lanes=args.serve_lanes, sgf_cache_bytes=1 << 30, policy=args.serve_policy)
     reqs = []
     with ClockSampler(0) as clk:
         t0 = time.perf_counter()
@@ -391,7 +393,8 @@ def run_serve(args):
                 time.sleep(0.001)
             reqs.append(srv.submit(r))
         for r in reqs:
-            r.wait()
+            if not r.wait(1800):                      # bounded: a stuck loop ends the run with an error
+                r.error = "not finished after 30 min"
         t_end = time.perf_counter()
     srv.close()
     ok = [r for r in reqs if r.error is None]
@@ -405,7 +408,8 @@ def run_serve(args):
         "config": {"workload": "serving stream: Poisson arrivals %.1f/s for %.0f s, blocks %s, layers %d-%d, "
                                "grids %d-%d log-uniform, 30%% LDOS requests, c0/c1 generators"
                                % (args.serve_rate, args.serve_seconds, blocks, lo, hi, g0, g1),
-                   "lanes": args.serve_lanes, "eta": 1e-4, "precision": "complex FP64 (plain form)"},
+                   "lanes": args.serve_lanes, "policy": args.serve_policy, "eta": 1e-4,
+                   "precision": "complex FP64 (plain form)"},
         "latency_s": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
                       "p99": float(np.percentile(lat, 99)) if lat.size else None,
                       "max": float(lat.max()) if lat.size else None},

@@ -10,11 +10,16 @@ feeds the GPU from a pool of pending energy points:
 - lanes: independent engine contexts on the same GPU, each with its own
   stream and workspace; a lane runs one persistent launch at a time, and
   the launches of different lanes run concurrently on the SMs;
-- batching: whenever a lane is free it takes the oldest pending points of
-  one solve kind (T or T+LDOS, same eta, dos_delta and pairs), whatever
-  request they belong to, up to `points_per_launch`; points of requests
-  that arrived while other launches were running join the next launch of
-  any free lane (continuous batching, not a queue of whole requests);
+- batching: whenever a lane is free it takes pending points of one solve
+  kind (T or T+LDOS, same eta, dos_delta and pairs), whatever request they
+  belong to, up to `points_per_launch`; points of requests that arrived
+  while other launches were running join the next launch of any free lane
+  (continuous batching, not a queue of whole requests).  The order is
+  `policy`: "fifo" takes the oldest points first; "srpt" (default) takes
+  first the points of the request with the least estimated remaining work
+  (pending points x a per-point cost of (layers + 80) x block order^3, the
+  sweep plus the two leads' decimation), which lowers the median latency of
+  a mixed stream without changing any result;
 - admission: a request is admitted when its device fits the HBM budget next
   to the resident devices (idle devices are evicted, least recently used
   first); a device larger than the budget on its own is rejected with
@@ -39,7 +44,7 @@ from . import native
 from .device import Device
 
 
-@dataclass
+@dataclass(eq=False)   # identity: requests hold arrays, and two requests are never "equal"
 class Request:
     device: Device
     energies: np.ndarray
@@ -69,7 +74,7 @@ class Request:
         return self._done.wait(timeout)
 
 
-@dataclass
+@dataclass(eq=False)
 class _Resident:
     ids: List[int]                        # device id in every lane
     nbytes: int
@@ -83,9 +88,13 @@ class Server:
 
     def __init__(self, cuda_device: int = 0, lanes: int = 2, points_per_launch: int = 0,
                  hbm_budget: int = 0, sgf_cache_bytes: int = 1 << 30, options: Optional[dict] = None,
-                 contexts: Optional[list] = None, sms: int = 0):
+                 contexts: Optional[list] = None, sms: int = 0, policy: str = "srpt"):
         """`contexts` (one per lane) and `sms` replace the engine contexts and
-        the device query, for driving the loop with stand-ins."""
+        the device query, for driving the loop with stand-ins.  `policy`:
+        "srpt" or "fifo" (see the module docstring)."""
+        if policy not in ("srpt", "fifo"):
+            raise ValueError("policy must be 'srpt' or 'fifo'")
+        self.policy = policy
         if contexts is not None:
             self.lanes = list(contexts)
             lanes = len(self.lanes)
@@ -211,18 +220,34 @@ class Server:
     def _group(req):
         return (bool(req.ldos), float(req.eta), float(req.dos_delta) if req.ldos else 0.0, tuple(req.pairs))
 
+    @staticmethod
+    def _point_cost(req) -> float:
+        """Relative cost of one point: the sweep over the layers plus the two
+        leads' decimation (about 40 iterations of a few products each)."""
+        n = max(req.device.pl_size)
+        return (req.device.nbl + 80.0) * float(n) ** 3
+
     def _take_batch(self):
-        """Oldest pending points of one solve kind, across requests."""
+        """Pending points of one solve kind, across requests, in policy order."""
         if not self._pending:
             return None
-        g = self._group(self._pending[0][0])
-        take, keep = [], []
-        for item in self._pending:
-            if len(take) < self.ppl and self._group(item[0]) == g:
+        if self.policy == "fifo":
+            order = self._pending
+        else:
+            left = {}
+            for r, _ in self._pending:
+                left[id(r)] = left.get(id(r), 0) + 1
+            # stable: within a request and among equal work, arrival order is kept
+            order = sorted(self._pending, key=lambda it: left[id(it[0])] * self._point_cost(it[0]))
+        g = self._group(order[0][0])
+        take, taken = [], set()
+        for item in order:
+            if len(take) >= self.ppl:
+                break
+            if self._group(item[0]) == g:
                 take.append(item)
-            else:
-                keep.append(item)
-        self._pending = keep
+                taken.add(id(item))
+        self._pending = [it for it in self._pending if id(it) not in taken]
         return take
 
     def _lane_loop(self, lane):
@@ -266,10 +291,11 @@ class Server:
     def _finish(self, r):
         r.t_done = time.perf_counter()
         k = self._key(r)
-        if k in self._resident and r in self._active:
+        active = any(x is r for x in self._active)
+        if k in self._resident and active:
             self._resident[k].users -= 1
             self._resident[k].last_use = r.t_done
-        if r in self._active:
-            self._active.remove(r)
+        if active:
+            self._active = [x for x in self._active if x is not r]
         self.completed.append(r)
         r._done.set()

@@ -113,3 +113,42 @@ def test_eviction_and_rejection():
         assert r3.wait(30) and r3.error is not None and np.all(r3.status == 8)
     finally:
         srv.close()
+
+
+def test_srpt_takes_the_least_remaining_work_first():
+    """The batch order: "srpt" starts with the request whose pending points
+    cost least in total, "fifo" with the oldest points; results are not
+    affected either way (every point is solved once, as above)."""
+    big_dev = G.transport_c0(nbl=6, n=8, seed=0)
+    small_dev = G.transport_c0(nbl=3, n=4, seed=1)
+    for policy, first in (("srpt", "small"), ("fifo", "big")):
+        srv = Server(contexts=[FakeContext()], sms=4, points_per_launch=16, hbm_budget=1 << 34, sgf_cache_bytes=0,
+                     policy=policy)
+        srv.close()                                   # drive _take_batch by hand
+        big = Request(big_dev, np.linspace(-1, 1, 100))
+        small = Request(small_dev, np.linspace(-1, 1, 5))
+        srv._pending = [(big, i) for i in range(100)] + [(small, i) for i in range(5)]
+        batch = srv._take_batch()
+        assert len(batch) == 16 and len(srv._pending) == 105 - 16
+        if first == "small":
+            assert [r is small for r, _ in batch[:5]] == [True] * 5
+            assert all(r is big for r, _ in batch[5:]) and [i for _, i in batch[5:]] == list(range(11))
+        else:
+            assert all(r is big for r, _ in batch) and [i for _, i in batch] == list(range(16))
+
+
+def test_out_of_order_completion():
+    """With "srpt" a small request that arrives after a large one finishes
+    first; the loop's bookkeeping of active requests must not compare
+    requests by value (they hold arrays)."""
+    ctxs = [FakeContext()]
+    srv = Server(contexts=ctxs, sms=4, points_per_launch=16, hbm_budget=1 << 34, sgf_cache_bytes=0, policy="srpt")
+    try:
+        big = srv.submit(Request(G.transport_c0(nbl=4, n=8, seed=0), np.linspace(-1, 1, 200)))
+        time.sleep(0.005)
+        small = srv.submit(Request(G.transport_c0(nbl=3, n=4, seed=1), np.linspace(-1, 1, 5)))
+        assert small.wait(30) and big.wait(30)
+        assert small.error is None and big.error is None
+        assert small.t_done < big.t_done
+    finally:
+        srv.close()
