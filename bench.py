@@ -69,7 +69,7 @@ def parse():
     p.add_argument("--serve-layers", default="10,60", help="layer count range (uniform)")
     p.add_argument("--serve-grid", default="64,1024", help="energy grid size range (log-uniform)")
     p.add_argument("--serve-lanes", type=int, default=2)
-    p.add_argument("--serve-policy", default="srpt", choices=["srpt", "fifo"],
+    p.add_argument("--serve-policy", default="fifo", choices=["fifo", "srpt"],
                    help="batching order: least remaining work first, or oldest first")
     return p.parse_args()
 

@@ -15,11 +15,14 @@ feeds the GPU from a pool of pending energy points:
   belong to, up to `points_per_launch`; points of requests that arrived
   while other launches were running join the next launch of any free lane
   (continuous batching, not a queue of whole requests).  The order is
-  `policy`: "fifo" takes the oldest points first; "srpt" (default) takes
+  `policy`: "fifo" (default) takes the oldest points first; "srpt" takes
   first the points of the request with the least estimated remaining work
   (pending points x a per-point cost of (layers + 80) x block order^3, the
-  sweep plus the two leads' decimation), which lowers the median latency of
-  a mixed stream without changing any result;
+  sweep plus the two leads' decimation), and fills the batch only with
+  points at most 4x as costly as its first one; no result changes.  On the
+  streams measured (B200, 2 lanes) srpt did not lower the latencies:
+  launches are not preempted, and waiting behind a running batch of large
+  points dominates;
 - admission: a request is admitted when its device fits the HBM budget next
   to the resident devices (idle devices are evicted, least recently used
   first); a device larger than the budget on its own is rejected with
@@ -88,7 +91,7 @@ class Server:
 
     def __init__(self, cuda_device: int = 0, lanes: int = 2, points_per_launch: int = 0,
                  hbm_budget: int = 0, sgf_cache_bytes: int = 1 << 30, options: Optional[dict] = None,
-                 contexts: Optional[list] = None, sms: int = 0, policy: str = "srpt"):
+                 contexts: Optional[list] = None, sms: int = 0, policy: str = "fifo"):
         """`contexts` (one per lane) and `sms` replace the engine contexts and
         the device query, for driving the loop with stand-ins.  `policy`:
         "srpt" or "fifo" (see the module docstring)."""
@@ -240,11 +243,15 @@ class Server:
             # stable: within a request and among equal work, arrival order is kept
             order = sorted(self._pending, key=lambda it: left[id(it[0])] * self._point_cost(it[0]))
         g = self._group(order[0][0])
+        # srpt: a batch ends when its slowest point does, so it takes only points
+        # at most 4x as costly as the first one's (cheap requests do not wait on
+        # expensive points launched beside them)
+        cap = 4.0 * self._point_cost(order[0][0]) if self.policy == "srpt" else float("inf")
         take, taken = [], set()
         for item in order:
             if len(take) >= self.ppl:
                 break
-            if self._group(item[0]) == g:
+            if self._group(item[0]) == g and self._point_cost(item[0]) <= cap:
                 take.append(item)
                 taken.add(id(item))
         self._pending = [it for it in self._pending if id(it) not in taken]
