@@ -129,3 +129,60 @@ def test_density_neq_parity(gpu_ctx, deph, three):
     finally:
         gpu_ctx.set_options()
         gpu_ctx.release(did)
+
+
+def _bond_currents(dev, E, outer):
+    """Current from device block cblk into each contact, from the outer
+    blocks of one real-axis point: Re[i Tr(Tlc Gn(c,cb) - Gn(cb,c) Tcl)],
+    Tlc = E SMC - HMC, Tcl = Tlc^dag (the layer-current formula of
+    iterative_layer_current, src/iterative.F90:427-461, on the device-contact
+    bond)."""
+    dc, cd = outer
+    J = []
+    for c in range(dev.ncont):
+        smc = dev.smc[c] if dev.smc is not None else 0.0
+        Tlc = E * smc - dev.hmc[c]
+        J.append(np.real(1j * np.trace(Tlc @ cd[c] - dc[c] @ Tlc.conj().T)))
+    return np.array(J)
+
+
+@pytest.mark.parametrize("case", ["two", "three", "c1_S"])
+def test_oracle_outer_blocks_carry_the_contact_currents(case):
+    """Known answer for calculate_Gn_outer: at one coherent real-axis point
+    (weight 1) the bond current between device block cblk and each contact,
+    formed from the outer blocks, is that contact's Meir-Wingreen current
+    (exact with S = I; with an overlap the broadening eta on the contact
+    side leaves an O(eta |S|) difference)."""
+    dev = {"two": lambda: G.transport_c0(nbl=4, n=6, seed=2),
+           "three": lambda: G.transport_c0(nbl=5, n=6, seed=1, cblk=[1, 5, 3]),
+           "c1_S": lambda: G.transport_c1(nbl=4, n=8, seed=3, density=0.4)}[case]()
+    nc = dev.ncont
+    for E in (0.05, -0.3, 0.7):
+        frm = np.array([[1.0] + [0.0] * (nc - 2) + [0.3]]) if nc > 2 else np.array([[1.0, 0.0]])
+        _, outer, _, st = O.density_neq(dev, [E], np.array([1.0 + 0j]), frm, eta=1e-6, scba_niter=0)
+        mw = O.meir_wingreen(dev, [E], frm, eta=1e-6, scba_niter=0)
+        J = _bond_currents(dev, E, outer)
+        tol = 1e-10 if case != "c1_S" else 1e-5
+        assert np.abs(J - mw["curr"][0]).max() <= tol * max(1.0, np.abs(mw["curr"][0]).max())
+        assert abs(J.sum()) <= tol                                  # current conservation
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("three", [False, True])
+def test_gpu_outer_blocks_carry_the_contact_currents(gpu_ctx, three):
+    """The same known answer on the CUDA path's outer blocks."""
+    dev = G.transport_c0(nbl=5, n=6, seed=1, cblk=[1, 5, 3]) if three else G.transport_c0(nbl=4, n=6, seed=2)
+    nc = dev.ncont
+    frm = np.array([[1.0] + [0.0] * (nc - 2) + [0.3]]) if nc > 2 else np.array([[1.0, 0.0]])
+    did = gpu_ctx.upload(dev)
+    try:
+        gpu_ctx.set_options(scba_niter=0)
+        for E in (0.05, -0.3, 0.7):
+            _, outer, _, st = gpu_ctx.density_neq(did, [E], np.array([1.0 + 0j]), frm, eta=1e-6)
+            mw = O.meir_wingreen(dev, [E], frm, eta=1e-6, scba_niter=0)
+            J = _bond_currents(dev, E, outer)
+            assert np.all(st == 0)
+            assert np.abs(J - mw["curr"][0]).max() <= 1e-9 * max(1.0, np.abs(mw["curr"][0]).max())
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
