@@ -669,7 +669,7 @@ __device__ __forceinline__ int cta_pivot(const double2* col, int j, int n, InvSc
 // One Gauss-Jordan step on a column panel P (n rows x w cols, ld = n) held in
 // shared memory: pivot row j (global row index), panel column jj.
 // f[] (n) and rowj[] (2w + 1) are shared scratch.  Returns the pivot row chosen.
-// Four barriers per step: pivot search (2), exchange + capture (1),
+// Three barriers per step: pivot search (1), exchange + capture (1),
 // scale + rank-1 update (1).
 // Thread layout of gj_step's update: rows spread over threads, columns
 // looped inside (computed once per inversion: integer divides).
@@ -763,7 +763,8 @@ struct LeafShared {
   double2 stage[2][2 * W * W];   // pivot rows of leaf_apply, two pieces (K up to 2W)
 };
 
-// One pivot step of gj_leaf_reg on panel column JJ (global column j).
+// One pivot step of the register leaves (gj_leaf2) on panel column JJ
+// (global column j).
 //
 // Every warp publishes its best candidate row, with the row itself and the
 // reciprocal of its pivot entry, before the one barrier of the step; after
