@@ -413,7 +413,7 @@ def run_serve(args):
         "latency_s": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
                       "p99": float(np.percentile(lat, 99)) if lat.size else None,
                       "max": float(lat.max()) if lat.size else None},
-        "requests": len(reqs), "rejected": len(reqs) - len(ok), "points": pts,
+        "requests": len(reqs), "rejected": len(reqs) - len(ok), "points": pts, "gpu_launches": srv.launches,
         "status_counts": {str(k): int(v) for k, v in
                           zip(*np.unique(np.concatenate([r.status for r in reqs]), return_counts=True))},
         "clocks": clk.summary(),

@@ -136,6 +136,7 @@ class Server:
         self._sched = threading.Thread(target=self._admit_loop, daemon=True)
         self.completed: List[Request] = []
         self.points_done = 0
+        self.launches = 0          # engine launches (one per lane batch)
         self._sched.start()
         for t in self._threads:
             t.start()
@@ -293,6 +294,7 @@ class Server:
                     if r._left == 0:
                         self._finish(r)
                 self.points_done += len(batch)
+                self.launches += 1
                 self._cv.notify_all()
 
     def _finish(self, r):

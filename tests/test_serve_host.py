@@ -75,6 +75,7 @@ def test_every_point_once_and_batches_mix_requests():
         assert all(n <= 16 for _, n, _ in launches)
         assert any(len(ids) > 1 for ids, _, _ in launches)          # points of several devices in one launch
         assert len(srv.latencies()) == 4
+        assert srv.launches == len(launches)
     finally:
         srv.close()
 
