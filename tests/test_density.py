@@ -46,6 +46,20 @@ def test_oracle_half_filled_chain_has_one_electron_per_site():
         assert np.abs(u - l.conj().T).max() < 1e-14
 
 
+def test_oracle_chain_bond_order_inside_and_across_the_contacts():
+    """Known answer for the equilibrium outer blocks (calculate_Gr_outer): in
+    a half-filled perfect chain every nearest-neighbour density-matrix
+    element is the bond order g_spin sin(k_F) / pi = 2 / pi, between device
+    sites (upper blocks) and between the device's end sites and the first
+    contact sites (outer blocks) alike; kT = 1e-3 moves it by O((pi kT)^2)."""
+    dev = G.chain(1, 6)
+    z, w = D.contour_points(elow=-4.0, muref=0.0, kT=0.001, n_kt=10, np1=48, np2=24, n_poles=3)
+    (rd, ru, rl), (odc, ocd), nc, st = O.density(dev, z, w)
+    assert np.all(st == 0)
+    bonds = [b[0, 0] for b in ru] + [b[0, 0] for b in odc] + [b[0, 0] for b in ocd]
+    assert np.allclose(bonds, 2.0 / np.pi, atol=1e-6)
+
+
 def test_restrict_to_pattern_is_blk2csr():
     dev = G.transport_c1(nbl=3, n=5, seed=4, density=0.4)
     H, S, plend, *_ = St.csr_from_device(dev)
