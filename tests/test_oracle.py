@@ -29,6 +29,29 @@ def test_chain_transmission_is_one_in_band(m, nbl, cblk):
     assert np.all(T2 < 1e-6)
 
 
+def _ladder(nbl=5, t=1.0, tperp=0.5):
+    """Perfect two-leg ladder, one rung per PL: H00 = [[0, -tp], [-tp, 0]],
+    rung-to-rung hopping -t on both legs.  Bands +-tp - 2t cos k."""
+    from libnegf_b200.device import Device
+    H0 = np.array([[0.0, -tperp], [-tperp, 0.0]], dtype=np.complex128)
+    V = -t * np.eye(2, dtype=np.complex128)
+    return Device([H0.copy() for _ in range(nbl)], [V.copy() for _ in range(nbl - 1)],
+                  [V.copy() for _ in range(nbl - 1)], [1, nbl], [H0.copy(), H0.copy()], [V.copy(), V.copy()],
+                  [V.copy(), V.copy()])
+
+
+def test_ladder_transmission_counts_open_channels():
+    """Known answer with two orbitals per PL: a perfect ladder transmits one
+    unit per open band, T(E) = #{s = +-1 : |E - s tp| < 2t} (2 in the
+    middle, 1 where only one band is open, 0 outside)."""
+    dev = _ladder()
+    E = np.array([-2.3, -1.8, -1.0, -0.2, 0.4, 1.2, 1.9, 2.2, 2.7])
+    expect = np.array([sum(abs(e - s * 0.5) < 2.0 for s in (1, -1)) for e in E], dtype=float)
+    T, nc, st = O.transmission(dev, E, eta=1e-7)
+    assert np.all(st == 0)
+    assert np.abs(T - expect).max() < 1e-4
+
+
 @pytest.mark.parametrize("e", [-1.7, -0.3, 0.0, 0.9, 1.95, 2.4, -3.0])
 def test_surface_green_closed_form(e):
     t = 1.0
