@@ -338,3 +338,22 @@ def test_elph_current_known_answer(gpu_ctx):
     finally:
         gpu_ctx.set_options()
         gpu_ctx.release(did)
+
+
+def test_ladder_known_answer(gpu_ctx):
+    """Two orbitals per layer: a perfect ladder transmits one unit per open
+    band (known answer, independent of the oracle)."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_oracle import _ladder
+    dev = _ladder()
+    E = np.array([-2.3, -1.8, -1.0, -0.2, 0.4, 1.2, 1.9, 2.2, 2.7])
+    expect = np.array([sum(abs(e - s * 0.5) < 2.0 for s in (1, -1)) for e in E], dtype=float)
+    did = gpu_ctx.upload(dev)
+    try:
+        T, nc, st = gpu_ctx.transmission(did, E, eta=1e-7)
+        assert np.all(st == 0)
+        assert np.abs(T - expect).max() < 1e-4
+    finally:
+        gpu_ctx.release(did)
