@@ -405,6 +405,30 @@ int negf_b200_zgemm_batched(int32_t batch, int32_t m, int32_t n, int32_t k,
  * 449-523) and zinv (src/inversions.F90:807-839).  `work` is a device buffer
  * of negf_b200_zinv_work_bytes(batch, n) bytes; info[b] = 0 or the 1-based
  * column of the first zero pivot. */
+/* C = alpha*A*B + beta*C, complex128, no transposes, on the integer tensor
+ * cores: every row of A and column of B is scaled by a power of two and cut
+ * into `slices` signed 7-bit digits (int8); the digit products accumulate
+ * exactly in int32 (tcgen05.mma kind::i8, accumulators in tensor memory)
+ * and are recombined in FP64.  The result carries about 7*slices - 1 bits
+ * relative to the row / column scales (slices = 7: within a few units of
+ * the rounding of an FP64 product; 4 <= slices <= 8).  Replaces, at FP64
+ * accuracy, the zgemm of prealloc_mult (src/sparsekit_drv.F90:1896-2081)
+ * and cu_ZmultMat with dagger = 0 (src/gpuroutines.cu:395-446).
+ * k <= 1024.  C may alias A or B.  `work` holds
+ * negf_b200_zgemm_i8_work_bytes(batch, m, n, k, slices) bytes; status
+ * (device, batch entries, may be NULL) gets NEGF_B200_ERR_NONFINITE for an
+ * operand with a NaN / Inf (C is NaN) and NEGF_B200_ERR_TIMEOUT if a
+ * pipeline wait inside the kernel ran out; other entries are left as they
+ * are. */
+size_t negf_b200_zgemm_i8_work_bytes(int32_t batch, int32_t m, int32_t n, int32_t k,
+                                     int32_t slices);
+int negf_b200_zgemm_batched_i8(int32_t batch, int32_t m, int32_t n, int32_t k,
+                               const double* alpha, const double* A,
+                               int64_t strideA, const double* B, int64_t strideB,
+                               const double* beta, double* C, int64_t strideC,
+                               int32_t slices, void* work, int32_t* status,
+                               void* stream);
+
 size_t negf_b200_zinv_work_bytes(int32_t batch, int32_t n);
 int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A,
                            double* Ainv, int32_t* info, void* work,
@@ -434,7 +458,8 @@ int negf_b200_decimation_batched(int32_t batch, int32_t n, const double* Ao,
  * batch * 15 * n * n * 16 bytes must fit (e.g. up to 4 problems of order
  * 256, 68 of order 64); larger requests return NEGF_B200_ERR_ADMISSION and
  * print the limit.  The first call on each device resolves the array's
- * address for that device; make it before any stream capture.  All calls
+ * address for that device (again after a device reset, when the CUDA
+ * context has changed); make it before any stream capture.  All calls
  * share the array: calls that can overlap on the GPU race, so serialise
  * them. */
 int negf_b200_decimation_noalloc(int32_t batch, int32_t n, const double* Ao,

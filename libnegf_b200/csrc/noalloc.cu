@@ -13,8 +13,12 @@
 // Every GPU on which this library's code is loaded holds it until the
 // process exits (at the latest from the first call on that GPU).  Its device
 // address is resolved on the host with cudaGetSymbolAddress, once per
-// device, by the first call made while that device is current; make that
-// first call before any stream capture.  All calls share the one array and
+// device and CUDA context, by the first call made while that device is
+// current; make that first call before any stream capture.  A device reset
+// (cudaDeviceReset, or a primary context torn down and made again) loads the
+// module afresh, so the address is keyed on the current context and
+// resolved again when the context changes; a failed launch also drops it.
+// All calls share the one array and
 // it keeps whatever the previous call left in it: calls whose kernels can
 // overlap on the GPU (different streams, different host threads) race on
 // it, so serialise them.  The decimation writes every scratch element it
@@ -34,6 +38,29 @@ __device__ __align__(256) unsigned char g_decimation_scratch[kScratchBytes];
 
 std::mutex g_mu;
 void* g_scratch_addr[kMaxDevices] = {nullptr};
+void* g_scratch_ctx[kMaxDevices] = {nullptr};   // context the address belongs to
+
+// The current CUDA context (CUcontext), through the runtime's driver entry
+// point so that the library needs no link against the driver library; null
+// if the driver does not provide it (then the address is kept per device).
+void* current_context() {
+  typedef int (*CtxGetCurrent)(void**);
+  static CtxGetCurrent fn = nullptr;
+  static bool looked = false;
+  if (!looked) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrent>(p);
+    else
+      cudaGetLastError();
+    looked = true;
+  }
+  void* ctx = nullptr;
+  if (fn && fn(&ctx) != 0) ctx = nullptr;
+  return ctx;
+}
 
 }  // namespace
 
@@ -60,19 +87,29 @@ extern "C" int negf_b200_decimation_noalloc(int32_t batch, int32_t n, const doub
   void* scratch = nullptr;
   {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
+    // (before the first lookup no context may be current yet: the lookup
+    // creates it, and the context stored is the one current after it)
+    void* ctx = current_context();
+    if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx) {
       void* p = nullptr;
       cudaError_t e = cudaGetSymbolAddress(&p, g_decimation_scratch);
       if (e != cudaSuccess || !p) {
         cudaGetLastError();
+        g_scratch_addr[dev] = nullptr;
         return NEGF_B200_ERR_CUDA;
       }
       g_scratch_addr[dev] = p;
+      g_scratch_ctx[dev] = current_context();
     }
     scratch = g_scratch_addr[dev];
   }
   cudaError_t e = negf::launch_decimation_batched(batch, n, (const double2*)Ao, (const double2*)Bo,
                                                   (const double2*)Co, (double2*)Go, ncyc, tol, max_iter,
                                                   (double2*)scratch, (cudaStream_t)stream);
-  return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;
+  if (e != cudaSuccess) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_scratch_addr[dev] = nullptr;   // resolve again on the next call
+    return NEGF_B200_ERR_CUDA;
+  }
+  return NEGF_B200_OK;
 }

@@ -30,15 +30,22 @@ def scatter_rows(local_rows: np.ndarray, idx: np.ndarray, npts: int) -> np.ndarr
 
 
 def reduce_rows(full: np.ndarray, dist=None) -> np.ndarray:
-    """Sum of every rank's scatter_rows() matrix (all ranks get the result)."""
+    """Sum of every rank's scatter_rows() matrix (all ranks get the result).
+    Complex rows (density or Gn blocks) keep their imaginary part: they are
+    reduced as their float64 (re, im) pairs and viewed back."""
     if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
         return full
     import torch
-    t = torch.from_numpy(np.ascontiguousarray(full, dtype=np.float64))
+    full = np.asarray(full)
+    cplx = np.iscomplexobj(full)
+    flat = (np.ascontiguousarray(full, dtype=np.complex128).view(np.float64) if cplx
+            else np.ascontiguousarray(full, dtype=np.float64))
+    t = torch.from_numpy(flat.copy())
     if dist.get_backend() == "nccl":
         t = t.cuda()
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
-    return t.cpu().numpy()
+    out = t.cpu().numpy()
+    return out.view(np.complex128) if cplx else out
 
 
 def max_over_ranks(value: float, dist=None) -> float:

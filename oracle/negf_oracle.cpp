@@ -851,6 +851,339 @@ void set_threads(int nthreads) {
 #endif
 }
 
+
+// ---------------------------------------------------------------------------
+// Independent-rounding restatements of the 2-contact T and T + DOS paths.
+//
+// The same steps as point_transmission / point_transmission_dos above
+// (decimation with the two-consecutive max|C1| rule, compute_contacts,
+// build_ESH, calculate_gsmr_blocks, Gr(1,1), the Gr sweep, the ct1 trace and
+// -Im Gr_ii / pi), written over a real type R with their own unblocked LU
+// (partial pivoting on max |Re|+|Im|, the izamax rule of zgetf2), triangular
+// solves against the identity (zgetrs) and plain triple-loop products:
+//   R = long double  (x87, 64-bit significand: unit roundoff 5.4e-20, about
+//                     2000x below FP64) -- a near-exact solution of the same
+//                     algorithm, used to measure how far each FP64 result
+//                     (this oracle's, the GPU's) lies from it;
+//   R = double       another FP64 rounding path than OpenBLAS's blocked
+//                     kernels: two CPU FP64 implementations side by side.
+namespace xp {
+
+template <typename R>
+struct C {
+  R re, im;
+};
+template <typename R>
+inline C<R> mk(R a, R b) { return C<R>{a, b}; }
+template <typename R>
+inline C<R> mul(C<R> a, C<R> b) { return mk<R>(a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re); }
+template <typename R>
+inline C<R> add(C<R> a, C<R> b) { return mk<R>(a.re + b.re, a.im + b.im); }
+template <typename R>
+inline C<R> sub(C<R> a, C<R> b) { return mk<R>(a.re - b.re, a.im - b.im); }
+template <typename R>
+inline C<R> cj(C<R> a) { return mk<R>(a.re, -a.im); }
+template <typename R>
+inline C<R> rcp(C<R> z) {   // Smith's algorithm
+  if (std::fabs(z.re) >= std::fabs(z.im)) {
+    R r = z.im / z.re, d = z.re + z.im * r;
+    return mk<R>(R(1) / d, -r / d);
+  }
+  R r = z.re / z.im, d = z.im + z.re * r;
+  return mk<R>(r / d, R(-1) / d);
+}
+
+template <typename R>
+struct Mat {
+  int nr = 0, nc = 0;
+  std::vector<C<R>> v;
+  Mat() = default;
+  Mat(int r, int c) : nr(r), nc(c), v((size_t)r * c, C<R>{0, 0}) {}
+  C<R>& at(int i, int j) { return v[(size_t)j * nr + i]; }
+  const C<R>& at(int i, int j) const { return v[(size_t)j * nr + i]; }
+};
+
+template <typename R>
+Mat<R> from(const Dns& d) {
+  Mat<R> m(d.nr, d.nc);
+  for (size_t q = 0; q < d.v.size(); ++q) m.v[q] = mk<R>((R)d.v[q].real(), (R)d.v[q].imag());
+  return m;
+}
+
+// C = s*A*B (acc = false) or C += s*A*B (acc = true): prealloc_mult
+template <typename R>
+void gemm(const Mat<R>& A, const Mat<R>& B, Mat<R>& Cm, C<R> s, bool acc) {
+  if (!acc) Cm = Mat<R>(A.nr, B.nc);
+  std::vector<C<R>> col(A.nr);
+  for (int j = 0; j < B.nc; ++j) {
+    for (int i = 0; i < A.nr; ++i) col[i] = C<R>{0, 0};
+    for (int k = 0; k < A.nc; ++k) {
+      const C<R> b = B.at(k, j);
+      const C<R>* a = &A.v[(size_t)k * A.nr];
+      for (int i = 0; i < A.nr; ++i) {
+        col[i].re += a[i].re * b.re - a[i].im * b.im;
+        col[i].im += a[i].re * b.im + a[i].im * b.re;
+      }
+    }
+    for (int i = 0; i < A.nr; ++i) Cm.at(i, j) = add(Cm.at(i, j), mul(s, col[i]));
+  }
+}
+
+// inverse by LU with partial pivoting + forward/backward solves against I
+template <typename R>
+int inv(const Mat<R>& A, Mat<R>& X) {
+  const int n = A.nr;
+  Mat<R> LU = A;
+  std::vector<int> piv(n);
+  int info = 0;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    R best = -1;
+    for (int i = k; i < n; ++i) {
+      R a = std::fabs(LU.at(i, k).re) + std::fabs(LU.at(i, k).im);
+      if (a > best) { best = a; p = i; }
+    }
+    piv[k] = p;
+    if (best == 0) { if (!info) info = k + 1; continue; }
+    if (p != k)
+      for (int j = 0; j < n; ++j) std::swap(LU.at(k, j), LU.at(p, j));
+    const C<R> r = rcp(LU.at(k, k));
+    for (int i = k + 1; i < n; ++i) LU.at(i, k) = mul(LU.at(i, k), r);
+    for (int j = k + 1; j < n; ++j) {
+      const C<R> u = LU.at(k, j);
+      for (int i = k + 1; i < n; ++i) LU.at(i, j) = sub(LU.at(i, j), mul(LU.at(i, k), u));
+    }
+  }
+  X = Mat<R>(n, n);
+  for (int i = 0; i < n; ++i) X.at(i, i) = C<R>{1, 0};
+  for (int k = 0; k < n; ++k)   // row interchanges of the right-hand sides
+    if (piv[k] != k)
+      for (int j = 0; j < n; ++j) std::swap(X.at(k, j), X.at(piv[k], j));
+  for (int j = 0; j < n; ++j) {
+    for (int k = 0; k < n; ++k) {   // L y = b (unit diagonal)
+      const C<R> y = X.at(k, j);
+      for (int i = k + 1; i < n; ++i) X.at(i, j) = sub(X.at(i, j), mul(LU.at(i, k), y));
+    }
+    for (int k = n - 1; k >= 0; --k) {   // U x = y
+      if (LU.at(k, k).re == 0 && LU.at(k, k).im == 0) continue;
+      const C<R> x = mul(X.at(k, j), rcp(LU.at(k, k)));
+      X.at(k, j) = x;
+      for (int i = 0; i < k; ++i) X.at(i, j) = sub(X.at(i, j), mul(LU.at(i, k), x));
+    }
+  }
+  return info;
+}
+
+// Gauss-Jordan inversion in place with partial pivoting (the same pivot
+// rule), row interchanges recorded and undone as column interchanges at the
+// end: the elimination order of the engine's inversion, unblocked.
+template <typename R>
+int inv_gj(const Mat<R>& A, Mat<R>& X) {
+  const int n = A.nr;
+  X = A;
+  std::vector<int> piv(n);
+  int info = 0;
+  for (int k = 0; k < n; ++k) {
+    int p = k;
+    R best = -1;
+    for (int i = k; i < n; ++i) {
+      R a = std::fabs(X.at(i, k).re) + std::fabs(X.at(i, k).im);
+      if (a > best) { best = a; p = i; }
+    }
+    piv[k] = p;
+    if (best == 0) { if (!info) info = k + 1; continue; }
+    if (p != k)
+      for (int j = 0; j < n; ++j) std::swap(X.at(k, j), X.at(p, j));
+    const C<R> r = rcp(X.at(k, k));
+    for (int j = 0; j < n; ++j) X.at(k, j) = (j == k) ? r : mul(X.at(k, j), r);
+    for (int i = 0; i < n; ++i) {
+      if (i == k) continue;
+      const C<R> f = X.at(i, k);
+      for (int j = 0; j < n; ++j)
+        if (j != k) X.at(i, j) = sub(X.at(i, j), mul(f, X.at(k, j)));
+      X.at(i, k) = mul(mk<R>(-f.re, -f.im), r);
+    }
+  }
+  for (int k = n - 1; k >= 0; --k)
+    if (piv[k] != k)
+      for (int i = 0; i < n; ++i) std::swap(X.at(i, k), X.at(i, piv[k]));
+  return info;
+}
+
+// inversion used by the restatement: LU + solves, or Gauss-Jordan
+inline int& inv_kind() { static thread_local int k = 0; return k; }
+template <typename R>
+int invert(const Mat<R>& A, Mat<R>& X) { return inv_kind() ? inv_gj(A, X) : inv(A, X); }
+
+template <typename R>
+Mat<R> dag(const Mat<R>& A) {
+  Mat<R> D(A.nc, A.nr);
+  for (int j = 0; j < A.nc; ++j)
+    for (int i = 0; i < A.nr; ++i) D.at(j, i) = cj(A.at(i, j));
+  return D;
+}
+
+template <typename R>
+R maxabs(const Mat<R>& M) {
+  R m = 0;
+  for (const C<R>& z : M.v) m = std::max(m, (R)std::sqrt(z.re * z.re + z.im * z.im));
+  return m;
+}
+
+// decimation (src/contselfenergy.F90:271-340)
+template <typename R>
+Mat<R> decimation(Mat<R> Ao, Mat<R> Bo, Mat<R> Co, R tol, int max_iter, int& ncyc, int& info) {
+  Mat<R> Aos = Ao, Go, X, C1, Sf, Y, B1;
+  const C<R> one{1, 0}, mone{-1, 0};
+  bool ok = false;
+  int it;
+  for (it = 1; it <= max_iter; ++it) {
+    if (invert(Ao, Go)) info = 1;
+    gemm(Go, Co, X, one, false);
+    gemm(Co, X, C1, one, false);
+    if (maxabs(C1) <= tol) {
+      if (ok) break;
+      ok = true;
+    } else {
+      ok = false;
+    }
+    gemm(Bo, X, Sf, one, false);
+    for (size_t q = 0; q < Ao.v.size(); ++q) {
+      Aos.v[q] = sub(Aos.v[q], Sf.v[q]);
+      Ao.v[q] = sub(Ao.v[q], Sf.v[q]);
+    }
+    gemm(Go, Bo, Y, one, false);
+    gemm(Bo, Y, B1, one, false);
+    gemm(Co, Y, Ao, mone, true);
+    Bo = B1;
+    Co = C1;
+  }
+  ncyc = it;
+  if (invert(Aos, Go)) info = 1;
+  return Go;
+}
+
+// one 2-contact point: T (dos == nullptr: ESH at E, gsmr down to block 2,
+// Gr(1,1), trace) or T + DOS (ESH at E + i dos_delta, full Gr sweep)
+template <typename R>
+double point(const DeviceBlocks& D, double E, double eta, double dos_delta, double* dos, double tol,
+             int max_iter, int& ncyc, int& info) {
+  const C<R> one{1, 0}, mone{-1, 0};
+  const C<R> Ec = mk<R>((R)E, (R)eta);
+  ncyc = 0;
+  std::vector<Mat<R>> Sig(D.ncont);
+  for (int c = 0; c < D.ncont; ++c) {
+    const int L = D.L[c];
+    Mat<R> Ao(L, L), Bo(L, L), Ct(L, L);
+    const Mat<R> H00 = from<R>(D.H00[c]), H01 = from<R>(D.H01[c]), S00 = from<R>(D.S00[c]),
+                 S01 = from<R>(D.S01[c]), HMC = from<R>(D.HMC[c]), SMC = from<R>(D.SMC[c]);
+    for (size_t q = 0; q < Ao.v.size(); ++q) {
+      Ao.v[q] = sub(mul(Ec, S00.v[q]), H00.v[q]);
+      Bo.v[q] = sub(mul(Ec, S01.v[q]), H01.v[q]);
+      Ct.v[q] = sub(mul(cj(Ec), S01.v[q]), H01.v[q]);
+    }
+    int nc = 0;
+    Mat<R> GS = decimation(Ao, Bo, dag(Ct), (R)tol, max_iter, nc, info);
+    ncyc += nc;
+    Mat<R> Tlc(HMC.nr, HMC.nc), TpMt(HMC.nr, HMC.nc), TG;
+    for (size_t q = 0; q < HMC.v.size(); ++q) {
+      Tlc.v[q] = sub(mul(Ec, SMC.v[q]), HMC.v[q]);
+      TpMt.v[q] = sub(mul(cj(Ec), SMC.v[q]), HMC.v[q]);
+    }
+    gemm(Tlc, GS, TG, one, false);
+    gemm(TG, dag(TpMt), Sig[c], one, false);
+  }
+  const int nbl = D.nbl;
+  const C<R> Ed = mk<R>((R)E, dos ? (R)dos_delta : (R)0);
+  std::vector<Mat<R>> d(nbl), u(nbl > 0 ? nbl - 1 : 0), l(nbl > 0 ? nbl - 1 : 0);
+  for (int i = 0; i < nbl; ++i) {
+    const Mat<R> H = from<R>(D.Hd[i]);
+    d[i] = Mat<R>(H.nr, H.nc);
+    for (size_t q = 0; q < H.v.size(); ++q) {
+      C<R> s = D.s_id ? C<R>{0, 0} : mk<R>((R)D.Sd[i].v[q].real(), (R)D.Sd[i].v[q].imag());
+      d[i].v[q] = sub(mul(Ed, s), H.v[q]);
+    }
+    if (D.s_id)
+      for (int k = 0; k < H.nr; ++k) d[i].at(k, k) = add(d[i].at(k, k), Ed);
+    if (i + 1 < nbl) {
+      const Mat<R> Hu = from<R>(D.Hu[i]), Hl = from<R>(D.Hl[i]);
+      u[i] = Mat<R>(Hu.nr, Hu.nc);
+      l[i] = Mat<R>(Hl.nr, Hl.nc);
+      for (size_t q = 0; q < Hu.v.size(); ++q) {
+        C<R> su = D.s_id ? C<R>{0, 0} : mk<R>((R)D.Su[i].v[q].real(), (R)D.Su[i].v[q].imag());
+        C<R> sl = D.s_id ? C<R>{0, 0} : mk<R>((R)D.Sl[i].v[q].real(), (R)D.Sl[i].v[q].imag());
+        u[i].v[q] = sub(mul(Ed, su), Hu.v[q]);
+        l[i].v[q] = sub(mul(Ed, sl), Hl.v[q]);
+      }
+    }
+  }
+  for (int c = 0; c < D.ncont; ++c) {
+    Mat<R>& B = d[D.cblk[c] - 1];
+    for (size_t q = 0; q < B.v.size(); ++q) B.v[q] = sub(B.v[q], Sig[c].v[q]);
+  }
+  // gsmr(nbl) .. gsmr(2)
+  std::vector<Mat<R>> g(nbl);
+  if (nbl > 1) {
+    if (invert(d[nbl - 1], g[nbl - 1])) info = 1;
+    for (int i = nbl - 2; i >= 1; --i) {
+      Mat<R> w1, w2;
+      gemm(u[i], g[i + 1], w1, mone, false);
+      gemm(w1, l[i], w2, one, false);
+      for (size_t q = 0; q < w2.v.size(); ++q) w2.v[q] = add(d[i].v[q], w2.v[q]);
+      if (invert(w2, g[i])) info = 1;
+    }
+  }
+  // Gr(1,1)
+  std::vector<Mat<R>> Gd(nbl);
+  {
+    Mat<R> w = d[0];
+    if (nbl > 1) {
+      Mat<R> w2, w3;
+      gemm(u[0], g[1], w2, one, false);
+      gemm(w2, l[0], w3, one, false);
+      for (size_t q = 0; q < w.v.size(); ++q) w.v[q] = sub(w.v[q], w3.v[q]);
+    }
+    if (invert(w, Gd[0])) info = 1;
+  }
+  if (dos)
+    for (int i = 1; i < nbl; ++i) {   // Gr(i,i) = gsmr_i - Gr(i,i-1) ESH(i-1,i) gsmr_i
+      Mat<R> w1, Gl, w2, w3;
+      gemm(g[i], l[i - 1], w1, one, false);
+      gemm(w1, Gd[i - 1], Gl, mone, false);
+      gemm(u[i - 1], g[i], w2, one, false);
+      gemm(Gl, w2, w3, mone, false);
+      Gd[i] = Mat<R>(g[i].nr, g[i].nc);
+      for (size_t q = 0; q < w3.v.size(); ++q) Gd[i].v[q] = add(g[i].v[q], w3.v[q]);
+    }
+  // calculate_single_transmission_2_contacts with ct1 = the contact on block 1
+  double tun = 0.0;
+  if (D.ncont == 2) {
+    const int ct1 = (D.cblk[0] < D.cblk[1]) ? 0 : 1;
+    const Mat<R>& G = Gd[D.cblk[ct1] - 1];
+    const Mat<R> GA = dag(G);
+    Mat<R> GAM1(Sig[ct1].nr, Sig[ct1].nc);
+    const Mat<R> SigA = dag(Sig[ct1]);
+    for (size_t q = 0; q < GAM1.v.size(); ++q) GAM1.v[q] = mul(mk<R>(0, 1), sub(Sig[ct1].v[q], SigA.v[q]));
+    Mat<R> w1, w2, w3, AA(G.nr, G.nc), w4;
+    gemm(GAM1, G, w1, one, false);
+    gemm(w1, GAM1, w2, one, false);
+    gemm(w2, GA, w3, one, false);
+    for (size_t q = 0; q < AA.v.size(); ++q) AA.v[q] = mul(mk<R>(0, 1), sub(G.v[q], GA.v[q]));
+    gemm(GAM1, AA, w4, one, false);
+    R tr = 0;
+    for (int k = 0; k < G.nr; ++k) tr += w4.at(k, k).re - w3.at(k, k).re;
+    tun = (double)std::fabs(tr);
+  }
+  if (dos) {
+    const R pi = (R)3.14159265358979323846264338327950288L;
+    for (int i = 0; i < nbl; ++i)
+      for (int k = 0; k < D.n[i]; ++k) dos[D.start[i] + k] = (double)(-Gd[i].at(k, k).im / pi);
+  }
+  return tun;
+}
+
+}  // namespace xp
+
 }  // namespace
 
 extern "C" {
@@ -1226,6 +1559,54 @@ double oracle_integrate_el(const double* tun, int ntun, double mu1, double mu2,
   }
   if (swapped) curr = -1.0 * curr;
   return curr;
+}
+
+// Independent-rounding restatement of the 2-contact T (dos == null) or T +
+// DOS path over `npts` energies: prec = 1 in long double (near-exact), 0 in
+// double with its own unblocked LU and products, 2 in double with
+// Gauss-Jordan inverses (the engine's elimination order, unblocked).  ncyc and status as in
+// oracle_transmission; status 1 on a zero pivot.
+int oracle_transmission_xp(const negf_b200_device* dev, int npts, const double* energy, double eta,
+                           double dos_delta, double sgf_tol, int sgf_max_iter, int prec, double* T,
+                           double* dos, int* ncyc, int* status, int nthreads) {
+  set_threads(nthreads);
+  DeviceBlocks D = unpack(dev);
+  if (D.ncont != 2) return NEGF_B200_ERR_BAD_ARG;
+  // the T-only path is the fast path of calculate_transmissions: Gr(1,1) only
+  if (!dos && std::min(D.cblk[0], D.cblk[1]) != 1) return NEGF_B200_ERR_BAD_ARG;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int p = 0; p < npts; ++p) {
+    int nc = 0, info = 0;
+    double* dp = dos ? dos + (size_t)p * D.norb : nullptr;
+    xp::inv_kind() = (prec == 2) ? 1 : 0;
+    T[p] = (prec == 1) ? xp::point<long double>(D, energy[p], eta, dos_delta, dp, sgf_tol, sgf_max_iter, nc, info)
+                       : xp::point<double>(D, energy[p], eta, dos_delta, dp, sgf_tol, sgf_max_iter, nc, info);
+    if (ncyc) ncyc[p] = nc;
+    if (status) status[p] = info;
+  }
+  return 0;
+}
+
+// Decimation restated over long double (prec 1) or double with its own LU
+// (prec 0) or Gauss-Jordan inverses (prec 2); arguments as oracle_decimation.
+int oracle_decimation_xp(int n, const double* Ao, const double* Bo, const double* Co, double tol, int max_iter,
+                         int prec, double* Go, int* ncyc) {
+  Dns A = from_ptr(Ao, n, n), B = from_ptr(Bo, n, n), C = from_ptr(Co, n, n);
+  int info = 0, nc = 0;
+  xp::inv_kind() = (prec == 2) ? 1 : 0;
+  if (prec == 1) {
+    xp::Mat<long double> G = xp::decimation<long double>(xp::from<long double>(A), xp::from<long double>(B),
+                                                         xp::from<long double>(C), (long double)tol, max_iter, nc,
+                                                         info);
+    for (size_t q = 0; q < G.v.size(); ++q) { Go[2 * q] = (double)G.v[q].re; Go[2 * q + 1] = (double)G.v[q].im; }
+  } else {
+    xp::Mat<double> G = xp::decimation<double>(xp::from<double>(A), xp::from<double>(B), xp::from<double>(C), tol,
+                                               max_iter, nc, info);
+    for (size_t q = 0; q < G.v.size(); ++q) { Go[2 * q] = G.v[q].re; Go[2 * q + 1] = G.v[q].im; }
+  }
+  xp::inv_kind() = 0;
+  if (ncyc) *ncyc = nc;
+  return info;
 }
 
 }  // extern "C"

@@ -33,6 +33,8 @@ def lib():
         vp = ctypes.c_void_p
         L.oracle_decimation.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int, dp, ip]
         L.oracle_zinv.argtypes = [ctypes.c_int, dp, dp]
+        L.oracle_decimation_xp.argtypes = [ctypes.c_int, dp, dp, dp, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_int, dp, ip]
         L.oracle_transmission.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double, ctypes.c_int, ctypes.c_double, dp, ip, ip, ctypes.c_int]
         L.oracle_transmission_dos.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double,
@@ -50,6 +52,9 @@ def lib():
         L.oracle_density_neq.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, dp, dp, dp, ctypes.c_int,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_int, dp, dp, dp, dp, dp, ip, ip,
                                          ctypes.c_int]
+        L.oracle_transmission_xp.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_int, ctypes.c_int, dp, dp, ip, ip,
+                                             ctypes.c_int]
         L.oracle_fermi.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double]
         L.oracle_fermi.restype = ctypes.c_double
         L.oracle_integrate_el.argtypes = [dp, ctypes.c_int] + [ctypes.c_double] * 8
@@ -80,6 +85,19 @@ def decimation(Ao, Bo, Co, tol=1e-9, max_iter=300):
     return g.reshape((n, n), order="F"), int(ncyc[0]), st
 
 
+def decimation_xp(Ao, Bo, Co, tol=1e-9, max_iter=300, extended=True, gauss_jordan=False):
+    """decimation restated over long double (extended) or over double with its
+    own unblocked LU (or Gauss-Jordan) inverses and triple-loop products."""
+    n = Ao.shape[0]
+    a, b, c = (_flatF(x) for x in (Ao, Bo, Co))
+    g = np.zeros(n * n, dtype=np.complex128)
+    ncyc = np.zeros(1, dtype=np.int32)
+    st = lib().oracle_decimation_xp(n, _d(a.view(np.float64)), _d(b.view(np.float64)), _d(c.view(np.float64)),
+                                    tol, max_iter, 1 if extended else (2 if gauss_jordan else 0),
+                                    _d(g.view(np.float64)), _i(ncyc))
+    return g.reshape((n, n), order="F"), int(ncyc[0]), st
+
+
 def zinv(A):
     n = A.shape[0]
     a = _flatF(A)
@@ -99,6 +117,31 @@ def transmission(dev: Device, energies, eta=1e-4, ni=1, nf=2, sgf_tol=1e-9, sgf_
     lib().oracle_transmission(ctypes.addressof(st), npts, _d(E), eta, ni, nf, sgf_tol, sgf_max_iter, eps,
                               _d(T), _i(ncyc), _i(status), nthreads)
     return T, ncyc, status
+
+
+def transmission_xp(dev: Device, energies, eta=1e-4, dos_delta=None, sgf_tol=1e-9, sgf_max_iter=300,
+                    extended=True, nthreads=0, gauss_jordan=False):
+    """The 2-contact T path (dos_delta None) or T + DOS path restated over
+    long double (extended=True: 64-bit significand, a near-exact solution of
+    the same algorithm) or over double with its own unblocked LU and
+    triple-loop products (extended=False: a second FP64 rounding path; with
+    gauss_jordan=True the inverses are Gauss-Jordan eliminations instead).
+    Returns T, dos (or None), ncyc, status."""
+    E = np.ascontiguousarray(energies, dtype=np.float64)
+    npts = E.size
+    T = np.zeros(npts)
+    dos = np.zeros((npts, dev.norb)) if dos_delta is not None else None
+    ncyc = np.zeros(npts, dtype=np.int32)
+    status = np.zeros(npts, dtype=np.int32)
+    st = dev.to_struct()
+    rc = lib().oracle_transmission_xp(ctypes.addressof(st), npts, _d(E), eta,
+                                      0.0 if dos_delta is None else dos_delta, sgf_tol, sgf_max_iter,
+                                      1 if extended else (2 if gauss_jordan else 0), _d(T),
+                                      _d(dos) if dos is not None else None,
+                                      _i(ncyc), _i(status), nthreads)
+    if rc != 0:
+        raise ValueError("oracle_transmission_xp: status %d (two contacts only)" % rc)
+    return T, dos, ncyc, status
 
 
 def transmission_dos(dev: Device, energies, eta=1e-4, dos_delta=1e-4, ni=1, nf=2, sgf_tol=1e-9,

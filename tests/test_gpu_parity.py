@@ -1,5 +1,13 @@
 """GPU parity: the CUDA path (through the C-ABI) against the CPU oracle on
-the same seeded inputs.  Bound: |T - T_oracle| <= max(1e-10 |T_oracle|, 1e-13)."""
+the same seeded inputs.
+
+Bound: |T - T_oracle| <= max(1e-10 |T_oracle|, 1e-13), strict at every point
+where three CPU FP64 paths of the algorithm (the oracle's and two restated
+ones) all lie within an eighth of it from the long-double solution; the
+decimation's iteration count equals the oracle's at every point.  At the
+other points (ill-conditioned device solves: the device blocks carry no
+broadening) the GPU result must lie as close to the long-double solution as
+the CPU FP64 paths do (conftest.assert_parity)."""
 import ctypes
 
 import numpy as np
@@ -8,7 +16,7 @@ import pytest
 from libnegf_b200 import generators as G
 from libnegf_b200 import native
 from oracle import oracle as O
-from conftest import assert_T_close, oracle_spread
+from conftest import assert_parity, assert_T_strict, xp_reference
 
 pytestmark = pytest.mark.gpu
 torch = pytest.importorskip("torch")
@@ -113,8 +121,14 @@ def test_decimation_batched(n):
     Gd = _host(dG, n, n)
     for i in range(b):
         g, nc, st = O.decimation(Ao[i], Bo[i], Co[i], tol=1e-9)
-        assert abs(int(ncyc[i]) - nc) <= 1
-        assert np.abs(Gd[i] - g).max() <= 1e-9 * max(1.0, np.abs(g).max())
+        assert int(ncyc[i]) == nc
+        gx = O.decimation_xp(Ao[i], Bo[i], Co[i], tol=1e-9)[0]
+        gd = O.decimation_xp(Ao[i], Bo[i], Co[i], tol=1e-9, extended=False)[0]
+        gg = O.decimation_xp(Ao[i], Bo[i], Co[i], tol=1e-9, extended=False, gauss_jordan=True)[0]
+        bound = 1e-10 * max(1.0, np.abs(g).max())
+        for part in (np.real, np.imag):
+            assert_parity(part(Gd[i]), part(g), bound, ref_x=part(gx), others=(part(gd), part(gg)),
+                          what="surface GF (n=%d, E=%g)" % (n, Es[i]))
 
 
 CASES = {
@@ -152,10 +166,10 @@ def test_transmission_parity(gpu_ctx, case):
     did = gpu_ctx.upload(dev)
     try:
         T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6)
-        ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev)
+        ref = _o_T(E, eta=1e-6)(dev)
         assert np.all(st == ref["status"])
-        assert np.all(np.abs(ncyc - ref["ncyc"]) <= 4)
-        assert_T_close(T, ref["T"], spread=spread["T"])
+        assert np.array_equal(ncyc, ref["ncyc"])
+        assert_T_strict(T, ref["T"], xp_reference(dev, E, 1e-6))
     finally:
         gpu_ctx.release(did)
 
@@ -171,10 +185,10 @@ def test_transmission_parity_band_edges(gpu_ctx, gen):
     did = gpu_ctx.upload(dev)
     try:
         T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6, check=False)
-        ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev)
+        ref = _o_T(E, eta=1e-6)(dev)
         assert np.all(st == ref["status"])
-        assert np.all(np.abs(ncyc - ref["ncyc"]) <= 4)
-        assert_T_close(T, ref["T"], spread=spread["T"])
+        assert np.array_equal(ncyc, ref["ncyc"])
+        assert_T_strict(T, ref["T"], xp_reference(dev, E, 1e-6))
     finally:
         gpu_ctx.release(did)
 
@@ -186,9 +200,10 @@ def test_transmission_parity_default_eta(gpu_ctx, case):
     did = gpu_ctx.upload(dev)
     try:
         T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-4)
-        ref, spread = oracle_spread(_o_T(E, eta=1e-4), dev)
+        ref = _o_T(E, eta=1e-4)(dev)
         assert np.all(st == ref["status"])
-        assert_T_close(T, ref["T"], spread=spread["T"])
+        assert np.array_equal(ncyc, ref["ncyc"])
+        assert_T_strict(T, ref["T"], xp_reference(dev, E, 1e-4))
     finally:
         gpu_ctx.release(did)
 
@@ -199,12 +214,15 @@ def test_transmission_dos_parity(gpu_ctx, case):
     did = gpu_ctx.upload(dev)
     try:
         T, dos, ncyc, st = gpu_ctx.transmission_dos(did, E, eta=1e-6, dos_delta=1e-4)
-        ref, spread = oracle_spread(_o_dos(E, eta=1e-6, dos_delta=1e-4), dev)
+        ref = _o_dos(E, eta=1e-6, dos_delta=1e-4)(dev)
         assert np.all(st == ref["status"])
-        assert_T_close(T, ref["T"], spread=spread["T"])
-        scale = max(np.abs(ref["dos"]).max(), 1.0)
-        bound = np.maximum(1e-10 * scale, 10 * spread["dos"])
-        assert np.all(np.abs(dos - ref["dos"]) <= bound)
+        assert np.array_equal(ncyc, ref["ncyc"])
+        x = xp_reference(dev, E, 1e-6, dos_delta=1e-4)
+        assert_T_strict(T, ref["T"], x)
+        # DOS: 1e-10 relative to the largest entry
+        bound = 1e-10 * max(np.abs(ref["dos"]).max(), 1.0)
+        assert_parity(dos, ref["dos"], bound, ref_x=None if x is None else x["dos_x"],
+                      others=() if x is None else (x["dos_d"], x["dos_g"]), what="DOS")
     finally:
         gpu_ctx.release(did)
 
@@ -217,11 +235,12 @@ def test_multi_device_batch(gpu_ctx):
     try:
         ids = np.array([i1] * len(E1) + [i2] * len(E2), dtype=np.int32)
         E = np.concatenate([E1, E2])
-        T, _, st = gpu_ctx.transmission(ids, E, eta=1e-6)
-        r1, s1 = oracle_spread(_o_T(E1, eta=1e-6), d1)
-        r2, s2 = oracle_spread(_o_T(E2, eta=1e-6), d2)
-        assert_T_close(T[:len(E1)], r1["T"], spread=s1["T"])
-        assert_T_close(T[len(E1):], r2["T"], spread=s2["T"])
+        T, nc, st = gpu_ctx.transmission(ids, E, eta=1e-6)
+        r1 = _o_T(E1, eta=1e-6)(d1)
+        r2 = _o_T(E2, eta=1e-6)(d2)
+        assert np.array_equal(nc, np.concatenate([r1["ncyc"], r2["ncyc"]]))
+        assert_T_strict(T[:len(E1)], r1["T"], xp_reference(d1, E1, 1e-6))
+        assert_T_strict(T[len(E1):], r2["T"], xp_reference(d2, E2, 1e-6))
     finally:
         gpu_ctx.release(i1)
         gpu_ctx.release(i2)
@@ -262,14 +281,15 @@ def test_meir_wingreen_parity(gpu_ctx, case):
     gpu_ctx.set_options(scba_niter=niter, scba_tol=tol, scba_mix=mix, scba_rule=rule)
     try:
         r = gpu_ctx.meir_wingreen(did, E, frm, coupling=cpl, eta=1e-4)
-        o, spread = oracle_spread(lambda d: O.meir_wingreen(d, E, frm, coupling=cpl, eta=1e-4, scba_niter=niter,
-                                                            scba_tol=tol, scba_mix=mix, scba_rule=rule), dev)
+        o = O.meir_wingreen(dev, E, frm, coupling=cpl, eta=1e-4, scba_niter=niter, scba_tol=tol,
+                            scba_mix=mix, scba_rule=rule)
         assert np.all(r["status"] == o["status"])
-        assert np.all(np.abs(r["scba_iter"] - o["scba_iter"]) <= 1)
+        assert np.array_equal(r["scba_iter"], o["scba_iter"])
+        assert np.array_equal(r["ncyc"], o["ncyc"])
         for key in ("curr", "layer_curr", "layer_dens"):
             a, b = r[key], o[key]
-            bound = np.maximum(1e-10 * max(1.0, np.abs(b).max()), 10 * spread[key])
-            assert np.all(np.abs(a - b) <= bound), key
+            bound = 1e-10 * max(1.0, np.abs(b).max())
+            assert np.all(np.abs(a - b) <= bound), (key, np.abs(a - b).max(), bound)
     finally:
         gpu_ctx.set_options()
         gpu_ctx.release(did)

@@ -33,8 +33,11 @@ def _worker(rank, world, port, out):
         idx = shard.shard_points(E.size, rank, world)
         rows = _fake_solve(E[idx])
         full = shard.reduce_rows(shard.scatter_rows(rows, idx, E.size), dist)
+        # complex rows (density / Gn blocks) keep their imaginary part
+        crow = rows[:, :1] * np.exp(1j * E[idx])[:, None]
+        cfull = shard.reduce_rows(shard.scatter_rows(crow, idx, E.size), dist)
         t = shard.max_over_ranks(1.0 + rank, dist)
-        out[rank] = (full, t, idx.tolist())
+        out[rank] = (full, t, idx.tolist(), cfull)
     finally:
         dist.destroy_process_group()
 
@@ -48,9 +51,11 @@ def test_two_gloo_ranks_rebuild_the_single_rank_result():
     mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
     E = np.linspace(-2, 2, 37)
     ref = _fake_solve(E)
+    cref = ref[:, :1] * np.exp(1j * E)[:, None]
     for r in range(world):
-        full, t, idx = out[r]
+        full, t, idx, cfull = out[r]
         assert np.array_equal(full, ref)
+        assert cfull.dtype == np.complex128 and np.array_equal(cfull, cref)
         assert t == float(world)               # the slowest rank's time
     assert sorted(out[0][2] + out[1][2]) == list(range(E.size))
 

@@ -64,6 +64,29 @@ def test_noalloc_decimation_matches_batched_on_two_calls():
         assert np.abs(g - g_ref).max() <= 1e-9 * scale
 
 
+def test_noalloc_calls_leave_free_device_memory_unchanged():
+    """After a first call (which loads the module and resolves the array's
+    address), further calls change the device's free memory by nothing: the
+    scratch is the fixed array, not an allocation."""
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    L = native.load()
+    n, Es = 64, [-1.1, 0.3, 1.7]
+    b = len(Es)
+    Ao, Bo, Co = _problem(n, Es, 5)
+    Go = torch.empty_like(Ao)
+    nc = torch.zeros(b, dtype=torch.int32, device="cuda")
+    call = lambda: L.negf_b200_decimation_noalloc(b, n, Ao.data_ptr(), Bo.data_ptr(), Co.data_ptr(),
+                                                  Go.data_ptr(), nc.data_ptr(), 1e-9, 300, None)
+    assert call() == 0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        assert call() == 0
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_noalloc_rejects_requests_beyond_the_fixed_scratch():
     if not torch.cuda.is_available():
         pytest.skip("no CUDA device")
