@@ -17,6 +17,7 @@
 
 #include "../../include/negf_b200.h"
 #include "engine.cuh"
+#include "ozaki.cuh"
 
 using negf::DevDesc;
 
@@ -1391,6 +1392,30 @@ int negf_b200_zgemm_batched(int32_t batch, int32_t m, int32_t n, int32_t k, cons
   cudaError_t e = negf::launch_zgemm_batched(
       batch, m, n, k, make_double2(alpha[0], alpha[1]), (const double2*)A, strideA / 2, (const double2*)B,
       strideB / 2, make_double2(beta[0], beta[1]), (double2*)C, strideC / 2, dagger, (cudaStream_t)stream);
+  return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;
+}
+
+size_t negf_b200_zgemm_i8_work_bytes(int32_t batch, int32_t m, int32_t n, int32_t k, int32_t slices) {
+  if (batch <= 0 || m <= 0 || n <= 0 || k <= 0 || slices < negf::kOzMinSlices || slices > negf::kOzMaxSlices)
+    return 0;
+  return negf::ozaki_layout(batch, m, n, k, slices).total + 256;
+}
+
+int negf_b200_zgemm_batched_i8(int32_t batch, int32_t m, int32_t n, int32_t k, const double* alpha,
+                               const double* A, int64_t strideA, const double* B, int64_t strideB,
+                               const double* beta, double* C, int64_t strideC, int32_t slices, void* work,
+                               int32_t* status, void* stream) {
+  if (batch < 0 || m < 0 || n < 0 || k < 0 || k > negf::kMaxOrder || batch > 65535 || !alpha || !beta ||
+      slices < negf::kOzMinSlices || slices > negf::kOzMaxSlices)
+    return NEGF_B200_ERR_BAD_ARG;
+  if (batch == 0 || m == 0 || n == 0) return NEGF_B200_OK;
+  if (!A || !B || !C || !work || k == 0) return NEGF_B200_ERR_BAD_ARG;
+  // the workspace is used from its first 256-byte boundary
+  uint8_t* w = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(work) + 255) & ~uintptr_t(255));
+  cudaError_t e = negf::launch_ozaki_zgemm(batch, m, n, k, make_double2(alpha[0], alpha[1]), (const double2*)A,
+                                           strideA / 2, (const double2*)B, strideB / 2,
+                                           make_double2(beta[0], beta[1]), (double2*)C, strideC / 2, slices, w,
+                                           nullptr, status, (cudaStream_t)stream);
   return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;
 }
 

@@ -1,0 +1,539 @@
+// Complex128 block products on the integer tensor cores of sm_100a: an exact
+// int8 splitting of the operands (see ozaki.cuh), tcgen05.mma kind::i8 with
+// the int32 accumulators in tensor memory, operand tiles staged by TMA.
+//
+// One product is three launches on the caller's stream:
+//   k_split_rows  A -> int8 digit planes of Ar, Ai, -Ai (K contiguous) and a
+//                 power-of-two exponent per row;
+//   k_split_cols  B -> digit planes of Br, Bi and an exponent per column;
+//   k_ozaki       one CTA per 128 x 64 tile of C: two passes (real, imaginary
+//                 part) over the concatenated K, one accumulator of 64
+//                 columns in TMEM per digit level l = t + u, then the FP64
+//                 epilogue C = alpha * 2^(eA+eB) sum_l 2^(-12-7l) acc_l + beta * C.
+// Roles inside k_ozaki: warp 0 lane 0 issues the TMA loads of a two-stage
+// ring, warp 1 lane 0 issues the MMAs and commits each stage back to the
+// producer; all eight warps read the accumulators (warp w reads TMEM lanes
+// 32 (w % 4) .. +31, columns 32 (w / 4) .. +31).  Every wait on an mbarrier is
+// bounded (about one second of SM clock); a wait that runs out marks the
+// item's status and the CTA frees its tensor memory and returns.
+//
+// Reference: the complex products this replaces are the zgemm calls of
+// prealloc_mult (src/sparsekit_drv.F90:1896-2081) and cu_ZmultMat
+// (src/gpuroutines.cu:395-446); libNEGF has no reduced-precision product
+// of its own besides the TF32 switch of cu_Zdecimation (:794-797).
+#include <cuda.h>   // CUtensorMap and its enums only; the encoder comes from the runtime's driver entry point
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+
+#include "ozaki.cuh"
+
+namespace negf {
+namespace {
+
+constexpr int kOzThreads = 256;
+constexpr long long kSpinCycles = 2000000000LL;   // bound of one mbarrier wait (~1 s)
+constexpr int kABytes = kOzTileM * kOzKChunk;      // one digit plane of an A tile
+constexpr int kBBytes = kOzTileN * kOzKChunk;      // one digit plane of a B tile
+
+__device__ __forceinline__ uint32_t s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// ---------------------------------------------------------------- mbarrier
+__device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(s32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for the completion of the phase with the given parity; false (and
+// *fail set) if it does not complete within kSpinCycles or another thread of
+// the CTA has already given up.
+__device__ bool mbar_wait(uint64_t* b, uint32_t parity, volatile int* fail) {
+  const long long t0 = clock64();
+  while (!mbar_test(b, parity)) {
+    if (*fail) return false;
+    if (clock64() - t0 > kSpinCycles) {
+      *fail = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// ---------------------------------------------------------------- TMA
+__device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(s32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(s32(bar))
+      : "memory");
+}
+
+// ---------------------------------------------------------------- tcgen05
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory operand descriptor: K-major, 64-byte swizzle, rows of 64 bytes,
+// 8-row groups 512 bytes apart (SBO), version 1 (sm_100).
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T, int8 x int8 -> int32, M = 128, N = 64, K = 32
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(s32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&v)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+constexpr uint32_t kTmemCols = 512;
+
+// instruction descriptor: D s32, A/B signed int8, both K-major, N = 64, M = 128
+constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kOzTileN >> 3) << 17) |
+                              ((uint32_t)(kOzTileM >> 4) << 24);
+
+// ---------------------------------------------------------------- splitting
+// Digits: x = a 2^-e in (-1, 1); d_0 = rint(64 x), then d_t = rint(128 r) of
+// the remainder r in [-1/2, 1/2]: every digit lies in [-64, 64] and
+// x = sum_t d_t 2^(-6-7t) + r 2^(-6-7(S-1)).  Rounding to nearest leaves the
+// cut-off remainders zero-mean.  A digit pair (t, u) has the weight
+// 2^(-12-7(t+u)), exact as a double.
+__device__ __forceinline__ double level_weight(int l) { return __longlong_as_double((long long)(1023 - 12 - 7 * l) << 52); }
+
+template <int S>
+__device__ __forceinline__ void digits(double x, int8_t (&d)[S]) {
+  double y = x * 64.0;
+  double r = rint(y);
+  d[0] = (int8_t)r;
+  x = y - r;
+#pragma unroll
+  for (int t = 1; t < S; ++t) {
+    y = x * 128.0;
+    r = rint(y);
+    d[t] = (int8_t)r;
+    x = y - r;
+  }
+}
+
+// levels kept: digit pairs (t, u) with t + u < levels(S); one TMEM accumulator each
+__host__ __device__ constexpr int oz_levels(int S) { return S + 1 < 8 ? S + 1 : 8; }
+
+// Rows of A (M x K, column major, lda = M): exponent per row, digit planes
+// of Ar, Ai, -Ai with K contiguous (row pitch kp bytes).  Block: 32 rows.
+template <int S>
+__global__ void __launch_bounds__(256) k_split_rows(int m, int k, int kp, const double2* A, int64_t sA, int8_t* qa,
+                                                   int* ea, int* flag) {
+  __shared__ double smax[8][32];
+  __shared__ int sexp[32];
+  __shared__ int sbad;
+  __shared__ __align__(16) int8_t sq[3][S][32][32];
+  const int item = blockIdx.y;
+  const int m0 = blockIdx.x * 32;
+  const int r = threadIdx.x & 31, g = threadIdx.x >> 5;
+  const double2* Ab = A + (int64_t)item * sA;
+  if (threadIdx.x == 0) sbad = 0;
+  __syncthreads();
+  double mx = 0.0;
+  bool bad = false;
+  if (m0 + r < m)
+    for (int kk = g; kk < k; kk += 8) {
+      const double2 v = Ab[(int64_t)(m0 + r) + (int64_t)kk * m];
+      bad |= !(isfinite(v.x) && isfinite(v.y));
+      mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+    }
+  smax[g][r] = mx;
+  if (bad) sbad = 1;
+  __syncthreads();
+  if (g == 0) {
+    double t = smax[0][r];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) t = fmax(t, smax[q][r]);
+    int e = 0;
+    if (t > 0.0 && isfinite(t)) frexp(t, &e);   // t = f 2^e, f in [0.5, 1): |row| < 2^e
+    sexp[r] = e;
+    if (m0 + r < m) ea[(int64_t)item * m + m0 + r] = e;
+  }
+  __syncthreads();
+  if (sbad && threadIdx.x == 0) atomicOr(flag + item, 1);
+  const int e = sexp[r];
+  const int64_t plane = (int64_t)m * kp;
+  for (int k0 = 0; k0 < kp; k0 += 32) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int kk = k0 + 4 * g + j;
+      double2 v = make_double2(0.0, 0.0);
+      if (m0 + r < m && kk < k) v = Ab[(int64_t)(m0 + r) + (int64_t)kk * m];
+      int8_t dr[S], di[S];
+      digits<S>(ldexp(v.x, -e), dr);
+      digits<S>(ldexp(v.y, -e), di);
+#pragma unroll
+      for (int t = 0; t < S; ++t) {
+        sq[0][t][r][4 * g + j] = dr[t];
+        sq[1][t][r][4 * g + j] = di[t];
+        sq[2][t][r][4 * g + j] = (int8_t)(-di[t]);
+      }
+    }
+    __syncthreads();
+    // 3 * S planes x 32 rows x 2 segments of 16 bytes
+    for (int idx = threadIdx.x; idx < 3 * S * 64; idx += 256) {
+      const int seg = idx & 1, row = (idx >> 1) & 31, pt = idx >> 6;   // pt = arr * S + t
+      const int arr = pt / S, t = pt % S;
+      if (m0 + row < m && k0 + 16 * seg < kp) {
+        int8_t* dst = qa + ((int64_t)(item * 3 + arr) * S + t) * plane + (int64_t)(m0 + row) * kp + k0 + 16 * seg;
+        *reinterpret_cast<int4*>(dst) = *reinterpret_cast<const int4*>(&sq[arr][t][row][16 * seg]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Columns of B (K x N, column major, ldb = K): exponent per column, digit
+// planes of Br, Bi with K contiguous.  One warp per column.
+template <int S>
+__global__ void __launch_bounds__(256) k_split_cols(int k, int n, int kp, const double2* B, int64_t sB, int8_t* qb,
+                                                   int* eb, int* flag) {
+  const int item = blockIdx.y;
+  const int c = blockIdx.x * 8 + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (c >= n) return;
+  const double2* col = B + (int64_t)item * sB + (int64_t)c * k;
+  double mx = 0.0;
+  bool bad = false;
+  for (int kk = lane; kk < k; kk += 32) {
+    const double2 v = col[kk];
+    bad |= !(isfinite(v.x) && isfinite(v.y));
+    mx = fmax(mx, fmax(fabs(v.x), fabs(v.y)));
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  bad = __any_sync(0xffffffffu, bad);
+  int e = 0;
+  if (mx > 0.0 && isfinite(mx)) frexp(mx, &e);
+  if (lane == 0) {
+    eb[(int64_t)item * n + c] = e;
+    if (bad) atomicOr(flag + item, 1);
+  }
+  const int64_t plane = (int64_t)n * kp;
+  int8_t* q0 = qb + (int64_t)(item * 2) * S * plane + (int64_t)c * kp;
+  for (int kk = lane; kk < kp; kk += 32) {
+    double2 v = make_double2(0.0, 0.0);
+    if (kk < k) v = col[kk];
+    int8_t dr[S], di[S];
+    digits<S>(ldexp(v.x, -e), dr);
+    digits<S>(ldexp(v.y, -e), di);
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+      q0[(int64_t)t * plane + kk] = dr[t];
+      q0[(int64_t)(S + t) * plane + kk] = di[t];
+    }
+  }
+}
+
+// ---------------------------------------------------------------- product
+struct OzArgs {
+  int m, n, k, nkc;   // nkc: K chunks of 64 bytes per half of the concatenated K
+  double2 alpha, beta;
+  double2* C;
+  int64_t sC;
+  const int* ea;
+  const int* eb;
+  const int* flag;
+  double* maxabs;
+  int* status;
+};
+
+template <int S>
+__global__ void __launch_bounds__(kOzThreads, 1)
+    k_ozaki(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, OzArgs a) {
+  constexpr int kStage = S * (kABytes + kBBytes);
+  constexpr int kLevels = oz_levels(S);
+  static_assert(kLevels * kOzTileN <= (int)kTmemCols, "level accumulators must fit the tensor memory");
+  extern __shared__ __align__(1024) uint8_t oz_raw[];
+  uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(oz_raw) + 1023) & ~uintptr_t(1023));
+  __shared__ __align__(8) uint64_t full[kOzStages], empty[kOzStages], accb;
+  __shared__ uint32_t tmem_base;
+  __shared__ volatile int fail;
+  __shared__ int issued[kOzStages];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = blockIdx.y;
+  const int tiles_n = (a.n + kOzTileN - 1) / kOzTileN;
+  const int m0 = (blockIdx.x / tiles_n) * kOzTileM, n0 = (blockIdx.x % tiles_n) * kOzTileN;
+  const int nchunk = 2 * a.nkc;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kOzStages; ++i) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], 1);
+      issued[i] = 0;
+    }
+    mbar_init(&accb, 1);
+    fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s32(&tmem_base)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = tmem_base;
+
+  // epilogue geometry: row r of the tile, 32 columns [cw, cw + 32)
+  const int quarter = warp & 3;
+  const int r = m0 + 32 * quarter + lane;
+  const int cw = 32 * (warp >> 2);
+  const bool row_ok = r < a.m;
+  const int ea_r = row_ok ? a.ea[(int64_t)item * a.m + r] : 0;
+  const bool nonfinite = a.flag[item] != 0;
+  double re[32];
+  double local_max = 0.0;
+
+  for (int pass = 0; pass < 2; ++pass) {
+    if (warp == 0 && lane == 0) {
+      // producer: TMA loads of the digit planes into the stage ring
+      for (int c = 0; c < nchunk; ++c) {
+        const int gidx = pass * nchunk + c, st = gidx % kOzStages, use = gidx / kOzStages;
+        if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, &fail)) break;
+        uint8_t* sa = sm + st * kStage;
+        uint8_t* sb = sa + S * kABytes;
+        const int h = c / a.nkc, k0 = (c % a.nkc) * kOzKChunk;
+        // real pass: [Ar | -Ai] x [Br ; Bi]; imaginary pass: [Ai | Ar] x [Br ; Bi]
+        const int arr_a = (pass == 0) ? (h == 0 ? 0 : 2) : (h == 0 ? 1 : 0);
+        mbar_arrive_tx(&full[st], (uint32_t)kStage);
+        for (int t = 0; t < S; ++t) {
+          tma_load_3d(sa + t * kABytes, &tA, &full[st], k0, m0, (item * 3 + arr_a) * S + t);
+          tma_load_3d(sb + t * kBBytes, &tB, &full[st], k0, n0, (item * 2 + h) * S + t);
+        }
+        issued[st] = use + 1;
+      }
+    } else if (warp == 1 && lane == 0) {
+      // MMA issuer: all digit pairs (t, u) with t + u < levels per K step
+      tc_fence_after();
+      for (int c = 0; c < nchunk; ++c) {
+        const int gidx = pass * nchunk + c, st = gidx % kOzStages, use = gidx / kOzStages;
+        if (!mbar_wait(&full[st], use & 1, &fail)) break;
+        tc_fence_after();
+        const uint32_t sa = s32(sm + st * kStage), sb = sa + S * kABytes;
+#pragma unroll
+        for (int ks = 0; ks < kOzKChunk / 32; ++ks) {
+#pragma unroll
+          for (int t = 0; t < S; ++t) {
+            const uint64_t da = sdesc(sa + t * kABytes + ks * 32);
+#pragma unroll
+            for (int u = 0; u < S && t + u < kLevels; ++u) {
+              const uint64_t db = sdesc(sb + u * kBBytes + ks * 32);
+              // the first pair of a level (smallest t) in a pass overwrites its accumulator
+              const int first_t = (t + u > S - 1) ? t + u - (S - 1) : 0;
+              const uint32_t acc = (c > 0 || ks > 0 || t > first_t) ? 1u : 0u;
+              umma_i8(tbase + (uint32_t)((t + u) * kOzTileN), da, db, kIdescI8, acc);
+            }
+          }
+        }
+        umma_commit(&empty[st]);   // the stage is free once these MMAs have read it
+      }
+      umma_commit(&accb);          // the level accumulators of this pass are complete
+    }
+    __syncwarp();
+    const bool ok = mbar_wait(&accb, pass & 1, &fail) && !fail;
+    tc_fence_after();
+    if (ok) {
+#pragma unroll
+      for (int grp = 0; grp < 4; ++grp) {
+        uint32_t v[kLevels][8];
+#pragma unroll
+        for (int l = 0; l < kLevels; ++l)
+          tmem_ld8(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(l * kOzTileN + cw + 8 * grp), v[l]);
+        tmem_wait_ld();
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          double x = 0.0;
+#pragma unroll
+          for (int l = kLevels - 1; l >= 0; --l) x += (double)(int)v[l][j] * level_weight(l);
+          const int c = n0 + cw + 8 * grp + j;
+          const int eb_c = (c < a.n) ? a.eb[(int64_t)item * a.n + c] : 0;
+          x = ldexp(x, ea_r + eb_c);
+          if (pass == 0) {
+            re[8 * grp + j] = x;
+          } else if (row_ok && c < a.n) {
+            double2* dst = a.C + (int64_t)item * a.sC + (int64_t)r + (int64_t)c * a.m;
+            const double pr = re[8 * grp + j], pi = x;
+            double2 out = make_double2(a.alpha.x * pr - a.alpha.y * pi, a.alpha.x * pi + a.alpha.y * pr);
+            if (a.beta.x != 0.0 || a.beta.y != 0.0) {
+              const double2 o = *dst;
+              out.x += a.beta.x * o.x - a.beta.y * o.y;
+              out.y += a.beta.x * o.y + a.beta.y * o.x;
+            }
+            if (nonfinite) {
+              const double qnan = __longlong_as_double(0x7ff8000000000000LL);
+              out = make_double2(qnan, qnan);
+            }
+            *dst = out;
+            local_max = fmax(local_max, hypot(out.x, out.y));
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();
+  }
+
+  if (fail) {
+    // let every TMA load this CTA issued land before its shared memory is released
+    if (threadIdx.x == 0)
+      for (int st = 0; st < kOzStages; ++st)
+        if (issued[st] > 0) {
+          const long long t0 = clock64();
+          while (!mbar_test(&full[st], (issued[st] - 1) & 1) && clock64() - t0 < kSpinCycles) {
+          }
+        }
+    if (threadIdx.x == 0 && a.status) a.status[item] = 7;
+  } else {
+    if (a.maxabs) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) local_max = fmax(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+      if (lane == 0 && local_max > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(a.maxabs + item),
+                  (unsigned long long)__double_as_longlong(local_max));
+    }
+    if (nonfinite && threadIdx.x == 0 && a.status) a.status[item] = 3;
+  }
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols)
+                              : "memory");
+}
+
+// ---------------------------------------------------------------- host
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encoder() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// 3-D map over digit planes: x = K byte (inner), y = row, z = plane
+bool make_map(CUtensorMap* map, void* base, int k, int rows, int kp, int planes, int box_rows) {
+  EncodeTiledFn fn = encoder();
+  if (!fn) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)k, (cuuint64_t)rows, (cuuint64_t)planes};
+  const cuuint64_t strides[2] = {(cuuint64_t)kp, (cuuint64_t)kp * (cuuint64_t)rows};
+  const cuuint32_t box[3] = {(cuuint32_t)kOzKChunk, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+template <int S>
+cudaError_t run(const OzakiLayout& L, double2 alpha, const double2* A, int64_t sA, const double2* B, int64_t sB,
+                double2 beta, double2* C, int64_t sC, uint8_t* w, double* maxabs, int* status, cudaStream_t s) {
+  int8_t* qa = reinterpret_cast<int8_t*>(w + L.qa_off);
+  int8_t* qb = reinterpret_cast<int8_t*>(w + L.qb_off);
+  int* ea = reinterpret_cast<int*>(w + L.ea_off);
+  int* eb = reinterpret_cast<int*>(w + L.eb_off);
+  int* flag = reinterpret_cast<int*>(w + L.flag_off);
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)L.batch, s);
+  if (e != cudaSuccess) return e;
+  k_split_rows<S><<<dim3((L.m + 31) / 32, L.batch), 256, 0, s>>>(L.m, L.k, L.kp, A, sA, qa, ea, flag);
+  k_split_cols<S><<<dim3((L.n + 7) / 8, L.batch), 256, 0, s>>>(L.k, L.n, L.kp, B, sB, qb, eb, flag);
+  CUtensorMap ta, tb;
+  if (!make_map(&ta, qa, L.k, L.m, L.kp, L.batch * 3 * S, kOzTileM) ||
+      !make_map(&tb, qb, L.k, L.n, L.kp, L.batch * 2 * S, kOzTileN))
+    return cudaErrorInvalidValue;
+  OzArgs a;
+  a.m = L.m; a.n = L.n; a.k = L.k; a.nkc = (L.k + kOzKChunk - 1) / kOzKChunk;
+  a.alpha = alpha; a.beta = beta; a.C = C; a.sC = sC;
+  a.ea = ea; a.eb = eb; a.flag = flag; a.maxabs = maxabs; a.status = status;
+  const size_t smem = (size_t)kOzStages * S * (kABytes + kBBytes) + 1024;
+  static std::mutex mu;
+  static bool attr_set[64] = {false};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+      e = cudaFuncSetAttribute(k_ozaki<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr_set[dev] = true;
+    }
+  }
+  const int tiles = ((L.m + kOzTileM - 1) / kOzTileM) * ((L.n + kOzTileN - 1) / kOzTileN);
+  k_ozaki<S><<<dim3(tiles, L.batch), kOzThreads, smem, s>>>(ta, tb, a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+OzakiLayout ozaki_layout(int batch, int m, int n, int k, int slices) {
+  OzakiLayout L;
+  L.batch = batch; L.m = m; L.n = n; L.k = k; L.slices = slices;
+  L.kp = (k + 15) & ~15;
+  size_t off = 0;
+  L.qa_off = off; off = align256(off + (size_t)batch * 3 * slices * m * L.kp);
+  L.qb_off = off; off = align256(off + (size_t)batch * 2 * slices * n * L.kp);
+  L.ea_off = off; off = align256(off + sizeof(int) * (size_t)batch * m);
+  L.eb_off = off; off = align256(off + sizeof(int) * (size_t)batch * n);
+  L.flag_off = off; off = align256(off + sizeof(int) * (size_t)batch);
+  L.total = off;
+  return L;
+}
+
+cudaError_t launch_ozaki_zgemm(int batch, int m, int n, int k, double2 alpha, const double2* A, int64_t sA,
+                               const double2* B, int64_t sB, double2 beta, double2* C, int64_t sC, int slices,
+                               void* work, double* maxabs, int* status, cudaStream_t s) {
+  if (batch <= 0 || m <= 0 || n <= 0) return cudaSuccess;
+  if (k <= 0 || k > 1024 || batch > 65535 || slices < kOzMinSlices || slices > kOzMaxSlices || !work ||
+      (reinterpret_cast<uintptr_t>(work) & 255))
+    return cudaErrorInvalidValue;
+  const OzakiLayout L = ozaki_layout(batch, m, n, k, slices);
+  uint8_t* w = static_cast<uint8_t*>(work);
+  switch (slices) {
+    case 4: return run<4>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
+    case 5: return run<5>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
+    case 6: return run<6>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
+    case 7: return run<7>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
+    default: return run<8>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
+  }
+}
+
+}  // namespace negf

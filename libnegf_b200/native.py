@@ -35,6 +35,7 @@ EXPORTED = [
     "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
     "negf_b200_set_workspace_limit", "negf_b200_density", "negf_b200_density_neq", "negf_b200_meir_wingreen_dev",
     "negf_b200_sgf_cache_save", "negf_b200_sgf_cache_load", "negf_b200_upload_csr",
+    "negf_b200_zgemm_i8_work_bytes", "negf_b200_zgemm_batched_i8",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -100,6 +101,10 @@ def load():
     L.negf_b200_meir_wingreen_dev.argtypes = [vp, i32, vp, vp, f64, vp, vp, vp, vp, vp, vp, vp, vp, vp, i32, i32, vp]
     L.negf_b200_zgemm_batched.argtypes = [i32, i32, i32, i32, dp, vp, ctypes.c_int64, vp, ctypes.c_int64, dp, vp,
                                           ctypes.c_int64, i32, vp]
+    L.negf_b200_zgemm_i8_work_bytes.restype = ctypes.c_size_t
+    L.negf_b200_zgemm_i8_work_bytes.argtypes = [i32, i32, i32, i32, i32]
+    L.negf_b200_zgemm_batched_i8.argtypes = [i32, i32, i32, i32, dp, vp, ctypes.c_int64, vp, ctypes.c_int64, dp,
+                                             vp, ctypes.c_int64, i32, vp, vp, vp]
     L.negf_b200_zinv_work_bytes.restype = ctypes.c_size_t
     L.negf_b200_zinv_work_bytes.argtypes = [i32, i32]
     L.negf_b200_zinv_batched.argtypes = [i32, i32, vp, vp, vp, vp, vp]
