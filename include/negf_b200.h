@@ -105,7 +105,16 @@ typedef struct negf_b200_options {
   double eps_drop;
   double scba_tol;
   int32_t scba_niter;
-  /* 0 = plain complex FP64 (the parity form). */
+  /* 0 = plain complex FP64 (the parity form).  4..8 = the mixed form for
+   * 2-contact transmission solves (negf_b200_transmission, _dev): every
+   * block product on the integer tensor cores with that many int8 digits
+   * per operand element (negf_b200_zgemm_batched_i8; 7 digits carry about
+   * the accuracy of an FP64 product, 8 a margin below it), the block
+   * inverses, the decimation's convergence test and the Caroli trace in
+   * FP64, all points of a call in lock step.  1 = the mixed form with 8
+   * digits.  The mixed form needs two
+   * contacts on blocks 1 and nbl, one PL size for every layer and both leads,
+   * no tun_proj; other solves return NEGF_B200_ERR_BAD_ARG under it. */
   int32_t precision;
   /* Resident CTAs per SM for the persistent point engine (0 = auto). */
   int32_t ctas_per_sm;

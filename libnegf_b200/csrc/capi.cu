@@ -17,6 +17,7 @@
 
 #include "../../include/negf_b200.h"
 #include "engine.cuh"
+#include "mixed.cuh"
 #include "ozaki.cuh"
 
 using negf::DevDesc;
@@ -401,7 +402,8 @@ int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* o) {
   if (o->sgf_tol <= 0.0 || o->sgf_max_iter < 1 || o->scba_niter < 0 || o->ctas_per_sm < 0 ||
       o->ctas_per_sm > 2)
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "invalid options");
-  if (o->precision != 0) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "only precision 0 (complex FP64) is built");
+  if (o->precision != 0 && o->precision != 1 && (o->precision < negf::kOzMinSlices || o->precision > negf::kOzMaxSlices))
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "precision must be 0 (FP64), 1 or 4..8 (int8 digits of the mixed form)");
   if (!(o->scba_mix > 0.0 && o->scba_mix <= 1.0) || (o->scba_rule != 0 && o->scba_rule != 1))
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "scba_mix must be in (0, 1] and scba_rule 0 or 1");
   ctx->opt = *o;
@@ -919,6 +921,71 @@ static int check_pairs(negf_b200_ctx* ctx, int npts, const int32_t* ids, int npa
   return NEGF_B200_OK;
 }
 
+// The mixed-precision form (options.precision != 0) for 2-contact transmission
+// solves: checks that every point's device fits it, sizes the batch to the
+// workspace and runs negf::mixed_run on device arrays of ids and energies.
+static int mixed_slices(const negf_b200_ctx* ctx) { return ctx->opt.precision == 1 ? 8 : ctx->opt.precision; }
+
+static int run_mixed(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_ids, const int32_t* d_ids, const double* d_E,
+                     double eta, double* d_T, int32_t* d_ncyc, int32_t* d_status, cudaStream_t s) {
+  // shape: from the host ids when given, else from the devices the context holds
+  std::vector<int> used;
+  if (h_ids) {
+    std::vector<char> seen(ctx->devs.size(), 0);
+    for (int p = 0; p < npts; ++p) {
+      if (h_ids[p] < 0 || h_ids[p] >= (int)ctx->devs.size() || !ctx->devs[h_ids[p]].live)
+        return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+      if (!seen[h_ids[p]]) { seen[h_ids[p]] = 1; used.push_back(h_ids[p]); }
+    }
+  } else {
+    for (int i = 0; i < (int)ctx->devs.size(); ++i)
+      if (ctx->devs[i].live) used.push_back(i);
+  }
+  if (used.empty()) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "no device");
+  const DeviceRec& r0 = ctx->devs[used[0]];
+  const int n = r0.nmax, nbl = r0.nbl;
+  int left = -1, right = -1;
+  for (int id : used) {
+    const DeviceRec& r = ctx->devs[id];
+    if (r.ncont != 2 || r.nbl < 2 || r.nbl != nbl || r.nmax != n || r.norb != nbl * n)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG,
+                  "the mixed form needs 2 contacts and one PL size n for all layers of every point's device");
+    int l = -1, rr = -1;
+    for (int c = 0; c < 2; ++c) {
+      if (r.desc.L[c] != n) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs lead PL size = n");
+      if (r.cblk[c] == 1) l = c;
+      if (r.cblk[c] == nbl) rr = c;
+    }
+    if (l < 0 || rr < 0 || l == rr)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs the contacts on blocks 1 and nbl");
+    if (left >= 0 && (l != left || rr != right))
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs the same contact order on every device");
+    if (r.desc.tun_mask) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no tun_proj");
+    left = l; right = rr;
+  }
+  int st = sync_descs(ctx);
+  if (st) return st;
+  const int slices = mixed_slices(ctx);
+  int batch = std::min<int>(npts, 2 * std::max(ctx->sms, 1) + 216);   // 512 on a B200
+  if (ctx->ws_limit) batch = std::min(batch, negf::mixed_batch_for(ctx->ws_limit, n, slices));
+  if (batch < 1) return fail(ctx, NEGF_B200_ERR_ADMISSION, "the workspace limit is below one point of the mixed form");
+  for (;;) {
+    st = grow(ctx, &ctx->ws, &ctx->ws_bytes, negf::mixed_ws_bytes(batch, n, slices));
+    if (st == NEGF_B200_OK) break;
+    if (batch == 1) return st;
+    batch = (batch + 1) / 2;
+  }
+  negf::MixedArgs a;
+  a.npts = npts; a.d_ids = d_ids; a.d_E = d_E; a.eta = eta; a.d_descs = ctx->d_descs;
+  a.n = n; a.nbl = nbl; a.left = left; a.right = right;
+  a.sgf_tol = ctx->opt.sgf_tol; a.sgf_max_iter = ctx->opt.sgf_max_iter; a.slices = slices;
+  a.d_T = d_T; a.d_ncyc = d_ncyc; a.d_status = d_status;
+  std::string msg;
+  st = negf::mixed_run(a, ctx->ws, batch, s, &msg);
+  if (st) return fail(ctx, st, "mixed form: " + msg);
+  return NEGF_B200_OK;
+}
+
 static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t* ids, const double* E,
                       double eta, double dos_delta, int32_t ni, int32_t nf, double* T, double* dos, int32_t* ncyc,
                       int32_t* status, const double* frm, const double* coupling, double* curr, double* lcurr,
@@ -1003,6 +1070,20 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
     plan_sgf(ctx, npts, ids, E, eta, sh.ncont_max, sgf_in, sgf_out);
     CK(cudaMemcpyAsync(d_sgf_in, sgf_in.data(), sgf_in.size() * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(d_sgf_out, sgf_out.data(), sgf_out.size() * 8, cudaMemcpyHostToDevice, s));
+  }
+  if (ctx->opt.precision != 0) {
+    if (mode != negf::MODE_T || npairs > 1 || ctx->sgf.mode)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG,
+                  "the mixed form (precision != 0) covers single-pair transmission solves without the SGF cache");
+    st = run_mixed(ctx, npts, ids, d_ids, d_E, eta, d_T, d_ncyc, d_st, s);
+    if (st) return st;
+    std::vector<int32_t> hst(npts);
+    if (T) CK(cudaMemcpyAsync(T, d_T, (size_t)npts * 8, cudaMemcpyDeviceToHost, s));
+    if (ncyc) CK(cudaMemcpyAsync(ncyc, d_ncyc, npts * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (status) std::memcpy(status, hst.data(), npts * 4);
+    return first_status(hst.data(), npts);
   }
   negf::EngineArgs a = base_args(ctx, mode, npts);
   a.dev_id = d_ids; a.energy = d_E; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
@@ -1297,6 +1378,11 @@ int negf_b200_transmission_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t* 
   if (npts == 0) return NEGF_B200_OK;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  if (ctx->opt.precision != 0) {
+    if (ctx->sgf.mode) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no SGF cache");
+    return run_mixed(ctx, npts, nullptr, d_device_id, d_energy, eta, d_T, d_ncyc, d_status,
+                     stream ? (cudaStream_t)stream : ctx->stream);
+  }
   LaunchShape sh;
   int st = shape_of(ctx, npts, nullptr, sh);
   if (st) return st;

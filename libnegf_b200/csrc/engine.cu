@@ -226,6 +226,32 @@ cudaError_t launch_zinv_batched(int batch, int n, const double2* A, double2* Ain
   return cudaGetLastError();
 }
 
+// Inverses of the problems map[b], b < batch (map null: b), matrices sA / sX
+// complex elements apart; work holds batch slots of zinv_batched_work_elems(n).
+// info[map[b]] gets the zgetrf-style singular column (0 = none).
+__global__ void __launch_bounds__(kThreads, 2)
+    k_zinv_mapped(int n, const double2* A, int64_t sA, double2* X, int64_t sX, const int* map, int* info,
+                  double2* work, int64_t wstride) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SmemMap sm = map_smem(smem_raw, n);
+  sm.tr.acc = nullptr;
+  const int b = blockIdx.x;
+  const int p = map ? map[b] : b;
+  int inf = zinv(n, A + (int64_t)p * sA, X + (int64_t)p * sX, work + (int64_t)b * wstride, sm);
+  if (threadIdx.x == 0 && info) info[p] = inf;
+}
+
+cudaError_t launch_zinv_mapped(int batch, int n, const double2* A, int64_t sA, double2* X, int64_t sX,
+                               const int* map, int* info, double2* work, cudaStream_t s) {
+  if (batch <= 0) return cudaSuccess;
+  const size_t smem = engine_smem_bytes(n);
+  cudaError_t e = cudaFuncSetAttribute(k_zinv_mapped, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_zinv_mapped<<<batch, kThreads, smem, s>>>(n, A, sA, X, sX, map, info, work,
+                                              (int64_t)zinv_batched_work_elems(n));
+  return cudaGetLastError();
+}
+
 __host__ __device__ inline size_t dec_work_elems(int n) { return (size_t)(S_INV + 3) * n * n; }
 size_t decimation_batched_work_elems(int n) { return dec_work_elems(n); }
 

@@ -1,0 +1,407 @@
+// Mixed-precision transmission solve (north-star precision form): the
+// 2-contact fast path of calculate_transmissions (src/iterative.F90:1697-1713)
+// for a batch of (E, k) points moved through the same steps together, so
+// that every block product is one batched product on the integer tensor
+// cores (launch_ozaki_zgemm: int8 digits, exact int32 accumulation, FP64
+// recombination) and every block inverse one batched FP64 Gauss-Jordan
+// inversion (launch_zinv_mapped).  FP64 throughout outside the products: the
+// decimation's convergence test on max|C1|, the inverses, and the Caroli
+// trace (whose two products are FP64 tensor-core products).
+//
+// Steps per batch, following the reference routine by routine:
+//   surface_green + decimation      src/contselfenergy.F90:184-210, 271-340
+//     (lock step over the points still iterating; a point leaves the active
+//     set on its second consecutive max|C1| <= SGFACC, as the CPU rule)
+//   compute_contacts / SelfEnergy   src/contselfenergy.F90:445-491, 552-566
+//   build_ESH (ESH at the real E)   src/iterative.F90:1956-1982
+//   calculate_gsmr_blocks(nbl, 2)   src/iterative_cpu.F90:51-124
+//   Gr(1,1)                         src/iterative_cpu.F90:134-170
+//   calculate_single_transmission_2_contacts   src/iterative_cpu.F90:399-470
+#include <algorithm>
+#include <vector>
+
+#include "../../include/negf_b200.h"
+#include "mixed.cuh"
+#include "ozaki.cuh"
+
+namespace negf {
+namespace {
+
+constexpr int kBlocks = 13;   // n x n complex work blocks per point
+
+__device__ __forceinline__ double2 cmulm(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 conjm(double2 a) { return make_double2(a.x, -a.y); }
+
+// Ao = Ec S00 - H00, Aos = Ao, Bo = Ec S01 - H01, Co = (conj(Ec) S01 - H01)^dag
+__global__ void k_lead_init(int n, int c, const int* ids, const double* E, double eta, const DevDesc* descs,
+                            double2* Ao, double2* Aos, double2* Bo, double2* Co, int64_t Q) {
+  const int p = blockIdx.y;
+  const DevDesc& d = descs[ids[p]];
+  const double2 ec = make_double2(E[p], eta);
+  const int64_t ol = d.olead[c], nn = (int64_t)n * n;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % n), j = (int)(q / n);
+    const int64_t qt = j + (int64_t)i * n;   // element (j, i)
+    const double2 s00 = d.has_s00 ? d.s00[ol + q] : make_double2(i == j ? 1.0 : 0.0, 0.0);
+    const double2 h00 = d.h00[ol + q];
+    const double2 s01 = d.has_s01 ? d.s01[ol + q] : make_double2(0.0, 0.0);
+    const double2 h01 = d.h01[ol + q];
+    const double2 s01t = d.has_s01 ? d.s01[ol + qt] : make_double2(0.0, 0.0);
+    const double2 h01t = d.h01[ol + qt];
+    double2 a = cmulm(ec, s00);
+    a.x -= h00.x; a.y -= h00.y;
+    double2 b = cmulm(ec, s01);
+    b.x -= h01.x; b.y -= h01.y;
+    double2 ct = cmulm(conjm(ec), s01t);
+    ct.x -= h01t.x; ct.y -= h01t.y;
+    Ao[p * Q + q] = a;
+    Aos[p * Q + q] = a;
+    Bo[p * Q + q] = b;
+    Co[p * Q + q] = conjm(ct);
+  }
+}
+
+// Ao -= Self, Aos -= Self for the points of the list
+__global__ void k_sub_self(int64_t nn, const int* list, const double2* Self, double2* Ao, double2* Aos, int64_t Q) {
+  const int p = list[blockIdx.y];
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
+    const double2 s = Self[p * Q + q];
+    double2 a = Ao[p * Q + q], b = Aos[p * Q + q];
+    a.x -= s.x; a.y -= s.y;
+    b.x -= s.x; b.y -= s.y;
+    Ao[p * Q + q] = a;
+    Aos[p * Q + q] = b;
+  }
+}
+
+// The CPU convergence rule (src/contselfenergy.F90:300-310): a point is done
+// on its second consecutive max|C1| <= tol.  Builds the list of the points
+// that go on (and zeroes their max for the next iteration).  One CTA.
+__global__ void k_dec_check(int na, const int* list, double* mx, int* ok, int* ncyc_c, double tol, int it,
+                            int* next, int* next_count) {
+  __shared__ int cnt;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < na; b += blockDim.x) {
+    const int p = list[b];
+    const double m = mx[p];
+    bool go = true;
+    if (m <= tol) {
+      if (ok[p]) {
+        go = false;
+        ncyc_c[p] = it;
+      }
+      ok[p] = 1;
+    } else {
+      ok[p] = 0;
+    }
+    if (go) {
+      next[atomicAdd(&cnt, 1)] = p;
+      mx[p] = 0.0;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) *next_count = cnt;
+}
+
+__global__ void k_info_to_status(int nb, const int* list, const int* info, int* status, int code) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
+    const int p = list ? list[b] : b;
+    if (info[p] != 0 && status[p] == 0) status[p] = code;
+  }
+}
+
+// Tlc = Ec SMC - HMC (n x L), Tcl = (conj(Ec) SMC - HMC)^dag (L x n); here L = n
+__global__ void k_tlc(int n, int c, const int* ids, const double* E, double eta, const DevDesc* descs,
+                      double2* Tlc, double2* Tcl, int64_t Q) {
+  const int p = blockIdx.y;
+  const DevDesc& d = descs[ids[p]];
+  const double2 ec = make_double2(E[p], eta);
+  const int64_t om = d.omc[c], nn = (int64_t)n * n;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % n), j = (int)(q / n);
+    const int64_t qt = j + (int64_t)i * n;
+    const double2 smc = d.has_smc ? d.smc[om + q] : make_double2(0.0, 0.0);
+    const double2 hmc = d.hmc[om + q];
+    double2 t = cmulm(ec, smc);
+    t.x -= hmc.x; t.y -= hmc.y;
+    const double2 smct = d.has_smc ? d.smc[om + qt] : make_double2(0.0, 0.0);
+    const double2 hmct = d.hmc[om + qt];
+    double2 u = cmulm(conjm(ec), smct);
+    u.x -= hmct.x; u.y -= hmct.y;
+    Tlc[p * Q + q] = t;
+    Tcl[p * Q + q] = conjm(u);
+  }
+}
+
+// ESH blocks at the real energy: which 0 = (i,i) minus sig (if given),
+// 1 = (i,i+1), 2 = (i+1,i); i 0-based
+__global__ void k_esh(int n, int which, int i, const int* ids, const double* E, const DevDesc* descs,
+                      const double2* sig, double2* out, int64_t Q) {
+  const int p = blockIdx.y;
+  const DevDesc& d = descs[ids[p]];
+  const double e = E[p];
+  const int64_t nn = (int64_t)n * n;
+  const int64_t off = (which == 0) ? d.od[i] : d.oo[i];
+  const double2* H = (which == 0) ? d.hd : (which == 1 ? d.hu : d.hl);
+  const double2* S = (which == 0) ? d.sd : (which == 1 ? d.su : d.sl);
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
+    const double2 h = H[off + q];
+    double2 v;
+    if (d.has_s) {
+      const double2 sv = S[off + q];
+      v = make_double2(e * sv.x - h.x, e * sv.y - h.y);
+    } else {
+      v = make_double2(-h.x, -h.y);
+      if (which == 0 && (q % n) == (q / n)) v.x += e;
+    }
+    if (sig) {
+      const double2 sg = sig[p * Q + q];
+      v.x -= sg.x; v.y -= sg.y;
+    }
+    out[p * Q + q] = v;
+  }
+}
+
+// Gamma = i (Sigma - Sigma^dag)   (zspectral_dns, src/sparsekit_drv.F90:2870-2890)
+__global__ void k_gamma(int n, const double2* Sig, double2* Gam, int64_t Q) {
+  const int p = blockIdx.y;
+  const int64_t nn = (int64_t)n * n;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(q % n), j = (int)(q / n);
+    const double2 a = Sig[p * Q + q], b = Sig[p * Q + j + (int64_t)i * n];
+    // i * (a - conj(b))
+    Gam[p * Q + q] = make_double2(-(a.y + b.y), a.x - b.x);
+  }
+}
+
+// T = |Re Tr[Gam i(G - G^dag)] - Re Tr[Gam G Gam G^dag]|
+//   Tr[Gam A]            = sum_ij Gam_ij i (G_ji - conj(G_ij))
+//   Tr[Gam G Gam G^dag]  = sum_ij M_ij conj(N_ij),  M = Gam G, N = G Gam
+// (calculate_single_transmission_2_contacts, src/iterative_cpu.F90:424-464).
+// One CTA per point; FP64.
+__global__ void k_trace(int n, const double2* Gam, const double2* G, const double2* M, const double2* N, double* T,
+                        int64_t Q) {
+  const int p = blockIdx.x;
+  const int64_t nn = (int64_t)n * n;
+  double t1 = 0.0, t2 = 0.0;
+  for (int64_t q = threadIdx.x; q < nn; q += blockDim.x) {
+    const int i = (int)(q % n), j = (int)(q / n);
+    const double2 g = Gam[p * Q + q];
+    const double2 gji = G[p * Q + j + (int64_t)i * n], gij = G[p * Q + q];
+    // A_ji = i (G_ji - conj(G_ij))
+    const double2 aji = make_double2(-(gji.y + gij.y), gji.x - gij.x);
+    t1 += g.x * aji.x - g.y * aji.y;
+    const double2 m = M[p * Q + q], nq = N[p * Q + q];
+    t2 += m.x * nq.x + m.y * nq.y;   // Re(m conj(n))
+  }
+  __shared__ double r1[32], r2[32];
+  for (int o = 16; o > 0; o >>= 1) {
+    t1 += __shfl_xor_sync(0xffffffffu, t1, o);
+    t2 += __shfl_xor_sync(0xffffffffu, t2, o);
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) { r1[w] = t1; r2[w] = t2; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) { s1 += r1[k]; s2 += r2[k]; }
+    T[p] = fabs(s1 - s2);
+  }
+}
+
+__global__ void k_iota(int n, int* v) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) v[b] = b;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+struct Carver {
+  char* p;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t n) {
+    T* r = p ? reinterpret_cast<T*>(p + off) : nullptr;
+    off = align256(off + n * sizeof(T));
+    return r;
+  }
+};
+
+struct Ws {
+  double2* blk[kBlocks];
+  double* mx;
+  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst;
+  double* tb;
+  double2* zwork;
+  void* oz;
+};
+
+Ws carve(void* base, int P, int n, int slices, size_t* total) {
+  Carver c{static_cast<char*>(base)};
+  Ws w;
+  const size_t Q = (size_t)n * n;
+  for (int b = 0; b < kBlocks; ++b) w.blk[b] = c.take<double2>((size_t)P * Q);
+  w.mx = c.take<double>(P);
+  w.ok = c.take<int>(P);
+  w.ncl = c.take<int>(P);
+  w.ncr = c.take<int>(P);
+  w.list0 = c.take<int>(P);
+  w.list1 = c.take<int>(P);
+  w.count = c.take<int>(4);
+  w.info = c.take<int>(P);
+  w.pst = c.take<int>(P);
+  w.tb = c.take<double>(P);
+  w.zwork = c.take<double2>((size_t)P * zinv_batched_work_elems(n) + 1);
+  w.oz = c.take<uint8_t>(ozaki_layout(P, n, n, n, slices).total);
+  *total = c.off + 256;
+  return w;
+}
+
+__global__ void k_finish(int P, const int* ncl, const int* ncr, const int* pst, const double* Tb, double* T,
+                         int* ncyc, int* status) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
+    T[p] = Tb[p];
+    if (ncyc) ncyc[p] = ncl[p] + ncr[p];
+    if (status) status[p] = pst[p];
+  }
+}
+
+__global__ void k_not_converged(int na, const int* list, int* ncyc_c, int* pst, int max_iter) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < na; b += gridDim.x * blockDim.x) {
+    const int p = list[b];
+    ncyc_c[p] = max_iter + 1;
+    if (pst[p] == 0) pst[p] = NEGF_B200_ERR_NOT_CONVERGED;
+  }
+}
+
+}  // namespace
+
+size_t mixed_ws_bytes(int batch, int n, int slices) {
+  size_t t = 0;
+  carve(nullptr, batch, n, slices, &t);
+  return t;
+}
+
+int mixed_batch_for(size_t bytes, int n, int slices) {
+  int lo = 0, hi = 1 << 14;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (mixed_ws_bytes(mid, n, slices) <= bytes) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::string* err) {
+  const int n = a.n;
+  const int64_t Q = (int64_t)n * n;
+  const double2 one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
+  size_t tot = 0;
+  Ws w = carve(ws, batch, n, a.slices, &tot);
+  double2** B = w.blk;
+  const dim3 eb(256);
+  const int gx = (int)std::min<int64_t>(64, (Q + 255) / 256);
+  auto ck = [&](cudaError_t e, const char* what) -> int {
+    if (e == cudaSuccess) return 0;
+    if (err) *err = std::string(what) + ": " + cudaGetErrorString(e);
+    return NEGF_B200_ERR_CUDA;
+  };
+#define MCK(x, what)             \
+  do {                           \
+    int r_ = ck((x), what);      \
+    if (r_) return r_;           \
+  } while (0)
+  auto prod = [&](int nb, const int* map, double2 alpha, const double2* A, const double2* Bm, double2 beta,
+                  double2* C, double* maxabs) -> cudaError_t {
+    return launch_ozaki_zgemm(nb, n, n, n, alpha, A, Q, Bm, Q, beta, C, Q, a.slices, w.oz, maxabs, w.pst, s, map);
+  };
+
+  for (int p0 = 0; p0 < a.npts; p0 += batch) {
+    const int P = std::min(batch, a.npts - p0);
+    const int* ids = a.d_ids + p0;
+    const double* E = a.d_E + p0;
+    MCK(cudaMemsetAsync(w.pst, 0, sizeof(int) * P, s), "memset status");
+    // ---- surface Green's function of each contact (B9 left, B10 right)
+    for (int side = 0; side < 2; ++side) {
+      const int c = side == 0 ? a.left : a.right;
+      int* ncyc_c = side == 0 ? w.ncl : w.ncr;
+      double2 *Ao = B[0], *Aos = B[1], *Bo = B[2], *Co = B[3], *Go = B[4], *X = B[5], *C1 = B[6], *Y = B[7],
+              *B1 = B[8];
+      k_lead_init<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, Ao, Aos, Bo, Co, Q);
+      MCK(cudaGetLastError(), "lead init");
+      MCK(cudaMemsetAsync(w.ok, 0, sizeof(int) * P, s), "memset ok");
+      MCK(cudaMemsetAsync(w.mx, 0, sizeof(double) * P, s), "memset mx");
+      MCK(cudaMemsetAsync(ncyc_c, 0, sizeof(int) * P, s), "memset ncyc");
+      k_iota<<<(P + 255) / 256, 256, 0, s>>>(P, w.list0);
+      int na = P;
+      int* cur = w.list0;
+      int* nxt = w.list1;
+      for (int it = 1; it <= a.sgf_max_iter && na > 0; ++it) {
+        MCK(launch_zinv_mapped(na, n, Ao, Q, Go, Q, cur, w.info, w.zwork, s), "zinv");
+        k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+        MCK(prod(na, cur, one, Go, Co, zero, X, nullptr), "GoXCo");
+        MCK(prod(na, cur, one, Co, X, zero, C1, w.mx), "C1");
+        k_dec_check<<<1, 1024, 0, s>>>(na, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt, w.count);
+        MCK(cudaGetLastError(), "check");
+        int h_count = 0;
+        MCK(cudaMemcpyAsync(&h_count, w.count, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
+        MCK(cudaStreamSynchronize(s), "sync");
+        std::swap(cur, nxt);
+        na = h_count;
+        if (na == 0) break;
+        MCK(prod(na, cur, one, Bo, X, zero, B1, nullptr), "Self");
+        k_sub_self<<<dim3(gx, na), eb, 0, s>>>(Q, cur, B1, Ao, Aos, Q);
+        MCK(prod(na, cur, one, Go, Bo, zero, Y, nullptr), "GoXBo");
+        MCK(prod(na, cur, one, Bo, Y, zero, B1, nullptr), "B1");
+        MCK(prod(na, cur, mone, Co, Y, one, Ao, nullptr), "Ao update");
+        // Bo = B1, Co = C1 for every point still iterating (the others are done with them)
+        std::swap(B[2], B[8]);
+        std::swap(B[3], B[6]);
+        Bo = B[2]; Co = B[3]; B1 = B[8]; C1 = B[6];
+      }
+      if (na > 0) k_not_converged<<<(na + 255) / 256, 256, 0, s>>>(na, cur, ncyc_c, w.pst, a.sgf_max_iter);
+      // gs = Aos^-1 for every point
+      MCK(launch_zinv_mapped(P, n, Aos, Q, B[9 + side], Q, nullptr, w.info, w.zwork, s), "gs");
+      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+    }
+    // ---- self-energies Sigma_c = Tlc gs Tcl (B11 left, B12 right)
+    for (int side = 0; side < 2; ++side) {
+      const int c = side == 0 ? a.left : a.right;
+      k_tlc<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, B[0], B[1], Q);
+      MCK(cudaGetLastError(), "tlc");
+      MCK(prod(P, nullptr, one, B[0], B[9 + side], zero, B[2], nullptr), "Tlc gs");
+      MCK(prod(P, nullptr, one, B[2], B[1], zero, B[11 + side], nullptr), "Sigma");
+    }
+    // ---- gsmr sweep from block nbl down to 2, then Gr(1,1)
+    double2 *g = B[4], *X = B[5], *W = B[6], *U = B[7], *Lb = B[8];
+    k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, a.nbl - 1, ids, E, a.d_descs, B[12], W, Q);
+    MCK(launch_zinv_mapped(P, n, W, Q, g, Q, nullptr, w.info, w.zwork, s), "gsmr N");
+    k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+    for (int i = a.nbl - 2; i >= 0; --i) {
+      // W = ESH(i,i) - ESH(i,i+1) gsmr(i+1) ESH(i+1,i)  (block i 0-based; Sigma_left on block 0)
+      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 1, i, ids, E, a.d_descs, nullptr, U, Q);
+      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 2, i, ids, E, a.d_descs, nullptr, Lb, Q);
+      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, i, ids, E, a.d_descs, i == 0 ? B[11] : nullptr, W, Q);
+      MCK(cudaGetLastError(), "esh");
+      MCK(prod(P, nullptr, one, U, g, zero, X, nullptr), "U g");
+      MCK(prod(P, nullptr, mone, X, Lb, one, W, nullptr), "W");
+      MCK(launch_zinv_mapped(P, n, W, Q, g, Q, nullptr, w.info, w.zwork, s), "gsmr");
+      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+    }
+    // g = Gr(1,1).  Trace with Gamma of the contact on block 1 (FP64 products)
+    k_gamma<<<dim3(gx, P), eb, 0, s>>>(n, B[11], B[0], Q);
+    MCK(launch_zgemm_batched(P, n, n, n, one, B[0], Q, g, Q, zero, B[1], Q, 0, s), "Gam G");
+    MCK(launch_zgemm_batched(P, n, n, n, one, g, Q, B[0], Q, zero, B[2], Q, 0, s), "G Gam");
+    k_trace<<<P, 512, 0, s>>>(n, B[0], g, B[1], B[2], w.tb, Q);
+    MCK(cudaGetLastError(), "trace");
+    k_finish<<<(P + 255) / 256, 256, 0, s>>>(P, w.ncl, w.ncr, w.pst, w.tb, a.d_T + p0,
+                                             a.d_ncyc ? a.d_ncyc + p0 : nullptr,
+                                             a.d_status ? a.d_status + p0 : nullptr);
+    MCK(cudaGetLastError(), "finish");
+  }
+#undef MCK
+  return NEGF_B200_OK;
+}
+
+}  // namespace negf

@@ -6,16 +6,24 @@
 //   k_split_rows  A -> int8 digit planes of Ar, Ai, -Ai (K contiguous) and a
 //                 power-of-two exponent per row;
 //   k_split_cols  B -> digit planes of Br, Bi and an exponent per column;
-//   k_ozaki       one CTA per 128 x 64 tile of C: two passes (real, imaginary
-//                 part) over the concatenated K, one accumulator of 64
-//                 columns in TMEM per digit level l = t + u, then the FP64
-//                 epilogue C = alpha * 2^(eA+eB) sum_l 2^(-12-7l) acc_l + beta * C.
-// Roles inside k_ozaki: warp 0 lane 0 issues the TMA loads of a two-stage
-// ring, warp 1 lane 0 issues the MMAs and commits each stage back to the
-// producer; all eight warps read the accumulators (warp w reads TMEM lanes
-// 32 (w % 4) .. +31, columns 32 (w / 4) .. +31).  Every wait on an mbarrier is
-// bounded (about one second of SM clock); a wait that runs out marks the
-// item's status and the CTA frees its tensor memory and returns.
+//   k_ozaki       persistent CTAs over 128 x 128 tiles of C.  Per tile four
+//                 mainloops over the concatenated K: (real, imaginary part) x
+//                 (digit levels 0-3, levels 4-7), each with one accumulator of
+//                 128 columns per level in tensor memory (4 x 128 = all 512
+//                 columns), then an FP64 epilogue: the four levels of a group
+//                 combine exactly (Horner, 2^7 apart, below 2^48); the first
+//                 group's sum stays in registers until the second group's is
+//                 added, scaled by 2^(eA_r + eB_c); the real part goes
+//                 through an FP64 buffer, C = alpha (re + i im) + beta C at
+//                 the end of the imaginary part.
+// Roles: warp 8 lane 0 issues the TMA loads of a three-stage ring (and runs
+// ahead into the next mainloop while the epilogue drains), warp 9 lane 0
+// issues the MMAs and commits each stage back to the producer, warps 0-7 read
+// the accumulators (warp w: TMEM lanes 32 (w % 4) .. +31, 64 columns each)
+// and hand the tensor memory back to the MMA warp as soon as it is in
+// registers.  Every wait on
+// an mbarrier is bounded (about one second of SM clock); a wait that runs
+// out marks the items' status and the CTA frees its tensor memory and returns.
 //
 // Reference: the complex products this replaces are the zgemm calls of
 // prealloc_mult (src/sparsekit_drv.F90:1896-2081) and cu_ZmultMat
@@ -32,16 +40,19 @@
 namespace negf {
 namespace {
 
-constexpr int kOzThreads = 256;
 constexpr long long kSpinCycles = 2000000000LL;   // bound of one mbarrier wait (~1 s)
-constexpr int kABytes = kOzTileM * kOzKChunk;      // one digit plane of an A tile
-constexpr int kBBytes = kOzTileN * kOzKChunk;      // one digit plane of a B tile
+constexpr int kPlaneBytes = kOzTileM * kOzKChunk;  // one digit plane of a 128-row tile (A and B alike)
+static_assert(kOzTileM == kOzTileN, "A and B tiles share the plane size");
+constexpr int kOzGroup = 4;                        // level accumulators held in TMEM at a time
 
 __device__ __forceinline__ uint32_t s32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 // ---------------------------------------------------------------- mbarrier
 __device__ __forceinline__ void mbar_init(uint64_t* b, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(s32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(s32(b)) : "memory");
 }
 __device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(s32(b)), "r"(bytes) : "memory");
@@ -83,14 +94,14 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-// Shared-memory operand descriptor: K-major, 64-byte swizzle, rows of 64 bytes,
-// 8-row groups 512 bytes apart (SBO), version 1 (sm_100).
+// Shared-memory operand descriptor: K-major, 32-byte swizzle, rows of 32 bytes
+// (one K step), 8-row groups 256 bytes apart (SBO), version 1 (sm_100).
 __device__ __forceinline__ uint64_t sdesc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
 }
 
-// D[tmem] (+)= A[smem] * B[smem]^T, int8 x int8 -> int32, M = 128, N = 64, K = 32
+// D[tmem] (+)= A[smem] * B[smem]^T, int8 x int8 -> int32, M = 128, N = 128, K = 32
 __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -111,7 +122,7 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 
 constexpr uint32_t kTmemCols = 512;
 
-// instruction descriptor: D s32, A/B signed int8, both K-major, N = 64, M = 128
+// instruction descriptor: D s32, A/B signed int8, both K-major, N = 128, M = 128
 constexpr uint32_t kIdescI8 = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kOzTileN >> 3) << 17) |
                               ((uint32_t)(kOzTileM >> 4) << 24);
 
@@ -145,7 +156,7 @@ __host__ __device__ constexpr int oz_levels(int S) { return S + 1 < 8 ? S + 1 : 
 // of Ar, Ai, -Ai with K contiguous (row pitch kp bytes).  Block: 32 rows.
 template <int S>
 __global__ void __launch_bounds__(256) k_split_rows(int m, int k, int kp, const double2* A, int64_t sA, int8_t* qa,
-                                                   int* ea, int* flag) {
+                                                   int* ea, int* flag, const int* item_map) {
   __shared__ double smax[8][32];
   __shared__ int sexp[32];
   __shared__ int sbad;
@@ -153,7 +164,7 @@ __global__ void __launch_bounds__(256) k_split_rows(int m, int k, int kp, const 
   const int item = blockIdx.y;
   const int m0 = blockIdx.x * 32;
   const int r = threadIdx.x & 31, g = threadIdx.x >> 5;
-  const double2* Ab = A + (int64_t)item * sA;
+  const double2* Ab = A + (int64_t)(item_map ? item_map[item] : item) * sA;
   if (threadIdx.x == 0) sbad = 0;
   __syncthreads();
   double mx = 0.0;
@@ -214,12 +225,12 @@ __global__ void __launch_bounds__(256) k_split_rows(int m, int k, int kp, const 
 // planes of Br, Bi with K contiguous.  One warp per column.
 template <int S>
 __global__ void __launch_bounds__(256) k_split_cols(int k, int n, int kp, const double2* B, int64_t sB, int8_t* qb,
-                                                   int* eb, int* flag) {
+                                                   int* eb, int* flag, const int* item_map) {
   const int item = blockIdx.y;
   const int c = blockIdx.x * 8 + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   if (c >= n) return;
-  const double2* col = B + (int64_t)item * sB + (int64_t)c * k;
+  const double2* col = B + (int64_t)(item_map ? item_map[item] : item) * sB + (int64_t)c * k;
   double mx = 0.0;
   bool bad = false;
   for (int kk = lane; kk < k; kk += 32) {
@@ -254,34 +265,58 @@ __global__ void __launch_bounds__(256) k_split_cols(int k, int n, int kp, const 
 
 // ---------------------------------------------------------------- product
 struct OzArgs {
-  int m, n, k, nkc;   // nkc: K chunks of 64 bytes per half of the concatenated K
+  int m, n, k, nkc;   // nkc: K chunks of kOzKChunk bytes per half of the concatenated K
+  int batch;
   double2 alpha, beta;
   double2* C;
   int64_t sC;
+  const int* item_map;   // launch item -> problem index for C / maxabs / status (null = identity)
   const int* ea;
   const int* eb;
   const int* flag;
+  double* t0;            // FP64 real part of C, m x n per launch item (read back for the final combine)
   double* maxabs;
   int* status;
 };
 
+// Warp roles: warps 0-7 read the accumulators (warp w owns TMEM lanes
+// 32 (w % 4) .. +31, i.e. rows m0 + 32 (w % 4) + lane, and the 64 columns
+// 64 (w / 4) .. +63), warp 8 lane 0 issues the TMA loads, warp 9 lane 0 the
+// MMAs.
+constexpr int kOzEpiWarps = 8;
+constexpr int kOzWarps = kOzEpiWarps + 2;
+constexpr int kOzEpiCols = kOzTileN / 2;   // columns per epilogue thread
+
+// int32 -> double without the conversion unit: 2^52 + 2^31 + v assembled from
+// bits (exact for every int32), minus 2^52 + 2^31 (exact): one FP64 add.
+__device__ __forceinline__ double i2d(uint32_t v) {
+  return __hiloint2double(0x43300000, (int)(v ^ 0x80000000u)) - 4503601774854144.0;
+}
+
+// 2^e as a double for the normal range, ldexp outside it
+__device__ __forceinline__ double pow2(int e) {
+  return (e > -1022 && e < 1023) ? __longlong_as_double((long long)(1023 + e) << 52) : ldexp(1.0, e);
+}
+
 template <int S>
-__global__ void __launch_bounds__(kOzThreads, 1)
+__global__ void __launch_bounds__(kOzWarps * 32, 1)
     k_ozaki(const __grid_constant__ CUtensorMap tA, const __grid_constant__ CUtensorMap tB, OzArgs a) {
-  constexpr int kStage = S * (kABytes + kBBytes);
   constexpr int kLevels = oz_levels(S);
-  static_assert(kLevels * kOzTileN <= (int)kTmemCols, "level accumulators must fit the tensor memory");
+  constexpr int kStage = 2 * S * kPlaneBytes;   // S planes of A and S of B
+  static_assert(kOzGroup * kOzTileN <= (int)kTmemCols, "a level group must fit the tensor memory");
+  static_assert(kLevels > kOzGroup && kLevels <= 2 * kOzGroup, "two level groups");
   extern __shared__ __align__(1024) uint8_t oz_raw[];
   uint8_t* sm = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(oz_raw) + 1023) & ~uintptr_t(1023));
-  __shared__ __align__(8) uint64_t full[kOzStages], empty[kOzStages], accb;
+  __shared__ __align__(8) uint64_t full[kOzStages], empty[kOzStages], accb, tfree;
   __shared__ uint32_t tmem_base;
   __shared__ volatile int fail;
   __shared__ int issued[kOzStages];
+  __shared__ double col_scale[kOzTileN];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int item = blockIdx.y;
-  const int tiles_n = (a.n + kOzTileN - 1) / kOzTileN;
-  const int m0 = (blockIdx.x / tiles_n) * kOzTileM, n0 = (blockIdx.x % tiles_n) * kOzTileN;
+  const int tiles_m = (a.m + kOzTileM - 1) / kOzTileM, tiles_n = (a.n + kOzTileN - 1) / kOzTileN;
+  const int per_item = tiles_m * tiles_n;
+  const int ntiles = per_item * a.batch;
   const int nchunk = 2 * a.nkc;
 
   if (threadIdx.x == 0) {
@@ -291,6 +326,7 @@ __global__ void __launch_bounds__(kOzThreads, 1)
       issued[i] = 0;
     }
     mbar_init(&accb, 1);
+    mbar_init(&tfree, kOzEpiWarps);
     fail = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -305,105 +341,185 @@ __global__ void __launch_bounds__(kOzThreads, 1)
   tc_fence_after();
   const uint32_t tbase = tmem_base;
 
-  // epilogue geometry: row r of the tile, 32 columns [cw, cw + 32)
-  const int quarter = warp & 3;
-  const int r = m0 + 32 * quarter + lane;
-  const int cw = 32 * (warp >> 2);
-  const bool row_ok = r < a.m;
-  const int ea_r = row_ok ? a.ea[(int64_t)item * a.m + r] : 0;
-  const bool nonfinite = a.flag[item] != 0;
-  double re[32];
-  double local_max = 0.0;
-
-  for (int pass = 0; pass < 2; ++pass) {
-    if (warp == 0 && lane == 0) {
-      // producer: TMA loads of the digit planes into the stage ring
-      for (int c = 0; c < nchunk; ++c) {
-        const int gidx = pass * nchunk + c, st = gidx % kOzStages, use = gidx / kOzStages;
-        if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, &fail)) break;
-        uint8_t* sa = sm + st * kStage;
-        uint8_t* sb = sa + S * kABytes;
-        const int h = c / a.nkc, k0 = (c % a.nkc) * kOzKChunk;
-        // real pass: [Ar | -Ai] x [Br ; Bi]; imaginary pass: [Ai | Ar] x [Br ; Bi]
-        const int arr_a = (pass == 0) ? (h == 0 ? 0 : 2) : (h == 0 ? 1 : 0);
-        mbar_arrive_tx(&full[st], (uint32_t)kStage);
-        for (int t = 0; t < S; ++t) {
-          tma_load_3d(sa + t * kABytes, &tA, &full[st], k0, m0, (item * 3 + arr_a) * S + t);
-          tma_load_3d(sb + t * kBBytes, &tB, &full[st], k0, n0, (item * 2 + h) * S + t);
-        }
-        issued[st] = use + 1;
-      }
-    } else if (warp == 1 && lane == 0) {
-      // MMA issuer: all digit pairs (t, u) with t + u < levels per K step
-      tc_fence_after();
-      for (int c = 0; c < nchunk; ++c) {
-        const int gidx = pass * nchunk + c, st = gidx % kOzStages, use = gidx / kOzStages;
-        if (!mbar_wait(&full[st], use & 1, &fail)) break;
-        tc_fence_after();
-        const uint32_t sa = s32(sm + st * kStage), sb = sa + S * kABytes;
-#pragma unroll
-        for (int ks = 0; ks < kOzKChunk / 32; ++ks) {
-#pragma unroll
-          for (int t = 0; t < S; ++t) {
-            const uint64_t da = sdesc(sa + t * kABytes + ks * 32);
-#pragma unroll
-            for (int u = 0; u < S && t + u < kLevels; ++u) {
-              const uint64_t db = sdesc(sb + u * kBBytes + ks * 32);
-              // the first pair of a level (smallest t) in a pass overwrites its accumulator
-              const int first_t = (t + u > S - 1) ? t + u - (S - 1) : 0;
-              const uint32_t acc = (c > 0 || ks > 0 || t > first_t) ? 1u : 0u;
-              umma_i8(tbase + (uint32_t)((t + u) * kOzTileN), da, db, kIdescI8, acc);
+  if (warp == kOzEpiWarps) {
+    // ---------------- producer: digit planes of every (tile, part, group, chunk)
+    if (lane == 0) {
+      int g = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
+        const int item = tile / per_item, tt = tile % per_item;
+        const int m0 = (tt / tiles_n) * kOzTileM, n0 = (tt % tiles_n) * kOzTileN;
+        for (int mi = 0; mi < 4 && !fail; ++mi) {
+          const int part = mi >> 1, grp = mi & 1;
+          // planes used by the group: digits t < 4 (levels 0-3) or all S
+          const int np = grp == 0 ? kOzGroup : S;
+          for (int c = 0; c < nchunk; ++c, ++g) {
+            const int st = g % kOzStages, use = g / kOzStages;
+            if (use > 0 && !mbar_wait(&empty[st], (use - 1) & 1, &fail)) break;
+            uint8_t* sa = sm + st * kStage;
+            uint8_t* sb = sa + S * kPlaneBytes;
+            const int h = c / a.nkc, k0 = (c % a.nkc) * kOzKChunk;
+            // real part: [Ar | -Ai] x [Br ; Bi]; imaginary part: [Ai | Ar] x [Br ; Bi]
+            const int arr_a = (part == 0) ? (h == 0 ? 0 : 2) : (h == 0 ? 1 : 0);
+            mbar_arrive_tx(&full[st], (uint32_t)(2 * np * kPlaneBytes));
+            for (int t = 0; t < np; ++t) {
+              tma_load_3d(sa + t * kPlaneBytes, &tA, &full[st], k0, m0, (item * 3 + arr_a) * S + t);
+              tma_load_3d(sb + t * kPlaneBytes, &tB, &full[st], k0, n0, (item * 2 + h) * S + t);
             }
+            issued[st] = use + 1;
           }
         }
-        umma_commit(&empty[st]);   // the stage is free once these MMAs have read it
       }
-      umma_commit(&accb);          // the level accumulators of this pass are complete
     }
-    __syncwarp();
-    const bool ok = mbar_wait(&accb, pass & 1, &fail) && !fail;
-    tc_fence_after();
-    if (ok) {
+  } else if (warp == kOzEpiWarps + 1) {
+    // ---------------- MMA issuer: the digit pairs of one level group per mainloop
+    if (lane == 0) {
+      int g = 0, ml = 0;
+      for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
+        for (int mi = 0; mi < 4 && !fail; ++mi, ++ml) {
+          const int l0 = (mi & 1) * kOzGroup;
+          // the accumulators are free once the epilogue has read the previous mainloop
+          if (ml > 0 && !mbar_wait(&tfree, (ml - 1) & 1, &fail)) break;
+          tc_fence_after();
+          for (int c = 0; c < nchunk; ++c, ++g) {
+            const int st = g % kOzStages, use = g / kOzStages;
+            if (!mbar_wait(&full[st], use & 1, &fail)) break;
+            tc_fence_after();
+            const uint32_t sa = s32(sm + st * kStage), sb = sa + S * kPlaneBytes;
 #pragma unroll
-      for (int grp = 0; grp < 4; ++grp) {
-        uint32_t v[kLevels][8];
+            for (int t = 0; t < S; ++t) {
 #pragma unroll
-        for (int l = 0; l < kLevels; ++l)
-          tmem_ld8(tbase + ((uint32_t)(32 * quarter) << 16) + (uint32_t)(l * kOzTileN + cw + 8 * grp), v[l]);
-        tmem_wait_ld();
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          double x = 0.0;
-#pragma unroll
-          for (int l = kLevels - 1; l >= 0; --l) x += (double)(int)v[l][j] * level_weight(l);
-          const int c = n0 + cw + 8 * grp + j;
-          const int eb_c = (c < a.n) ? a.eb[(int64_t)item * a.n + c] : 0;
-          x = ldexp(x, ea_r + eb_c);
-          if (pass == 0) {
-            re[8 * grp + j] = x;
-          } else if (row_ok && c < a.n) {
-            double2* dst = a.C + (int64_t)item * a.sC + (int64_t)r + (int64_t)c * a.m;
-            const double pr = re[8 * grp + j], pi = x;
-            double2 out = make_double2(a.alpha.x * pr - a.alpha.y * pi, a.alpha.x * pi + a.alpha.y * pr);
-            if (a.beta.x != 0.0 || a.beta.y != 0.0) {
-              const double2 o = *dst;
-              out.x += a.beta.x * o.x - a.beta.y * o.y;
-              out.y += a.beta.x * o.y + a.beta.y * o.x;
+              for (int u = 0; u < S; ++u) {
+                const int l = t + u;
+                if (l < l0 || l >= l0 + kOzGroup || l >= kLevels) continue;
+                // the first pair of a level (smallest t) in a mainloop overwrites its accumulator
+                const int first_t = (l > S - 1) ? l - (S - 1) : 0;
+                const uint32_t acc = (c > 0 || t > first_t) ? 1u : 0u;
+                umma_i8(tbase + (uint32_t)((l - l0) * kOzTileN), sdesc(sa + t * kPlaneBytes),
+                        sdesc(sb + u * kPlaneBytes), kIdescI8, acc);
+              }
             }
+            umma_commit(&empty[st]);   // the stage is free once these MMAs have read it
+          }
+          umma_commit(&accb);          // this group's level accumulators are complete
+        }
+      }
+    }
+  } else {
+    // ---------------- epilogue: warps 0-7
+    const int quarter = warp & 3, cw = kOzEpiCols * (warp >> 2);
+    const uint32_t tlane = (uint32_t)(32 * quarter) << 16;
+    constexpr int nlev1 = kLevels - kOzGroup;
+    const double w0 = level_weight(kOzGroup - 1);   // units of the level-0..3 Horner sum
+    const double w1 = level_weight(kLevels - 1);    // units of the level-4.. Horner sum
+    int ml = 0;
+    double part0[kOzEpiCols];                       // levels 0-3 of the current part, exact
+    for (int tile = blockIdx.x; tile < ntiles && !fail; tile += gridDim.x) {
+      const int item = tile / per_item, tt = tile % per_item;
+      const int prob = a.item_map ? a.item_map[item] : item;
+      const int m0 = (tt / tiles_n) * kOzTileM, n0 = (tt % tiles_n) * kOzTileN;
+      const int r = m0 + 32 * quarter + lane;
+      const bool row_ok = r < a.m;
+      const double rs = row_ok ? pow2(a.ea[(int64_t)item * a.m + r]) : 0.0;
+      const bool nonfinite = a.flag[item] != 0;
+      // column scales of this tile (the epilogue warps' named barrier 1)
+      asm volatile("bar.sync 1, %0;" ::"n"(kOzEpiWarps * 32));
+      if (threadIdx.x < kOzTileN) {
+        const int c = n0 + threadIdx.x;
+        col_scale[threadIdx.x] = (c < a.n) ? pow2(a.eb[(int64_t)item * a.n + c]) : 0.0;
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(kOzEpiWarps * 32));
+      double* T0 = a.t0 + (int64_t)item * a.m * a.n;
+      double local_max = 0.0;
+      for (int mi = 0; mi < 4; ++mi, ++ml) {
+        const int part = mi >> 1, grp = mi & 1;
+        if (!mbar_wait(&accb, ml & 1, &fail)) break;
+        tc_fence_after();
+#pragma unroll
+        for (int j8 = 0; j8 < kOzEpiCols / 8; ++j8) {
+          uint32_t v[kOzGroup][8];
+          const uint32_t col = (uint32_t)(cw + 8 * j8);
+          if (grp == 0) {
+#pragma unroll
+            for (int l = 0; l < kOzGroup; ++l) tmem_ld8(tbase + tlane + (uint32_t)(l * kOzTileN) + col, v[l]);
+          } else {
+#pragma unroll
+            for (int l = 0; l < nlev1; ++l) tmem_ld8(tbase + tlane + (uint32_t)(l * kOzTileN) + col, v[l]);
+          }
+          tmem_wait_ld();
+          if (j8 == kOzEpiCols / 8 - 1) {
+            // every accumulator of this group is in registers: hand the tensor memory back
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tfree);
+          }
+          if (grp == 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+              // exact: |acc| < 2^26, four levels 2^7 apart stay below 2^48
+              double x = i2d(v[0][j]);
+#pragma unroll
+              for (int l = 1; l < kOzGroup; ++l) x = fma(x, 128.0, i2d(v[l][j]));
+              part0[8 * j8 + j] = x;
+            }
+            continue;
+          }
+          // group 1: the part is complete
+          double val[8];
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            double y = i2d(v[0][j]);
+#pragma unroll
+            for (int l = 1; l < nlev1; ++l) y = fma(y, 128.0, i2d(v[l][j]));
+            val[j] = fma(part0[8 * j8 + j], w0, y * w1) * rs * col_scale[col + j];
+          }
+          if (!row_ok) continue;
+          const int c0 = n0 + (int)col;
+          if (part == 0) {
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              if (c0 + j < a.n) T0[(int64_t)r + (int64_t)(c0 + j) * a.m] = val[j];
+            continue;
+          }
+          double pr[8];
+          double2 old[8];
+          const bool use_beta = (a.beta.x != 0.0 || a.beta.y != 0.0);
+          double2* Cp = a.C + (int64_t)prob * a.sC;
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            const int64_t o = (int64_t)r + (int64_t)(c0 + j) * a.m;
+            const bool ok = c0 + j < a.n;
+            pr[j] = ok ? T0[o] : 0.0;
+            old[j] = (ok && use_beta) ? Cp[o] : make_double2(0.0, 0.0);
+          }
+#pragma unroll
+          for (int j = 0; j < 8; ++j) {
+            if (c0 + j >= a.n) continue;
+            const double pi = val[j];
+            double2 out = make_double2(a.alpha.x * pr[j] - a.alpha.y * pi, a.alpha.x * pi + a.alpha.y * pr[j]);
+            out.x += a.beta.x * old[j].x - a.beta.y * old[j].y;
+            out.y += a.beta.x * old[j].y + a.beta.y * old[j].x;
             if (nonfinite) {
               const double qnan = __longlong_as_double(0x7ff8000000000000LL);
               out = make_double2(qnan, qnan);
             }
-            *dst = out;
-            local_max = fmax(local_max, hypot(out.x, out.y));
+            Cp[(int64_t)r + (int64_t)(c0 + j) * a.m] = out;
+            if (a.maxabs) local_max = fmax(local_max, hypot(out.x, out.y));
           }
         }
       }
+      if (fail) break;
+      if (a.maxabs) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) local_max = fmax(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+        if (lane == 0 && local_max > 0.0)
+          atomicMax(reinterpret_cast<unsigned long long*>(a.maxabs + prob),
+                    (unsigned long long)__double_as_longlong(local_max));
+      }
+      if (nonfinite && threadIdx.x == 0 && a.status && tt == 0) a.status[prob] = 3;
     }
-    tc_fence_before();
-    __syncthreads();
   }
 
+  __syncthreads();
   if (fail) {
     // let every TMA load this CTA issued land before its shared memory is released
     if (threadIdx.x == 0)
@@ -413,17 +529,13 @@ __global__ void __launch_bounds__(kOzThreads, 1)
           while (!mbar_test(&full[st], (issued[st] - 1) & 1) && clock64() - t0 < kSpinCycles) {
           }
         }
-    if (threadIdx.x == 0 && a.status) a.status[item] = 7;
-  } else {
-    if (a.maxabs) {
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) local_max = fmax(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
-      if (lane == 0 && local_max > 0.0)
-        atomicMax(reinterpret_cast<unsigned long long*>(a.maxabs + item),
-                  (unsigned long long)__double_as_longlong(local_max));
-    }
-    if (nonfinite && threadIdx.x == 0 && a.status) a.status[item] = 3;
+    if (threadIdx.x == 0 && a.status)
+      for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        const int item = tile / per_item;
+        a.status[a.item_map ? a.item_map[item] : item] = 7;
+      }
   }
+  tc_fence_before();
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(kTmemCols)
                               : "memory");
@@ -458,15 +570,28 @@ bool make_map(CUtensorMap* map, void* base, int k, int rows, int kp, int planes,
   const cuuint32_t box[3] = {(cuuint32_t)kOzKChunk, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_SWIZZLE_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
+int num_sms() {
+  static int n[64] = {0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64) return 148;
+  if (!n[dev] && cudaDeviceGetAttribute(&n[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    n[dev] = 148;
+  }
+  return n[dev];
+}
+
 template <int S>
 cudaError_t run(const OzakiLayout& L, double2 alpha, const double2* A, int64_t sA, const double2* B, int64_t sB,
-                double2 beta, double2* C, int64_t sC, uint8_t* w, double* maxabs, int* status, cudaStream_t s) {
+                double2 beta, double2* C, int64_t sC, uint8_t* w, double* maxabs, int* status, cudaStream_t s,
+                const int* item_map) {
   int8_t* qa = reinterpret_cast<int8_t*>(w + L.qa_off);
   int8_t* qb = reinterpret_cast<int8_t*>(w + L.qb_off);
   int* ea = reinterpret_cast<int*>(w + L.ea_off);
@@ -474,17 +599,20 @@ cudaError_t run(const OzakiLayout& L, double2 alpha, const double2* A, int64_t s
   int* flag = reinterpret_cast<int*>(w + L.flag_off);
   cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int) * (size_t)L.batch, s);
   if (e != cudaSuccess) return e;
-  k_split_rows<S><<<dim3((L.m + 31) / 32, L.batch), 256, 0, s>>>(L.m, L.k, L.kp, A, sA, qa, ea, flag);
-  k_split_cols<S><<<dim3((L.n + 7) / 8, L.batch), 256, 0, s>>>(L.k, L.n, L.kp, B, sB, qb, eb, flag);
+  k_split_rows<S><<<dim3((L.m + 31) / 32, L.batch), 256, 0, s>>>(L.m, L.k, L.kp, A, sA, qa, ea, flag, item_map);
+  k_split_cols<S><<<dim3((L.n + 7) / 8, L.batch), 256, 0, s>>>(L.k, L.n, L.kp, B, sB, qb, eb, flag, item_map);
   CUtensorMap ta, tb;
   if (!make_map(&ta, qa, L.k, L.m, L.kp, L.batch * 3 * S, kOzTileM) ||
       !make_map(&tb, qb, L.k, L.n, L.kp, L.batch * 2 * S, kOzTileN))
     return cudaErrorInvalidValue;
   OzArgs a;
   a.m = L.m; a.n = L.n; a.k = L.k; a.nkc = (L.k + kOzKChunk - 1) / kOzKChunk;
-  a.alpha = alpha; a.beta = beta; a.C = C; a.sC = sC;
-  a.ea = ea; a.eb = eb; a.flag = flag; a.maxabs = maxabs; a.status = status;
-  const size_t smem = (size_t)kOzStages * S * (kABytes + kBBytes) + 1024;
+  a.batch = L.batch;
+  a.alpha = alpha; a.beta = beta; a.C = C; a.sC = sC; a.item_map = item_map;
+  a.ea = ea; a.eb = eb; a.flag = flag;
+  a.t0 = reinterpret_cast<double*>(w + L.t0_off);
+  a.maxabs = maxabs; a.status = status;
+  const size_t smem = (size_t)kOzStages * 2 * S * kPlaneBytes + 1024;
   static std::mutex mu;
   static bool attr_set[64] = {false};
   int dev = 0;
@@ -497,8 +625,9 @@ cudaError_t run(const OzakiLayout& L, double2 alpha, const double2* A, int64_t s
       if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
   }
-  const int tiles = ((L.m + kOzTileM - 1) / kOzTileM) * ((L.n + kOzTileN - 1) / kOzTileN);
-  k_ozaki<S><<<dim3(tiles, L.batch), kOzThreads, smem, s>>>(ta, tb, a);
+  const long long tiles = (long long)((L.m + kOzTileM - 1) / kOzTileM) * ((L.n + kOzTileN - 1) / kOzTileN) * L.batch;
+  const int grid = (int)(tiles < num_sms() ? tiles : num_sms());
+  k_ozaki<S><<<grid, kOzWarps * 32, smem, s>>>(ta, tb, a);
   return cudaGetLastError();
 }
 
@@ -514,13 +643,14 @@ OzakiLayout ozaki_layout(int batch, int m, int n, int k, int slices) {
   L.ea_off = off; off = align256(off + sizeof(int) * (size_t)batch * m);
   L.eb_off = off; off = align256(off + sizeof(int) * (size_t)batch * n);
   L.flag_off = off; off = align256(off + sizeof(int) * (size_t)batch);
+  L.t0_off = off; off = align256(off + sizeof(double) * (size_t)batch * m * n);
   L.total = off;
   return L;
 }
 
 cudaError_t launch_ozaki_zgemm(int batch, int m, int n, int k, double2 alpha, const double2* A, int64_t sA,
                                const double2* B, int64_t sB, double2 beta, double2* C, int64_t sC, int slices,
-                               void* work, double* maxabs, int* status, cudaStream_t s) {
+                               void* work, double* maxabs, int* status, cudaStream_t s, const int* item_map) {
   if (batch <= 0 || m <= 0 || n <= 0) return cudaSuccess;
   if (k <= 0 || k > 1024 || batch > 65535 || slices < kOzMinSlices || slices > kOzMaxSlices || !work ||
       (reinterpret_cast<uintptr_t>(work) & 255))
@@ -528,11 +658,11 @@ cudaError_t launch_ozaki_zgemm(int batch, int m, int n, int k, double2 alpha, co
   const OzakiLayout L = ozaki_layout(batch, m, n, k, slices);
   uint8_t* w = static_cast<uint8_t*>(work);
   switch (slices) {
-    case 4: return run<4>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
-    case 5: return run<5>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
-    case 6: return run<6>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
-    case 7: return run<7>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
-    default: return run<8>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s);
+    case 4: return run<4>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s, item_map);
+    case 5: return run<5>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s, item_map);
+    case 6: return run<6>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s, item_map);
+    case 7: return run<7>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s, item_map);
+    default: return run<8>(L, alpha, A, sA, B, sB, beta, C, sC, w, maxabs, status, s, item_map);
   }
 }
 

@@ -22,27 +22,31 @@
 namespace negf {
 
 constexpr int kOzTileM = 128;       // UMMA M (one CTA)
-constexpr int kOzTileN = 64;        // UMMA N; S level accumulators of 64 columns in TMEM
-constexpr int kOzKChunk = 64;       // bytes of K per pipeline stage (one 64-byte swizzle row)
-constexpr int kOzStages = 2;
+constexpr int kOzTileN = 128;       // UMMA N (the full-rate width); 4 levels x 128 columns of TMEM
+constexpr int kOzKChunk = 32;       // bytes of K per pipeline stage (one 32-byte swizzle row, one MMA K step)
+constexpr int kOzStages = 3;
 constexpr int kOzMinSlices = 4, kOzMaxSlices = 8;
 
-// Workspace of one batched product (bytes), laid out by ozaki_layout().
+// Workspace of one batched product (bytes), laid out by ozaki_layout():
+// digit planes of A and B, exponents, non-finite flags, an FP64 m x n
+// buffer per item for the real part.
 struct OzakiLayout {
   int m, n, k, kp, slices, batch;
-  size_t qa_off, qb_off, ea_off, eb_off, flag_off, total;
+  size_t qa_off, qb_off, ea_off, eb_off, flag_off, t0_off, total;
 };
 OzakiLayout ozaki_layout(int batch, int m, int n, int k, int slices);
 
-// C_b = alpha * A_b * B_b + beta * C_b for b < batch (complex128, column
-// major, element strides sA/sB/sC in complex elements).  beta == 0: C is
-// not read.  C may alias A or B (the operands are split into the workspace
-// first).  maxabs (optional, one double per item, non-negative, updated
-// with atomicMax on its bit pattern): max |C_b| over the stored elements.
-// status (optional, one int per item): 3 on a non-finite operand (C is NaN),
-// 7 when a pipeline wait ran out (C is not written).
+// C_p = alpha * A_p * B_p + beta * C_p for the problems p = item_map[b],
+// b < batch (item_map null: p = b); complex128, column major, element
+// strides sA/sB/sC in complex elements.  beta == 0: C is not read.  C may
+// alias A or B (the operands are split into the workspace first).  maxabs
+// (optional, one double per problem, non-negative, updated with atomicMax on
+// its bit pattern): max |C_p| over the stored elements.  status (optional,
+// one int per problem): 3 on a non-finite operand (C is NaN), 7 when a
+// pipeline wait ran out (C is not written).
 cudaError_t launch_ozaki_zgemm(int batch, int m, int n, int k, double2 alpha, const double2* A, int64_t sA,
                                const double2* B, int64_t sB, double2 beta, double2* C, int64_t sC, int slices,
-                               void* work, double* maxabs, int* status, cudaStream_t s);
+                               void* work, double* maxabs, int* status, cudaStream_t s,
+                               const int* item_map = nullptr);
 
 }  // namespace negf

@@ -99,54 +99,59 @@ def fp64_scatter(ref, ref_x, others=()):
     return e
 
 
-def assert_parity(got, ref, bound, ref_x=None, others=(), what="T", kx=10.0):
+def assert_parity(got, ref, bound, ref_x=None, others=(), spread=None, what="T", kx=10.0):
     """Parity of `got` against the oracle `ref` at the bound (an array).
 
-    Without an extended-precision solution: |got - ref| <= bound everywhere.
-    With one (`ref_x`, plus the other CPU FP64 paths in `others`): strict
-    wherever every CPU FP64 result lies within an eighth of the bound of the
-    long-double solution.  The other points are listed (returned, and named
-    in a failure message): there the FP64 rounding of the reference path
-    itself scatters beyond the bound's margin, and the result must be as
-    close to the long-double solution as the CPU FP64 paths are:
-    |got - ref_x| <= max(bound, kx * their largest distance from it)."""
+    The FP64 rounding of the reference path is sampled per point by the CPU
+    FP64 paths' distances from the long-double solution `ref_x` (the
+    oracle's and the restated ones in `others`) and by `spread`, the
+    oracle's own change under rounding-level (1e-15 relative) input
+    perturbations.  Strict, |got - ref| <= bound, wherever every sample is
+    within an eighth of the bound.  The other points are listed (returned,
+    and named in a failure message): there the reference path's own FP64
+    result scatters beyond the bound's margin, and the result must be as
+    close to the long-double solution as the CPU FP64 paths are,
+    |got - ref_x| <= max(bound, kx * the largest sample), or, without a
+    long-double solution, |got - ref| <= max(bound, kx * spread)."""
     got = np.asarray(got, dtype=float)
     ref = np.asarray(ref, dtype=float)
     bound = np.broadcast_to(np.asarray(bound, dtype=float), ref.shape)
     assert got.shape == ref.shape
-    if ref_x is None:
-        listed = np.zeros(ref.shape, dtype=bool)
-        e_cpu = None
-    else:
+    e_cpu = np.zeros(ref.shape)
+    if ref_x is not None:
         ref_x = np.asarray(ref_x, dtype=float)
         e_cpu = fp64_scatter(ref, ref_x, others)
-        listed = e_cpu > LIST_FRACTION * bound
+    if spread is not None:
+        e_cpu = np.maximum(e_cpu, np.asarray(spread, dtype=float))
+    listed = e_cpu > LIST_FRACTION * bound
     err = np.abs(got - ref)
     bad = (~listed) & (err > bound)
     assert not bad.any(), "%s: %d of %d points beyond the strict bound; worst err %.3e (bound %.3e) at ref=%.6e" % (
         what, int(bad.sum()), bad.size, err[bad].max(), bound[bad][np.argmax(err[bad])],
         ref[bad][np.argmax(err[bad])])
     if listed.any():
-        e_x = np.abs(got - ref_x)
+        e_x = np.abs(got - (ref_x if ref_x is not None else ref))
         lim = np.maximum(bound, kx * e_cpu)
         badx = listed & (e_x > lim)
         assert not badx.any(), (
-            "%s: %d listed points farther from the long-double solution than %gx the CPU FP64 paths: "
-            "worst |got - x| %.3e against CPU %.3e" % (what, int(badx.sum()), kx, e_x[badx].max(),
-                                                      e_cpu[badx][np.argmax(e_x[badx])]))
+            "%s: %d listed points farther from the %s than %gx the FP64 rounding samples: "
+            "worst %.3e against %.3e" % (what, int(badx.sum()),
+                                         "long-double solution" if ref_x is not None else "oracle",
+                                         kx, e_x[badx].max(), e_cpu[badx][np.argmax(e_x[badx])]))
     return np.nonzero(listed.ravel())[0]
 
 
-def assert_T_strict(T, Tref, xref=None, rtol=1e-10, atol=1e-13, what="T"):
+def assert_T_strict(T, Tref, xref=None, spread=None, rtol=1e-10, atol=1e-13, what="T"):
     """The transmission bound |T - Tref| <= max(rtol |Tref|, atol), strict
-    except at the points where the CPU FP64 paths themselves scatter beyond
-    an eighth of it around the long-double solution (`xref` from
-    xp_reference or the fixture)."""
+    except at the points where the reference path's FP64 rounding scatters
+    beyond an eighth of it (`xref` from xp_reference or the fixture, `spread`
+    from oracle_spread)."""
     Tref = np.asarray(Tref, dtype=float)
     bound = np.maximum(rtol * np.abs(Tref), atol)
     if xref is None:
-        return assert_parity(T, Tref, bound, what=what)
-    return assert_parity(T, Tref, bound, ref_x=xref["T_x"], others=(xref["T_d"], xref.get("T_g")), what=what)
+        return assert_parity(T, Tref, bound, spread=spread, what=what)
+    return assert_parity(T, Tref, bound, ref_x=xref["T_x"], others=(xref["T_d"], xref.get("T_g")), spread=spread,
+                         what=what)
 
 
 @pytest.fixture(scope="session")

@@ -22,7 +22,9 @@ For the T and T + DOS shapes four CPU solutions are stored per point:
   T_g   the same in double with Gauss-Jordan inverses (a third one, with the
         elimination order of the engine's inversion);
   T_x   the same algorithm in long double (64-bit significand), a near-exact
-        solution: |T_o - T_x| is the reference path's own rounding error.
+        solution: |T_o - T_x| is the reference path's own rounding error;
+  T_s   the oracle's largest change under two rounding-level (1e-15
+        relative) perturbations of every input block.
 At energies where the device solve is ill-conditioned (the device blocks
 carry no broadening, src/integrations.F90:1747-1752, so narrow resonances
 are only as wide as the lead coupling makes them) the FP64 paths land up to
@@ -123,7 +125,20 @@ def c3_occupations(E):
 CASES = {"c0": c0_case, "c1": c1_case, "c2": c2_case, "c3": c3_case}
 
 
-KINDS = ("o", "d", "g", "x")
+KINDS = ("o", "d", "g", "x", "s")
+
+
+def perturbed(dev, rng, rel=1e-15):
+    """Copy of `dev` with every block element scaled by (1 + rel N(0,1))."""
+    import copy
+    d = copy.deepcopy(dev)
+    for name in BLOCK_LISTS:
+        lst = getattr(d, name)
+        if lst is None:
+            continue
+        for i in range(len(lst)):
+            lst[i] = lst[i] * (1.0 + rel * rng.standard_normal(lst[i].shape))
+    return d
 
 
 def run_shape(name, out, kinds=KINDS):
@@ -152,7 +167,22 @@ def run_shape(name, out, kinds=KINDS):
                 continue
             Ek = E[sel]
             t0 = time.time()
-            if key == "o" and p["dos"]:
+            if key == "s":
+                rng = np.random.default_rng(17)
+                t = np.zeros(sel.size)
+                ds = None
+                base = (O.transmission_dos(d, Ek, eta=p["eta"], dos_delta=0.0, sgf_tol=p["sgf_tol"]) if p["dos"]
+                        else O.transmission(d, Ek, eta=p["eta"], sgf_tol=p["sgf_tol"]))
+                for _ in range(2):
+                    dp = perturbed(d, rng)
+                    r = (O.transmission_dos(dp, Ek, eta=p["eta"], dos_delta=0.0, sgf_tol=p["sgf_tol"]) if p["dos"]
+                         else O.transmission(dp, Ek, eta=p["eta"], sgf_tol=p["sgf_tol"]))
+                    t = np.maximum(t, np.abs(r[0] - base[0]))
+                    if p["dos"]:
+                        dd = np.abs(r[1] - base[1])
+                        ds = dd if ds is None else np.maximum(ds, dd)
+                c, st = base[-2], base[-1]
+            elif key == "o" and p["dos"]:
                 t, ds, c, st = O.transmission_dos(d, Ek, eta=p["eta"], dos_delta=0.0, sgf_tol=p["sgf_tol"])
             elif key == "o":
                 t, c, st = O.transmission(d, Ek, eta=p["eta"], sgf_tol=p["sgf_tol"])
