@@ -36,15 +36,18 @@ sys.path.insert(0, ROOT)
 WORKLOADS = {
     # name: (nbl, n, nE, emin, emax, nk, eta, dos)
     "c1": dict(nbl=100, n=256, nE=2048, emin=-2.0, emax=2.0, nk=16, eta=1e-6, dos=True, gen="c1"),
-    "c0": dict(nbl=20, n=32, nE=512, emin=-3.0, emax=3.0, nk=1, eta=1e-6, dos=False, gen="c0"),
+    # the CPU-runnable config states its surface Green's functions converged to 1e-12
+    "c0": dict(nbl=20, n=32, nE=512, emin=-3.0, emax=3.0, nk=1, eta=1e-6, dos=False, gen="c0", sgf_tol=1e-12),
     "c2": dict(nbl=60, n=512, nE=1024, emin=-2.0, emax=2.0, nk=8, eta=1e-6, dos=False, gen="c1"),
     # elastic-dephasing SCBA: dephasing coupling 0.1 eV (D = 0.01 eV^2) on every orbital, bias 0.2 eV
     # symmetric, 300 K leads; linear mixing 0.5 until the contact-1 current changes by < 1e-8, at most
     # 100 sweeps; one step = the whole 1024-point grid
     "c3": dict(nbl=40, n=128, nE=1024, emin=-1.0, emax=1.0, nk=1, eta=1e-4, dos=False, gen="c0", pps=1024,
                scba=dict(coupling=0.1, bias=0.2, temp_k=300.0, niter=100, tol=1e-8, mix=0.5, rule=1)),
-    # small case of the c1 kernel for profiler captures (few GB on the device)
+    # small cases of the c1 kernel for profiler captures (a few GB on the device): DRAM bytes per
+    # point at 4 and 8 layers give the per-layer and per-point parts that scale it to c1
     "prof": dict(nbl=8, n=256, nE=256, emin=-2.0, emax=2.0, nk=1, eta=1e-6, dos=True, gen="c1"),
+    "prof4": dict(nbl=4, n=256, nE=256, emin=-2.0, emax=2.0, nk=1, eta=1e-6, dos=True, gen="c1"),
     # serving stream (Poisson arrivals of transmission / LDOS requests; see run_serve)
     "serve": dict(nbl=0, n=0, nE=0, emin=-2.0, emax=2.0, nk=1, eta=1e-4, dos=False, gen="serve"),
 }
@@ -71,6 +74,9 @@ def parse():
     p.add_argument("--serve-lanes", type=int, default=2)
     p.add_argument("--serve-policy", default="fifo", choices=["fifo", "srpt"],
                    help="batching order: least remaining work first, or oldest first")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the c2 plain / mixed and serving segments of the default line")
+    p.add_argument("--mixed-digits", type=int, default=8, help="int8 digits of the mixed form (4..8)")
     return p.parse_args()
 
 
@@ -92,9 +98,20 @@ def point_list(wl, seed=11):
     return ids[perm], en[perm]
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one k_engine
-# launch, from an ncu capture of the default c1 command (592 points per step)
-DRAM_BYTES_PER_LAUNCH = {("c1", 592): 8.028e12}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the k_engine
+# launch per point, modelled as a + b N for a device of N layers of n = 256
+# (T + DOS), from one-pass ncu captures of two small cases of the same kernel
+# ("prof4": N = 4 and "prof": N = 8, 296 points each, a few GB on the device);
+# scaled to a launch by its points.  None until measured.
+DRAM_PER_POINT_MODEL = {256: None}
+
+
+def dram_bytes_per_launch(wl, points):
+    m = DRAM_PER_POINT_MODEL.get(wl["n"]) if wl.get("dos") and not wl.get("scba") else None
+    if m is None:
+        return None
+    a, b = m
+    return points * (a + b * wl["nbl"])
 
 
 def flops_per_point(wl, ncyc_total, ncont=2):
@@ -237,6 +254,8 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
     from oracle import oracle as O
     O.lib()
     T = np.zeros(nsamp)
+    ncyc = np.zeros(nsamp, dtype=np.int32)
+    tol = wl.get("sgf_tol", 1e-9)
     sc = wl.get("scba")
     if sc:
         out = {"curr": np.zeros((nsamp, 2)), "layer_dens": np.zeros((nsamp, wl["nbl"])),
@@ -255,12 +274,16 @@ def cpu_baseline(wl, devs, ids, E, nsamp, nthreads):
             done += sel.size
             continue
         if wl["dos"]:
-            t, _, _, _ = O.transmission_dos(devs[k], E[sel], eta=wl["eta"], dos_delta=0.0, nthreads=nthreads)
+            t, _, nc, _ = O.transmission_dos(devs[k], E[sel], eta=wl["eta"], dos_delta=0.0, sgf_tol=tol,
+                                             nthreads=nthreads)
         else:
-            t, _, _ = O.transmission(devs[k], E[sel], eta=wl["eta"], nthreads=nthreads)
+            t, nc, _ = O.transmission(devs[k], E[sel], eta=wl["eta"], sgf_tol=tol, nthreads=nthreads)
         T[sel] = t
+        ncyc[sel] = nc
         done += sel.size
     dt = time.perf_counter() - t0
+    if not sc:
+        cpu_baseline.last_ncyc = ncyc
     return done / dt, (out if sc else T), dt
 
 
@@ -306,47 +329,71 @@ def scba_parity_summary(wl, devs, ids, E, got, ref, cores):
     return out
 
 
-def parity_summary(wl, devs, ids, E, Tg, Tc, cores, nworst=64):
-    """GPU vs oracle on the CPU-baseline sample, with the parity bound of the
-    tests: |dT| <= max(1e-10 |T|, 1e-13, 10 * spread), spread being the
-    oracle's own change under 1e-15 relative perturbations of the device
-    blocks, computed for the worst points (the eta = 1e-6 solve is
-    ill-conditioned at lead band edges)."""
+def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ctx=None, dids=None, nworst=16):
+    """GPU vs oracle on the CPU-baseline sample with the rule of the tests:
+    |dT| <= max(1e-10 |T|, 1e-13) wherever the oracle's own change under
+    rounding-level (1e-15 relative) perturbations of every input block stays
+    within an eighth of that bound; the points where it does not are listed
+    (the reference path's FP64 result scatters there) and must lie within
+    10x that spread.  Also: how many decimation iteration counts differ from
+    the oracle's, and the worst points solved again on both sides with the
+    surface Green's functions converged to SGFACC = 1e-12 (the stopping
+    iteration then does not matter: what remains is rounding)."""
     import copy
     from oracle import oracle as O
     err = np.abs(Tg - Tc)
     plain = np.maximum(1e-10 * np.abs(Tc), 1e-13)
     out = {"points": int(E.size), "max_abs_dT": float(err.max()),
            "within_1e-10_rel_or_1e-13_abs": int((err <= plain).sum())}
+    if ncyc_g is not None and ncyc_c is not None:
+        out["decimation_ncyc_mismatches"] = int((np.asarray(ncyc_g) != np.asarray(ncyc_c)).sum())
     worst = [int(q) for q in np.argsort(-(err / plain))[:nworst] if err[q] > plain[q]]
-    if worst:
-        rng = np.random.default_rng(0)
-        spread = np.zeros(len(worst))
-        wq = np.asarray(worst)
-        for _ in range(2):
-            for k in sorted(set(ids[wq].tolist())):          # one call per k-point, OpenMP over its points
-                j = np.nonzero(ids[wq] == k)[0]
-                d = copy.deepcopy(devs[k])
-                for name in ("h_diag", "h_upper", "h_lower", "s_diag", "s_upper", "s_lower", "lead_h00", "lead_h01",
-                             "lead_s00", "lead_s01", "hmc", "smc"):
-                    lst = getattr(d, name)
-                    if lst is None:
-                        continue
-                    for i in range(len(lst)):
-                        lst[i] = lst[i] * (1.0 + 1e-15 * rng.standard_normal(lst[i].shape))
-                if wl["dos"]:
-                    t = O.transmission_dos(d, E[wq[j]], eta=wl["eta"], dos_delta=0.0, nthreads=cores)[0]
-                else:
-                    t = O.transmission(d, E[wq[j]], eta=wl["eta"], nthreads=cores)[0]
-                spread[j] = np.maximum(spread[j], np.abs(t - Tc[wq[j]]))
-        ok = [bool(err[q] <= max(plain[q], 10 * spread[j])) for j, q in enumerate(worst)]
-        out["beyond_1e-10"] = int((err > plain).sum())
-        out["beyond_1e-10_within_10x_oracle_spread"] = int(sum(ok))
-        out["worst"] = [{"E": float(E[q]), "T": float(Tc[q]), "abs_dT": float(err[q]),
-                         "oracle_spread": float(spread[j])} for j, q in enumerate(worst[:4])]
-        out["all_within_test_bound"] = bool(all(ok)) and len(worst) == int((err > plain).sum())
-    else:
+    out["beyond_1e-10"] = int((err > plain).sum())
+    if not worst:
         out["all_within_test_bound"] = True
+        return out
+    tol = wl.get("sgf_tol", 1e-9)
+    run = (lambda d, e, t: O.transmission_dos(d, e, eta=wl["eta"], dos_delta=0.0, sgf_tol=t, nthreads=cores)[0]) \
+        if wl["dos"] else (lambda d, e, t: O.transmission(d, e, eta=wl["eta"], sgf_tol=t, nthreads=cores)[0])
+    rng = np.random.default_rng(0)
+    wq = np.asarray(worst)
+    spread = np.zeros(len(worst))
+    for _ in range(2):
+        for k in sorted(set(ids[wq].tolist())):          # one call per k-point, OpenMP over its points
+            j = np.nonzero(ids[wq] == k)[0]
+            d = copy.deepcopy(devs[k])
+            for name in ("h_diag", "h_upper", "h_lower", "s_diag", "s_upper", "s_lower", "lead_h00", "lead_h01",
+                         "lead_s00", "lead_s01", "hmc", "smc"):
+                lst = getattr(d, name)
+                if lst is None:
+                    continue
+                for i in range(len(lst)):
+                    lst[i] = lst[i] * (1.0 + 1e-15 * rng.standard_normal(lst[i].shape))
+            spread[j] = np.maximum(spread[j], np.abs(run(d, E[wq[j]], tol) - Tc[wq[j]]))
+    listed = spread > plain[wq] / 8
+    ok = [bool(listed[j] and err[q] <= max(plain[q], 10 * spread[j])) for j, q in enumerate(worst)]
+    out["beyond_1e-10_listed_by_oracle_spread"] = int(listed.sum())
+    out["listed_within_10x_spread"] = int(sum(ok))
+    # the four worst again at SGFACC = 1e-12, oracle and GPU
+    w4 = wq[:4]
+    recheck = []
+    if ctx is not None and dids is not None:
+        ctx.set_options(sgf_tol=1e-12)
+        try:
+            for q in w4:
+                k = int(ids[q])
+                tc12 = float(run(devs[k], E[q:q + 1], 1e-12)[0])
+                if wl["dos"]:
+                    tg12 = float(ctx.transmission_dos(dids[k], E[q:q + 1], eta=wl["eta"], dos_delta=0.0,
+                                                      check=False)[0][0])
+                else:
+                    tg12 = float(ctx.transmission(dids[k], E[q:q + 1], eta=wl["eta"], check=False)[0][0])
+                recheck.append({"E": float(E[q]), "T": float(Tc[q]), "abs_dT_at_sgf_tol": float(err[q]),
+                                "abs_dT_at_1e-12": abs(tg12 - tc12), "oracle_spread": float(spread[list(wq).index(q)])})
+        finally:
+            ctx.set_options(sgf_tol=tol)
+    out["worst_rechecked_at_sgfacc_1e-12"] = recheck
+    out["all_within_test_bound"] = bool(all(ok)) and len(worst) == out["beyond_1e-10"]
     return out
 
 
@@ -359,18 +406,24 @@ def run_serve(args):
     default command line runs a bounded slice of it so that the run ends in
     about a minute (the flags widen it).  Reported: served energy-point
     solves/s over the whole stream, p50 / p99 request latency."""
-    import torch
+    line = serve_stream(args.serve_rate, args.serve_seconds, [int(x) for x in args.serve_blocks.split(",")],
+                        tuple(int(x) for x in args.serve_layers.split(",")),
+                        tuple(int(x) for x in args.serve_grid.split(",")), args.serve_lanes, args.serve_policy)
+    print(json.dumps(line), flush=True)
+
+
+def serve_stream(rate, seconds, blocks, layers, grid, lanes, policy):
+    import torch  # noqa: F401
     from libnegf_b200 import generators as G
     from libnegf_b200.serve import Request, Server
     rng = np.random.default_rng(7)
-    blocks = [int(x) for x in args.serve_blocks.split(",")]
-    lo, hi = (int(x) for x in args.serve_layers.split(","))
-    g0, g1 = (int(x) for x in args.serve_grid.split(","))
+    lo, hi = layers
+    g0, g1 = grid
     t = 0.0
     plan = []
     while True:
-        t += rng.exponential(1.0 / args.serve_rate)
-        if t > args.serve_seconds:
+        t += rng.exponential(1.0 / rate)
+        if t > seconds:
             break
         n = int(rng.choice(blocks))
         nbl = int(rng.integers(lo, hi + 1))
@@ -378,7 +431,7 @@ def run_serve(args):
         kind = "ldos" if rng.random() < 0.3 else "T"
         gen = "c1" if rng.random() < 0.5 else "c0"
         plan.append((t, n, nbl, npts, kind, gen, int(rng.integers(1 << 30))))
-    srv = Server(lanes=args.serve_lanes, sgf_cache_bytes=1 << 30, policy=args.serve_policy)
+    srv = Server(lanes=lanes, sgf_cache_bytes=1 << 30, policy=policy)
     reqs = []
     with ClockSampler(0) as clk:
         t0 = time.perf_counter()
@@ -407,8 +460,8 @@ def run_serve(args):
         "vs_baseline": None, "dtype": "c128", "data": "synthetic",
         "config": {"workload": "serving stream: Poisson arrivals %.1f/s for %.0f s, blocks %s, layers %d-%d, "
                                "grids %d-%d log-uniform, 30%% LDOS requests, c0/c1 generators"
-                               % (args.serve_rate, args.serve_seconds, blocks, lo, hi, g0, g1),
-                   "lanes": args.serve_lanes, "policy": args.serve_policy, "eta": 1e-4,
+                               % (rate, seconds, blocks, lo, hi, g0, g1),
+                   "lanes": lanes, "policy": policy, "eta": 1e-4,
                    "precision": "complex FP64 (plain form)"},
         "latency_s": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
                       "p99": float(np.percentile(lat, 99)) if lat.size else None,
@@ -423,7 +476,93 @@ def run_serve(args):
                 "d2h_bytes_per_step": int(sum(r.T.nbytes + (r.ledos.nbytes if r.ledos is not None else 0)
                                               for r in reqs))},
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def c2_segments(local, peak, digits):
+    """Bounded segments of the block-512 workload (60 layers x 512 orbitals,
+    S = I + 0.05 R, eta = 1e-6) on one launch-sized batch of 296 points: 232
+    energies of the 1024-point grid over two of the 8 transverse k-points and
+    64 energies within 1e-3 eV of a lead band edge.  The plain FP64 form
+    (solves/s, fraction of the FP64 tensor peak under the reference flop
+    model) and the mixed form (int8 tensor-core products): solves/s, speed-up,
+    and its error against the plain FP64 GPU form on the same points."""
+    import torch
+    from libnegf_b200 import generators as G
+    from libnegf_b200 import native
+    wl = WORKLOADS["c2"]
+    L = native.load()
+    ks = [0.0, np.pi / wl["nk"]]
+    devs = G.transport_c1_kpoints(ks, nbl=wl["nbl"], n=wl["n"], seed=1)
+    grid = G.energy_grid(wl["emin"], wl["emax"], wl["nE"])
+    rng = np.random.default_rng(5)
+    g0, g1 = rng.choice(grid.size, 116, replace=False), rng.choice(grid.size, 116, replace=False)
+    edge = G.band_edge_energies(devs[0], contact=0, nk=64, n_edges=64, window=1e-3)[:64]
+    ids = np.concatenate([np.zeros(116), np.ones(116), np.zeros(edge.size)]).astype(np.int32)
+    E = np.concatenate([grid[g0], grid[g1], edge])
+    is_edge = np.concatenate([np.zeros(232, bool), np.ones(edge.size, bool)])
+    perm = rng.permutation(E.size)
+    ids, E, is_edge = ids[perm], E[perm], is_edge[perm]
+    P = E.size
+    out = {}
+    with native.Context(local) as ctx:
+        h = np.asarray([ctx.upload(d) for d in devs], dtype=np.int32)
+        d_ids = torch.from_numpy(h[ids]).cuda()
+        d_E = torch.from_numpy(E).cuda()
+        d_T = torch.zeros(P, dtype=torch.float64, device="cuda")
+        d_nc = torch.zeros(P, dtype=torch.int32, device="cuda")
+        d_st = torch.zeros(P, dtype=torch.int32, device="cuda")
+        stream = torch.cuda.Stream()
+        res = {}
+        for name, prec in (("plain", 0), ("mixed", digits)):
+            ctx.set_options(precision=prec)
+
+            def call():
+                rc = L.negf_b200_transmission_dev(ctx.handle, P, d_ids.data_ptr(), d_E.data_ptr(), wl["eta"], 1, 2,
+                                                  d_T.data_ptr(), d_nc.data_ptr(), d_st.data_ptr(),
+                                                  ctypes.c_void_p(stream.cuda_stream))
+                if rc != 0:
+                    raise RuntimeError("c2 %s solve failed: %d %s" % (name, rc, ctx.last_error()))
+            call()                        # warm-up (workspace, shared-memory opt-in)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with ClockSampler(local) as clk:
+                e0.record(stream)
+                call()
+                e1.record(stream)
+                torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1)
+            res[name] = (d_T.cpu().numpy().copy(), d_nc.cpu().numpy().copy(), d_st.cpu().numpy().copy(), ms,
+                         clk.summary())
+        ctx.set_options()
+    Tp, ncp, stp, msp, clkp = res["plain"]
+    Tm, ncm, stm, msm, clkm = res["mixed"]
+    flops = float(sum(flops_per_point(wl, int(c)) for c in ncp))
+    achieved = flops / (msp * 1e-3) / 1e12
+    out["c2_plain"] = {"solves_per_s": P / (msp * 1e-3), "ms": msp, "points": P, "achieved_tflops": achieved,
+                       "frac_of_fp64_peak": achieved / peak, "status_counts": _counts(stp), "clocks": clkp}
+    big = np.abs(Tp) > 1e-6
+    rel = np.abs(Tm - Tp) / np.where(big, np.abs(Tp), 1.0)
+    absd = np.abs(Tm - Tp)
+    out["c2_mixed"] = {
+        "solves_per_s": P / (msm * 1e-3), "ms": msm, "points": P, "digits": digits,
+        "speedup_vs_plain": msp / msm,
+        "error_vs_plain_fp64_gpu": {
+            "max_rel_T_gt_1e-6": float(rel[big].max()) if big.any() else None,
+            "mean_rel_T_gt_1e-6": float(rel[big].mean()) if big.any() else None,
+            "max_abs_T_le_1e-6": float(absd[~big].max()) if (~big).any() else None,
+            "beyond_1e-8": int(((rel > 1e-8) & big).sum() + ((absd > 1e-11) & ~big).sum()),
+            "band_edge_points": int(is_edge.sum()),
+            "band_edge_max_rel": float(rel[is_edge & big].max()) if (is_edge & big).any() else None},
+        "decimation_ncyc_equal_to_plain": int((ncm == ncp).sum()),
+        "status_counts": _counts(stm), "clocks": clkm,
+        "form": "every block product on the int8 tensor cores (Ozaki digits, exact int32 accumulation), "
+                "FP64 Gauss-Jordan inverses, FP64 decimation test and Caroli trace, all points in lock step"}
+    return out
+
+
+def _counts(st):
+    return {str(k): int(v) for k, v in zip(*np.unique(st, return_counts=True))}
 
 
 def run_reference(args, wl, rank, world):
@@ -463,14 +602,18 @@ def config_of(args, wl, pts):
                             "bias %g eV, %g K; Meir-Wingreen currents, layer currents and densities"
                             % (args.workload, wl["nbl"], wl["n"], wl["nE"], wl["emin"], wl["emax"], sc["coupling"],
                                sc["coupling"] ** 2, sc["bias"], sc["temp_k"]),
-                "points_per_step": pts, "eta": wl["eta"], "sgf_tol": 1e-9,
+                "points_per_step": pts, "eta": wl["eta"], "sgf_tol": wl.get("sgf_tol", 1e-9),
                 "scba_rule": ("linear mixing %g, stop when the contact-1 current changes by < %g, at most %d sweeps"
                               % (sc["mix"], sc["tol"], sc["niter"])) if sc["rule"] == 1 else
                              ("mixing %g, max|dGn| < %g, at most %d sweeps" % (sc["mix"], sc["tol"], sc["niter"])),
                 "l2": "inputs and workspace larger than L2 (126 MB)", "parallelism": "dp%d (E shards)" % args.gpus}
+    grid = wl["nE"] * wl["nk"]
     return {"workload": "transport_%s: N=%d PLs x n=%d, complex128, %d energies x %d k-points%s" % (
         args.workload, wl["nbl"], wl["n"], wl["nE"], wl["nk"], ", T(E,k) + diagonal DOS" if wl["dos"] else
-        ", T(E,k)"), "points_per_step": pts, "eta": wl["eta"], "sgf_tol": 1e-9,
+        ", T(E,k)"), "points_per_step": pts, "eta": wl["eta"], "sgf_tol": wl.get("sgf_tol", 1e-9),
+        "launches": "each step is one persistent launch of %d of the %d (E,k) points of the grid (energies and "
+                    "k-points mixed in every launch); the grid runs as %d such launches"
+                    % (pts, grid, -(-grid // pts)),
         "l2": "inputs and workspace larger than L2 (126 MB)", "parallelism": "dp%d (E,k shards)" % args.gpus}
 
 
@@ -506,6 +649,7 @@ def main():
     ids_r, E_r = ids_all[shard], E_all[shard]
 
     ctx = native.Context(local)
+    ctx.set_options(sgf_tol=wl.get("sgf_tol", 1e-9))
     dids = [ctx.upload(d) for d in devs]
     norb = devs[0].norb
     sms = torch.cuda.get_device_properties(local).multi_processor_count
@@ -526,7 +670,8 @@ def main():
     sc = wl.get("scba")
     nbl = devs[0].nbl
     if sc:
-        ctx.set_options(scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"], scba_rule=sc["rule"])
+        ctx.set_options(scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"], scba_rule=sc["rule"],
+                        sgf_tol=wl.get("sgf_tol", 1e-9))
         frm_run = scba_occupations(wl, E_run)
         cpl = np.full(norb, sc["coupling"])
         d_frm = torch.from_numpy(frm_run).cuda()
@@ -641,8 +786,9 @@ def main():
             "gpu_launches": args.steps,
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
-                         "traffic": DRAM_BYTES_PER_LAUNCH.get((args.workload, P)),
-                         "traffic_unit": "bytes per launch (one step)",
+                         "traffic": dram_bytes_per_launch(wl, P),
+                         "traffic_unit": "bytes per launch (one step), per-point model a + b N from two small-case "
+                                         "captures (prof4, prof), scaled by the launch's points",
                          "peak_source": "measured in-run: cuBLAS ZGEMM 4096^3 complex128 (FP64 DMMA pipe)",
                          "flop_model": "reference operation sequence, inverse = zgetrf+zgetrs 32/3 n^3",
                          "flops_per_step": flops / args.steps,
@@ -694,9 +840,20 @@ def main():
                 got = {"curr": curr_g[sel], "layer_dens": ldens_g[sel], "scba_iter": sweeps[sel]}
                 line["parity_sample"] = scba_parity_summary(wl, devs, ids_run[sel], E_run[sel], got, Tc, cores)
             else:
-                line["parity_sample"] = parity_summary(wl, devs, ids_run[sel], E_run[sel], Tgpu[sel], Tc, cores)
-        print(json.dumps(line), flush=True)
+                line["parity_sample"] = parity_summary(wl, devs, ids_run[sel], E_run[sel], Tgpu[sel], Tc, cores,
+                                                       ncyc_g=nc[sel], ncyc_c=cpu_baseline.last_ncyc, ctx=ctx,
+                                                       dids=dids)
     ctx.close()
+    if rank == 0:
+        if world == 1 and args.workload == "c1" and not args.no_extras:
+            # the rest of the metric on the same box and clock record: the block-512 plain and mixed
+            # forms, and a bounded serving stream over all five block sizes
+            line.update(c2_segments(local, peak, args.mixed_digits))
+            srv = serve_stream(1.0, 10.0, [16, 64, 128, 256, 512], (10, 40), (64, 512), 2, "fifo")
+            line["serve"] = {k: srv[k] for k in ("value", "unit", "latency_s", "requests", "rejected", "points",
+                                                 "status_counts", "clocks")}
+            line["serve"]["config"] = srv["config"]["workload"]
+        print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
 

@@ -49,3 +49,34 @@ def test_bad_arguments_are_rejected_without_gpu():
     assert L.negf_b200_ctx_create(0, None) == native.BAD_ARG
     assert L.negf_b200_zinv_batched(1, -1, None, None, None, None, None) == native.BAD_ARG
     assert L.negf_b200_decimation_batched(1, 4, None, None, None, None, None, -1.0, 10, None, None) == native.BAD_ARG
+
+
+def test_fortran_binding_covers_the_header():
+    """fortran/negf_b200_bind.F90 (uncompiled on this image) binds every
+    function the header declares, under the header's names, and nothing else
+    of this library; its derived types list the C structs' fields in order."""
+    src = open(os.path.join(ROOT, "fortran", "negf_b200_bind.F90")).read()
+    bound = set(re.findall(r"bind\(C,\s*name='(negf_b200_\w+)'\)", src))
+    assert bound == set(declared_symbols())
+    hdr = re.sub(r"/\*.*?\*/", "", open(os.path.join(ROOT, "include", "negf_b200.h")).read(), flags=re.S)
+    for cname, ftype in (("negf_b200_device", "negf_b200_device"), ("negf_b200_options", "negf_b200_options")):
+        body = re.search(r"typedef struct %s \{(.*?)\}" % cname, hdr, flags=re.S).group(1)
+        cfields = re.findall(r"(\w+)\s*;", body)
+        fbody = re.search(r"type, bind\(C\) :: %s(.*?)end type" % ftype, src, flags=re.S).group(1)
+        ffields = []
+        for line in fbody.splitlines():
+            if "::" in line:
+                ffields += [f.strip() for f in line.split("::")[1].split(",")]
+        assert ffields == cfields, (cname, ffields, cfields)
+
+
+def test_fortran_backend_exports_the_seam_names():
+    """fortran/iterative_b200.F90 exports the public names of libNEGF's GPU
+    RGF backend (src/iterative_gpu.F90:44-50) and the decimation seam."""
+    src = open(os.path.join(ROOT, "fortran", "iterative_b200.F90")).read()
+    public = set(re.findall(r"public :: (\w+)", src))
+    assert {"calculate_gsmr_blocks", "calculate_Gr_tridiag_blocks", "calculate_Gn_tridiag_blocks",
+            "calculate_single_transmission_2_contacts", "calculate_single_transmission_N_contacts",
+            "check_convergence_trid", "check_convergence_vec", "decimation_b200"} <= public
+    for name in public:
+        assert re.search(r"subroutine %s\(" % name, src), name
