@@ -802,6 +802,9 @@ def main():
         if sc:
             line["scba_sweeps_mean"] = float(sweeps[timed].mean())
             line["scba_sweeps_max"] = int(sweeps[timed].max())
+            # points that stopped at the sweep cap without meeting the current rule (linear mixing
+            # contracts slowly inside the bias window: the current still drifts by ~1e-2 per 40 sweeps)
+            line["scba_not_converged"] = int((sweeps[timed] > sc["niter"]).sum())
         if trace:
             line["trace_phase_share"] = trace
         if world == 1 and not args.no_cpu_baseline:

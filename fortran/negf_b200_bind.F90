@@ -17,6 +17,7 @@ module negf_b200_bind
     type(c_ptr) :: pl_size, h_diag, h_upper, h_lower, s_diag, s_upper, s_lower
     integer(c_int32_t) :: ncont
     type(c_ptr) :: cblk, lead_size, lead_h00, lead_h01, lead_s00, lead_s01, hmc, smc
+    type(c_ptr) :: surf_size, lead_hs, lead_ss
   end type
 
   ! negf_b200_options

@@ -70,6 +70,19 @@ extern "C" {
  *   lead_h01/s01 : contact PL1 -> PL2 coupling, L_c x L_c
  *   hmc/smc      : device block cblk[c] -> contact PL1, n_cblk x L_c
  *   lead_s00/lead_s01/smc NULL means identity / zero overlap.
+ * Bound surface layers (libNEGF's surfdim > 0, src/contselfenergy.F90:
+ * 150-156, 226-243): a contact may start with n0_c orbitals ahead of its
+ * periodic principal layers (Surf | PL1 | PL2).  Then
+ *   surf_size[c] : n0_c (surf_size NULL = no surface anywhere)
+ *   lead_hs/ss   : H and S over Surf followed by PL1, (n0_c + L_c)^2, for
+ *                  the contacts with n0_c > 0 only, concatenated in contact
+ *                  order (lead_ss NULL: S = I there); only the entries in a
+ *                  Surf row or column are used (the PL1 block is the lead's)
+ *   hmc/smc      : for such a contact n_cblk x (n0_c + L_c), device block
+ *                  cblk[c] -> Surf and PL1
+ * and the contact's surface Green's function is the inverse of
+ * [E S - H over Surf+PL1 with the PL1 block replaced by gs^-1], gs the
+ * decimation's (the bound-state block of surface_green).
  */
 typedef struct negf_b200_device {
   int32_t nbl;
@@ -89,6 +102,9 @@ typedef struct negf_b200_device {
   const double* lead_s01;
   const double* hmc;
   const double* smc;
+  const int32_t* surf_size;
+  const double* lead_hs;
+  const double* lead_ss;
 } negf_b200_device;
 
 /* ---- solver options ------------------------------------------------------

@@ -441,24 +441,35 @@ int upload_impl(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_
       no += (int64_t)pl[i] * pl[i + 1];
     }
   }
-  int64_t nl = 0, nm = 0;
-  std::vector<int64_t> olead(ncont), omc(ncont);
+  int64_t nl = 0, nm = 0, nsf = 0;
+  std::vector<int64_t> olead(ncont), omc(ncont), osurf(ncont, 0);
+  std::vector<int> surf(ncont, 0);
   for (int c = 0; c < ncont; ++c) {
     const int cb = dv->cblk[c], L = dv->lead_size[c];
     if (cb < 1 || cb > nbl || L < 1)
       return fail(ctx, NEGF_B200_ERR_BAD_ARG, "contact " + std::to_string(c + 1) + ": bad cblk or lead size");
-    nmax = std::max(nmax, L);
+    surf[c] = dv->surf_size ? dv->surf_size[c] : 0;
+    if (surf[c] < 0 || (surf[c] > 0 && !dv->lead_hs))
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "contact " + std::to_string(c + 1) + ": bad surface block");
+    const int ngs = L + surf[c];   // orbitals of the contact the device couples to (Surf + PL1)
+    nmax = std::max(nmax, ngs);
     olead[c] = nl;
     nl += (int64_t)L * L;
     omc[c] = nm;
-    nm += (int64_t)pl[cb - 1] * L;
+    nm += (int64_t)pl[cb - 1] * ngs;
+    if (surf[c] > 0) {
+      osurf[c] = nsf;
+      nsf += (int64_t)ngs * ngs;
+    }
   }
   if (nmax > negf::kMaxOrder)
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "block order above " + std::to_string(negf::kMaxOrder));
   // blob layout (complex elements): hd sd | hu hl su sl | h00 h01 s00 s01 | hmc smc | ints
   const int64_t ns = has_s ? 1 : 0;
   const int64_t has00 = dv->lead_s00 ? 1 : 0, has01 = dv->lead_s01 ? 1 : 0, hasmc = dv->smc ? 1 : 0;
-  int64_t elems = nd * (1 + ns) + no * (2 + 2 * ns) + nl * (2 + has00 + has01) + nm * (1 + hasmc);
+  const int64_t hasss = (nsf > 0 && dv->lead_ss) ? 1 : 0;
+  int64_t elems = nd * (1 + ns) + no * (2 + 2 * ns) + nl * (2 + has00 + has01) + nm * (1 + hasmc) +
+                  nsf * (1 + hasss);
   size_t bytes = (size_t)elems * 16 + (size_t)nbl * (4 + 4 + 8) + (size_t)std::max(1, nbl - 1) * 8 + 64;
   int st;
   if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
@@ -496,6 +507,9 @@ int upload_impl(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_
   d.s01 = has01 ? (const double2*)put(dv->lead_s01, nl * 16) : nullptr;
   d.hmc = (const double2*)put(dv->hmc, nm * 16);
   d.smc = hasmc ? (const double2*)put(dv->smc, nm * 16) : nullptr;
+  d.hs = nsf > 0 ? (const double2*)put(dv->lead_hs, nsf * 16) : nullptr;
+  d.ss = hasss ? (const double2*)put(dv->lead_ss, nsf * 16) : nullptr;
+  d.has_ss = (int)hasss;
   d.pl = (const int*)put(pl.data(), nbl * 4);
   d.pstart = (const int*)put(pstart.data(), nbl * 4);
   d.od = (const int64_t*)put(od.data(), nbl * 8);
@@ -505,6 +519,8 @@ int upload_impl(negf_b200_ctx* ctx, const negf_b200_device* dv, int32_t* device_
     d.L[c] = dv->lead_size[c];
     d.olead[c] = olead[c];
     d.omc[c] = omc[c];
+    d.surf[c] = surf[c];
+    d.osurf[c] = osurf[c];
   }
   if (perr != cudaSuccess || off > bytes) {
     cudaGetLastError();
@@ -961,6 +977,8 @@ static int run_mixed(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_ids, con
     if (left >= 0 && (l != left || rr != right))
       return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs the same contact order on every device");
     if (r.desc.tun_mask) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no tun_proj");
+    if (r.desc.surf[0] > 0 || r.desc.surf[1] > 0)
+      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no bound surface layers");
     left = l; right = rr;
   }
   int st = sync_descs(ctx);
@@ -1172,6 +1190,10 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
   for (int c = 0; c < r.ncont; ++c) nm += (int64_t)pl[r.desc.cblk[c] - 1] * r.desc.L[c];
   if (nm_out) *nm_out = nm;
   if (outer) outer->assign((size_t)(2 * nm), make_double2(0.0, 0.0));
+  if (outer)
+    for (int c = 0; c < r.ncont; ++c)
+      if (r.desc.surf[c] > 0)
+        return fail(ctx, NEGF_B200_ERR_BAD_ARG, "outer blocks of a contact with bound surface layers are not built");
   if (npts == 0) return NEGF_B200_OK;
   if (mode == negf::MODE_GN && r.nbl < 2) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the Gn solve needs nbl >= 2");
   std::vector<int32_t> ids(npts, device_id);

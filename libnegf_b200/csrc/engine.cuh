@@ -40,6 +40,12 @@ struct DevDesc {
   const int* ldos_ptr;             // [nldos+1] LDOS set k = ldos_idx[ldos_ptr[k] .. ldos_ptr[k+1])
   const int* ldos_idx;             // 1-based orbital indices
   int nldos, pad2;
+  // bound surface layers (surfdim, src/contselfenergy.F90:226-243): surf[c] orbitals
+  // ahead of the periodic PLs; H / S over Surf + PL1 at osurf[c] in hs / ss
+  int surf[kMaxCont];
+  int64_t osurf[kMaxCont];
+  const double2* hs; const double2* ss;
+  int has_ss, pad3;
 };
 
 struct EngineArgs {

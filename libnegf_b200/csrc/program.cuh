@@ -115,6 +115,7 @@ enum OpKind : int {
   K_TRDIAG,    // res[slot] = Re Tr A, order m
   K_LDOS,      // out[k] = sum over LDOS set k of dos[i-1] (A = dos row as doubles, device sets)
   K_ACCUM,     // C[q] += alpha * A[q], q < m (atomic: C is shared by all CTAs)
+  K_SUBCOPY,   // C(flag + r, flag + c) = A(r, c), A m x m, C leading dimension ldc
 };
 
 struct Op {
@@ -298,6 +299,12 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       }
       break;
     }
+    case K_SUBCOPY:
+      for (int q = tid; q < o.m * o.m; q += blockDim.x) {
+        const int r = q % o.m, c = q / o.m;
+        o.C[(int64_t)(o.flag + r) + (int64_t)(o.flag + c) * o.ldc] = o.A[q];
+      }
+      break;
     case K_ACCUM:
       for (int q = tid; q < o.m; q += blockDim.x) {
         const double2 v = cmul(o.alpha, o.A[q]);
@@ -482,6 +489,23 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           PT_EMIT(s);
         }
       sgf_ready:
+        if (s.d->surf[s.c] > 0) {
+          // bound-surface block of surface_green (src/contselfenergy.F90:226-243): GS is the
+          // inverse of E S - H over Surf + PL1 with the PL1 block replaced by gs^-1
+          o.kind = K_ZINV; o.m = s.L; o.A = w.slot(4); o.C = w.slot(5);
+          PT_EMIT(s);
+          if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          set_esh(o, w.slot(0), s.L + s.d->surf[s.c], s.L + s.d->surf[s.c], s.d->hs + s.d->osurf[s.c],
+                  s.d->has_ss ? s.d->ss + s.d->osurf[s.c] : nullptr, s.ecs, 1, nullptr, nullptr, OP_N);
+          PT_EMIT(s);
+          o.kind = K_SUBCOPY; o.m = s.L; o.ldc = s.L + s.d->surf[s.c]; o.flag = s.d->surf[s.c];
+          o.A = w.slot(5); o.C = w.slot(0);
+          PT_EMIT(s);
+          s.L += s.d->surf[s.c];
+          o.kind = K_ZINV; o.m = s.L; o.A = w.slot(0); o.C = w.slot(4);
+          PT_EMIT(s);
+          if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+        }
         if (a.acc_lc && (a.mode == MODE_RHO || a.mode == MODE_GN)) {
           set_simple(o, K_COPY, s.L * s.L, w.slot(4), a.mode == MODE_RHO ? w.gskeep(s.c) : w.gnkeep(s.c));
           PT_EMIT(s);

@@ -43,6 +43,9 @@ class NegfDeviceStruct(ctypes.Structure):
         ("lead_s01", c_double_p),
         ("hmc", c_double_p),
         ("smc", c_double_p),
+        ("surf_size", c_int32_p),
+        ("lead_hs", c_double_p),
+        ("lead_ss", c_double_p),
     ]
 
 
@@ -87,6 +90,12 @@ class Device:
     lead_s00: Optional[List[np.ndarray]] = None
     lead_s01: Optional[List[np.ndarray]] = None
     smc: Optional[List[np.ndarray]] = None
+    # bound surface layers (surfdim > 0): per contact n0 (0 = none) and, for
+    # n0 > 0, H / S over Surf + PL1 ((n0 + L) x (n0 + L)); hmc / smc of such a
+    # contact are n_cblk x (n0 + L)
+    surf_size: Optional[List[int]] = None
+    lead_hs: Optional[List[Optional[np.ndarray]]] = None
+    lead_ss: Optional[List[Optional[np.ndarray]]] = None
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -108,6 +117,9 @@ class Device:
     @property
     def lead_size(self) -> List[int]:
         return [b.shape[0] for b in self.lead_h00]
+
+    def surf(self, c: int) -> int:
+        return int(self.surf_size[c]) if self.surf_size is not None else 0
 
     def validate(self) -> None:
         n = self.pl_size
@@ -132,8 +144,14 @@ class Device:
             L = self.lead_h00[c].shape[0]
             if self.lead_h01[c].shape != (L, L):
                 raise ValueError("lead_h01[%d] must be %dx%d" % (c, L, L))
-            if self.hmc[c].shape != (n[cb - 1], L):
-                raise ValueError("hmc[%d] must be %dx%d" % (c, n[cb - 1], L))
+            ngs = L + self.surf(c)
+            if self.hmc[c].shape != (n[cb - 1], ngs):
+                raise ValueError("hmc[%d] must be %dx%d" % (c, n[cb - 1], ngs))
+            if self.surf(c) > 0:
+                if self.lead_hs is None or self.lead_hs[c] is None or self.lead_hs[c].shape != (ngs, ngs):
+                    raise ValueError("lead_hs[%d] must be %dx%d" % (c, ngs, ngs))
+                if self.lead_ss is not None and self.lead_ss[c] is not None and self.lead_ss[c].shape != (ngs, ngs):
+                    raise ValueError("lead_ss[%d] must be %dx%d" % (c, ngs, ngs))
 
     def to_struct(self) -> NegfDeviceStruct:
         """Packs the blocks; the returned struct references arrays kept alive
@@ -153,6 +171,13 @@ class Device:
                      "lead_h00", "lead_h01", "lead_s00", "lead_s01", "hmc", "smc"):
             arrs[name] = k(_pack(getattr(self, name))) if getattr(self, name) is not None else None
         st = NegfDeviceStruct()
+        if self.surf_size is not None and any(self.surf(c) > 0 for c in range(self.ncont)):
+            ss = k(np.ascontiguousarray([self.surf(c) for c in range(self.ncont)], dtype=np.int32))
+            st.surf_size = ss.ctypes.data_as(c_int32_p)
+            with_s = [c for c in range(self.ncont) if self.surf(c) > 0]
+            st.lead_hs = _ptr(k(_pack([self.lead_hs[c] for c in with_s])))
+            if self.lead_ss is not None and all(self.lead_ss[c] is not None for c in with_s):
+                st.lead_ss = _ptr(k(_pack([self.lead_ss[c] for c in with_s])))
         st.nbl = self.nbl
         st.pl_size = pl.ctypes.data_as(c_int32_p)
         st.ncont = self.ncont

@@ -261,3 +261,50 @@ def transport_c1_kpoints(kpoints: Sequence[float], nbl: int = 100, n: int = 256,
         out.append(Device(hd, hu, hl, list(cblk), lh00, lh01, hmc, s_diag=sd, s_upper=su, s_lower=sl,
                           lead_s00=ls00, lead_s01=ls01, smc=smc))
     return out
+
+
+def with_periodic_surface(dev: Device, contact: int, layers: int = 1) -> Device:
+    """The same device with `layers` principal layers of contact `contact`
+    moved into a bound surface block (surfdim = layers * L): the contact's
+    region becomes Surf | PL1 | PL2 with Surf made of periodic copies of the
+    lead PL.  The surface Green's function of Surf + PL1 then restricts to the
+    lead's own surface GF on Surf, so every result equals the original
+    device's (a known answer for the bound-surface block)."""
+    import copy
+    d = copy.deepcopy(dev)
+    c = contact
+    L = d.lead_h00[c].shape[0]
+    n0 = layers * L
+    ngs = n0 + L
+    H00, H01 = d.lead_h00[c], d.lead_h01[c]
+    S00 = None if d.lead_s00 is None else d.lead_s00[c]
+    S01 = None if d.lead_s01 is None else d.lead_s01[c]
+    nl = layers + 1   # surface layers + PL1
+    hs = np.zeros((ngs, ngs), np.complex128)
+    ss = np.zeros((ngs, ngs), np.complex128)
+    for k in range(nl):
+        sl = slice(k * L, (k + 1) * L)
+        hs[sl, sl] = H00
+        ss[sl, sl] = np.eye(L) if S00 is None else S00
+        if k + 1 < nl:
+            nx = slice((k + 1) * L, (k + 2) * L)
+            hs[sl, nx] = H01
+            hs[nx, sl] = H01.conj().T
+            if S01 is not None:
+                ss[sl, nx] = S01
+                ss[nx, sl] = S01.conj().T
+    hmc = np.zeros((d.hmc[c].shape[0], ngs), np.complex128)
+    hmc[:, :L] = d.hmc[c]
+    d.hmc[c] = hmc
+    if d.smc is not None:
+        smc = np.zeros_like(hmc)
+        smc[:, :L] = d.smc[c]
+        d.smc[c] = smc
+    d.surf_size = [0] * d.ncont if d.surf_size is None else list(d.surf_size)
+    d.surf_size[c] = n0
+    d.lead_hs = [None] * d.ncont if d.lead_hs is None else list(d.lead_hs)
+    d.lead_hs[c] = hs
+    if S00 is not None or S01 is not None:
+        d.lead_ss = [None] * d.ncont if d.lead_ss is None else list(d.lead_ss)
+        d.lead_ss[c] = ss
+    return d

@@ -38,9 +38,10 @@ def device_from_csr(H, S, plend: Sequence[int], cblk: Sequence[int], surfstart: 
     """Blocks of H (and S; None = identity, as negf_set_s_id) for the
     structure of negf_init_structure (1-based indices).  H and S may be
     scipy.sparse matrices or dense arrays over device + contact orbitals.
-    Surface blocks (surfend >= surfstart) are rejected: the bound-surface
-    correction of surface_green (src/contselfenergy.F90:226-243) is not
-    built."""
+    A contact with surface orbitals (surfend >= surfstart: libNEGF's
+    surfdim = surfend - surfstart + 1 > 0, Surf | PL1 | PL2) gets its bound
+    surface block (H and S over Surf + PL1, the block surface_green inverts,
+    src/contselfenergy.F90:226-243) and a coupling to Surf + PL1."""
     plend = [int(x) for x in plend]
     npl = len(plend)
     if npl < 1:
@@ -62,31 +63,39 @@ def device_from_csr(H, S, plend: Sequence[int], cblk: Sequence[int], surfstart: 
         sd = su = sl = None
     lh00, lh01, hmc = [], [], []
     ls00, ls01, smc = [], [], []
+    surf, lhs, lss = [], [], []
     for c in range(ncont):
         b0, c_start, c_end = int(surfstart[c]), int(surfend[c]) + 1, int(contend[c])
-        surfdim = c_start - b0
-        if surfdim != 0:
-            raise NotImplementedError("contact %d: surface blocks (surfdim = %d > 0) are not supported"
-                                      % (c + 1, surfdim))
-        ncdim = c_end - b0 + 1
-        if ncdim < 2 or ncdim % 2:
-            raise ValueError("contact %d: its two PLs must have equal size (dimension %d)" % (c + 1, ncdim))
-        L = ncdim // 2
-        j0 = b0 - 1                                 # 0-based first orbital of the contact
-        lh00.append(_dense(H, j0, j0 + L, j0, j0 + L))
-        lh01.append(_dense(H, j0, j0 + L, j0 + L, j0 + 2 * L))
+        n0 = c_start - b0                            # surfdim
+        if n0 < 0:
+            raise ValueError("contact %d: surfend < surfstart - 1" % (c + 1))
+        nd = c_end - c_start + 1                     # the two periodic PLs
+        if nd < 2 or nd % 2:
+            raise ValueError("contact %d: its two PLs must have equal size (dimension %d)" % (c + 1, nd))
+        L = nd // 2
+        j0 = b0 - 1                                  # 0-based first orbital of the contact (surface first)
+        p1 = j0 + n0                                 # 0-based first orbital of PL1
+        ngs = n0 + L
+        lh00.append(_dense(H, p1, p1 + L, p1, p1 + L))
+        lh01.append(_dense(H, p1, p1 + L, p1 + L, p1 + 2 * L))
         cb = int(cblk[c])
         if not 1 <= cb <= npl:
             raise ValueError("cblk[%d] = %d outside 1..%d" % (c, cb, npl))
-        hmc.append(_dense(H, starts[cb - 1], plend[cb - 1], j0, j0 + L))
+        hmc.append(_dense(H, starts[cb - 1], plend[cb - 1], j0, j0 + ngs))
+        surf.append(n0)
+        lhs.append(_dense(H, j0, j0 + ngs, j0, j0 + ngs) if n0 > 0 else None)
+        lss.append(_dense(S, j0, j0 + ngs, j0, j0 + ngs) if (n0 > 0 and S is not None) else None)
         if S is not None:
-            ls00.append(_dense(S, j0, j0 + L, j0, j0 + L))
-            ls01.append(_dense(S, j0, j0 + L, j0 + L, j0 + 2 * L))
-            smc.append(_dense(S, starts[cb - 1], plend[cb - 1], j0, j0 + L))
+            ls00.append(_dense(S, p1, p1 + L, p1, p1 + L))
+            ls01.append(_dense(S, p1, p1 + L, p1 + L, p1 + 2 * L))
+            smc.append(_dense(S, starts[cb - 1], plend[cb - 1], j0, j0 + ngs))
+    any_surf = any(n > 0 for n in surf)
     dev = Device(hd, hu, hl, [int(x) for x in cblk], lh00, lh01, hmc,
                  s_diag=sd, s_upper=su, s_lower=sl,
                  lead_s00=ls00 if S is not None else None, lead_s01=ls01 if S is not None else None,
-                 smc=smc if S is not None else None)
+                 smc=smc if S is not None else None,
+                 surf_size=surf if any_surf else None, lead_hs=lhs if any_surf else None,
+                 lead_ss=lss if (any_surf and S is not None) else None)
     dev.validate()
     return dev
 
@@ -127,7 +136,8 @@ def csr_from_device(dev: Device):
     plend = list(np.cumsum(n))
     starts = [0] + plend[:-1]
     L = dev.lead_size
-    ntot = norb + 2 * sum(L)
+    n0s = [dev.surf(c) for c in range(dev.ncont)]
+    ntot = norb + sum(2 * L[c] + n0s[c] for c in range(dev.ncont))
     H = sp.lil_matrix((ntot, ntot), dtype=np.complex128)
     S = sp.lil_matrix((ntot, ntot), dtype=np.complex128) if dev.s_diag is not None else None
     for i in range(dev.nbl):
@@ -143,27 +153,33 @@ def csr_from_device(dev: Device):
     surfstart, surfend, contend = [], [], []
     off = norb
     for c in range(dev.ncont):
-        l = L[c]
+        l, n0 = L[c], n0s[c]
         j0 = off
+        p1 = j0 + n0                                  # first orbital of PL1 (after the surface)
         surfstart.append(j0 + 1)
-        surfend.append(j0)
-        contend.append(j0 + 2 * l)
-        H[j0:j0 + l, j0:j0 + l] = dev.lead_h00[c]
-        H[j0 + l:j0 + 2 * l, j0 + l:j0 + 2 * l] = dev.lead_h00[c]
-        H[j0:j0 + l, j0 + l:j0 + 2 * l] = dev.lead_h01[c]
-        H[j0 + l:j0 + 2 * l, j0:j0 + l] = dev.lead_h01[c].conj().T
+        surfend.append(j0 + n0)
+        contend.append(j0 + n0 + 2 * l)
+        H[p1:p1 + l, p1:p1 + l] = dev.lead_h00[c]
+        H[p1 + l:p1 + 2 * l, p1 + l:p1 + 2 * l] = dev.lead_h00[c]
+        H[p1:p1 + l, p1 + l:p1 + 2 * l] = dev.lead_h01[c]
+        H[p1 + l:p1 + 2 * l, p1:p1 + l] = dev.lead_h01[c].conj().T
+        if n0 > 0:
+            H[j0:p1 + l, j0:p1 + l] = dev.lead_hs[c]
         cb = dev.cblk[c]
-        H[starts[cb - 1]:plend[cb - 1], j0:j0 + l] = dev.hmc[c]
-        H[j0:j0 + l, starts[cb - 1]:plend[cb - 1]] = dev.hmc[c].conj().T
+        H[starts[cb - 1]:plend[cb - 1], j0:p1 + l] = dev.hmc[c]
+        H[j0:p1 + l, starts[cb - 1]:plend[cb - 1]] = dev.hmc[c].conj().T
         if S is not None:
             s00 = dev.lead_s00[c] if dev.lead_s00 is not None else np.eye(l)
             s01 = dev.lead_s01[c] if dev.lead_s01 is not None else np.zeros((l, l))
-            smc = dev.smc[c] if dev.smc is not None else np.zeros((n[cb - 1], l))
-            S[j0:j0 + l, j0:j0 + l] = s00
-            S[j0 + l:j0 + 2 * l, j0 + l:j0 + 2 * l] = s00
-            S[j0:j0 + l, j0 + l:j0 + 2 * l] = s01
-            S[j0 + l:j0 + 2 * l, j0:j0 + l] = s01.conj().T
-            S[starts[cb - 1]:plend[cb - 1], j0:j0 + l] = smc
-            S[j0:j0 + l, starts[cb - 1]:plend[cb - 1]] = smc.conj().T
-        off += 2 * l
+            smc = dev.smc[c] if dev.smc is not None else np.zeros((n[cb - 1], n0 + l))
+            S[p1:p1 + l, p1:p1 + l] = s00
+            S[p1 + l:p1 + 2 * l, p1 + l:p1 + 2 * l] = s00
+            S[p1:p1 + l, p1 + l:p1 + 2 * l] = s01
+            S[p1 + l:p1 + 2 * l, p1:p1 + l] = s01.conj().T
+            if n0 > 0:
+                S[j0:p1 + l, j0:p1 + l] = (dev.lead_ss[c] if dev.lead_ss is not None and dev.lead_ss[c] is not None
+                                           else np.eye(n0 + l))
+            S[starts[cb - 1]:plend[cb - 1], j0:p1 + l] = smc
+            S[j0:p1 + l, starts[cb - 1]:plend[cb - 1]] = smc.conj().T
+        off += n0 + 2 * l
     return (H.tocsr(), S.tocsr() if S is not None else None, plend, list(dev.cblk), surfstart, surfend, contend)

@@ -169,6 +169,8 @@ struct DeviceBlocks {
   bool s_id = true;
   std::vector<int> cblk, L;
   std::vector<Dns> H00, H01, S00, S01, HMC, SMC;
+  std::vector<int> surf;          // bound surface orbitals per contact (surfdim)
+  std::vector<Dns> HS, SS;        // H, S over Surf + PL1 (surf > 0 only)
   int norb = 0;
   std::vector<int> start;       // 0-based start orbital of each PL
 };
@@ -199,12 +201,26 @@ DeviceBlocks unpack(const negf_b200_device* d) {
       oo += (size_t)ni * nj;
     }
   }
-  size_t ol = 0, om = 0;
+  size_t ol = 0, om = 0, os = 0;
   for (int c = 0; c < B.ncont; ++c) {
     int L = d->lead_size[c];
     int cb = d->cblk[c];
     B.cblk.push_back(cb);
     B.L.push_back(L);
+    const int n0 = d->surf_size ? d->surf_size[c] : 0;
+    B.surf.push_back(n0);
+    const int ngs = L + n0;
+    if (n0 > 0) {
+      B.HS.push_back(from_ptr(d->lead_hs + 2 * os, ngs, ngs));
+      Dns ss = from_ptr(d->lead_ss ? d->lead_ss + 2 * os : nullptr, ngs, ngs);
+      if (!d->lead_ss)
+        for (int i = 0; i < ngs; ++i) ss.at(i, i) = 1.0;
+      B.SS.push_back(ss);
+      os += (size_t)ngs * ngs;
+    } else {
+      B.HS.push_back(Dns());
+      B.SS.push_back(Dns());
+    }
     int ncb = B.n[cb - 1];
     B.H00.push_back(from_ptr(d->lead_h00 + 2 * ol, L, L));
     B.H01.push_back(from_ptr(d->lead_h01 + 2 * ol, L, L));
@@ -213,10 +229,10 @@ DeviceBlocks unpack(const negf_b200_device* d) {
       for (int i = 0; i < L; ++i) s00.at(i, i) = 1.0;
     B.S00.push_back(s00);
     B.S01.push_back(from_ptr(d->lead_s01 ? d->lead_s01 + 2 * ol : nullptr, L, L));
-    B.HMC.push_back(from_ptr(d->hmc + 2 * om, ncb, L));
-    B.SMC.push_back(from_ptr(d->smc ? d->smc + 2 * om : nullptr, ncb, L));
+    B.HMC.push_back(from_ptr(d->hmc + 2 * om, ncb, ngs));
+    B.SMC.push_back(from_ptr(d->smc ? d->smc + 2 * om : nullptr, ncb, ngs));
     ol += (size_t)L * L;
-    om += (size_t)ncb * L;
+    om += (size_t)ncb * ngs;
   }
   return B;
 }
@@ -258,7 +274,26 @@ void decimation(Dns& Go, Dns& Ao, Dns& Bo, Dns& Co, int n, int& ncyc,
   (void)n;
 }
 
-// surface_green, surfdim = 0, no cache (src/contselfenergy.F90:115-268)
+// The bound-surface block of surface_green (src/contselfenergy.F90:226-243):
+// with n0 surface orbitals ahead of the periodic PLs, GS (n0+L square) is
+// the inverse of E S - H over Surf + PL1 whose PL1 block is replaced by the
+// inverse of the decimation's Go.
+void bound_surface(cplx E, const DeviceBlocks& D, int c, Dns& GS, Err& err) {
+  const int n0 = D.surf[c];
+  if (n0 == 0) return;
+  const int L = D.L[c], ngs = n0 + L;
+  Dns Ginv;
+  zinv(Ginv, GS, err);
+  Dns gt;
+  gt.create(ngs, ngs);
+  for (size_t q = 0; q < gt.v.size(); ++q) gt.v[q] = E * D.SS[c].v[q] - D.HS[c].v[q];
+  for (int j = 0; j < L; ++j)
+    for (int i = 0; i < L; ++i) gt.at(n0 + i, n0 + j) = Ginv.at(i, j);
+  GS.destroy();
+  zinv(GS, gt, err);
+}
+
+// surface_green, no cache (src/contselfenergy.F90:115-268)
 void surface_green(cplx E, const DeviceBlocks& D, int c, Dns& GS, int& ncyc,
                    double sgf_acc, int max_iter, Err& err) {
   int L = D.L[c];
@@ -271,6 +306,7 @@ void surface_green(cplx E, const DeviceBlocks& D, int c, Dns& GS, int& ncyc,
   }
   dagger(Ct, Co);
   decimation(GS, Ao, Bo, Co, L, ncyc, sgf_acc, max_iter, err);
+  bound_surface(E, D, c, GS, err);
 }
 
 // compute_contacts_dns (src/contselfenergy.F90:445-491) + SelfEnergy_dns
@@ -1085,6 +1121,16 @@ double point(const DeviceBlocks& D, double E, double eta, double dos_delta, doub
     int nc = 0;
     Mat<R> GS = decimation(Ao, Bo, dag(Ct), (R)tol, max_iter, nc, info);
     ncyc += nc;
+    if (D.surf[c] > 0) {   // bound-surface block (src/contselfenergy.F90:226-243)
+      const int n0 = D.surf[c], ngs = n0 + L;
+      Mat<R> Ginv, gt(ngs, ngs);
+      if (invert(GS, Ginv)) info = 1;
+      const Mat<R> HS = from<R>(D.HS[c]), SS = from<R>(D.SS[c]);
+      for (size_t q = 0; q < gt.v.size(); ++q) gt.v[q] = sub(mul(Ec, SS.v[q]), HS.v[q]);
+      for (int j = 0; j < L; ++j)
+        for (int i = 0; i < L; ++i) gt.at(n0 + i, n0 + j) = Ginv.at(i, j);
+      if (invert(gt, GS)) info = 1;
+    }
     Mat<R> Tlc(HMC.nr, HMC.nc), TpMt(HMC.nr, HMC.nc), TG;
     for (size_t q = 0; q < HMC.v.size(); ++q) {
       Tlc.v[q] = sub(mul(Ec, SMC.v[q]), HMC.v[q]);

@@ -59,6 +59,12 @@ def contact_sigma(dev, c, Ec, tol=1e-9, max_iter=300):
     Bo = Ec * S01 - dev.lead_h01[c]
     Co = dag(np.conj(Ec) * S01 - dev.lead_h01[c])
     gs, ncyc = decimation(Ao, Bo, Co, tol, max_iter)
+    n0 = dev.surf(c)
+    if n0 > 0:   # bound-surface block (src/contselfenergy.F90:226-243)
+        SS = np.eye(n0 + L) if dev.lead_ss is None or dev.lead_ss[c] is None else dev.lead_ss[c]
+        gt = Ec * SS - dev.lead_hs[c]
+        gt[n0:, n0:] = inv(gs)
+        gs = inv(gt)
     SMC = np.zeros_like(dev.hmc[c]) if dev.smc is None else dev.smc[c]
     Tlc = Ec * SMC - dev.hmc[c]
     Tcl = dag(np.conj(Ec) * SMC - dev.hmc[c])

@@ -80,3 +80,37 @@ def test_decimation_iteration_cap(gpu_ctx):
     finally:
         gpu_ctx.set_options()
         gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("where", ["device", "lead"])
+def test_nonfinite_input_gives_a_status_not_a_trap(gpu_ctx, where):
+    """A NaN planted on the host in H (a device block, or a lead block) comes
+    back as a non-finite result with a non-zero per-point status for every
+    point, through the FP64 engine and the mixed form alike; the context
+    stays usable: a clean device solved right after matches the oracle.  The
+    reference has no such status (its GPU path sums |A| to look for NaN and
+    stops, src/gpuroutines.cu:697-739)."""
+    bad = G.transport_c0(nbl=4, n=128, seed=8)
+    if where == "device":
+        bad.h_diag[2][5, 7] = np.nan
+    else:
+        bad.lead_h00[0][3, 3] = np.nan
+    E = np.linspace(-1.5, 1.5, 6)
+    clean = G.transport_c0(nbl=4, n=128, seed=9)
+    b, c = gpu_ctx.upload(bad), gpu_ctx.upload(clean)
+    try:
+        for precision in (0, 8):
+            gpu_ctx.set_options(precision=precision)
+            T, nc, st = gpu_ctx.transmission(b, E, eta=1e-6, check=False)
+            assert np.all(st != 0), (precision, st)
+            assert not np.isfinite(T).all() or np.all(st == 3), (precision, T, st)
+            T2, nc2, st2 = gpu_ctx.transmission(c, E, eta=1e-6)
+            assert np.all(st2 == 0)
+            Tr, ncr, _ = O.transmission(clean, E, eta=1e-6)
+            assert np.array_equal(nc2, ncr)
+            assert np.all(np.abs(T2 - Tr) <= np.maximum(1e-8 * np.abs(Tr), 1e-11))
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(b)
+        gpu_ctx.release(c)

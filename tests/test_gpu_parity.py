@@ -378,3 +378,47 @@ def test_ladder_known_answer(gpu_ctx):
         assert np.abs(T - expect).max() < 1e-4
     finally:
         gpu_ctx.release(did)
+
+
+@pytest.mark.parametrize("gen", ["c0", "c1_S"])
+def test_bound_surface_parity(gpu_ctx, gen):
+    """Contacts with bound surface layers (surfdim > 0, the bound-state block
+    of surface_green, src/contselfenergy.F90:226-243): T and DOS against the
+    oracle at the strict rule; periodic surface layers give the plain device's
+    T; the mixed form declines them."""
+    dev0 = (G.transport_c0(nbl=5, n=16, seed=4) if gen == "c0"
+            else G.transport_c1(nbl=4, n=12, seed=4, density=0.3))
+    dev = G.with_periodic_surface(G.with_periodic_surface(dev0, 0, 1), 1, 2)
+    # an irregular surface too: perturb the surface-only entries so the answer is not the plain one
+    rng = np.random.default_rng(3)
+    n0 = dev.surf_size[0]
+    bump = 0.05 * (rng.standard_normal((n0, n0)) + 1j * rng.standard_normal((n0, n0)))
+    dev.lead_hs[0][:n0, :n0] += bump + bump.conj().T
+    E = np.linspace(-1.8, 1.8, 13)
+    did, d0 = gpu_ctx.upload(dev), gpu_ctx.upload(dev0)
+    try:
+        T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6)
+        ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev, nsamp=2)
+        assert np.all(st == ref["status"])
+        assert np.array_equal(ncyc, ref["ncyc"])
+        assert_T_strict(T, ref["T"], xp_reference(dev, E, 1e-6), spread=spread["T"], what="surface T")
+        Td, dos, ncd, std = gpu_ctx.transmission_dos(did, E, eta=1e-6, dos_delta=1e-4)
+        rd, sd = oracle_spread(_o_dos(E, eta=1e-6, dos_delta=1e-4), dev, nsamp=2)
+        assert np.array_equal(ncd, rd["ncyc"])
+        assert_parity(dos, rd["dos"], 1e-10 * max(np.abs(rd["dos"]).max(), 1.0), spread=sd["dos"], what="surface DOS")
+        # periodic surface layers: the plain device's T
+        per = gpu_ctx.upload(G.with_periodic_surface(dev0, 1, 1))
+        try:
+            Tp = gpu_ctx.transmission(per, E, eta=1e-4)[0]
+            T0 = gpu_ctx.transmission(d0, E, eta=1e-4)[0]
+            assert np.all(np.abs(Tp - T0) <= np.maximum(1e-10 * np.abs(T0), 1e-11))
+        finally:
+            gpu_ctx.release(per)
+        gpu_ctx.set_options(precision=8)
+        with pytest.raises(native.NegfError) as e:
+            gpu_ctx.transmission(did, E, eta=1e-6)
+        assert e.value.code == native.BAD_ARG
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
+        gpu_ctx.release(d0)

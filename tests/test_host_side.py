@@ -118,12 +118,30 @@ def test_upload_csr_matches_block_upload(gpu_ctx, case):
         gpu_ctx.release(d2)
 
 
-def test_csr_extraction_rejects_surface_blocks():
-    dev = G.transport_c0(nbl=3, n=4, seed=3)
+@pytest.mark.parametrize("gen", ["c0", "c1_S"])
+def test_bound_surface_known_answer(gen):
+    """surfdim > 0 (src/contselfenergy.F90:226-243): surface orbitals that are
+    periodic copies of the lead PL leave every result unchanged, through the
+    oracle, its long-double path and the NumPy twin; the CSR round trip with
+    surface orbitals (negf_init_structure's surfstart/surfend) is exact."""
+    from oracle import twin as TW
+    dev0 = (G.transport_c0(nbl=5, n=8, seed=4) if gen == "c0"
+            else G.transport_c1(nbl=4, n=10, seed=4, density=0.3))
+    dev = G.with_periodic_surface(G.with_periodic_surface(dev0, 0, 1), 1, 2)
+    assert dev.surf_size == [dev0.lead_size[0], 2 * dev0.lead_size[1]]
+    E = np.linspace(-1.5, 1.5, 9)
+    T0 = O.transmission(dev0, E, eta=1e-4)[0]
+    T, nc, st = O.transmission(dev, E, eta=1e-4)
+    assert np.all(st == 0)
+    assert np.all(np.abs(T - T0) <= np.maximum(1e-10 * np.abs(T0), 1e-11))
+    Tx = O.transmission_xp(dev, E, eta=1e-4)[0]
+    assert np.all(np.abs(Tx - T) <= np.maximum(1e-10 * np.abs(T), 1e-12))
+    Tt = np.array([TW.point_transmission(dev, e, eta=1e-4)[0] for e in E], dtype=float)
+    assert np.all(np.abs(Tt - T) <= np.maximum(1e-10 * np.abs(T), 1e-12))
     H, S, plend, cblk, ss, se, ce = St.csr_from_device(dev)
-    se = [s + 1 for s in ss]            # a one-orbital surface block
-    with pytest.raises(NotImplementedError):
-        St.device_from_csr(H, S, plend, cblk, ss, se, ce)
+    assert [e - s + 1 for s, e in zip(ss, se)] == dev.surf_size
+    back = St.device_from_csr(H, S, plend, cblk, ss, se, ce)
+    assert np.array_equal(O.transmission(back, E, eta=1e-4)[0], T)
 
 
 @pytest.mark.gpu
