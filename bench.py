@@ -50,6 +50,8 @@ WORKLOADS = {
     "prof4": dict(nbl=4, n=256, nE=256, emin=-2.0, emax=2.0, nk=1, eta=1e-6, dos=True, gen="c1"),
     # serving stream (Poisson arrivals of transmission / LDOS requests; see run_serve)
     "serve": dict(nbl=0, n=0, nE=0, emin=-2.0, emax=2.0, nk=1, eta=1e-4, dos=False, gen="serve"),
+    # block products alone (see run_gemm): order --gemm-n, --gemm-batch products per launch
+    "gemm": dict(nbl=0, n=0, nE=0, emin=0.0, emax=0.0, nk=1, eta=0.0, dos=False, gen="gemm"),
 }
 
 
@@ -77,6 +79,8 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the c2 plain / mixed and serving segments of the default line")
     p.add_argument("--mixed-digits", type=int, default=8, help="int8 digits of the mixed form (4..8)")
+    p.add_argument("--gemm-n", type=int, default=512, help="order of the products of --workload gemm")
+    p.add_argument("--gemm-batch", type=int, default=296, help="products per launch of --workload gemm")
     return p.parse_args()
 
 
@@ -102,8 +106,10 @@ def point_list(wl, seed=11):
 # launch per point, modelled as a + b N for a device of N layers of n = 256
 # (T + DOS), from one-pass ncu captures of two small cases of the same kernel
 # ("prof4": N = 4 and "prof": N = 8, 296 points each, a few GB on the device);
-# scaled to a launch by its points.  None until measured.
-DRAM_PER_POINT_MODEL = {256: None}
+# scaled to a launch by its points.  Measured on B200: prof4 1.2345e12 B,
+# prof 1.3457e12 B per launch -> a = 3.795e9 B (contacts: decimation and
+# self-energies), b = 9.40e7 B per layer.
+DRAM_PER_POINT_MODEL = {256: (3.795e9, 9.40e7)}
 
 
 def dram_bytes_per_launch(wl, points):
@@ -397,6 +403,94 @@ def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ct
     return out
 
 
+def ozaki_pairs(digits):
+    """Digit pairs (t, u) of the int8 product: t, u < digits, t + u < min(digits + 1, 8)."""
+    lv = min(digits + 1, 8)
+    return sum(1 for t in range(digits) for u in range(digits) if t + u < lv)
+
+
+def run_gemm(args, local):
+    """Block products alone: a batch of complex128 products C = A B of order
+    n on the integer tensor cores (negf_b200_zgemm_batched_i8: int8 digits,
+    tcgen05.mma kind::i8, exact int32 accumulation in tensor memory, FP64
+    recombination) beside the FP64 tensor-core product
+    (negf_b200_zgemm_batched, DMMA) on the same operands.  `value` is the
+    integer product's FP64-equivalent rate (8 n^3 flops per product); the
+    roofline counts its int8 operations (2 x 2 x pairs x n^2 x 2n per
+    product: real and imaginary part over the concatenated K, every kept
+    digit pair) against twice the measured dense bf16 rate (B200's dense
+    int8 rate is twice its bf16 rate).  Inputs (3 x batch x n^2 x 16 bytes)
+    exceed the L2 at the default sizes."""
+    import torch
+    from libnegf_b200 import native
+    torch.cuda.set_device(local)
+    L = native.load()
+    n, b, S = args.gemm_n, args.gemm_batch, args.mixed_digits
+    g = torch.Generator(device="cuda")
+    g.manual_seed(7)
+    A = torch.randn(b, n, n, dtype=torch.complex128, device="cuda", generator=g)
+    B = torch.randn(b, n, n, dtype=torch.complex128, device="cuda", generator=g)
+    C8 = torch.empty_like(A)
+    C64 = torch.empty_like(A)
+    work = torch.empty(L.negf_b200_zgemm_i8_work_bytes(b, n, n, n, S), dtype=torch.uint8, device="cuda")
+    st = torch.zeros(b, dtype=torch.int32, device="cuda")
+    one = (ctypes.c_double * 2)(1.0, 0.0)
+    zero = (ctypes.c_double * 2)(0.0, 0.0)
+    stream = torch.cuda.Stream()
+    sh = ctypes.c_void_p(stream.cuda_stream)
+    nn = 2 * n * n                      # product stride in doubles
+
+    def i8():
+        rc = L.negf_b200_zgemm_batched_i8(b, n, n, n, one, A.data_ptr(), nn, B.data_ptr(), nn, zero,
+                                          C8.data_ptr(), nn, S, work.data_ptr(), st.data_ptr(), sh)
+        if rc != 0:
+            raise RuntimeError("int8 product failed: %d" % rc)
+
+    def f64():
+        rc = L.negf_b200_zgemm_batched(b, n, n, n, one, A.data_ptr(), nn, B.data_ptr(), nn, zero,
+                                       C64.data_ptr(), nn, 0, sh)
+        if rc != 0:
+            raise RuntimeError("FP64 product failed: %d" % rc)
+
+    def timed(f, clocks=False):
+        for _ in range(args.warmup):
+            f()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            e0.record(stream)
+            for _ in range(args.steps):
+                f()
+            e1.record(stream)
+            torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, clk.summary()
+
+    ms8, clk = timed(i8)
+    ms64, clk64 = timed(f64)
+    assert int(st.abs().max()) == 0
+    err = float((C8 - C64).abs().max() / C64.abs().max())
+    ops = 2.0 * 2.0 * ozaki_pairs(S) * n * n * 2 * n * b
+    peak = 2.0 * json.load(open(os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                                             "MEASURED_PEAKS.json")))["bf16_tflops"]
+    achieved = ops / (ms8 * 1e-3) / 1e12
+    line = {"metric": "complex_product_fp64_equiv_tflops", "value": 8.0 * n ** 3 * b / (ms8 * 1e-3) / 1e12,
+            "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms8,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8 digits, c128 in/out",
+            "data": "synthetic", "clocks": clk,
+            "config": {"workload": "batched complex128 products C = A B, order %d, %d products per launch, "
+                                   "%d int8 digits (%d digit pairs); inputs larger than L2" % (n, b, S, ozaki_pairs(S)),
+                       "launches": "three per product: digit split of A, of B, the tcgen05 product kernel"},
+            "fp64_dmma": {"ms": ms64, "tflops": 8.0 * n ** 3 * b / (ms64 * 1e-3) / 1e12, "clocks": clk64},
+            "speedup_vs_fp64_dmma": ms64 / ms8,
+            "max_abs_diff_over_max_abs_c": err,
+            "gpu_launches": 3 * args.steps,
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOPS (int8)",
+                         "frac": achieved / peak, "traffic": None,
+                         "note": "whole call (split + product kernels) timed; peak = 2 x the measured dense "
+                                 "bf16 TFLOP/s"}}
+    print(json.dumps(line), flush=True)
+
+
 def run_serve(args):
     """Serving stream: requests arrive as a Poisson process; each draws a
     device from the c0 / c1 generators (layer count uniform in a range, block
@@ -630,6 +724,10 @@ def main():
         if rank == 0:
             run_serve(args)
         return
+    if wl["gen"] == "gemm":
+        if rank == 0:
+            run_gemm(args, local)
+        return
 
     import torch
     torch.cuda.set_device(local)
@@ -825,6 +923,7 @@ def main():
             sel = np.sort(np.asarray(picks[:nsamp], dtype=np.int64))
             nsamp = sel.size
             v, Tc, dt = cpu_baseline(wl, devs, ids_run[sel], E_run[sel], nsamp, cores)
+            ncyc_c = getattr(cpu_baseline, "last_ncyc", None)
             # one host core: one or two of the same points, single-threaded (SCBA: the point whose sweep
             # count on the GPU is closest to the sample's mean)
             n1 = 1 if sc else 2
@@ -844,7 +943,7 @@ def main():
                 line["parity_sample"] = scba_parity_summary(wl, devs, ids_run[sel], E_run[sel], got, Tc, cores)
             else:
                 line["parity_sample"] = parity_summary(wl, devs, ids_run[sel], E_run[sel], Tgpu[sel], Tc, cores,
-                                                       ncyc_g=nc[sel], ncyc_c=cpu_baseline.last_ncyc, ctx=ctx,
+                                                       ncyc_g=nc[sel], ncyc_c=ncyc_c, ctx=ctx,
                                                        dids=dids)
     ctx.close()
     if rank == 0:

@@ -412,8 +412,9 @@ int negf_b200_get_trace(negf_b200_ctx* ctx, uint64_t* cycles);
 
 /* ---- device-pointer primitives (mirror src/gpuroutines.cu) ---------------
  * All pointers are device pointers, `stream` is a cudaStream_t (NULL =
- * legacy default stream); `batch` independent problems with the given
- * element strides.  No allocation inside except where stated. */
+ * legacy default stream); `batch` independent problems, problem b of an
+ * operand starting b * stride doubles (2 per complex element) after its
+ * pointer.  No allocation inside except where stated. */
 
 /* C = alpha*op(A)*op(B) + beta*C, complex128.  dagger: 0 = (N,N),
  * 1 = (C,N), 2 = (N,C) -- the `dagger` argument of cu_ZmultMat
@@ -424,12 +425,6 @@ int negf_b200_zgemm_batched(int32_t batch, int32_t m, int32_t n, int32_t k,
                             const double* beta, double* C, int64_t strideC,
                             int32_t dagger, void* stream);
 
-/* Ainv = A^-1 (n x n) by Gauss-Jordan elimination with partial pivoting
- * (pivot = max |Re|+|Im|, the izamax rule of zgetrf).  Replaces cu_Zinverse
- * = cusolverDnZgetrf + Zgetrs against the identity (src/gpuroutines.cu:
- * 449-523) and zinv (src/inversions.F90:807-839).  `work` is a device buffer
- * of negf_b200_zinv_work_bytes(batch, n) bytes; info[b] = 0 or the 1-based
- * column of the first zero pivot. */
 /* C = alpha*A*B + beta*C, complex128, no transposes, on the integer tensor
  * cores: every row of A and column of B is scaled by a power of two and cut
  * into `slices` signed 7-bit digits (int8); the digit products accumulate
@@ -454,6 +449,12 @@ int negf_b200_zgemm_batched_i8(int32_t batch, int32_t m, int32_t n, int32_t k,
                                int32_t slices, void* work, int32_t* status,
                                void* stream);
 
+/* Ainv = A^-1 (n x n) by Gauss-Jordan elimination with partial pivoting
+ * (pivot = max |Re|+|Im|, the izamax rule of zgetrf).  Replaces cu_Zinverse
+ * = cusolverDnZgetrf + Zgetrs against the identity (src/gpuroutines.cu:
+ * 449-523) and zinv (src/inversions.F90:807-839).  `work` is a device buffer
+ * of negf_b200_zinv_work_bytes(batch, n) bytes; info[b] = 0 or the 1-based
+ * column of the first zero pivot. */
 size_t negf_b200_zinv_work_bytes(int32_t batch, int32_t n);
 int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A,
                            double* Ainv, int32_t* info, void* work,

@@ -65,7 +65,7 @@ def test_config_shape_transmission(gpu_ctx, fixture, shape):
             bound = 1e-10 * max(np.abs(ref).max(), 1.0)
             assert_parity(dos[:, ::DOS_STRIDE], ref, bound, ref_x=z[shape + "__dos_x"],
                           others=(z[shape + "__dos_d"], z[shape + "__dos_g"]), spread=z[shape + "__dos_s"],
-                          what=shape + " DOS")
+                          what=shape + " DOS", rows=True)
     finally:
         gpu_ctx.set_options()
         for h in handles:

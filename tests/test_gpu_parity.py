@@ -222,7 +222,8 @@ def test_transmission_dos_parity(gpu_ctx, case):
         # DOS: 1e-10 relative to the largest entry
         bound = 1e-10 * max(np.abs(ref["dos"]).max(), 1.0)
         assert_parity(dos, ref["dos"], bound, ref_x=None if x is None else x["dos_x"],
-                      others=() if x is None else (x["dos_d"], x["dos_g"]), spread=spread["dos"], what="DOS")
+                      others=() if x is None else (x["dos_d"], x["dos_g"]), spread=spread["dos"], what="DOS",
+                      rows=True)
     finally:
         gpu_ctx.release(did)
 
@@ -405,7 +406,8 @@ def test_bound_surface_parity(gpu_ctx, gen):
         Td, dos, ncd, std = gpu_ctx.transmission_dos(did, E, eta=1e-6, dos_delta=1e-4)
         rd, sd = oracle_spread(_o_dos(E, eta=1e-6, dos_delta=1e-4), dev, nsamp=2)
         assert np.array_equal(ncd, rd["ncyc"])
-        assert_parity(dos, rd["dos"], 1e-10 * max(np.abs(rd["dos"]).max(), 1.0), spread=sd["dos"], what="surface DOS")
+        assert_parity(dos, rd["dos"], 1e-10 * max(np.abs(rd["dos"]).max(), 1.0), spread=sd["dos"], what="surface DOS",
+                      rows=True)
         # periodic surface layers: the plain device's T
         per = gpu_ctx.upload(G.with_periodic_surface(dev0, 1, 1))
         try:
