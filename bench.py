@@ -79,6 +79,8 @@ def parse():
     p.add_argument("--no-extras", action="store_true",
                    help="skip the c2 plain / mixed and serving segments of the default line")
     p.add_argument("--mixed-digits", type=int, default=8, help="int8 digits of the mixed form (4..8)")
+    p.add_argument("--schedule", type=int, default=0, choices=[0, 1, 2],
+                   help="options.schedule: 0 auto (lock step for 2-contact T at n <= 32), 1 engine, 2 lock step")
     p.add_argument("--gemm-n", type=int, default=512, help="order of the products of --workload gemm")
     p.add_argument("--gemm-batch", type=int, default=296, help="products per launch of --workload gemm")
     return p.parse_args()
@@ -384,7 +386,7 @@ def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ct
     w4 = wq[:4]
     recheck = []
     if ctx is not None and dids is not None:
-        ctx.set_options(sgf_tol=1e-12)
+        ctx.update_options(sgf_tol=1e-12)
         try:
             for q in w4:
                 k = int(ids[q])
@@ -397,7 +399,7 @@ def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ct
                 recheck.append({"E": float(E[q]), "T": float(Tc[q]), "abs_dT_at_sgf_tol": float(err[q]),
                                 "abs_dT_at_1e-12": abs(tg12 - tc12), "oracle_spread": float(spread[list(wq).index(q)])})
         finally:
-            ctx.set_options(sgf_tol=tol)
+            ctx.update_options(sgf_tol=tol)
     out["worst_rechecked_at_sgfacc_1e-12"] = recheck
     out["all_within_test_bound"] = bool(all(ok)) and len(worst) == out["beyond_1e-10"]
     return out
@@ -705,10 +707,12 @@ def config_of(args, wl, pts):
     return {"workload": "transport_%s: N=%d PLs x n=%d, complex128, %d energies x %d k-points%s" % (
         args.workload, wl["nbl"], wl["n"], wl["nE"], wl["nk"], ", T(E,k) + diagonal DOS" if wl["dos"] else
         ", T(E,k)"), "points_per_step": pts, "eta": wl["eta"], "sgf_tol": wl.get("sgf_tol", 1e-9),
-        "launches": "each step is one persistent launch of %d of the %d (E,k) points of the grid (energies and "
-                    "k-points mixed in every launch); the grid runs as %d such launches"
+        "launches": "each step is one solve call on %d of the %d (E,k) points of the grid (energies and "
+                    "k-points mixed in every call); the grid runs as %d such calls"
                     % (pts, grid, -(-grid // pts)),
-        "l2": "inputs and workspace larger than L2 (126 MB)", "parallelism": "dp%d (E,k shards)" % args.gpus}
+        "l2": ("L2 flushed before every timed step (256 MB written, outside the step's events)" if wl["n"] <= 64
+               else "inputs and workspace larger than L2 (126 MB)"),
+        "parallelism": "dp%d (E,k shards)" % args.gpus}
 
 
 def main():
@@ -747,7 +751,7 @@ def main():
     ids_r, E_r = ids_all[shard], E_all[shard]
 
     ctx = native.Context(local)
-    ctx.set_options(sgf_tol=wl.get("sgf_tol", 1e-9))
+    ctx.set_options(sgf_tol=wl.get("sgf_tol", 1e-9), schedule=args.schedule)
     dids = [ctx.upload(d) for d in devs]
     norb = devs[0].norb
     sms = torch.cuda.get_device_properties(local).multi_processor_count
@@ -768,7 +772,7 @@ def main():
     sc = wl.get("scba")
     nbl = devs[0].nbl
     if sc:
-        ctx.set_options(scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"], scba_rule=sc["rule"],
+        ctx.update_options(scba_niter=sc["niter"], scba_tol=sc["tol"], scba_mix=sc["mix"], scba_rule=sc["rule"],
                         sgf_tol=wl.get("sgf_tol", 1e-9))
         frm_run = scba_occupations(wl, E_run)
         cpl = np.full(norb, sc["coupling"])
@@ -805,15 +809,24 @@ def main():
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    # small orders (c0): a step's device blocks and workspace can sit in the L2, so the L2 is flushed
+    # (256 MB written on the solve's stream) before every timed step, outside its events
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if wl["n"] <= 64 else None
+    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    nl0 = ctx.launch_count()
     with ClockSampler(local) as clk:
-        ev[0].record(stream)
         for j in range(args.steps):
+            if flush is not None:
+                with torch.cuda.stream(stream):
+                    flush.zero_()
+            ev0[j].record(stream)
             step(args.warmup + j)
-            ev[j + 1].record(stream)
+            ev1[j].record(stream)
         torch.cuda.synchronize()
-    per_step = [ev[j].elapsed_time(ev[j + 1]) for j in range(args.steps)]
-    ms = ev[0].elapsed_time(ev[-1])
+    gpu_launches = ctx.launch_count() - nl0
+    per_step = [ev0[j].elapsed_time(ev1[j]) for j in range(args.steps)]
+    ms = sum(per_step)
     if dist:
         ms = max_over_ranks(ms, dist)
         dist.barrier()
@@ -881,7 +894,10 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
             "config": config_of(args, wl, P),
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": args.steps,
+            "gpu_launches": gpu_launches,
+            "schedule": ("lock step: every point of a step through each batched block operation at once, one "
+                         "warp per point (n <= 32)") if gpu_launches > args.steps else
+                        "persistent engine: one launch per step, one CTA per point",
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
                          "traffic": dram_bytes_per_launch(wl, P),

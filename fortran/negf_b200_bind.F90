@@ -31,6 +31,7 @@ module negf_b200_bind
     integer(c_int32_t) :: ctas_per_sm
     real(c_double) :: scba_mix
     integer(c_int32_t) :: scba_rule
+    integer(c_int32_t) :: schedule
   end type
 
   interface
@@ -51,6 +52,9 @@ module negf_b200_bind
     end function
     function negf_b200_last_error(ctx) bind(C, name='negf_b200_last_error')
       import; type(c_ptr), value :: ctx; type(c_ptr) :: negf_b200_last_error
+    end function
+    integer(c_int) function negf_b200_launch_count(ctx, count) bind(C, name='negf_b200_launch_count')
+      import; type(c_ptr), value :: ctx; integer(c_int64_t) :: count
     end function
     integer(c_int) function negf_b200_upload_device(ctx, d, id) bind(C, name='negf_b200_upload_device')
       import; type(c_ptr), value :: ctx; type(negf_b200_device) :: d; integer(c_int32_t) :: id

@@ -144,6 +144,22 @@ typedef struct negf_b200_options {
    * between sweeps.  Neither alternative exists in the reference. */
   double scba_mix;
   int32_t scba_rule;
+  /* How the points of a 2-contact transmission solve (negf_b200_transmission,
+   * _dev; single pair, no SGF cache) are scheduled under precision = 0:
+   *   1 = the persistent engine: one CTA per point, its whole solve;
+   *   2 = lock step: every point of the call through the same block
+   *       operation at once, one warp per point and operation (orders
+   *       n <= 32; the call needs the shape rules of the mixed form);
+   *   0 (default) = lock step when the call's points all fit it and n <= 32
+   *       (for _dev calls: every device the context holds) and the stream is
+   *       not capturing, else the engine.
+   * Lock step synchronises its stream a few times per call (the
+   * decimation's active count is read back), so a captured call takes the
+   * engine (schedule 2 under capture: NEGF_B200_ERR_BAD_ARG).
+   * Both compute the reference's operation sequence in complex FP64; their
+   * last bits differ (summation order).  Under precision != 0 the mixed
+   * form runs in lock step whatever this says. */
+  int32_t schedule;
 } negf_b200_options;
 
 typedef struct negf_b200_ctx negf_b200_ctx;
@@ -161,6 +177,10 @@ int negf_b200_ctx_destroy(negf_b200_ctx* ctx);
 int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* opt);
 /* Last error message of this context (empty if none). */
 const char* negf_b200_last_error(const negf_b200_ctx* ctx);
+/* Kernels launched by this context's solve calls since it was created: one
+ * per persistent-engine call, one per batched block operation of lock step
+ * (three per product of the mixed form: two digit splits and the product). */
+int negf_b200_launch_count(negf_b200_ctx* ctx, uint64_t* count);
 
 /* Uploads a device description to HBM once (H/S blocks, contact blocks) and
  * returns a handle.  One description per k-point: libNEGF keeps one H(k),S(k)

@@ -11,8 +11,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libnegf_b200.so")
 SOURCES = [os.path.join(HERE, "csrc", f) for f in ("engine.cu", "program.cu", "capi.cu", "noalloc.cu", "gemm_dev.cu", "leaf_dev.cu",
-                                                     "csr.cu", "ozaki.cu", "mixed.cu")]
-DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cta_ops.cuh", "engine.cuh", "program.cuh", "ozaki.cuh", "mixed.cuh")] + [
+                                                     "csr.cu", "ozaki.cu", "mixed.cu", "small.cu")]
+DEPS = SOURCES + [os.path.join(HERE, "csrc", f) for f in ("cta_ops.cuh", "engine.cuh", "program.cuh", "ozaki.cuh", "mixed.cuh", "small.cuh")] + [
     os.path.join(ROOT, "include", "negf_b200.h")]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

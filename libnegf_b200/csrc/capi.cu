@@ -18,6 +18,7 @@
 #include "../../include/negf_b200.h"
 #include "engine.cuh"
 #include "mixed.cuh"
+#include "small.cuh"
 #include "ozaki.cuh"
 
 using negf::DevDesc;
@@ -115,6 +116,7 @@ struct negf_b200_ctx {
   unsigned long long* d_trace = nullptr;
   SgfCache sgf;
   size_t ws_limit = 0;   // 0 = none
+  uint64_t launches = 0; // kernels launched by solve calls (negf_b200_launch_count)
   std::mutex mu;
 };
 
@@ -231,6 +233,7 @@ int run_device(negf_b200_ctx* ctx, negf::EngineArgs a, const LaunchShape& sh, cu
   CK(cudaMemsetAsync(a.counter, 0, sizeof(int), s));
   cudaError_t e = negf::launch_engine(a, grid, s);
   if (e != cudaSuccess) return cuda_fail(ctx, e, "launch_engine");
+  ++ctx->launches;
   return NEGF_B200_OK;
 }
 
@@ -352,6 +355,7 @@ void negf_b200_default_options(negf_b200_options* o) {
   o->ctas_per_sm = 0;
   o->scba_mix = 1.0;
   o->scba_rule = 0;
+  o->schedule = 0;
 }
 
 const char* negf_b200_version(void) { return "negf_b200 0.1 (sm_100a, complex FP64)"; }
@@ -406,11 +410,20 @@ int negf_b200_set_options(negf_b200_ctx* ctx, const negf_b200_options* o) {
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "precision must be 0 (FP64), 1 or 4..8 (int8 digits of the mixed form)");
   if (!(o->scba_mix > 0.0 && o->scba_mix <= 1.0) || (o->scba_rule != 0 && o->scba_rule != 1))
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "scba_mix must be in (0, 1] and scba_rule 0 or 1");
+  if (o->schedule < 0 || o->schedule > 2)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG, "schedule must be 0 (auto), 1 (engine) or 2 (lock step)");
   ctx->opt = *o;
   return NEGF_B200_OK;
 }
 
 const char* negf_b200_last_error(const negf_b200_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int negf_b200_launch_count(negf_b200_ctx* ctx, uint64_t* count) {
+  if (!ctx || !count) return NEGF_B200_ERR_BAD_ARG;
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  *count = ctx->launches;
+  return NEGF_B200_OK;
+}
 
 namespace {
 // The block arrays of `dv` may be host or device memory (copies with
@@ -937,56 +950,121 @@ static int check_pairs(negf_b200_ctx* ctx, int npts, const int32_t* ids, int npa
   return NEGF_B200_OK;
 }
 
-// The mixed-precision form (options.precision != 0) for 2-contact transmission
-// solves: checks that every point's device fits it, sizes the batch to the
-// workspace and runs negf::mixed_run on device arrays of ids and energies.
+// The lock-step forms of 2-contact transmission solves (negf::mixed_run):
+// the mixed-precision form (options.precision != 0: int8 tensor-core
+// products) and the small-order FP64 form (precision 0, n <= 32, by
+// options.schedule).  Both need one shape for every point of a call.
 static int mixed_slices(const negf_b200_ctx* ctx) { return ctx->opt.precision == 1 ? 8 : ctx->opt.precision; }
 
-static int run_mixed(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_ids, const int32_t* d_ids, const double* d_E,
-                     double eta, double* d_T, int32_t* d_ncyc, int32_t* d_status, cudaStream_t s) {
-  // shape: from the host ids when given, else from the devices the context holds
+struct LockShape {
+  int n = 0, nbl = 0, left = -1, right = -1;
+};
+
+// Whether the points (host ids; null: every device the context holds) fit
+// the lock-step forms: 2 contacts on blocks 1 and nbl in the same order, one
+// PL size n for all layers and both leads, the same nbl, no tun_proj, no
+// bound surface layers.  The reason in *why when not.
+static bool lockstep_shape(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_ids, LockShape* sh, std::string* why,
+                           bool* bad_id) {
+  *bad_id = false;
   std::vector<int> used;
   if (h_ids) {
     std::vector<char> seen(ctx->devs.size(), 0);
     for (int p = 0; p < npts; ++p) {
-      if (h_ids[p] < 0 || h_ids[p] >= (int)ctx->devs.size() || !ctx->devs[h_ids[p]].live)
-        return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
+      if (h_ids[p] < 0 || h_ids[p] >= (int)ctx->devs.size() || !ctx->devs[h_ids[p]].live) {
+        *bad_id = true;
+        *why = "unknown device id";
+        return false;
+      }
       if (!seen[h_ids[p]]) { seen[h_ids[p]] = 1; used.push_back(h_ids[p]); }
     }
   } else {
     for (int i = 0; i < (int)ctx->devs.size(); ++i)
       if (ctx->devs[i].live) used.push_back(i);
   }
-  if (used.empty()) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "no device");
+  if (used.empty()) { *why = "a device"; return false; }
   const DeviceRec& r0 = ctx->devs[used[0]];
   const int n = r0.nmax, nbl = r0.nbl;
   int left = -1, right = -1;
   for (int id : used) {
     const DeviceRec& r = ctx->devs[id];
-    if (r.ncont != 2 || r.nbl < 2 || r.nbl != nbl || r.nmax != n || r.norb != nbl * n)
-      return fail(ctx, NEGF_B200_ERR_BAD_ARG,
-                  "the mixed form needs 2 contacts and one PL size n for all layers of every point's device");
+    if (r.ncont != 2 || r.nbl < 2 || r.nbl != nbl || r.nmax != n || r.norb != nbl * n) {
+      *why = "2 contacts and one PL size n for all layers of every point's device";
+      return false;
+    }
     int l = -1, rr = -1;
     for (int c = 0; c < 2; ++c) {
-      if (r.desc.L[c] != n) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs lead PL size = n");
+      if (r.desc.L[c] != n) { *why = "lead PL size = n"; return false; }
       if (r.cblk[c] == 1) l = c;
       if (r.cblk[c] == nbl) rr = c;
     }
-    if (l < 0 || rr < 0 || l == rr)
-      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs the contacts on blocks 1 and nbl");
-    if (left >= 0 && (l != left || rr != right))
-      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form needs the same contact order on every device");
-    if (r.desc.tun_mask) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no tun_proj");
-    if (r.desc.surf[0] > 0 || r.desc.surf[1] > 0)
-      return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no bound surface layers");
+    if (l < 0 || rr < 0 || l == rr) { *why = "the contacts on blocks 1 and nbl"; return false; }
+    if (left >= 0 && (l != left || rr != right)) { *why = "the same contact order on every device"; return false; }
+    if (r.desc.tun_mask) { *why = "no tun_proj"; return false; }
+    if (r.desc.surf[0] > 0 || r.desc.surf[1] > 0) { *why = "no bound surface layers"; return false; }
     left = l; right = rr;
   }
+  sh->n = n; sh->nbl = nbl; sh->left = left; sh->right = right;
+  return true;
+}
+
+// Decides how a 2-contact transmission call runs: returns true when a
+// lock-step form takes it (*slices = the int8 digits, 0 = the small-order
+// FP64 form) or when the call must fail (*st set); false for the engine.
+static bool lockstep_choice(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_ids, bool single_pair, LockShape* sh,
+                            int* slices, int* st, cudaStream_t stream) {
+  *st = NEGF_B200_OK;
+  const bool mixed = ctx->opt.precision != 0;
+  if (!mixed && ctx->opt.schedule == 1) return false;
+  const bool forced = mixed || ctx->opt.schedule == 2;
+  const char* form = mixed ? "the mixed form (precision != 0)" : "lock step (schedule 2)";
+  // lock step reads the decimation's active count back to the host, which a
+  // stream capture cannot hold: the engine takes captured calls
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) {
+    cudaGetLastError();
+    cap = cudaStreamCaptureStatusNone;
+  }
+  if (cap != cudaStreamCaptureStatusNone) {
+    if (!forced) return false;
+    *st = fail(ctx, NEGF_B200_ERR_BAD_ARG, std::string(form) + " cannot run under stream capture");
+    return true;
+  }
+  if (!single_pair || ctx->sgf.mode) {
+    if (!forced) return false;
+    *st = fail(ctx, NEGF_B200_ERR_BAD_ARG,
+               std::string(form) + " covers single-pair transmission solves without the SGF cache");
+    return true;
+  }
+  std::string why;
+  bool bad_id = false;
+  bool ok = lockstep_shape(ctx, npts, h_ids, sh, &why, &bad_id);
+  if (ok && !mixed && sh->n > negf::kSmallMax) {
+    ok = false;
+    why = "orders n <= 32";
+  }
+  if (!ok && (forced || bad_id)) {
+    *st = fail(ctx, NEGF_B200_ERR_BAD_ARG, bad_id ? why : std::string(form) + " needs " + why);
+    return true;
+  }
+  if (!ok) return false;
+  *slices = mixed ? mixed_slices(ctx) : 0;
+  return true;
+}
+
+// Runs a lock-step form on device arrays of ids and energies: sizes the batch
+// to the workspace and calls negf::mixed_run.
+static int run_lockstep(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_ids, const double* d_E, double eta,
+                        double* d_T, int32_t* d_ncyc, int32_t* d_status, cudaStream_t s, const LockShape& sh,
+                        int slices) {
   int st = sync_descs(ctx);
   if (st) return st;
-  const int slices = mixed_slices(ctx);
-  int batch = std::min<int>(npts, 2 * std::max(ctx->sms, 1) + 216);   // 512 on a B200
+  const int n = sh.n;
+  // the mixed form: two waves of resident Ozaki tiles plus a margin (512 on a
+  // B200); the small form: the whole call at once up to 8192 points
+  int batch = std::min<int>(npts, slices ? 2 * std::max(ctx->sms, 1) + 216 : 8192);
   if (ctx->ws_limit) batch = std::min(batch, negf::mixed_batch_for(ctx->ws_limit, n, slices));
-  if (batch < 1) return fail(ctx, NEGF_B200_ERR_ADMISSION, "the workspace limit is below one point of the mixed form");
+  if (batch < 1) return fail(ctx, NEGF_B200_ERR_ADMISSION, "the workspace limit is below one point of lock step");
   for (;;) {
     st = grow(ctx, &ctx->ws, &ctx->ws_bytes, negf::mixed_ws_bytes(batch, n, slices));
     if (st == NEGF_B200_OK) break;
@@ -995,12 +1073,13 @@ static int run_mixed(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_ids, con
   }
   negf::MixedArgs a;
   a.npts = npts; a.d_ids = d_ids; a.d_E = d_E; a.eta = eta; a.d_descs = ctx->d_descs;
-  a.n = n; a.nbl = nbl; a.left = left; a.right = right;
+  a.n = n; a.nbl = sh.nbl; a.left = sh.left; a.right = sh.right;
   a.sgf_tol = ctx->opt.sgf_tol; a.sgf_max_iter = ctx->opt.sgf_max_iter; a.slices = slices;
   a.d_T = d_T; a.d_ncyc = d_ncyc; a.d_status = d_status;
+  a.launches = &ctx->launches;
   std::string msg;
   st = negf::mixed_run(a, ctx->ws, batch, s, &msg);
-  if (st) return fail(ctx, st, "mixed form: " + msg);
+  if (st) return fail(ctx, st, (slices ? "mixed form: " : "lock step: ") + msg);
   return NEGF_B200_OK;
 }
 
@@ -1089,11 +1168,14 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
     CK(cudaMemcpyAsync(d_sgf_in, sgf_in.data(), sgf_in.size() * 8, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(d_sgf_out, sgf_out.data(), sgf_out.size() * 8, cudaMemcpyHostToDevice, s));
   }
-  if (ctx->opt.precision != 0) {
-    if (mode != negf::MODE_T || npairs > 1 || ctx->sgf.mode)
-      return fail(ctx, NEGF_B200_ERR_BAD_ARG,
-                  "the mixed form (precision != 0) covers single-pair transmission solves without the SGF cache");
-    st = run_mixed(ctx, npts, ids, d_ids, d_E, eta, d_T, d_ncyc, d_st, s);
+  LockShape lsh;
+  int lslices = 0;
+  if (mode != negf::MODE_T && ctx->opt.precision != 0)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG,
+                "the mixed form (precision != 0) covers single-pair transmission solves without the SGF cache");
+  if (mode == negf::MODE_T && lockstep_choice(ctx, npts, ids, npairs == 1, &lsh, &lslices, &st, s)) {
+    if (st) return st;
+    st = run_lockstep(ctx, npts, d_ids, d_E, eta, d_T, d_ncyc, d_st, s, lsh, lslices);
     if (st) return st;
     std::vector<int32_t> hst(npts);
     if (T) CK(cudaMemcpyAsync(T, d_T, (size_t)npts * 8, cudaMemcpyDeviceToHost, s));
@@ -1400,10 +1482,14 @@ int negf_b200_transmission_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t* 
   if (npts == 0) return NEGF_B200_OK;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
-  if (ctx->opt.precision != 0) {
-    if (ctx->sgf.mode) return fail(ctx, NEGF_B200_ERR_BAD_ARG, "the mixed form has no SGF cache");
-    return run_mixed(ctx, npts, nullptr, d_device_id, d_energy, eta, d_T, d_ncyc, d_status,
-                     stream ? (cudaStream_t)stream : ctx->stream);
+  {
+    LockShape lsh;
+    int lslices = 0, lst = 0;
+    const cudaStream_t ls = stream ? (cudaStream_t)stream : ctx->stream;
+    if (lockstep_choice(ctx, npts, nullptr, true, &lsh, &lslices, &lst, ls)) {
+      if (lst) return lst;
+      return run_lockstep(ctx, npts, d_device_id, d_energy, eta, d_T, d_ncyc, d_status, ls, lsh, lslices);
+    }
   }
   LaunchShape sh;
   int st = shape_of(ctx, npts, nullptr, sh);

@@ -23,6 +23,7 @@
 #include "../../include/negf_b200.h"
 #include "mixed.cuh"
 #include "ozaki.cuh"
+#include "small.cuh"
 
 namespace negf {
 namespace {
@@ -63,8 +64,11 @@ __global__ void k_lead_init(int n, int c, const int* ids, const double* E, doubl
   }
 }
 
-// Ao -= Self, Aos -= Self for the points of the list
-__global__ void k_sub_self(int64_t nn, const int* list, const double2* Self, double2* Ao, double2* Aos, int64_t Q) {
+// Ao -= Self, Aos -= Self for the points of the list (its first *count
+// entries when count is given)
+__global__ void k_sub_self(int64_t nn, const int* list, const int* count, const double2* Self, double2* Ao,
+                           double2* Aos, int64_t Q) {
+  if (count && (int)blockIdx.y >= *count) return;
   const int p = list[blockIdx.y];
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
     const double2 s = Self[p * Q + q];
@@ -78,10 +82,12 @@ __global__ void k_sub_self(int64_t nn, const int* list, const double2* Self, dou
 
 // The CPU convergence rule (src/contselfenergy.F90:300-310): a point is done
 // on its second consecutive max|C1| <= tol.  Builds the list of the points
-// that go on (and zeroes their max for the next iteration).  One CTA.
-__global__ void k_dec_check(int na, const int* list, double* mx, int* ok, int* ncyc_c, double tol, int it,
-                            int* next, int* next_count) {
+// that go on (and zeroes their max for the next iteration).  One CTA.  The
+// list's length is na, or *count when count is given.
+__global__ void k_dec_check(int na, const int* count, const int* list, double* mx, int* ok, int* ncyc_c, double tol,
+                            int it, int* next, int* next_count) {
   __shared__ int cnt;
+  if (count) na = *count;
   if (threadIdx.x == 0) cnt = 0;
   __syncthreads();
   for (int b = threadIdx.x; b < na; b += blockDim.x) {
@@ -106,7 +112,8 @@ __global__ void k_dec_check(int na, const int* list, double* mx, int* ok, int* n
   if (threadIdx.x == 0) *next_count = cnt;
 }
 
-__global__ void k_info_to_status(int nb, const int* list, const int* info, int* status, int code) {
+__global__ void k_info_to_status(int nb, const int* count, const int* list, const int* info, int* status, int code) {
+  if (count) nb = min(nb, *count);
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nb; b += gridDim.x * blockDim.x) {
     const int p = list ? list[b] : b;
     if (info[p] != 0 && status[p] == 0) status[p] = code;
@@ -212,8 +219,9 @@ __global__ void k_trace(int n, const double2* Gam, const double2* G, const doubl
   }
 }
 
-__global__ void k_iota(int n, int* v) {
+__global__ void k_iota(int n, int* v, int* count) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) v[b] = b;
+  if (count && blockIdx.x == 0 && threadIdx.x == 0) *count = n;
 }
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
@@ -253,8 +261,9 @@ Ws carve(void* base, int P, int n, int slices, size_t* total) {
   w.info = c.take<int>(P);
   w.pst = c.take<int>(P);
   w.tb = c.take<double>(P);
-  w.zwork = c.take<double2>((size_t)P * zinv_batched_work_elems(n) + 1);
-  w.oz = c.take<uint8_t>(ozaki_layout(P, n, n, n, slices).total);
+  const bool small = slices == 0;        // the lock-step FP64 form: one-warp kernels, no splitting
+  w.zwork = c.take<double2>(small ? 1 : (size_t)P * zinv_batched_work_elems(n) + 1);
+  w.oz = small ? nullptr : c.take<uint8_t>(ozaki_layout(P, n, n, n, slices).total);
   *total = c.off + 256;
   return w;
 }
@@ -264,11 +273,13 @@ __global__ void k_finish(int P, const int* ncl, const int* ncr, const int* pst, 
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x) {
     T[p] = Tb[p];
     if (ncyc) ncyc[p] = ncl[p] + ncr[p];
-    if (status) status[p] = pst[p];
+    // a non-finite T that no step flagged (NaN in the device blocks) is reported as such
+    if (status) status[p] = (pst[p] == 0 && !isfinite(Tb[p])) ? NEGF_B200_ERR_NONFINITE : pst[p];
   }
 }
 
-__global__ void k_not_converged(int na, const int* list, int* ncyc_c, int* pst, int max_iter) {
+__global__ void k_not_converged(int na, const int* count, const int* list, int* ncyc_c, int* pst, int max_iter) {
+  if (count) na = min(na, *count);
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < na; b += gridDim.x * blockDim.x) {
     const int p = list[b];
     ncyc_c[p] = max_iter + 1;
@@ -297,6 +308,7 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
   const int n = a.n;
   const int64_t Q = (int64_t)n * n;
   const double2 one = make_double2(1, 0), zero = make_double2(0, 0), mone = make_double2(-1, 0);
+  const bool small = a.slices == 0;
   size_t tot = 0;
   Ws w = carve(ws, batch, n, a.slices, &tot);
   double2** B = w.blk;
@@ -312,10 +324,32 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
     int r_ = ck((x), what);      \
     if (r_) return r_;           \
   } while (0)
-  auto prod = [&](int nb, const int* map, double2 alpha, const double2* A, const double2* Bm, double2 beta,
-                  double2* C, double* maxabs) -> cudaError_t {
+  // products and inverses of the problems map[b], b < nb (or b < *count)
+  uint64_t nl = 0;                 // kernels launched (reported through a.launches)
+  auto prod = [&](int nb, const int* map, const int* count, double2 alpha, const double2* A, const double2* Bm,
+                  double2 beta, double2* C, double* maxabs) -> cudaError_t {
+    if (small) {
+      ++nl;
+      return launch_small_zgemm(nb, n, alpha, A, Bm, beta, C, Q, map, count, maxabs, s);
+    }
+    nl += 3;                       // digit split of A, of B, the product
     return launch_ozaki_zgemm(nb, n, n, n, alpha, A, Q, Bm, Q, beta, C, Q, a.slices, w.oz, maxabs, w.pst, s, map);
   };
+  auto inv = [&](int nb, const int* map, const int* count, const double2* A, double2* X) -> cudaError_t {
+    ++nl;
+    if (small) return launch_small_zinv(nb, n, A, X, Q, map, count, w.info, s);
+    return launch_zinv_mapped(nb, n, A, Q, X, Q, map, w.info, w.zwork, s);
+  };
+  // FP64 products of the trace (the one-warp kernel at small orders, else the DMMA product)
+  auto prod64 = [&](int nb, const double2* A, const double2* Bm, double2* C) -> cudaError_t {
+    ++nl;
+    if (small) return launch_small_zgemm(nb, n, one, A, Bm, zero, C, Q, nullptr, nullptr, nullptr, s);
+    return launch_zgemm_batched(nb, n, n, n, one, A, Q, Bm, Q, zero, C, Q, 0, s);
+  };
+  // the small form runs the decimation without a host round trip per
+  // iteration: the kernels read the active count on the device, and the host
+  // looks at it every kPoll iterations
+  constexpr int kPoll = 8;
 
   for (int p0 = 0; p0 < a.npts; p0 += batch) {
     const int P = std::min(batch, a.npts - p0);
@@ -328,79 +362,98 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       int* ncyc_c = side == 0 ? w.ncl : w.ncr;
       double2 *Ao = B[0], *Aos = B[1], *Bo = B[2], *Co = B[3], *Go = B[4], *X = B[5], *C1 = B[6], *Y = B[7],
               *B1 = B[8];
-      k_lead_init<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, Ao, Aos, Bo, Co, Q);
+      k_lead_init<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, Ao, Aos, Bo, Co, Q); ++nl;
       MCK(cudaGetLastError(), "lead init");
       MCK(cudaMemsetAsync(w.ok, 0, sizeof(int) * P, s), "memset ok");
       MCK(cudaMemsetAsync(w.mx, 0, sizeof(double) * P, s), "memset mx");
       MCK(cudaMemsetAsync(ncyc_c, 0, sizeof(int) * P, s), "memset ncyc");
-      k_iota<<<(P + 255) / 256, 256, 0, s>>>(P, w.list0);
-      int na = P;
+      int* cnt_cur = small ? w.count : nullptr;        // device active counts (small form)
+      int* cnt_nxt = small ? w.count + 1 : nullptr;
+      k_iota<<<(P + 255) / 256, 256, 0, s>>>(P, w.list0, cnt_cur); ++nl;
+      int na = P;                                      // host bound of the active list
       int* cur = w.list0;
       int* nxt = w.list1;
-      for (int it = 1; it <= a.sgf_max_iter && na > 0; ++it) {
-        MCK(launch_zinv_mapped(na, n, Ao, Q, Go, Q, cur, w.info, w.zwork, s), "zinv");
-        k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
-        MCK(prod(na, cur, one, Go, Co, zero, X, nullptr), "GoXCo");
-        MCK(prod(na, cur, one, Co, X, zero, C1, w.mx), "C1");
-        k_dec_check<<<1, 1024, 0, s>>>(na, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt, w.count);
+      int it = 1;
+      for (; it <= a.sgf_max_iter && na > 0; ++it) {
+        MCK(inv(na, cur, cnt_cur, Ao, Go), "zinv");
+        k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
+        MCK(prod(na, cur, cnt_cur, one, Go, Co, zero, X, nullptr), "GoXCo");
+        MCK(prod(na, cur, cnt_cur, one, Co, X, zero, C1, w.mx), "C1");
+        k_dec_check<<<1, 1024, 0, s>>>(na, cnt_cur, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt,
+                                       small ? cnt_nxt : w.count); ++nl;
         MCK(cudaGetLastError(), "check");
-        int h_count = 0;
-        MCK(cudaMemcpyAsync(&h_count, w.count, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
-        MCK(cudaStreamSynchronize(s), "sync");
         std::swap(cur, nxt);
-        na = h_count;
-        if (na == 0) break;
-        MCK(prod(na, cur, one, Bo, X, zero, B1, nullptr), "Self");
-        k_sub_self<<<dim3(gx, na), eb, 0, s>>>(Q, cur, B1, Ao, Aos, Q);
-        MCK(prod(na, cur, one, Go, Bo, zero, Y, nullptr), "GoXBo");
-        MCK(prod(na, cur, one, Bo, Y, zero, B1, nullptr), "B1");
-        MCK(prod(na, cur, mone, Co, Y, one, Ao, nullptr), "Ao update");
+        if (small) {
+          std::swap(cnt_cur, cnt_nxt);
+          if (it % kPoll == 0) {
+            MCK(cudaMemcpyAsync(&na, cnt_cur, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
+            MCK(cudaStreamSynchronize(s), "sync");
+            if (na == 0) break;
+          }
+        } else {
+          int h_count = 0;
+          MCK(cudaMemcpyAsync(&h_count, w.count, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
+          MCK(cudaStreamSynchronize(s), "sync");
+          na = h_count;
+          if (na == 0) break;
+        }
+        MCK(prod(na, cur, cnt_cur, one, Bo, X, zero, B1, nullptr), "Self");
+        k_sub_self<<<dim3(gx, na), eb, 0, s>>>(Q, cur, cnt_cur, B1, Ao, Aos, Q); ++nl;
+        MCK(prod(na, cur, cnt_cur, one, Go, Bo, zero, Y, nullptr), "GoXBo");
+        MCK(prod(na, cur, cnt_cur, one, Bo, Y, zero, B1, nullptr), "B1");
+        MCK(prod(na, cur, cnt_cur, mone, Co, Y, one, Ao, nullptr), "Ao update");
         // Bo = B1, Co = C1 for every point still iterating (the others are done with them)
         std::swap(B[2], B[8]);
         std::swap(B[3], B[6]);
         Bo = B[2]; Co = B[3]; B1 = B[8]; C1 = B[6];
       }
-      if (na > 0) k_not_converged<<<(na + 255) / 256, 256, 0, s>>>(na, cur, ncyc_c, w.pst, a.sgf_max_iter);
+      if (small && na > 0) {         // the loop ran to the cap: how many are left
+        MCK(cudaMemcpyAsync(&na, cnt_cur, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
+        MCK(cudaStreamSynchronize(s), "sync");
+      }
+      if (na > 0)
+        k_not_converged<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, ncyc_c, w.pst, a.sgf_max_iter); ++nl;
       // gs = Aos^-1 for every point
-      MCK(launch_zinv_mapped(P, n, Aos, Q, B[9 + side], Q, nullptr, w.info, w.zwork, s), "gs");
-      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+      MCK(inv(P, nullptr, nullptr, Aos, B[9 + side]), "gs");
+      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
     }
     // ---- self-energies Sigma_c = Tlc gs Tcl (B11 left, B12 right)
     for (int side = 0; side < 2; ++side) {
       const int c = side == 0 ? a.left : a.right;
-      k_tlc<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, B[0], B[1], Q);
+      k_tlc<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, B[0], B[1], Q); ++nl;
       MCK(cudaGetLastError(), "tlc");
-      MCK(prod(P, nullptr, one, B[0], B[9 + side], zero, B[2], nullptr), "Tlc gs");
-      MCK(prod(P, nullptr, one, B[2], B[1], zero, B[11 + side], nullptr), "Sigma");
+      MCK(prod(P, nullptr, nullptr, one, B[0], B[9 + side], zero, B[2], nullptr), "Tlc gs");
+      MCK(prod(P, nullptr, nullptr, one, B[2], B[1], zero, B[11 + side], nullptr), "Sigma");
     }
     // ---- gsmr sweep from block nbl down to 2, then Gr(1,1)
     double2 *g = B[4], *X = B[5], *W = B[6], *U = B[7], *Lb = B[8];
-    k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, a.nbl - 1, ids, E, a.d_descs, B[12], W, Q);
-    MCK(launch_zinv_mapped(P, n, W, Q, g, Q, nullptr, w.info, w.zwork, s), "gsmr N");
-    k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+    k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, a.nbl - 1, ids, E, a.d_descs, B[12], W, Q); ++nl;
+    MCK(inv(P, nullptr, nullptr, W, g), "gsmr N");
+    k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
     for (int i = a.nbl - 2; i >= 0; --i) {
       // W = ESH(i,i) - ESH(i,i+1) gsmr(i+1) ESH(i+1,i)  (block i 0-based; Sigma_left on block 0)
-      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 1, i, ids, E, a.d_descs, nullptr, U, Q);
-      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 2, i, ids, E, a.d_descs, nullptr, Lb, Q);
-      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, i, ids, E, a.d_descs, i == 0 ? B[11] : nullptr, W, Q);
+      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 1, i, ids, E, a.d_descs, nullptr, U, Q); ++nl;
+      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 2, i, ids, E, a.d_descs, nullptr, Lb, Q); ++nl;
+      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, i, ids, E, a.d_descs, i == 0 ? B[11] : nullptr, W, Q); ++nl;
       MCK(cudaGetLastError(), "esh");
-      MCK(prod(P, nullptr, one, U, g, zero, X, nullptr), "U g");
-      MCK(prod(P, nullptr, mone, X, Lb, one, W, nullptr), "W");
-      MCK(launch_zinv_mapped(P, n, W, Q, g, Q, nullptr, w.info, w.zwork, s), "gsmr");
-      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+      MCK(prod(P, nullptr, nullptr, one, U, g, zero, X, nullptr), "U g");
+      MCK(prod(P, nullptr, nullptr, mone, X, Lb, one, W, nullptr), "W");
+      MCK(inv(P, nullptr, nullptr, W, g), "gsmr");
+      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
     }
     // g = Gr(1,1).  Trace with Gamma of the contact on block 1 (FP64 products)
-    k_gamma<<<dim3(gx, P), eb, 0, s>>>(n, B[11], B[0], Q);
-    MCK(launch_zgemm_batched(P, n, n, n, one, B[0], Q, g, Q, zero, B[1], Q, 0, s), "Gam G");
-    MCK(launch_zgemm_batched(P, n, n, n, one, g, Q, B[0], Q, zero, B[2], Q, 0, s), "G Gam");
-    k_trace<<<P, 512, 0, s>>>(n, B[0], g, B[1], B[2], w.tb, Q);
+    k_gamma<<<dim3(gx, P), eb, 0, s>>>(n, B[11], B[0], Q); ++nl;
+    MCK(prod64(P, B[0], g, B[1]), "Gam G");
+    MCK(prod64(P, g, B[0], B[2]), "G Gam");
+    k_trace<<<P, 512, 0, s>>>(n, B[0], g, B[1], B[2], w.tb, Q); ++nl;
     MCK(cudaGetLastError(), "trace");
     k_finish<<<(P + 255) / 256, 256, 0, s>>>(P, w.ncl, w.ncr, w.pst, w.tb, a.d_T + p0,
                                              a.d_ncyc ? a.d_ncyc + p0 : nullptr,
-                                             a.d_status ? a.d_status + p0 : nullptr);
+                                             a.d_status ? a.d_status + p0 : nullptr); ++nl;
     MCK(cudaGetLastError(), "finish");
   }
 #undef MCK
+  if (a.launches) *a.launches += nl;
   return NEGF_B200_OK;
 }
 

@@ -23,10 +23,11 @@ struct MixedArgs {
   int left, right;           // 0-based contact indices on block 1 and on block nbl
   double sgf_tol;
   int sgf_max_iter;
-  int slices;                // int8 digits per operand element (4..8)
+  int slices;                // int8 digits per operand element (4..8); 0 = the small-order FP64 form (n <= 32)
   double* d_T;
   int* d_ncyc;               // decimation iterations summed over the contacts
   int* d_status;
+  uint64_t* launches = nullptr;  // host counter of kernels launched (may be null)
 };
 
 // bytes of workspace for a batch of `batch` points of order n

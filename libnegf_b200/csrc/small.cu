@@ -1,0 +1,211 @@
+// Small-order block operations for the lock-step FP64 form (small.cuh): one
+// warp per problem, lane i holding row i (inversion) or computing row i of
+// the product.  Reference operations replaced: the zgemm of prealloc_mult
+// (src/sparsekit_drv.F90:1896-2081) and zinv = zgetrf + zgetrs against the
+// identity (src/inversions.F90:807-839), at orders n <= 32.
+#include <cuda_runtime.h>
+
+#include "cta_ops.cuh"
+#include "small.cuh"
+
+namespace negf {
+namespace {
+
+constexpr int kWarps = 4;                  // problems per CTA
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ int batch_limit(int batch, const int* count) {
+  return count ? min(*count, batch) : batch;
+}
+
+// Row `lane` of C = alpha A B + beta C, JB columns of C per pass held in
+// registers; A's column k is one coalesced load per k, B's row k uniform
+// (broadcast) loads.
+template <int N, int JB>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_small_zgemm(int batch, int n, double2 alpha, const double2* __restrict__ A, const double2* __restrict__ B,
+                  double2 beta, double2* C, int64_t Q, const int* map, const int* count, double* maxabs) {
+  const int lane = threadIdx.x & 31;
+  const int b = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  if (b >= batch_limit(batch, count)) return;
+  const int p = map ? map[b] : b;
+  const double2* Ap = A + p * Q;
+  const double2* Bp = B + p * Q;
+  double2* Cp = C + p * Q;
+  const bool row = lane < n;
+  const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
+  double mx = 0.0;
+  bool bad = false;
+  for (int j0 = 0; j0 < n; j0 += JB) {
+    double2 acc[JB];
+#pragma unroll
+    for (int jj = 0; jj < JB; ++jj) acc[jj] = make_double2(0.0, 0.0);
+    for (int k = 0; k < n; ++k) {
+      const double2 a = row ? __ldg(Ap + lane + (int64_t)k * n) : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) {
+        const int j = j0 + jj;
+        if (j < n) {
+          const double2 bv = __ldg(Bp + k + (int64_t)j * n);
+          acc[jj].x = fma(a.x, bv.x, acc[jj].x);
+          acc[jj].x = fma(-a.y, bv.y, acc[jj].x);
+          acc[jj].y = fma(a.x, bv.y, acc[jj].y);
+          acc[jj].y = fma(a.y, bv.x, acc[jj].y);
+        }
+      }
+    }
+    if (row) {
+#pragma unroll
+      for (int jj = 0; jj < JB; ++jj) {
+        const int j = j0 + jj;
+        if (j < n) {
+          double2* el = Cp + lane + (int64_t)j * n;
+          double2 v = cmul(alpha, acc[jj]);
+          if (use_beta) v = cadd(v, cmul(beta, *el));
+          *el = v;
+          const double h = hypot(v.x, v.y);
+          mx = fmax(mx, h);
+          bad |= !(h <= 1.7976931348623157e308);   // NaN or Inf
+        }
+      }
+    }
+  }
+  if (maxabs) {
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(kFull, mx, o));
+    // a non-finite element makes the maximum NaN (fmax would drop it): the
+    // positive quiet NaN is above every finite bit pattern, so it stays
+    if (__any_sync(kFull, bad)) mx = __longlong_as_double(0x7ff8000000000000LL);
+    if (lane == 0)
+      atomicMax(reinterpret_cast<unsigned long long*>(maxabs + p), (unsigned long long)__double_as_longlong(mx));
+  }
+}
+
+// In-place Gauss-Jordan on the rows held by the lanes.  Rows are never moved
+// between lanes: each lane carries the logical (pivot-order) index of its
+// row, the pivot of column k is the unused row with the largest |Re|+|Im|
+// (lowest logical index on a tie), and the column interchanges that undo the
+// row order are applied to the store addresses at the end.  Per step the
+// pivot row is published through shared memory; the pivot row becomes
+// row * d (d = 1 / pivot, entry k = d), every other row r - (r_k d) * row
+// (entry k = -(r_k d)), the update order of the engine's Gauss-Jordan.
+template <int N>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count,
+                 int* info) {
+  __shared__ double2 prow[kWarps][N];
+  __shared__ int sidx[kWarps][N];
+  __shared__ int scm[kWarps][N];
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int b = blockIdx.x * kWarps + w;
+  if (b >= batch_limit(batch, count)) return;
+  const int p = map ? map[b] : b;
+  const double2* Ap = A + p * Q;
+  double2 r[N];
+#pragma unroll
+  for (int c = 0; c < N; ++c)
+    r[c] = (lane < n && c < n) ? Ap[lane + (int64_t)c * n] : make_double2(0.0, 0.0);
+  int lg = lane;
+  bool used = lane >= n;
+  int inf = 0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    if (k < n) {
+      // NaN ranks above everything (every lane must see one total order, and
+      // a NaN should spread to the whole inverse rather than be skipped)
+      double bv = used ? -1.0 : cabs1(r[k]);
+      if (bv != bv) bv = __longlong_as_double(0x7ff0000000000000LL);
+      int blg = lg, bl = lane;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(kFull, bv, o);
+        const int olg = __shfl_xor_sync(kFull, blg, o);
+        const int ol = __shfl_xor_sync(kFull, bl, o);
+        if (ov > bv || (ov == bv && olg < blg)) {
+          bv = ov;
+          blg = olg;
+          bl = ol;
+        }
+      }
+      if (lane == bl) {
+#pragma unroll
+        for (int c = 0; c < N; ++c)
+          if (c < n) prow[w][c] = r[c];
+      }
+      __syncwarp();
+      const double2 pv = prow[w][k];
+      if (pv.x == 0.0 && pv.y == 0.0 && inf == 0) inf = k + 1;
+      const double2 d = crecip(pv);
+      if (lane == bl) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) r[c] = (c == k) ? d : cmul(r[c], d);
+      } else {
+        const double2 fd = cmul(r[k], d);
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+          if (c == k) {
+            r[c] = make_double2(-fd.x, -fd.y);
+          } else if (c < n) {
+            r[c] = csub(r[c], cmul(fd, prow[w][c]));
+          }
+        }
+      }
+      if (lg == k) lg = blg;
+      if (lane == bl) {
+        lg = k;
+        used = true;
+      }
+      if (lane == 0) sidx[w][k] = blg;
+      __syncwarp();
+    }
+  }
+  // column interchanges in reverse pivot order: output column dest[c] takes
+  // internal column c
+  if (lane == 0) {
+    for (int j = 0; j < n; ++j) scm[w][j] = j;
+    for (int l = n - 1; l >= 0; --l) {
+      const int il = sidx[w][l];
+      if (il != l) {
+        const int t = scm[w][il];
+        scm[w][il] = scm[w][l];
+        scm[w][l] = t;
+      }
+    }
+    for (int j = 0; j < n; ++j) sidx[w][scm[w][j]] = j;
+  }
+  __syncwarp();
+  if (lane < n) {
+    double2* Xp = X + p * Q;
+#pragma unroll
+    for (int c = 0; c < N; ++c)
+      if (c < n) Xp[lg + (int64_t)sidx[w][c] * n] = r[c];
+  }
+  if (lane == 0 && info) info[p] = inf;
+}
+
+}  // namespace
+
+cudaError_t launch_small_zgemm(int batch, int n, double2 alpha, const double2* A, const double2* B, double2 beta,
+                               double2* C, int64_t Q, const int* map, const int* count, double* maxabs,
+                               cudaStream_t s) {
+  if (batch <= 0) return cudaSuccess;
+  if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
+  const int grid = (batch + kWarps - 1) / kWarps;
+  if (n <= 16)
+    k_small_zgemm<16, 16><<<grid, kWarps * 32, 0, s>>>(batch, n, alpha, A, B, beta, C, Q, map, count, maxabs);
+  else
+    k_small_zgemm<32, 16><<<grid, kWarps * 32, 0, s>>>(batch, n, alpha, A, B, beta, C, Q, map, count, maxabs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
+                              const int* count, int* info, cudaStream_t s) {
+  if (batch <= 0) return cudaSuccess;
+  if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
+  const int grid = (batch + kWarps - 1) / kWarps;
+  if (n <= 16)
+    k_small_zinv<16><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info);
+  else
+    k_small_zinv<32><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info);
+  return cudaGetLastError();
+}
+
+}  // namespace negf

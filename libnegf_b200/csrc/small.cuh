@@ -1,0 +1,32 @@
+// Small-order block operations (n <= 32) for the lock-step FP64 form: one
+// warp per problem, every problem of a batch in one launch.  At these orders
+// a product or an inversion is a few microseconds of dependent steps, so a
+// CTA working through one point's chain of them (the persistent engine)
+// leaves the FP64 pipe idle; a batch of warps, each holding one problem's
+// rows in registers, keeps it fed.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace negf {
+
+constexpr int kSmallMax = 32;      // largest order of the one-warp kernels
+
+// C_p = alpha A_p B_p + beta C_p (complex128, column major, n x n) for the
+// problems p = map[b] (map null: p = b), b < *count (count null: batch).
+// A, B, C: problem p at p * Q complex elements.  beta == 0: C is not read.
+// maxabs (optional): max |C_p| (modulus) of the written elements, folded
+// into maxabs[p] by atomicMax on the bit pattern (non-negative doubles); a
+// NaN or Inf element makes it NaN.  C must not alias A or B.
+cudaError_t launch_small_zgemm(int batch, int n, double2 alpha, const double2* A, const double2* B, double2 beta,
+                               double2* C, int64_t Q, const int* map, const int* count, double* maxabs,
+                               cudaStream_t s);
+
+// X_p = A_p^-1 by Gauss-Jordan elimination with partial pivoting (pivot =
+// max |Re|+|Im| over the rows not yet used, the lowest row on a tie: the
+// izamax rule of zgetrf) for the same problem selection; info[p] = 0 or the
+// 1-based column of the first zero pivot.  X may alias A.
+cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
+                              const int* count, int* info, cudaStream_t s);
+
+}  // namespace negf

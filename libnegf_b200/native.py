@@ -35,7 +35,7 @@ EXPORTED = [
     "negf_b200_transmissions", "negf_b200_set_sgf_cache", "negf_b200_sgf_cache_stats",
     "negf_b200_set_workspace_limit", "negf_b200_density", "negf_b200_density_neq", "negf_b200_meir_wingreen_dev",
     "negf_b200_sgf_cache_save", "negf_b200_sgf_cache_load", "negf_b200_upload_csr",
-    "negf_b200_zgemm_i8_work_bytes", "negf_b200_zgemm_batched_i8",
+    "negf_b200_zgemm_i8_work_bytes", "negf_b200_zgemm_batched_i8", "negf_b200_launch_count",
 ]
 TRACE_PHASES = ["gemm", "inv_panel", "inv_update", "inv_other", "elementwise", "total", "points", "unused"]
 
@@ -64,7 +64,8 @@ class Options(ctypes.Structure):
     """Mirror of negf_b200_options."""
     _fields_ = [("sgf_tol", ctypes.c_double), ("sgf_max_iter", ctypes.c_int32), ("eps_drop", ctypes.c_double),
                 ("scba_tol", ctypes.c_double), ("scba_niter", ctypes.c_int32), ("precision", ctypes.c_int32),
-                ("ctas_per_sm", ctypes.c_int32), ("scba_mix", ctypes.c_double), ("scba_rule", ctypes.c_int32)]
+                ("ctas_per_sm", ctypes.c_int32), ("scba_mix", ctypes.c_double), ("scba_rule", ctypes.c_int32),
+                ("schedule", ctypes.c_int32)]
 
 
 _lib = None
@@ -105,6 +106,7 @@ def load():
     L.negf_b200_zgemm_i8_work_bytes.argtypes = [i32, i32, i32, i32, i32]
     L.negf_b200_zgemm_batched_i8.argtypes = [i32, i32, i32, i32, dp, vp, ctypes.c_int64, vp, ctypes.c_int64, dp,
                                              vp, ctypes.c_int64, i32, vp, vp, vp]
+    L.negf_b200_launch_count.argtypes = [vp, ctypes.POINTER(ctypes.c_uint64)]
     L.negf_b200_zinv_work_bytes.restype = ctypes.c_size_t
     L.negf_b200_zinv_work_bytes.argtypes = [i32, i32]
     L.negf_b200_zinv_batched.argtypes = [i32, i32, vp, vp, vp, vp, vp]
@@ -151,6 +153,7 @@ class Context:
         self._L = L
         self.devices = {}
         self._nldos = {}
+        self.options = {}
         if options:
             self.set_options(**options)
 
@@ -184,6 +187,7 @@ class Context:
             raise NegfError(rc, "%s: %s" % (what, self.last_error()))
 
     def set_options(self, **kw):
+        """The library defaults (negf_b200_default_options) with `kw` on top."""
         o = Options()
         self._L.negf_b200_default_options(ctypes.byref(o))
         for k, v in kw.items():
@@ -191,6 +195,17 @@ class Context:
                 raise TypeError("unknown option %s" % k)
             setattr(o, k, v)
         self._check(self._L.negf_b200_set_options(self._h, ctypes.byref(o)), "set_options")
+        self.options = dict(kw)
+
+    def update_options(self, **kw):
+        """The options set so far with `kw` on top."""
+        self.set_options(**{**self.options, **kw})
+
+    def launch_count(self) -> int:
+        """Kernels this context's solve calls have launched so far."""
+        c = ctypes.c_uint64()
+        self._check(self._L.negf_b200_launch_count(self._h, ctypes.byref(c)), "launch_count")
+        return int(c.value)
 
     def set_tracing(self, enable=True):
         self._check(self._L.negf_b200_set_tracing(self._h, 1 if enable else 0), "set_tracing")

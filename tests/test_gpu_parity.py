@@ -160,10 +160,14 @@ def _o_dos(E, **kw):
     return run
 
 
+@pytest.mark.parametrize("schedule", [0, 1])
 @pytest.mark.parametrize("case", sorted(CASES))
-def test_transmission_parity(gpu_ctx, case):
+def test_transmission_parity(gpu_ctx, case, schedule):
+    """schedule 0: lock step where the call fits it (2 contacts on blocks 1
+    and nbl, one PL size n <= 32), else the engine; schedule 1: the engine."""
     dev, E = CASES[case]()
     did = gpu_ctx.upload(dev)
+    gpu_ctx.set_options(schedule=schedule)
     try:
         T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6)
         ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev, nsamp=2)
@@ -171,6 +175,7 @@ def test_transmission_parity(gpu_ctx, case):
         assert np.array_equal(ncyc, ref["ncyc"])
         assert_T_strict(T, ref["T"], xp_reference(dev, E, 1e-6), spread=spread["T"])
     finally:
+        gpu_ctx.set_options()
         gpu_ctx.release(did)
 
 

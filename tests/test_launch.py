@@ -10,24 +10,45 @@ from libnegf_b200 import generators as G
 
 @pytest.mark.gpu
 def test_autotune_picks_a_schedule_without_changing_results(gpu_ctx, tmp_path):
+    """The tuner times the engine at 2 and 1 CTAs per SM and lock step where
+    the shape admits it, applies the fastest on top of the caller's options,
+    and reads its choice back from the file.  The engine's CTA counts give
+    identical bits; every schedule is at strict parity with the oracle."""
+    from conftest import assert_T_strict, oracle_spread, xp_reference
     from libnegf_b200 import autotune
+    from oracle import oracle as O
     dev = G.transport_c0(nbl=6, n=16, seed=2)
     E = np.linspace(-2, 2, 300)
     did = gpu_ctx.upload(dev)
     try:
-        T0, _, _ = gpu_ctx.transmission(did, E, eta=1e-4)
+        got = {}
+        for name, c in (("engine_2", autotune.ENGINE_2), ("engine_1", autotune.ENGINE_1),
+                        ("lockstep", autotune.LOCKSTEP)):
+            gpu_ctx.set_options(sgf_tol=1e-10, **c)
+            got[name] = gpu_ctx.transmission(did, E, eta=1e-4)
+        assert np.array_equal(got["engine_1"][0], got["engine_2"][0])
+        ref, spread = oracle_spread(lambda d: dict(zip(("T", "ncyc"), O.transmission(d, E, eta=1e-4,
+                                                                                         sgf_tol=1e-10)[:2])),
+                                    dev, nsamp=2)
+        x = xp_reference(dev, E, 1e-4, sgf_tol=1e-10)
+        for name, (T, nc, st) in got.items():
+            assert np.array_equal(nc, ref["ncyc"]), name
+            assert_T_strict(T, ref["T"], x, spread=spread["T"], what=name)
+        gpu_ctx.set_options(sgf_tol=1e-10)
         autotune.forget()
         rec = autotune.tune(gpu_ctx, did, E[:200], mode="T", cache_file=str(tmp_path / "sched.json"))
-        assert rec["ctas_per_sm"] in (1, 2) and set(rec["timings"]) == {"1", "2"}
-        T1, _, _ = gpu_ctx.transmission(did, E, eta=1e-4)
-        assert np.array_equal(T0, T1)
-        for c in (1, 2):
-            gpu_ctx.set_options(ctas_per_sm=c)
-            assert np.array_equal(gpu_ctx.transmission(did, E, eta=1e-4)[0], T0)
+        assert set(rec["timings"]) == {"engine_2", "engine_1", "lockstep"}
+        assert gpu_ctx.options["sgf_tol"] == 1e-10                 # the caller's options stay
+        assert np.array_equal(gpu_ctx.transmission(did, E, eta=1e-4)[0], got[rec["choice"]][0])
         autotune.forget()
         rec2 = autotune.tune(gpu_ctx, did, E[:200], mode="T", cache_file=str(tmp_path / "sched.json"))
         assert rec2 == rec                                   # read back from the file
+        # the DOS solve has no lock step: only the engine's candidates
+        autotune.forget()
+        rec3 = autotune.tune(gpu_ctx, did, E[:200], mode="DOS")
+        assert set(rec3["timings"]) == {"engine_2", "engine_1"} and rec3["schedule"] == 1
     finally:
+        autotune.forget()
         gpu_ctx.set_options()
         gpu_ctx.release(did)
 

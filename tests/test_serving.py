@@ -83,6 +83,7 @@ def test_workspace_limit_runs_fewer_ctas(gpu_ctx):
     dev = G.transport_c0(nbl=8, n=32, seed=3)
     E = np.linspace(-2, 2, 64)
     did = gpu_ctx.upload(dev)
+    gpu_ctx.set_options(schedule=1)                               # the persistent engine's CTAs
     try:
         T0, _, _ = gpu_ctx.transmission(did, E, eta=1e-6)
         slot = 32 * 32 * 16
@@ -94,6 +95,7 @@ def test_workspace_limit_runs_fewer_ctas(gpu_ctx):
             gpu_ctx.transmission(did, E, eta=1e-6)
         assert ei.value.code == native.ADMISSION
     finally:
+        gpu_ctx.set_options()
         gpu_ctx.set_workspace_limit(0)
         gpu_ctx.release(did)
 
