@@ -1052,6 +1052,18 @@ static bool lockstep_choice(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_i
   return true;
 }
 
+// The solves that only the engine runs (DOS, N-contact pairs, SCBA, the
+// density matrix) refuse the options that ask for a lock-step form.
+static int engine_only(negf_b200_ctx* ctx, const char* what) {
+  if (ctx->opt.precision != 0)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG,
+                std::string("the mixed form (precision != 0) covers single-pair transmission solves, not ") + what);
+  if (ctx->opt.schedule == 2)
+    return fail(ctx, NEGF_B200_ERR_BAD_ARG,
+                std::string("lock step (schedule 2) covers single-pair transmission solves, not ") + what);
+  return NEGF_B200_OK;
+}
+
 // Runs a lock-step form on device arrays of ids and energies: sizes the batch
 // to the workspace and calls negf::mixed_run.
 static int run_lockstep(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_ids, const double* d_E, double eta,
@@ -1170,9 +1182,10 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   }
   LockShape lsh;
   int lslices = 0;
-  if (mode != negf::MODE_T && ctx->opt.precision != 0)
-    return fail(ctx, NEGF_B200_ERR_BAD_ARG,
-                "the mixed form (precision != 0) covers single-pair transmission solves without the SGF cache");
+  if (mode != negf::MODE_T) {
+    st = engine_only(ctx, "this solve");
+    if (st) return st;
+  }
   if (mode == negf::MODE_T && lockstep_choice(ctx, npts, ids, npairs == 1, &lsh, &lslices, &st, s)) {
     if (st) return st;
     st = run_lockstep(ctx, npts, d_ids, d_E, eta, d_T, d_ncyc, d_st, s, lsh, lslices);
@@ -1256,6 +1269,7 @@ int accumulate_blocks(negf_b200_ctx* ctx, int mode, int32_t device_id, int32_t n
                       const double* coupling, std::vector<double2>& T, std::vector<int>& pl, int64_t& nd,
                       int64_t& no, int32_t* ncyc, int32_t* status, std::vector<double2>* outer = nullptr,
                       int64_t* nm_out = nullptr) {
+  if (int e = engine_only(ctx, "the density matrix")) return e;
   if (device_id < 0 || device_id >= (int)ctx->devs.size() || !ctx->devs[device_id].live)
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "unknown device id");
   const DeviceRec& r = ctx->devs[device_id];
@@ -1508,8 +1522,10 @@ int negf_b200_transmission_dos_dev(negf_b200_ctx* ctx, int32_t npts, const int32
   if (npts == 0) return NEGF_B200_OK;
   std::lock_guard<std::mutex> lk(ctx->mu);
   if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
+  int st = engine_only(ctx, "the DOS solve");
+  if (st) return st;
   LaunchShape sh;
-  int st = shape_of(ctx, npts, nullptr, sh);
+  st = shape_of(ctx, npts, nullptr, sh);
   if (st) return st;
   negf::EngineArgs a = base_args(ctx, negf::MODE_DOS, npts);
   a.dev_id = d_device_id; a.energy = d_energy; a.eta = eta; a.dos_delta = dos_delta; a.ni = ni; a.nf = nf;
@@ -1528,6 +1544,7 @@ int negf_b200_meir_wingreen_dev(negf_b200_ctx* ctx, int32_t npts, const int32_t*
   if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, NEGF_B200_ERR_CUDA, "cudaSetDevice");
   if (!d_device_id || !d_energy || !d_frm || !d_scba_iter || !d_scba_err || !d_status)
     return fail(ctx, NEGF_B200_ERR_BAD_ARG, "device_id, energy, frm, scba_iter, scba_err and status are required");
+  if (int e = engine_only(ctx, "the SCBA solve")) return e;
   LaunchShape sh;
   int st = shape_of(ctx, npts, nullptr, sh);
   if (st) return st;

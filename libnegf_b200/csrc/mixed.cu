@@ -172,6 +172,39 @@ __global__ void k_esh(int n, int which, int i, const int* ids, const double* E, 
   }
 }
 
+// The three ESH blocks of one sweep step in one pass: U = ESH(i,i+1),
+// L = ESH(i+1,i), W = ESH(i,i) - sig (sig may be null)
+__global__ void k_esh_step(int n, int i, const int* ids, const double* E, const DevDesc* descs, const double2* sig,
+                           double2* U, double2* Lo, double2* W, int64_t Q) {
+  const int p = blockIdx.y;
+  const DevDesc& d = descs[ids[p]];
+  const double e = E[p];
+  const int64_t nn = (int64_t)n * n;
+  const int64_t od = d.od[i], oo = d.oo[i];
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
+    const double2 hu = d.hu[oo + q], hl = d.hl[oo + q], hd = d.hd[od + q];
+    double2 u, l, w;
+    if (d.has_s) {
+      const double2 su = d.su[oo + q], sl = d.sl[oo + q], sd = d.sd[od + q];
+      u = make_double2(e * su.x - hu.x, e * su.y - hu.y);
+      l = make_double2(e * sl.x - hl.x, e * sl.y - hl.y);
+      w = make_double2(e * sd.x - hd.x, e * sd.y - hd.y);
+    } else {
+      u = make_double2(-hu.x, -hu.y);
+      l = make_double2(-hl.x, -hl.y);
+      w = make_double2(-hd.x, -hd.y);
+      if ((q % n) == (q / n)) w.x += e;
+    }
+    if (sig) {
+      const double2 sg = sig[p * Q + q];
+      w.x -= sg.x; w.y -= sg.y;
+    }
+    U[p * Q + q] = u;
+    Lo[p * Q + q] = l;
+    W[p * Q + q] = w;
+  }
+}
+
 // Gamma = i (Sigma - Sigma^dag)   (zspectral_dns, src/sparsekit_drv.F90:2870-2890)
 __global__ void k_gamma(int n, const double2* Sig, double2* Gam, int64_t Q) {
   const int p = blockIdx.y;
@@ -337,7 +370,7 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
   };
   auto inv = [&](int nb, const int* map, const int* count, const double2* A, double2* X) -> cudaError_t {
     ++nl;
-    if (small) return launch_small_zinv(nb, n, A, X, Q, map, count, w.info, s);
+    if (small) return launch_small_zinv(nb, n, A, X, Q, map, count, w.info, w.pst, NEGF_B200_ERR_SINGULAR, s);
     return launch_zinv_mapped(nb, n, A, Q, X, Q, map, w.info, w.zwork, s);
   };
   // FP64 products of the trace (the one-warp kernel at small orders, else the DMMA product)
@@ -376,7 +409,10 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       int it = 1;
       for (; it <= a.sgf_max_iter && na > 0; ++it) {
         MCK(inv(na, cur, cnt_cur, Ao, Go), "zinv");
-        k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
+        if (!small) {
+          k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+          ++nl;
+        }
         MCK(prod(na, cur, cnt_cur, one, Go, Co, zero, X, nullptr), "GoXCo");
         MCK(prod(na, cur, cnt_cur, one, Co, X, zero, C1, w.mx), "C1");
         k_dec_check<<<1, 1024, 0, s>>>(na, cnt_cur, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt,
@@ -415,7 +451,10 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
         k_not_converged<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, ncyc_c, w.pst, a.sgf_max_iter); ++nl;
       // gs = Aos^-1 for every point
       MCK(inv(P, nullptr, nullptr, Aos, B[9 + side]), "gs");
-      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
+      if (!small) {
+        k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+        ++nl;
+      }
     }
     // ---- self-energies Sigma_c = Tlc gs Tcl (B11 left, B12 right)
     for (int side = 0; side < 2; ++side) {
@@ -429,17 +468,21 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
     double2 *g = B[4], *X = B[5], *W = B[6], *U = B[7], *Lb = B[8];
     k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, a.nbl - 1, ids, E, a.d_descs, B[12], W, Q); ++nl;
     MCK(inv(P, nullptr, nullptr, W, g), "gsmr N");
-    k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
+    if (!small) {
+      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+      ++nl;
+    }
     for (int i = a.nbl - 2; i >= 0; --i) {
       // W = ESH(i,i) - ESH(i,i+1) gsmr(i+1) ESH(i+1,i)  (block i 0-based; Sigma_left on block 0)
-      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 1, i, ids, E, a.d_descs, nullptr, U, Q); ++nl;
-      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 2, i, ids, E, a.d_descs, nullptr, Lb, Q); ++nl;
-      k_esh<<<dim3(gx, P), eb, 0, s>>>(n, 0, i, ids, E, a.d_descs, i == 0 ? B[11] : nullptr, W, Q); ++nl;
+      k_esh_step<<<dim3(gx, P), eb, 0, s>>>(n, i, ids, E, a.d_descs, i == 0 ? B[11] : nullptr, U, Lb, W, Q); ++nl;
       MCK(cudaGetLastError(), "esh");
       MCK(prod(P, nullptr, nullptr, one, U, g, zero, X, nullptr), "U g");
       MCK(prod(P, nullptr, nullptr, mone, X, Lb, one, W, nullptr), "W");
       MCK(inv(P, nullptr, nullptr, W, g), "gsmr");
-      k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR); ++nl;
+      if (!small) {
+        k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+        ++nl;
+      }
     }
     // g = Gr(1,1).  Trace with Gamma of the contact on block 1 (FP64 products)
     k_gamma<<<dim3(gx, P), eb, 0, s>>>(n, B[11], B[0], Q); ++nl;

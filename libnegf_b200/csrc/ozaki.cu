@@ -434,6 +434,10 @@ __global__ void __launch_bounds__(kOzWarps * 32, 1)
         const int part = mi >> 1, grp = mi & 1;
         if (!mbar_wait(&accb, ml & 1, &fail)) break;
         tc_fence_after();
+        // pass 1: every accumulator of the group into registers, combined to
+        // one double per element (group 0: the exact level-0..3 Horner sum;
+        // group 1: the part's value, scaled), then the tensor memory goes
+        // back to the MMA warp before any global memory is touched
 #pragma unroll
         for (int j8 = 0; j8 < kOzEpiCols / 8; ++j8) {
           uint32_t v[kOzGroup][8];
@@ -446,12 +450,6 @@ __global__ void __launch_bounds__(kOzWarps * 32, 1)
             for (int l = 0; l < nlev1; ++l) tmem_ld8(tbase + tlane + (uint32_t)(l * kOzTileN) + col, v[l]);
           }
           tmem_wait_ld();
-          if (j8 == kOzEpiCols / 8 - 1) {
-            // every accumulator of this group is in registers: hand the tensor memory back
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&tfree);
-          }
           if (grp == 0) {
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
@@ -461,18 +459,25 @@ __global__ void __launch_bounds__(kOzWarps * 32, 1)
               for (int l = 1; l < kOzGroup; ++l) x = fma(x, 128.0, i2d(v[l][j]));
               part0[8 * j8 + j] = x;
             }
-            continue;
-          }
-          // group 1: the part is complete
-          double val[8];
+          } else {
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            double y = i2d(v[0][j]);
+            for (int j = 0; j < 8; ++j) {
+              double y = i2d(v[0][j]);
 #pragma unroll
-            for (int l = 1; l < nlev1; ++l) y = fma(y, 128.0, i2d(v[l][j]));
-            val[j] = fma(part0[8 * j8 + j], w0, y * w1) * rs * col_scale[col + j];
+              for (int l = 1; l < nlev1; ++l) y = fma(y, 128.0, i2d(v[l][j]));
+              part0[8 * j8 + j] = fma(part0[8 * j8 + j], w0, y * w1) * rs * col_scale[col + j];
+            }
           }
-          if (!row_ok) continue;
+        }
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&tfree);
+        if (grp == 0 || !row_ok) continue;
+        // pass 2 (group 1, the part complete): global memory while the next mainloop runs
+#pragma unroll
+        for (int j8 = 0; j8 < kOzEpiCols / 8; ++j8) {
+          const uint32_t col = (uint32_t)(cw + 8 * j8);
+          const double* val = part0 + 8 * j8;
           const int c0 = n0 + (int)col;
           if (part == 0) {
 #pragma unroll

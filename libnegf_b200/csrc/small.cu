@@ -1,6 +1,6 @@
 // Small-order block operations for the lock-step FP64 form (small.cuh): one
-// warp per problem, lane i holding row i (inversion) or computing row i of
-// the product.  Reference operations replaced: the zgemm of prealloc_mult
+// CTA per product (operands staged in shared memory), one warp per
+// inversion (lane i holding row i).  Reference operations replaced: the zgemm of prealloc_mult
 // (src/sparsekit_drv.F90:1896-2081) and zinv = zgetrf + zgetrs against the
 // identity (src/inversions.F90:807-839), at orders n <= 32.
 #include <cuda_runtime.h>
@@ -18,35 +18,42 @@ __device__ __forceinline__ int batch_limit(int batch, const int* count) {
   return count ? min(*count, batch) : batch;
 }
 
-// Row `lane` of C = alpha A B + beta C, JB columns of C per pass held in
-// registers; A's column k is one coalesced load per k, B's row k uniform
-// (broadcast) loads.
-template <int N, int JB>
+// One CTA (4 warps) per problem: A and B staged in shared memory by
+// coalesced loads (one memory latency per operand), then warp w computes
+// columns [w CW, (w + 1) CW) of C and lane i row i: A's column k is read
+// conflict-free, B's row k by broadcast.
+template <int N>
 __global__ void __launch_bounds__(kWarps * 32)
     k_small_zgemm(int batch, int n, double2 alpha, const double2* __restrict__ A, const double2* __restrict__ B,
                   double2 beta, double2* C, int64_t Q, const int* map, const int* count, double* maxabs) {
-  const int lane = threadIdx.x & 31;
-  const int b = blockIdx.x * kWarps + (threadIdx.x >> 5);
+  constexpr int CW = N / kWarps;   // columns per warp
+  __shared__ double2 sA[N * N], sB[N * N];
+  __shared__ double smx[kWarps];
+  __shared__ int sbad[kWarps];
+  const int b = blockIdx.x;
   if (b >= batch_limit(batch, count)) return;
   const int p = map ? map[b] : b;
+  const int nn = n * n;
   const double2* Ap = A + p * Q;
   const double2* Bp = B + p * Q;
-  double2* Cp = C + p * Q;
-  const bool row = lane < n;
-  const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
-  double mx = 0.0;
-  bool bad = false;
-  for (int j0 = 0; j0 < n; j0 += JB) {
-    double2 acc[JB];
+  for (int q = threadIdx.x; q < nn; q += kWarps * 32) {
+    sA[q] = __ldg(Ap + q);
+    sB[q] = __ldg(Bp + q);
+  }
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int j0 = w * CW;
+  double2 acc[CW];
 #pragma unroll
-    for (int jj = 0; jj < JB; ++jj) acc[jj] = make_double2(0.0, 0.0);
+  for (int jj = 0; jj < CW; ++jj) acc[jj] = make_double2(0.0, 0.0);
+  if (lane < n) {
     for (int k = 0; k < n; ++k) {
-      const double2 a = row ? __ldg(Ap + lane + (int64_t)k * n) : make_double2(0.0, 0.0);
+      const double2 a = sA[lane + k * n];
 #pragma unroll
-      for (int jj = 0; jj < JB; ++jj) {
+      for (int jj = 0; jj < CW; ++jj) {
         const int j = j0 + jj;
         if (j < n) {
-          const double2 bv = __ldg(Bp + k + (int64_t)j * n);
+          const double2 bv = sB[k + j * n];
           acc[jj].x = fma(a.x, bv.x, acc[jj].x);
           acc[jj].x = fma(-a.y, bv.y, acc[jj].x);
           acc[jj].y = fma(a.x, bv.y, acc[jj].y);
@@ -54,29 +61,45 @@ __global__ void __launch_bounds__(kWarps * 32)
         }
       }
     }
-    if (row) {
+  }
+  const bool use_beta = beta.x != 0.0 || beta.y != 0.0;
+  double mx = 0.0;
+  bool bad = false;
+  if (lane < n) {
+    double2* Cp = C + p * Q;
 #pragma unroll
-      for (int jj = 0; jj < JB; ++jj) {
-        const int j = j0 + jj;
-        if (j < n) {
-          double2* el = Cp + lane + (int64_t)j * n;
-          double2 v = cmul(alpha, acc[jj]);
-          if (use_beta) v = cadd(v, cmul(beta, *el));
-          *el = v;
-          const double h = hypot(v.x, v.y);
-          mx = fmax(mx, h);
-          bad |= !(h <= 1.7976931348623157e308);   // NaN or Inf
-        }
+    for (int jj = 0; jj < CW; ++jj) {
+      const int j = j0 + jj;
+      if (j < n) {
+        double2* el = Cp + lane + (int64_t)j * n;
+        double2 v = cmul(alpha, acc[jj]);
+        if (use_beta) v = cadd(v, cmul(beta, *el));
+        *el = v;
+        const double h = hypot(v.x, v.y);
+        mx = fmax(mx, h);
+        bad |= !(h <= 1.7976931348623157e308);   // NaN or Inf
       }
     }
   }
   if (maxabs) {
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(kFull, mx, o));
-    // a non-finite element makes the maximum NaN (fmax would drop it): the
-    // positive quiet NaN is above every finite bit pattern, so it stays
-    if (__any_sync(kFull, bad)) mx = __longlong_as_double(0x7ff8000000000000LL);
-    if (lane == 0)
+    bad = __any_sync(kFull, bad);
+    if (lane == 0) {
+      smx[w] = mx;
+      sbad[w] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      bool any = false;
+      for (int q = 0; q < kWarps; ++q) {
+        mx = fmax(mx, smx[q]);
+        any |= sbad[q] != 0;
+      }
+      // a non-finite element makes the maximum NaN (fmax would drop it): the
+      // positive quiet NaN is above every finite bit pattern, so it stays
+      if (any) mx = __longlong_as_double(0x7ff8000000000000LL);
       atomicMax(reinterpret_cast<unsigned long long*>(maxabs + p), (unsigned long long)__double_as_longlong(mx));
+    }
   }
 }
 
@@ -91,7 +114,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 template <int N>
 __global__ void __launch_bounds__(kWarps * 32)
     k_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count,
-                 int* info) {
+                 int* info, int* status, int singular_code) {
   __shared__ double2 prow[kWarps][N];
   __shared__ int sidx[kWarps][N];
   __shared__ int scm[kWarps][N];
@@ -110,21 +133,20 @@ __global__ void __launch_bounds__(kWarps * 32)
 #pragma unroll
   for (int k = 0; k < N; ++k) {
     if (k < n) {
-      // NaN ranks above everything (every lane must see one total order, and
-      // a NaN should spread to the whole inverse rather than be skipped)
-      double bv = used ? -1.0 : cabs1(r[k]);
-      if (bv != bv) bv = __longlong_as_double(0x7ff0000000000000LL);
-      int blg = lg, bl = lane;
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ov = __shfl_xor_sync(kFull, bv, o);
-        const int olg = __shfl_xor_sync(kFull, blg, o);
-        const int ol = __shfl_xor_sync(kFull, bl, o);
-        if (ov > bv || (ov == bv && olg < blg)) {
-          bv = ov;
-          blg = olg;
-          bl = ol;
-        }
-      }
+      // pivot search by integer warp reductions on the bit pattern of
+      // |Re|+|Im| (non-negative doubles order as their bits), + 1 so that an
+      // unused row with a zero entry still beats the used rows (key 0); NaN
+      // ranks above everything, so every lane sees one total order and a NaN
+      // spreads to the whole inverse rather than being skipped
+      double v = cabs1(r[k]);
+      if (v != v) v = __longlong_as_double(0x7ff0000000000000LL);
+      const unsigned long long key = used ? 0ull : (unsigned long long)__double_as_longlong(v) + 1ull;
+      const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+      const unsigned mhi = __reduce_max_sync(kFull, hi);
+      const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+      const bool cand = hi == mhi && lo == mlo;
+      const int blg = (int)__reduce_min_sync(kFull, cand ? (unsigned)lg : 0xffffffffu);
+      const int bl = __ffs(__ballot_sync(kFull, cand && lg == blg)) - 1;
       if (lane == bl) {
 #pragma unroll
         for (int c = 0; c < N; ++c)
@@ -179,6 +201,7 @@ __global__ void __launch_bounds__(kWarps * 32)
       if (c < n) Xp[lg + (int64_t)sidx[w][c] * n] = r[c];
   }
   if (lane == 0 && info) info[p] = inf;
+  if (lane == 0 && status && inf != 0 && status[p] == 0) status[p] = singular_code;
 }
 
 }  // namespace
@@ -188,23 +211,22 @@ cudaError_t launch_small_zgemm(int batch, int n, double2 alpha, const double2* A
                                cudaStream_t s) {
   if (batch <= 0) return cudaSuccess;
   if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
-  const int grid = (batch + kWarps - 1) / kWarps;
   if (n <= 16)
-    k_small_zgemm<16, 16><<<grid, kWarps * 32, 0, s>>>(batch, n, alpha, A, B, beta, C, Q, map, count, maxabs);
+    k_small_zgemm<16><<<batch, kWarps * 32, 0, s>>>(batch, n, alpha, A, B, beta, C, Q, map, count, maxabs);
   else
-    k_small_zgemm<32, 16><<<grid, kWarps * 32, 0, s>>>(batch, n, alpha, A, B, beta, C, Q, map, count, maxabs);
+    k_small_zgemm<32><<<batch, kWarps * 32, 0, s>>>(batch, n, alpha, A, B, beta, C, Q, map, count, maxabs);
   return cudaGetLastError();
 }
 
 cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
-                              const int* count, int* info, cudaStream_t s) {
+                              const int* count, int* info, int* status, int singular_code, cudaStream_t s) {
   if (batch <= 0) return cudaSuccess;
   if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
   const int grid = (batch + kWarps - 1) / kWarps;
   if (n <= 16)
-    k_small_zinv<16><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info);
+    k_small_zinv<16><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info, status, singular_code);
   else
-    k_small_zinv<32><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info);
+    k_small_zinv<32><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info, status, singular_code);
   return cudaGetLastError();
 }
 

@@ -1,5 +1,6 @@
 // Small-order block operations (n <= 32) for the lock-step FP64 form: one
-// warp per problem, every problem of a batch in one launch.  At these orders
+// CTA per product, one warp per inversion, every problem of a batch in one
+// launch.  At these orders
 // a product or an inversion is a few microseconds of dependent steps, so a
 // CTA working through one point's chain of them (the persistent engine)
 // leaves the FP64 pipe idle; a batch of warps, each holding one problem's
@@ -25,8 +26,9 @@ cudaError_t launch_small_zgemm(int batch, int n, double2 alpha, const double2* A
 // X_p = A_p^-1 by Gauss-Jordan elimination with partial pivoting (pivot =
 // max |Re|+|Im| over the rows not yet used, the lowest row on a tie: the
 // izamax rule of zgetrf) for the same problem selection; info[p] = 0 or the
-// 1-based column of the first zero pivot.  X may alias A.
+// 1-based column of the first zero pivot, and status[p] (optional) gets
+// singular_code there unless it holds a code already.  X may alias A.
 cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
-                              const int* count, int* info, cudaStream_t s);
+                              const int* count, int* info, int* status, int singular_code, cudaStream_t s);
 
 }  // namespace negf

@@ -12,9 +12,12 @@ from oracle import oracle as O
 
 @pytest.mark.gpu
 def test_sgf_cache_reuses_surface_gf(gpu_ctx):
+    """The cache lives in the persistent engine: the uncached reference call
+    runs there too (schedule 1), so the bits compare."""
     dev = G.transport_c0(nbl=6, n=8, seed=0)
     E = np.linspace(-2.5, 2.5, 21)
     did = gpu_ctx.upload(dev)
+    gpu_ctx.set_options(schedule=1)
     try:
         T0, nc0, st0 = gpu_ctx.transmission(did, E, eta=1e-6)
         gpu_ctx.set_sgf_cache(1, 64 << 20)
@@ -38,6 +41,7 @@ def test_sgf_cache_reuses_surface_gf(gpu_ctx):
         T4, nc4, _ = gpu_ctx.transmission(did, E, eta=1e-6)
         assert np.all(nc4 > 0) and np.array_equal(T4, T0)
     finally:
+        gpu_ctx.set_options()
         gpu_ctx.set_sgf_cache(0)
         gpu_ctx.release(did)
 
