@@ -20,6 +20,7 @@ oracle restatement, LAPACK zgetrf/zgetrs + zgemm, OpenMP over points) on the
 host cores on a bounded sample of the same workload.
 """
 import argparse
+import copy
 import ctypes
 import json
 import os
@@ -337,7 +338,8 @@ def scba_parity_summary(wl, devs, ids, E, got, ref, cores):
     return out
 
 
-def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ctx=None, dids=None, nworst=16):
+def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ctx=None, dids=None, nworst=64,
+                   nsamp=3):
     """GPU vs oracle on the CPU-baseline sample with the rule of the tests:
     |dT| <= max(1e-10 |T|, 1e-13) wherever the oracle's own change under
     rounding-level (1e-15 relative) perturbations of every input block stays
@@ -366,7 +368,7 @@ def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ct
     rng = np.random.default_rng(0)
     wq = np.asarray(worst)
     spread = np.zeros(len(worst))
-    for _ in range(2):
+    for _ in range(nsamp):
         for k in sorted(set(ids[wq].tolist())):          # one call per k-point, OpenMP over its points
             j = np.nonzero(ids[wq] == k)[0]
             d = copy.deepcopy(devs[k])
@@ -382,6 +384,9 @@ def parity_summary(wl, devs, ids, E, Tg, Tc, cores, ncyc_g=None, ncyc_c=None, ct
     ok = [bool(listed[j] and err[q] <= max(plain[q], 10 * spread[j])) for j, q in enumerate(worst)]
     out["beyond_1e-10_listed_by_oracle_spread"] = int(listed.sum())
     out["listed_within_10x_spread"] = int(sum(ok))
+    out["listing"] = ("a point beyond 1e-10 is listed when the oracle's own change under %d samples of 1e-15 "
+                      "relative input perturbations exceeds an eighth of the bound (the tests also sample the "
+                      "long-double and two FP64 restatements, too slow here)" % nsamp)
     # the four worst again at SGFACC = 1e-12, oracle and GPU
     w4 = wq[:4]
     recheck = []
@@ -630,7 +635,24 @@ def c2_segments(local, peak, digits):
             ms = e0.elapsed_time(e1)
             res[name] = (d_T.cpu().numpy().copy(), d_nc.cpu().numpy().copy(), d_st.cpu().numpy().copy(), ms,
                          clk.summary())
+        # the plain FP64 form's own change under 1e-15 relative perturbations of every
+        # device block (seeded): the conditioning of each point, measured on the GPU
         ctx.set_options()
+        rngp = np.random.default_rng(17)
+        hp = []
+        for d in devs:
+            dp = copy.deepcopy(d)
+            for name in ("h_diag", "h_upper", "h_lower", "s_diag", "s_upper", "s_lower", "lead_h00", "lead_h01",
+                         "lead_s00", "lead_s01", "hmc", "smc"):
+                lst = getattr(dp, name)
+                if lst is None:
+                    continue
+                for i in range(len(lst)):
+                    lst[i] = lst[i] * (1.0 + 1e-15 * rngp.standard_normal(lst[i].shape))
+            hp.append(ctx.upload(dp))
+        Tpert = ctx.transmission(np.asarray(hp, dtype=np.int32)[ids], E, eta=wl["eta"], check=False)[0]
+        for q in hp:
+            ctx.release(q)
     Tp, ncp, stp, msp, clkp = res["plain"]
     Tm, ncm, stm, msm, clkm = res["mixed"]
     flops = float(sum(flops_per_point(wl, int(c)) for c in ncp))
@@ -638,18 +660,36 @@ def c2_segments(local, peak, digits):
     out["c2_plain"] = {"solves_per_s": P / (msp * 1e-3), "ms": msp, "points": P, "achieved_tflops": achieved,
                        "frac_of_fp64_peak": achieved / peak, "status_counts": _counts(stp), "clocks": clkp}
     big = np.abs(Tp) > 1e-6
+    ok = (stm == 0) & np.isfinite(Tm)
     rel = np.abs(Tm - Tp) / np.where(big, np.abs(Tp), 1.0)
     absd = np.abs(Tm - Tp)
+    bound = np.maximum(1e-8 * np.abs(Tp), 1e-11)
+    spread = np.abs(Tpert - Tp)
+    listed = spread > bound / 8          # the FP64 form itself moves by more than an eighth of the bound
+    strict = ok & ~listed
+    lst_ok = ok & listed
+
+    def _mx(v, m):
+        return float(v[m].max()) if m.any() else None
     out["c2_mixed"] = {
         "solves_per_s": P / (msm * 1e-3), "ms": msm, "points": P, "digits": digits,
         "speedup_vs_plain": msp / msm,
         "error_vs_plain_fp64_gpu": {
-            "max_rel_T_gt_1e-6": float(rel[big].max()) if big.any() else None,
-            "mean_rel_T_gt_1e-6": float(rel[big].mean()) if big.any() else None,
-            "max_abs_T_le_1e-6": float(absd[~big].max()) if (~big).any() else None,
-            "beyond_1e-8": int(((rel > 1e-8) & big).sum() + ((absd > 1e-11) & ~big).sum()),
+            "bound": "max(1e-8 |T|, 1e-11)",
+            "points_with_status": int((~ok).sum()),
+            "strict_points": int(strict.sum()),
+            "strict_within_bound": int((strict & (absd <= bound)).sum()),
+            "strict_max_rel_T_gt_1e-6": _mx(rel, strict & big),
+            "strict_mean_rel_T_gt_1e-6": float(rel[strict & big].mean()) if (strict & big).any() else None,
+            "listed_points": int(listed.sum()),
+            "listed_within_10x_spread": int((lst_ok & (absd <= np.maximum(bound, 10 * spread))).sum()),
+            "listing": "a point is listed where the plain FP64 GPU form's own T moves by more than an eighth of "
+                       "the bound under 1e-15 relative perturbations of every device block (ill-conditioned at "
+                       "eta = 1e-6)",
+            "max_rel_T_gt_1e-6_all": _mx(rel, ok & big),
             "band_edge_points": int(is_edge.sum()),
-            "band_edge_max_rel": float(rel[is_edge & big].max()) if (is_edge & big).any() else None},
+            "band_edge_listed": int((is_edge & listed).sum()),
+            "band_edge_strict_max_rel": _mx(rel, is_edge & strict & big)},
         "decimation_ncyc_equal_to_plain": int((ncm == ncp).sum()),
         "status_counts": _counts(stm), "clocks": clkm,
         "form": "every block product on the int8 tensor cores (Ozaki digits, exact int32 accumulation), "

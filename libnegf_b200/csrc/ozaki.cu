@@ -430,6 +430,7 @@ __global__ void __launch_bounds__(kOzWarps * 32, 1)
       asm volatile("bar.sync 1, %0;" ::"n"(kOzEpiWarps * 32));
       double* T0 = a.t0 + (int64_t)item * a.m * a.n;
       double local_max = 0.0;
+      bool any_bad = false;
       for (int mi = 0; mi < 4; ++mi, ++ml) {
         const int part = mi >> 1, grp = mi & 1;
         if (!mbar_wait(&accb, ml & 1, &fail)) break;
@@ -508,7 +509,11 @@ __global__ void __launch_bounds__(kOzWarps * 32, 1)
               out = make_double2(qnan, qnan);
             }
             Cp[(int64_t)r + (int64_t)(c0 + j) * a.m] = out;
-            if (a.maxabs) local_max = fmax(local_max, hypot(out.x, out.y));
+            if (a.maxabs) {
+              const double h = hypot(out.x, out.y);
+              local_max = fmax(local_max, h);
+              any_bad |= !(h <= 1.7976931348623157e308);   // NaN or Inf
+            }
           }
         }
       }
@@ -516,7 +521,10 @@ __global__ void __launch_bounds__(kOzWarps * 32, 1)
       if (a.maxabs) {
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) local_max = fmax(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
-        if (lane == 0 && local_max > 0.0)
+        // a NaN or Inf element makes the maximum NaN (fmax drops it), which stays
+        // above every finite bit pattern under atomicMax: a convergence test on it fails
+        if (__any_sync(0xffffffffu, any_bad)) local_max = __longlong_as_double(0x7ff8000000000000LL);
+        if (lane == 0 && !(local_max <= 0.0))
           atomicMax(reinterpret_cast<unsigned long long*>(a.maxabs + prob),
                     (unsigned long long)__double_as_longlong(local_max));
       }

@@ -41,7 +41,8 @@ OzakiLayout ozaki_layout(int batch, int m, int n, int k, int slices);
 // strides sA/sB/sC in complex elements.  beta == 0: C is not read.  C may
 // alias A or B (the operands are split into the workspace first).  maxabs
 // (optional, one double per problem, non-negative, updated with atomicMax on
-// its bit pattern): max |C_p| over the stored elements.  status (optional,
+// its bit pattern): max |C_p| over the stored elements, NaN when one of them
+// is NaN or Inf.  status (optional,
 // one int per problem): 3 on a non-finite operand (C is NaN), 7 when a
 // pipeline wait ran out (C is not written).
 cudaError_t launch_ozaki_zgemm(int batch, int m, int n, int k, double2 alpha, const double2* A, int64_t sA,

@@ -130,54 +130,59 @@ __global__ void __launch_bounds__(kWarps * 32)
   int lg = lane;
   bool used = lane >= n;
   int inf = 0;
+  // the step loop stays rolled (a fully unrolled N x N body overflows the
+  // instruction cache); the register row is indexed by the unrolled column
+  // loop only, the pivot column picked out with selects
+#pragma unroll 1
+  for (int k = 0; k < n; ++k) {
+    double2 rk = r[0];
 #pragma unroll
-  for (int k = 0; k < N; ++k) {
-    if (k < n) {
-      // pivot search by integer warp reductions on the bit pattern of
-      // |Re|+|Im| (non-negative doubles order as their bits), + 1 so that an
-      // unused row with a zero entry still beats the used rows (key 0); NaN
-      // ranks above everything, so every lane sees one total order and a NaN
-      // spreads to the whole inverse rather than being skipped
-      double v = cabs1(r[k]);
-      if (v != v) v = __longlong_as_double(0x7ff0000000000000LL);
-      const unsigned long long key = used ? 0ull : (unsigned long long)__double_as_longlong(v) + 1ull;
-      const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
-      const unsigned mhi = __reduce_max_sync(kFull, hi);
-      const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
-      const bool cand = hi == mhi && lo == mlo;
-      const int blg = (int)__reduce_min_sync(kFull, cand ? (unsigned)lg : 0xffffffffu);
-      const int bl = __ffs(__ballot_sync(kFull, cand && lg == blg)) - 1;
-      if (lane == bl) {
+    for (int c = 1; c < N; ++c)
+      if (c == k) rk = r[c];
+    // pivot search by integer warp reductions on the bit pattern of
+    // |Re|+|Im| (non-negative doubles order as their bits), + 1 so that an
+    // unused row with a zero entry still beats the used rows (key 0); NaN
+    // ranks above everything, so every lane sees one total order and a NaN
+    // spreads to the whole inverse rather than being skipped
+    double v = cabs1(rk);
+    if (v != v) v = __longlong_as_double(0x7ff0000000000000LL);
+    const unsigned long long key = used ? 0ull : (unsigned long long)__double_as_longlong(v) + 1ull;
+    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+    const unsigned mhi = __reduce_max_sync(kFull, hi);
+    const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+    const bool cand = hi == mhi && lo == mlo;
+    const int blg = (int)__reduce_min_sync(kFull, cand ? (unsigned)lg : 0xffffffffu);
+    const int bl = __ffs(__ballot_sync(kFull, cand && lg == blg)) - 1;
+    if (lane == bl) {
 #pragma unroll
-        for (int c = 0; c < N; ++c)
-          if (c < n) prow[w][c] = r[c];
-      }
-      __syncwarp();
-      const double2 pv = prow[w][k];
-      if (pv.x == 0.0 && pv.y == 0.0 && inf == 0) inf = k + 1;
-      const double2 d = crecip(pv);
-      if (lane == bl) {
+      for (int c = 0; c < N; ++c)
+        if (c < n) prow[w][c] = r[c];
+    }
+    __syncwarp();
+    const double2 pv = prow[w][k];
+    if (pv.x == 0.0 && pv.y == 0.0 && inf == 0) inf = k + 1;
+    const double2 d = crecip(pv);
+    if (lane == bl) {
 #pragma unroll
-        for (int c = 0; c < N; ++c) r[c] = (c == k) ? d : cmul(r[c], d);
-      } else {
-        const double2 fd = cmul(r[k], d);
+      for (int c = 0; c < N; ++c) r[c] = (c == k) ? d : cmul(r[c], d);
+    } else {
+      const double2 fd = cmul(rk, d);
 #pragma unroll
-        for (int c = 0; c < N; ++c) {
-          if (c == k) {
-            r[c] = make_double2(-fd.x, -fd.y);
-          } else if (c < n) {
-            r[c] = csub(r[c], cmul(fd, prow[w][c]));
-          }
+      for (int c = 0; c < N; ++c) {
+        if (c == k) {
+          r[c] = make_double2(-fd.x, -fd.y);
+        } else if (c < n) {
+          r[c] = csub(r[c], cmul(fd, prow[w][c]));
         }
       }
-      if (lg == k) lg = blg;
-      if (lane == bl) {
-        lg = k;
-        used = true;
-      }
-      if (lane == 0) sidx[w][k] = blg;
-      __syncwarp();
     }
+    if (lg == k) lg = blg;
+    if (lane == bl) {
+      lg = k;
+      used = true;
+    }
+    if (lane == 0) sidx[w][k] = blg;
+    __syncwarp();
   }
   // column interchanges in reverse pivot order: output column dest[c] takes
   // internal column c

@@ -20,6 +20,9 @@ LIB_PATH = os.path.join(HERE, "libnegf_b200.so")
 
 OK, SINGULAR, NOT_CONVERGED, NONFINITE, NOMEM, BAD_ARG, CUDA, TIMEOUT, ADMISSION, NO_GPU = range(10)
 SCBA_NOT_CONVERGED = 10
+# codes that concern the whole call (nothing was solved): raised even with check=False, which
+# only lets per-point codes (SINGULAR, NOT_CONVERGED, NONFINITE, TIMEOUT, ...) through
+CALL_ERRORS = (BAD_ARG, NOMEM, CUDA, ADMISSION, NO_GPU)
 STATUS_NAMES = {0: "OK", 1: "SINGULAR", 2: "NOT_CONVERGED", 3: "NONFINITE", 4: "NOMEM", 5: "BAD_ARG",
                 6: "CUDA", 7: "TIMEOUT", 8: "ADMISSION", 9: "NO_GPU", 10: "SCBA_NOT_CONVERGED"}
 
@@ -274,7 +277,7 @@ class Context:
         st = np.zeros(n, dtype=np.int32)
         rc = self._L.negf_b200_transmissions(self._h, n, _i(ids), _d(E), eta, dos_delta, ni.size, _i(ni), _i(nf),
                                              _d(T), _d(led) if ldos else None, _i(ncyc), _i(st))
-        if check and rc not in (OK, NOT_CONVERGED):
+        if (check or rc in CALL_ERRORS) and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "transmissions: " + self.last_error())
         return T, (led[:, :nsets] if ldos else None), ncyc, st
 
@@ -330,7 +333,7 @@ class Context:
         rc = self._L.negf_b200_density(self._h, device_id, z.size, _d(er), _d(ei), _d(wt.view(np.float64)),
                                        _d(rd.view(np.float64)), _d(ru.view(np.float64)), _d(rl.view(np.float64)),
                                        _d(rdc.view(np.float64)), _d(rcd.view(np.float64)), _i(nc), _i(st))
-        if check and rc not in (OK, NOT_CONVERGED):
+        if (check or rc in CALL_ERRORS) and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "density: " + self.last_error())
         return split_blocks(pl, rd, ru, rl), split_outer(dev, rdc, rcd), nc, st
 
@@ -360,7 +363,7 @@ class Context:
                                            _d(cp) if cp is not None else None, _d(rd.view(np.float64)),
                                            _d(ru.view(np.float64)), _d(rl.view(np.float64)),
                                            _d(rdc.view(np.float64)), _d(rcd.view(np.float64)), _i(nc), _i(st))
-        if check and rc not in (OK, NOT_CONVERGED, SCBA_NOT_CONVERGED):
+        if (check or rc in CALL_ERRORS) and rc not in (OK, NOT_CONVERGED, SCBA_NOT_CONVERGED):
             raise NegfError(rc, "density_neq: " + self.last_error())
         return split_blocks(pl, rd, ru, rl), split_outer(dev, rdc, rcd), nc, st
 
@@ -381,7 +384,7 @@ class Context:
         ncyc = np.zeros(n, dtype=np.int32)
         st = np.zeros(n, dtype=np.int32)
         rc = self._L.negf_b200_transmission(self._h, n, _i(ids), _d(E), eta, ni, nf, _d(T), _i(ncyc), _i(st))
-        if check and rc not in (OK, NOT_CONVERGED):
+        if (check or rc in CALL_ERRORS) and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "transmission: " + self.last_error())
         return T, ncyc, st
 
@@ -396,7 +399,7 @@ class Context:
         st = np.zeros(n, dtype=np.int32)
         rc = self._L.negf_b200_transmission_dos(self._h, n, _i(ids), _d(E), eta, dos_delta, ni, nf, _d(T), _d(dos),
                                                 _i(ncyc), _i(st))
-        if check and rc not in (OK, NOT_CONVERGED):
+        if (check or rc in CALL_ERRORS) and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "transmission_dos: " + self.last_error())
         return T, dos, ncyc, st
 
@@ -420,7 +423,7 @@ class Context:
         st = np.zeros(n, dtype=np.int32)
         rc = self._L.negf_b200_meir_wingreen(self._h, n, _i(ids), _d(E), eta, _d(frm), _d(cp), _d(curr), _d(lcurr),
                                              _d(ldens), _i(it), _d(err), _i(ncyc), _i(st))
-        if check and rc not in (OK, NOT_CONVERGED):
+        if (check or rc in CALL_ERRORS) and rc not in (OK, NOT_CONVERGED):
             raise NegfError(rc, "meir_wingreen: " + self.last_error())
         return dict(curr=curr, layer_curr=lcurr[:, :nbl - 1], layer_dens=ldens, scba_iter=it, scba_err=err,
                     ncyc=ncyc, status=st)
