@@ -582,6 +582,40 @@ __device__ __forceinline__ double cta_max(double v, double* red) {
   return s;
 }
 
+// An inverse whose residual probe exceeds this gets a Newton step
+// X <- X + X (I - A X) (at most two): Gauss-Jordan is not backward stable,
+// and on a nearly singular matrix (the decimation's Ao near a lead
+// resonance) its residual can exceed the broadening eta that selects the
+// retarded solution, which the iteration then loses.  Backward-stable
+// inverses probe at 1e-14 .. 1e-10.
+constexpr double kInvProbeTol = 1e-7;
+
+// The fixed probe vector of cta_inv_probe: v_k = (1 + (k mod 7) / 8) - i (k mod 5) / 8.
+__device__ __forceinline__ double2 probe_v(int k) { return make_double2(1.0 + 0.125 * (k % 7), -0.125 * (k % 5)); }
+
+// Residual probe of a computed inverse X of A (order n, column major):
+// max_i |(A (X v))_i - v_i| for the fixed vector v above (|v_k| ~ 1): of the
+// order of the rounding of the product for an inverse that is backward
+// stable, far above it where the inversion lost accuracy (Gauss-Jordan on a
+// nearly singular matrix).  Two matrix-vector products; y is an n-element
+// shared-memory buffer.  NaN or Inf anywhere gives +Inf.
+__device__ __forceinline__ double cta_inv_probe(int n, const double2* A, const double2* X, double2* y, double* red) {
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(X[(size_t)r + (size_t)c * n], probe_v(c)));
+    y[r] = acc;
+  }
+  __syncthreads();
+  double e = 0.0;
+  for (int r = threadIdx.x; r < n; r += blockDim.x) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(A[(size_t)r + (size_t)c * n], y[c]));
+    const double d = cabs(csub(acc, probe_v(r)));
+    e = (d <= 1.7976931348623157e308) ? fmax(e, d) : __longlong_as_double(0x7ff0000000000000LL);
+  }
+  return cta_max(e, red);
+}
+
 // Re Tr(X Y) = sum_{i,j} Re(X(i,j) Y(j,i)); op applies to Y (OP_C: Y = Z^dag)
 __device__ __forceinline__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red,
                                                    const unsigned char* mask = nullptr) {

@@ -47,6 +47,29 @@ __device__ __forceinline__ int zinv(int n, const double2* A, double2* out, doubl
   return cta_zinv(n, A, out, ws, sm.main, sm.inv);
 }
 
+// zinv, then the residual probe and up to two Newton steps
+// X <- X + X (I - A X) where the probe exceeds kInvProbeTol (the engine's
+// refine block); R and Xn are n x n scratch.
+__device__ __noinline__ int zinv_refined(int n, const double2* A, double2* X, double2* ws, double2* R, double2* Xn,
+                                         SmemMap& sm) {
+  const int bad = zinv(n, A, X, ws, sm);
+  const double2 one = make_double2(1, 0), mone = make_double2(-1, 0);
+  const int nn = n * n;
+  for (int k = 0; k < 2; ++k) {
+    const double e = cta_inv_probe(n, A, X, sm.main, sm.red);
+    if (!(e > kInvProbeTol) || !(e <= 1.7976931348623157e308)) break;
+    for (int q = threadIdx.x; q < nn; q += blockDim.x) R[q] = make_double2((q % n) == (q / n) ? 1.0 : 0.0, 0.0);
+    __syncthreads();
+    gemm(n, n, n, opN(A, n), opN(X, n), R, n, mone, one, sm);     // R = I - A X
+    cta_copy(Xn, X, nn);
+    __syncthreads();
+    gemm(n, n, n, opN(X, n), opN(R, n), Xn, n, one, one, sm);     // X + X R
+    cta_copy(X, Xn, nn);
+    __syncthreads();
+  }
+  return bad;
+}
+
 // Sancho-Rubio decimation (src/contselfenergy.F90:271-340), CTA-cooperative.
 // In: Ao, Bo, Co in slot 0, 2, 3 (consumed).  Out: surface GF in *go_out
 // (one of the slots).  Returns a status.
@@ -68,7 +91,7 @@ __device__ __noinline__ int cta_decimation(int L, const Ws& w, double tol, int m
   int it;
   const double2 one = cz(1, 0), zero = cz(0, 0), mone = cz(-1, 0);
   for (it = 1; it <= max_iter; ++it) {
-    if (zinv(L, Ao, Go, w.inv(), sm)) st = ST_SINGULAR;
+    if (zinv_refined(L, Ao, Go, w.inv(), w.slot(8), w.slot(9), sm)) st = ST_SINGULAR;
     gemm(L, L, L, opN(Go, L), opN(Co, L), X, L, one, zero, sm);            // GoXCo
     gemm(L, L, L, opN(Co, L), opN(X, L), C1, L, one, zero, sm, true);      // C1 = Co GoXCo
     const double mx = *sm.maxv;
@@ -92,7 +115,7 @@ __device__ __noinline__ int cta_decimation(int L, const Ws& w, double tol, int m
   }
   ncyc = done ? it : max_iter + 1;
   if (!done && st == ST_OK) st = ST_NOT_CONVERGED;
-  if (zinv(L, Aos, Go, w.inv(), sm)) st = ST_SINGULAR;
+  if (zinv_refined(L, Aos, Go, w.inv(), w.slot(8), w.slot(9), sm)) st = ST_SINGULAR;
   *go_out = Go;
   return st;
 }
@@ -204,7 +227,8 @@ cudaError_t launch_zgemm_batched(int batch, int m, int n, int k, double2 alpha, 
   return cudaGetLastError();
 }
 
-size_t zinv_batched_work_elems(int n) { return zinv_ws_elems(n, kSmemMain); }
+// per matrix: the inversion's own buffers, then two n x n refinement buffers
+size_t zinv_batched_work_elems(int n) { return zinv_ws_elems(n, kSmemMain) + 2 * (size_t)n * n; }
 
 __global__ void __launch_bounds__(kThreads, 2)
     k_zinv_batched(int n, const double2* A, double2* Ainv, int* info, double2* work, int64_t wstride) {
@@ -213,7 +237,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   sm.tr.acc = nullptr;
   const int b = blockIdx.x;
   const int64_t nn = (int64_t)n * n;
-  int inf = zinv(n, A + b * nn, Ainv + b * nn, work + b * wstride, sm);
+  double2* wb = work + b * wstride;
+  double2* R = wb + zinv_ws_elems(n, kSmemMain);
+  int inf = zinv_refined(n, A + b * nn, Ainv + b * nn, wb, R, R + nn, sm);
   if (threadIdx.x == 0 && info) info[b] = inf;
 }
 
@@ -237,7 +263,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   sm.tr.acc = nullptr;
   const int b = blockIdx.x;
   const int p = map ? map[b] : b;
-  int inf = zinv(n, A + (int64_t)p * sA, X + (int64_t)p * sX, work + (int64_t)b * wstride, sm);
+  double2* wb = work + (int64_t)b * wstride;
+  double2* R = wb + zinv_ws_elems(n, kSmemMain);
+  int inf = zinv_refined(n, A + (int64_t)p * sA, X + (int64_t)p * sX, wb, R, R + (int64_t)n * n, sm);
   if (threadIdx.x == 0 && info) info[p] = inf;
 }
 

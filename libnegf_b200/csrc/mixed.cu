@@ -370,8 +370,14 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
   };
   auto inv = [&](int nb, const int* map, const int* count, const double2* A, double2* X) -> cudaError_t {
     ++nl;
-    if (small) return launch_small_zinv(nb, n, A, X, Q, map, count, w.info, w.pst, NEGF_B200_ERR_SINGULAR, s);
-    return launch_zinv_mapped(nb, n, A, Q, X, Q, map, w.info, w.zwork, s);
+    if (small) {
+      // the one-warp inversion, then its residual probe and Newton steps where needed
+      cudaError_t e = launch_small_zinv(nb, n, A, X, Q, map, count, w.info, w.pst, NEGF_B200_ERR_SINGULAR, s);
+      if (e != cudaSuccess) return e;
+      ++nl;
+      return launch_small_refine(nb, n, A, X, Q, map, count, s);
+    }
+    return launch_zinv_mapped(nb, n, A, Q, X, Q, map, w.info, w.zwork, s);   // probe and refinement inside
   };
   // FP64 products of the trace (the one-warp kernel at small orders, else the DMMA product)
   auto prod64 = [&](int nb, const double2* A, const double2* Bm, double2* C) -> cudaError_t {

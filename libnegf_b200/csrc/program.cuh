@@ -116,7 +116,10 @@ enum OpKind : int {
   K_LDOS,      // out[k] = sum over LDOS set k of dos[i-1] (A = dos row as doubles, device sets)
   K_ACCUM,     // C[q] += alpha * A[q], q < m (atomic: C is shared by all CTAs)
   K_SUBCOPY,   // C(flag + r, flag + c) = A(r, c), A m x m, C leading dimension ldc
+  K_RESPROBE,  // res[slot] = max_i |(A (B v))_i - v_i|, order m (cta_inv_probe: B a computed inverse of A)
+  K_EYE,       // C = identity, order m
 };
+
 
 struct Op {
   int kind;
@@ -305,6 +308,15 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
         o.C[(int64_t)(o.flag + r) + (int64_t)(o.flag + c) * o.ldc] = o.A[q];
       }
       break;
+    case K_RESPROBE: {
+      const double e = cta_inv_probe(o.m, o.A, o.B, sm.main, sm.red);
+      if (tid == 0) sm.res[o.slot] = e;
+      break;
+    }
+    case K_EYE:
+      for (int q = tid; q < o.m * o.m; q += blockDim.x)
+        o.C[q] = make_double2((q % o.m) == (q / o.m) ? 1.0 : 0.0, 0.0);
+      break;
     case K_ACCUM:
       for (int q = tid; q < o.m; q += blockDim.x) {
         const double2 v = cmul(o.alpha, o.A[q]);
@@ -329,6 +341,10 @@ struct Prog {
   double2 ec, ecs;      // ES-H energy, contact energy
   // contacts / decimation
   int c, L, ncb, it, ok, done, ib, ix, ic, ic1;
+  // inverse refinement (the `refine` block): matrix, its computed inverse, order, return point
+  const double2* rA;
+  double2* rX;
+  int rm, rret, rk;
   // sweeps
   int i, j, sub_first, cur, cc, last, tiny, pp, lo;
   double2* gnext;
@@ -345,6 +361,13 @@ struct Prog {
 };
 
 #define PT_EMIT(s) do { (s).pc = __LINE__; return true; case __LINE__:; } while (0)
+// Runs the `refine` block on the inverse X_ of A_ (order m_) and resumes here.
+#define PT_REFINE(s, A_, X_, m_)                                        \
+  do {                                                                  \
+    (s).rA = (A_); (s).rX = (X_); (s).rm = (m_); (s).rret = __LINE__;   \
+    goto refine;                                                        \
+    case __LINE__:;                                                     \
+  } while (0)
 
 __device__ __forceinline__ const double2* sig_on_block(const DevDesc* d, const Ws& w, int i, int& first) {
   first = -1;
@@ -405,6 +428,7 @@ __device__ __forceinline__ const unsigned char* tun_mask_of(const DevDesc* d, in
 __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& sm, const Ws& w, Op& o) {
   const double2 one = cz(1, 0), zero = cz(0, 0), mone = cz(-1, 0);
   double mx;
+dispatch:
   switch (s.pc) {
     case 0:
     for (;;) {
@@ -454,6 +478,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           o.kind = K_ZINV; o.m = s.L; o.A = w.slot(0); o.C = w.slot(4);
           PT_EMIT(s);
           if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          PT_REFINE(s, w.slot(0), w.slot(4), s.L);
           set_gemm(o, s.L, s.L, s.L, w.slot(4), s.L, OP_N, w.slot(s.ic), s.L, OP_N, w.slot(s.ix), s.L, one, zero);
           PT_EMIT(s);                                                                    // GoXCo
           set_gemm(o, s.L, s.L, s.L, w.slot(s.ic), s.L, OP_N, w.slot(s.ix), s.L, OP_N, w.slot(s.ic1), s.L, one,
@@ -483,6 +508,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         o.kind = K_ZINV; o.m = s.L; o.A = w.slot(1); o.C = w.slot(4);
         PT_EMIT(s);                                                                      // gs = Ao_s^-1
         if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+        PT_REFINE(s, w.slot(1), w.slot(4), s.L);
         if (a.sgf_out && a.sgf_out[(int64_t)s.p * a.ncont_max + s.c] >= 0) {
           // surface_green's add (:251-256)
           set_simple(o, K_COPY, s.L * s.L, w.slot(4), a.sgf_arena + a.sgf_out[(int64_t)s.p * a.ncont_max + s.c]);
@@ -495,6 +521,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           o.kind = K_ZINV; o.m = s.L; o.A = w.slot(4); o.C = w.slot(5);
           PT_EMIT(s);
           if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          PT_REFINE(s, w.slot(4), w.slot(5), s.L);
           set_esh(o, w.slot(0), s.L + s.d->surf[s.c], s.L + s.d->surf[s.c], s.d->hs + s.d->osurf[s.c],
                   s.d->has_ss ? s.d->ss + s.d->osurf[s.c] : nullptr, s.ecs, 1, nullptr, nullptr, OP_N);
           PT_EMIT(s);
@@ -505,6 +532,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           o.kind = K_ZINV; o.m = s.L; o.A = w.slot(0); o.C = w.slot(4);
           PT_EMIT(s);
           if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          PT_REFINE(s, w.slot(0), w.slot(4), s.L);
         }
         if (a.acc_lc && (a.mode == MODE_RHO || a.mode == MODE_GN)) {
           set_simple(o, K_COPY, s.L * s.L, w.slot(4), a.mode == MODE_RHO ? w.gskeep(s.c) : w.gnkeep(s.c));
@@ -562,6 +590,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
           o.kind = K_ZINV; o.m = s.d->pl[s.d->nbl - 1]; o.A = w.slot(0); o.C = s.gnext;
           PT_EMIT(s);
           if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+          PT_REFINE(s, w.slot(0), s.gnext, s.d->pl[s.d->nbl - 1]);
           s.pp = 1;
           for (s.i = s.d->nbl - 2; s.i >= 1; --s.i) {
             if (s.d->has_s) {
@@ -591,6 +620,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
             s.gnext = o.C;
             PT_EMIT(s);
             if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+            PT_REFINE(s, w.slot(0), s.gnext, s.d->pl[s.i]);
           }
         }
         // -------------------------------------- Gr(1,1)
@@ -619,6 +649,7 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
         o.kind = K_ZINV; o.m = s.d->pl[0]; o.A = w.slot(0); o.C = s.gsv;
         PT_EMIT(s);
         if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
+        PT_REFINE(s, w.slot(0), s.gsv, s.d->pl[0]);
         if (s.fast) {
           // ------------------------------------ 2-contact trace (iterative_cpu.F90:399-470)
           s.lo = s.d->pl[0];
@@ -1076,11 +1107,34 @@ __device__ __forceinline__ bool next_op(const EngineArgs& a, Prog& s, SmemMap& s
       }
       __syncthreads();
     }
+    goto program_end;
+
+    refine:
+      // residual probe of the inverse just formed; a Newton step where it failed
+      for (s.rk = 0; s.rk < 2; ++s.rk) {
+        o.kind = K_RESPROBE; o.m = s.rm; o.A = s.rA; o.B = s.rX; o.slot = 7;
+        PT_EMIT(s);
+        if (!(sm.res[7] > kInvProbeTol) || !(sm.res[7] <= 1.7976931348623157e308)) break;   // fine, or non-finite
+        o.kind = K_EYE; o.m = s.rm; o.C = w.slot(S_INV);
+        PT_EMIT(s);
+        set_gemm(o, s.rm, s.rm, s.rm, s.rA, s.rm, OP_N, s.rX, s.rm, OP_N, w.slot(S_INV), s.rm, mone, one);
+        PT_EMIT(s);                                                                      // R = I - A X
+        set_simple(o, K_COPY, s.rm * s.rm, s.rX, w.slot(S_INV + 1));
+        PT_EMIT(s);
+        set_gemm(o, s.rm, s.rm, s.rm, s.rX, s.rm, OP_N, w.slot(S_INV), s.rm, OP_N, w.slot(S_INV + 1), s.rm, one, one);
+        PT_EMIT(s);                                                                      // X + X R
+        set_simple(o, K_COPY, s.rm * s.rm, w.slot(S_INV + 1), s.rX);
+        PT_EMIT(s);
+      }
+      s.pc = s.rret;
+      goto dispatch;
   }
+program_end:
   s.pc = -1;
   return false;
 }
 
+#undef PT_REFINE
 #undef PT_EMIT
 
 // ---------------------------------------------------------------- stepping

@@ -5,6 +5,8 @@
 // identity (src/inversions.F90:807-839), at orders n <= 32.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "cta_ops.cuh"
 #include "small.cuh"
 
@@ -209,7 +211,106 @@ __global__ void __launch_bounds__(kWarps * 32)
   if (lane == 0 && status && inf != 0 && status[p] == 0) status[p] = singular_code;
 }
 
+// Residual probe of the inverse X of A and up to two Newton steps
+// X <- X + X (I - A X) where it exceeds kInvProbeTol (cta_inv_probe, the
+// engine's refine block), one CTA per problem with A, X and I - A X staged
+// in shared memory.  A problem whose probe passes costs two matrix-vector
+// products and leaves X untouched.
+template <int N>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count) {
+  extern __shared__ __align__(16) double2 sref[];
+  double2* sA = sref;
+  double2* sX = sA + N * N;
+  double2* sR = sX + N * N;
+  double2* y = sR + N * N;
+  __shared__ double red[kWarps];
+  const int b = blockIdx.x;
+  if (b >= batch_limit(batch, count)) return;
+  const int p = map ? map[b] : b;
+  const int nn = n * n;
+  const double2* Ap = A + p * Q;
+  double2* Xp = X + p * Q;
+  for (int q = threadIdx.x; q < nn; q += kWarps * 32) {
+    sA[q] = Ap[q];
+    sX[q] = Xp[q];
+  }
+  __syncthreads();
+  bool changed = false;
+  for (int round = 0; round < 2; ++round) {
+    // probe: y = X v, then max |A y - v|
+    for (int r = threadIdx.x; r < n; r += kWarps * 32) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(sX[r + c * n], probe_v(c)));
+      y[r] = acc;
+    }
+    __syncthreads();
+    double e = 0.0;
+    for (int r = threadIdx.x; r < n; r += kWarps * 32) {
+      double2 acc = make_double2(0.0, 0.0);
+      for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(sA[r + c * n], y[c]));
+      const double d = cabs(csub(acc, probe_v(r)));
+      e = (d <= 1.7976931348623157e308) ? fmax(e, d) : __longlong_as_double(0x7ff0000000000000LL);
+    }
+    for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(kFull, e, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    __syncthreads();
+    double em = 0.0;
+    for (int q = 0; q < kWarps; ++q) em = fmax(em, red[q]);
+    __syncthreads();
+    if (!(em > kInvProbeTol) || !(em <= 1.7976931348623157e308)) break;
+    // R = I - A X
+    for (int q = threadIdx.x; q < nn; q += kWarps * 32) {
+      const int i = q % n, j = q / n;
+      double2 acc = make_double2(i == j ? 1.0 : 0.0, 0.0);
+      for (int k = 0; k < n; ++k) acc = csub(acc, cmul(sA[i + k * n], sX[k + j * n]));
+      sR[q] = acc;
+    }
+    __syncthreads();
+    // X + X R, element by element into registers, then back into sX
+    double2 nx[N * N / (kWarps * 32) + 1];
+    int cnt = 0;
+    for (int q = threadIdx.x; q < nn; q += kWarps * 32, ++cnt) {
+      const int i = q % n, j = q / n;
+      double2 acc = sX[q];
+      for (int k = 0; k < n; ++k) acc = cadd(acc, cmul(sX[i + k * n], sR[k + j * n]));
+      nx[cnt] = acc;
+    }
+    __syncthreads();
+    cnt = 0;
+    for (int q = threadIdx.x; q < nn; q += kWarps * 32, ++cnt) sX[q] = nx[cnt];
+    __syncthreads();
+    changed = true;
+  }
+  if (changed)
+    for (int q = threadIdx.x; q < nn; q += kWarps * 32) Xp[q] = sX[q];
+}
+
 }  // namespace
+
+cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
+                                const int* count, cudaStream_t s) {
+  if (batch <= 0) return cudaSuccess;
+  if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
+  if (n <= 16) {
+    const size_t smem = (3 * 16 * 16 + 16) * sizeof(double2);
+    k_small_refine<16><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count);
+  } else {
+    const size_t smem = (3 * 32 * 32 + 32) * sizeof(double2);   // above the 48 KB default: opt in per device
+    static std::mutex mu;
+    static bool attr[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
+      cudaError_t e = cudaFuncSetAttribute(k_small_refine<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      if (dev >= 0 && dev < 64) attr[dev] = true;
+    }
+    k_small_refine<32><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count);
+  }
+  return cudaGetLastError();
+}
 
 cudaError_t launch_small_zgemm(int batch, int n, double2 alpha, const double2* A, const double2* B, double2 beta,
                                double2* C, int64_t Q, const int* map, const int* count, double* maxabs,

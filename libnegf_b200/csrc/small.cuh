@@ -31,4 +31,10 @@ cudaError_t launch_small_zgemm(int batch, int n, double2 alpha, const double2* A
 cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
                               const int* count, int* info, int* status, int singular_code, cudaStream_t s);
 
+// The residual probe of each inverse X_p of A_p (same problem selection) and
+// up to two Newton steps X <- X + X (I - A X) where it shows a loss of
+// accuracy (kInvProbeTol); X_p is left untouched where it does not.
+cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
+                                const int* count, cudaStream_t s);
+
 }  // namespace negf

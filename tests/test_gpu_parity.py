@@ -62,6 +62,38 @@ def test_zgemm_batched(m, n, k, dagger):
     assert np.abs(got - ref).max() <= 1e-13 * max(1.0, np.abs(ref).max()) * np.sqrt(k)
 
 
+@pytest.mark.parametrize("n", [24, 96, 256, 512])
+def test_zinv_residual_on_nearly_singular_matrices(n):
+    """Gauss-Jordan is not backward stable: on a matrix with condition number
+    1e9-1e11 its residual A X - I can reach 1e-5 where an LU inverse stays at
+    1e-10.  The inverse comes back with the residual of a backward-stable
+    one (residual probe, Newton steps where it fails), the forward error
+    within cond * eps."""
+    rng = np.random.default_rng(100 + n)
+    b = 3
+    A = np.empty((b, n, n), dtype=np.complex128)
+    for i, c in enumerate((1e9, 1e10, 1e11)):
+        U = np.linalg.qr(_rand(rng, (n, n)))[0]
+        V = np.linalg.qr(_rand(rng, (n, n)))[0]
+        A[i] = (U * np.geomspace(1.0, 1.0 / c, n)) @ V
+    dA = _dev(A)
+    dX = torch.empty_like(dA)
+    info = torch.zeros(b, dtype=torch.int32, device="cuda")
+    L = native.load()
+    work = torch.empty(L.negf_b200_zinv_work_bytes(b, n), dtype=torch.uint8, device="cuda")
+    rc = L.negf_b200_zinv_batched(b, n, dA.data_ptr(), dX.data_ptr(), info.data_ptr(), work.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0 and int(info.abs().sum()) == 0
+    X = _host(dX, n, n)
+    for i in range(b):
+        Xr = np.linalg.inv(A[i])
+        res = np.abs(A[i] @ X[i] - np.eye(n)).max()
+        res_lu = np.abs(A[i] @ Xr - np.eye(n)).max()
+        assert res <= max(100 * res_lu, 1e-9), (i, res, res_lu)
+        cond = np.linalg.cond(A[i])
+        assert np.abs(X[i] - Xr).max() <= 1e-14 * cond * np.abs(Xr).max() * n
+
+
 @pytest.mark.parametrize("n", [1, 2, 5, 16, 33, 64, 65, 100, 128, 200, 256, 257, 512, 513, 777, 1024])
 def test_zinv_batched(n):
     rng = np.random.default_rng(n)
@@ -429,3 +461,47 @@ def test_bound_surface_parity(gpu_ctx, gen):
         gpu_ctx.set_options()
         gpu_ctx.release(did)
         gpu_ctx.release(d0)
+
+
+def test_c2_point_near_a_lead_resonance(gpu_ctx):
+    """The block-512 device (60 layers, k = 0, S = I + 0.05 R) at grid point
+    296 of 1024 on [-2, 2] eV, eta = 1e-6.  The second contact's decimation
+    meets a nearly singular Ao (condition 4e8) on its second iteration; a
+    Gauss-Jordan inverse with a 1e-5 residual there (far above eta) once
+    drove the iteration to a wrong, non-retarded surface Green's function
+    (T = 10.01 against 2.22700 in long double).  The engine's T and the
+    decimation primitive's gs must stay on the retarded solution, within
+    the oracle's own FP64 scatter there (the CPU FP64 paths take 47, 48
+    and 57 iterations at this point)."""
+    dev = G.transport_c1_kpoints([0.0], nbl=60, n=512, seed=1)[0]
+    E = np.array([-0.8426197458455522])
+    did = gpu_ctx.upload(dev)
+    try:
+        T, ncyc, st = gpu_ctx.transmission(did, E, eta=1e-6)
+        ref, spread = oracle_spread(_o_T(E, eta=1e-6), dev, nsamp=2)
+        assert np.all(st == 0)
+        assert abs(T[0] - 2.22700145) <= max(10 * spread["T"][0], 2e-3), (T, ref["T"], spread["T"])
+        assert abs(T[0] - ref["T"][0]) <= max(10 * spread["T"][0], 2e-3)
+    finally:
+        gpu_ctx.release(did)
+    # the failing contact's surface Green's function from the decimation primitive
+    n = dev.lead_size[1]
+    Ec = E[0] + 1e-6j
+    S00 = np.eye(n) if dev.lead_s00 is None else dev.lead_s00[1]
+    S01 = np.zeros((n, n)) if dev.lead_s01 is None else dev.lead_s01[1]
+    Ao = Ec * S00 - dev.lead_h00[1]
+    Bo = Ec * S01 - dev.lead_h01[1]
+    Co = np.conj(np.conj(Ec) * S01 - dev.lead_h01[1]).T
+    L = native.load()
+    dA, dB, dC = _dev(Ao[None]), _dev(Bo[None]), _dev(Co[None])
+    dG = torch.empty_like(dA)
+    nc = torch.zeros(1, dtype=torch.int32, device="cuda")
+    work = torch.empty(L.negf_b200_decimation_work_bytes(1, n), dtype=torch.uint8, device="cuda")
+    rc = L.negf_b200_decimation_batched(1, n, dA.data_ptr(), dB.data_ptr(), dC.data_ptr(), dG.data_ptr(),
+                                        nc.data_ptr(), 1e-9, 300, work.data_ptr(), None)
+    torch.cuda.synchronize()
+    assert rc == 0
+    Gg = _host(dG, n, n)[0]
+    Gc, ncc, _ = O.decimation(Ao, Bo, Co, 1e-9, 300)
+    assert np.abs(Gg - Gc).max() <= 1e-2 * np.abs(Gc).max()       # FP64 paths differ by ~6e-4 here
+    assert abs(np.trace(Gg).imag - np.trace(Gc).imag) <= 1e-2 * abs(np.trace(Gc).imag)
