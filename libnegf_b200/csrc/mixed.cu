@@ -415,35 +415,44 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       int it = 1;
       for (; it <= a.sgf_max_iter && na > 0; ++it) {
         MCK(inv(na, cur, cnt_cur, Ao, Go), "zinv");
-        if (!small) {
-          k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
-          ++nl;
-        }
-        MCK(prod(na, cur, cnt_cur, one, Go, Co, zero, X, nullptr), "GoXCo");
-        MCK(prod(na, cur, cnt_cur, one, Co, X, zero, C1, w.mx), "C1");
-        k_dec_check<<<1, 1024, 0, s>>>(na, cnt_cur, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt,
-                                       small ? cnt_nxt : w.count); ++nl;
-        MCK(cudaGetLastError(), "check");
-        std::swap(cur, nxt);
         if (small) {
+          // the rest of the iteration in two fused launches, one CTA per point
+          MCK(cudaMemsetAsync(cnt_nxt, 0, sizeof(int), s), "memset count");
+          MCK(launch_small_dec_a(na, n, cur, cnt_cur, Go, Co, Bo, C1, Ao, Aos, Q, w.ok, ncyc_c, a.sgf_tol, it, nxt,
+                                 cnt_nxt, s), "decimation a");
+          MCK(launch_small_dec_b(na, n, nxt, cnt_nxt, Go, Bo, Co, B1, Ao, Q, s), "decimation b");
+          nl += 2;
+          std::swap(cur, nxt);
           std::swap(cnt_cur, cnt_nxt);
+          std::swap(B[2], B[8]);
+          std::swap(B[3], B[6]);
+          Bo = B[2]; Co = B[3]; B1 = B[8]; C1 = B[6];
           if (it % kPoll == 0) {
             MCK(cudaMemcpyAsync(&na, cnt_cur, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
             MCK(cudaStreamSynchronize(s), "sync");
-            if (na == 0) break;
           }
-        } else {
+          continue;
+        }
+        // the mixed form: one batched product per step, the active list compacted on the host
+        k_info_to_status<<<(na + 255) / 256, 256, 0, s>>>(na, nullptr, cur, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+        ++nl;
+        MCK(prod(na, cur, nullptr, one, Go, Co, zero, X, nullptr), "GoXCo");
+        MCK(prod(na, cur, nullptr, one, Co, X, zero, C1, w.mx), "C1");
+        k_dec_check<<<1, 1024, 0, s>>>(na, nullptr, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt, w.count); ++nl;
+        MCK(cudaGetLastError(), "check");
+        std::swap(cur, nxt);
+        {
           int h_count = 0;
           MCK(cudaMemcpyAsync(&h_count, w.count, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
           MCK(cudaStreamSynchronize(s), "sync");
           na = h_count;
           if (na == 0) break;
         }
-        MCK(prod(na, cur, cnt_cur, one, Bo, X, zero, B1, nullptr), "Self");
-        k_sub_self<<<dim3(gx, na), eb, 0, s>>>(Q, cur, cnt_cur, B1, Ao, Aos, Q); ++nl;
-        MCK(prod(na, cur, cnt_cur, one, Go, Bo, zero, Y, nullptr), "GoXBo");
-        MCK(prod(na, cur, cnt_cur, one, Bo, Y, zero, B1, nullptr), "B1");
-        MCK(prod(na, cur, cnt_cur, mone, Co, Y, one, Ao, nullptr), "Ao update");
+        MCK(prod(na, cur, nullptr, one, Bo, X, zero, B1, nullptr), "Self");
+        k_sub_self<<<dim3(gx, na), eb, 0, s>>>(Q, cur, nullptr, B1, Ao, Aos, Q); ++nl;
+        MCK(prod(na, cur, nullptr, one, Go, Bo, zero, Y, nullptr), "GoXBo");
+        MCK(prod(na, cur, nullptr, one, Bo, Y, zero, B1, nullptr), "B1");
+        MCK(prod(na, cur, nullptr, mone, Co, Y, one, Ao, nullptr), "Ao update");
         // Bo = B1, Co = C1 for every point still iterating (the others are done with them)
         std::swap(B[2], B[8]);
         std::swap(B[3], B[6]);

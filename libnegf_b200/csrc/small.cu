@@ -211,6 +211,175 @@ __global__ void __launch_bounds__(kWarps * 32)
   if (lane == 0 && status && inf != 0 && status[p] == 0) status[p] = singular_code;
 }
 
+// ---------------------------------------------------------------- decimation steps
+// Row `lane` of columns [w CW, (w + 1) CW) of A B, A and B n x n in shared
+// memory (the product of k_small_zgemm, for the fused steps below).
+template <int N>
+__device__ __forceinline__ void mm_rows(int n, const double2* sA, const double2* sB, double2 (&acc)[N / kWarps]) {
+  constexpr int CW = N / kWarps;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int jj = 0; jj < CW; ++jj) acc[jj] = make_double2(0.0, 0.0);
+  if (lane >= n) return;
+  for (int k = 0; k < n; ++k) {
+    const double2 a = sA[lane + k * n];
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj) {
+      const int j = w * CW + jj;
+      if (j < n) {
+        const double2 bv = sB[k + j * n];
+        acc[jj].x = fma(a.x, bv.x, acc[jj].x);
+        acc[jj].x = fma(-a.y, bv.y, acc[jj].x);
+        acc[jj].y = fma(a.x, bv.y, acc[jj].y);
+        acc[jj].y = fma(a.y, bv.x, acc[jj].y);
+      }
+    }
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void stage(int n, double2* dst, const double2* src) {
+  for (int q = threadIdx.x; q < n * n; q += kWarps * 32) dst[q] = src[q];
+}
+
+// First half of a decimation iteration (src/contselfenergy.F90:271-340) for
+// the points list[b], b < *count, one CTA each: X = Go Co, C1 = Co X, the
+// CPU convergence rule on max|C1| (a point is done on its second
+// consecutive max|C1| <= tol: ncyc = it; the others go on to next[]), and
+// for the points that go on Self = Bo X, Ao -= Self, Aos -= Self.
+template <int N>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_small_dec_a(int n, const int* list, const int* count, int P, const double2* Go, const double2* Co,
+                  const double2* Bo, double2* C1, double2* Ao, double2* Aos, int64_t Q, int* ok, int* ncyc_c,
+                  double tol, int it, int* next, int* next_count) {
+  constexpr int CW = N / kWarps;
+  extern __shared__ __align__(16) double2 sdec[];
+  double2* sG = sdec;
+  double2* sC = sG + N * N;
+  double2* sB = sC + N * N;
+  double2* sX = sB + N * N;
+  __shared__ double smx[kWarps];
+  __shared__ int sgo;
+  const int b = blockIdx.x;
+  if (b >= min(*count, P)) return;
+  const int p = list[b];
+  const int64_t o = p * Q;
+  stage<N>(n, sG, Go + o);
+  stage<N>(n, sC, Co + o);
+  stage<N>(n, sB, Bo + o);
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 acc[CW];
+  mm_rows<N>(n, sG, sC, acc);                      // X = Go Co
+  if (lane < n)
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj)
+      if (w * CW + jj < n) sX[lane + (w * CW + jj) * n] = acc[jj];
+  __syncthreads();
+  mm_rows<N>(n, sC, sX, acc);                      // C1 = Co X
+  double mx = 0.0;
+  bool bad = false;
+  if (lane < n)
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj) {
+      const int j = w * CW + jj;
+      if (j < n) {
+        C1[o + lane + j * n] = acc[jj];
+        const double h = hypot(acc[jj].x, acc[jj].y);
+        mx = fmax(mx, h);
+        bad |= !(h <= 1.7976931348623157e308);
+      }
+    }
+  for (int s = 16; s > 0; s >>= 1) mx = fmax(mx, __shfl_xor_sync(kFull, mx, s));
+  if (__any_sync(kFull, bad)) mx = __longlong_as_double(0x7ff8000000000000LL);
+  if (lane == 0) smx[w] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = smx[0];
+    for (int q = 1; q < kWarps; ++q) m = (m != m || smx[q] != smx[q]) ? m + smx[q] : fmax(m, smx[q]);
+    bool go = true;
+    if (m <= tol) {
+      if (ok[p]) {
+        go = false;
+        ncyc_c[p] = it;
+      }
+      ok[p] = 1;
+    } else {
+      ok[p] = 0;
+    }
+    if (go) next[atomicAdd(next_count, 1)] = p;
+    sgo = go;
+  }
+  __syncthreads();
+  if (!sgo) return;
+  mm_rows<N>(n, sB, sX, acc);                      // Self = Bo X
+  if (lane < n)
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj) {
+      const int j = w * CW + jj;
+      if (j < n) {
+        const int64_t q = o + lane + j * n;
+        Ao[q] = csub(Ao[q], acc[jj]);
+        Aos[q] = csub(Aos[q], acc[jj]);
+      }
+    }
+}
+
+// Second half, for the points that go on (list, count): Y = Go Bo,
+// B1 = Bo Y, Ao -= Co Y (Co before this iteration's update).
+template <int N>
+__global__ void __launch_bounds__(kWarps * 32)
+    k_small_dec_b(int n, const int* list, const int* count, int P, const double2* Go, const double2* Bo,
+                  const double2* Co, double2* B1, double2* Ao, int64_t Q) {
+  constexpr int CW = N / kWarps;
+  extern __shared__ __align__(16) double2 sdec[];
+  double2* sG = sdec;
+  double2* sB = sG + N * N;
+  double2* sC = sB + N * N;
+  double2* sY = sC + N * N;
+  const int b = blockIdx.x;
+  if (b >= min(*count, P)) return;
+  const int p = list[b];
+  const int64_t o = p * Q;
+  stage<N>(n, sG, Go + o);
+  stage<N>(n, sB, Bo + o);
+  stage<N>(n, sC, Co + o);
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 acc[CW];
+  mm_rows<N>(n, sG, sB, acc);                      // Y = Go Bo
+  if (lane < n)
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj)
+      if (w * CW + jj < n) sY[lane + (w * CW + jj) * n] = acc[jj];
+  __syncthreads();
+  mm_rows<N>(n, sB, sY, acc);                      // B1 = Bo Y
+  if (lane < n)
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj)
+      if (w * CW + jj < n) B1[o + lane + (w * CW + jj) * n] = acc[jj];
+  mm_rows<N>(n, sC, sY, acc);                      // Ao -= Co Y
+  if (lane < n)
+#pragma unroll
+    for (int jj = 0; jj < CW; ++jj) {
+      const int j = w * CW + jj;
+      if (j < n) Ao[o + lane + j * n] = csub(Ao[o + lane + j * n], acc[jj]);
+    }
+}
+
+// Dynamic shared memory above the 48 KB default needs an opt-in per device.
+template <typename K>
+cudaError_t opt_in(K kernel, size_t smem, bool (&done)[64], std::mutex& mu) {
+  if (smem <= 48 * 1024) return cudaSuccess;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev >= 0 && dev < 64 && done[dev]) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && dev >= 0 && dev < 64) done[dev] = true;
+  return e;
+}
+
 // Residual probe of the inverse X of A and up to two Newton steps
 // X <- X + X (I - A X) where it exceeds kInvProbeTol (cta_inv_probe, the
 // engine's refine block), one CTA per problem with A, X and I - A X staged
@@ -308,6 +477,51 @@ cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, 
       if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     k_small_refine<32><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_small_dec_a(int P, int n, const int* list, const int* count, const double2* Go,
+                               const double2* Co, const double2* Bo, double2* C1, double2* Ao, double2* Aos,
+                               int64_t Q, int* ok, int* ncyc_c, double tol, int it, int* next, int* next_count,
+                               cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
+  static std::mutex mu;
+  static bool done16[64] = {false}, done32[64] = {false};
+  if (n <= 16) {
+    const size_t smem = 4 * 16 * 16 * sizeof(double2);
+    cudaError_t e = opt_in(k_small_dec_a<16>, smem, done16, mu);
+    if (e != cudaSuccess) return e;
+    k_small_dec_a<16><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, Ao, Aos, Q, ok, ncyc_c, tol,
+                                                   it, next, next_count);
+  } else {
+    const size_t smem = 4 * 32 * 32 * sizeof(double2);
+    cudaError_t e = opt_in(k_small_dec_a<32>, smem, done32, mu);
+    if (e != cudaSuccess) return e;
+    k_small_dec_a<32><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, Ao, Aos, Q, ok, ncyc_c, tol,
+                                                   it, next, next_count);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_small_dec_b(int P, int n, const int* list, const int* count, const double2* Go,
+                               const double2* Bo, const double2* Co, double2* B1, double2* Ao, int64_t Q,
+                               cudaStream_t s) {
+  if (P <= 0) return cudaSuccess;
+  if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
+  static std::mutex mu;
+  static bool done16[64] = {false}, done32[64] = {false};
+  if (n <= 16) {
+    const size_t smem = 4 * 16 * 16 * sizeof(double2);
+    cudaError_t e = opt_in(k_small_dec_b<16>, smem, done16, mu);
+    if (e != cudaSuccess) return e;
+    k_small_dec_b<16><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Bo, Co, B1, Ao, Q);
+  } else {
+    const size_t smem = 4 * 32 * 32 * sizeof(double2);
+    cudaError_t e = opt_in(k_small_dec_b<32>, smem, done32, mu);
+    if (e != cudaSuccess) return e;
+    k_small_dec_b<32><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Bo, Co, B1, Ao, Q);
   }
   return cudaGetLastError();
 }
