@@ -474,7 +474,11 @@ int negf_b200_zgemm_batched_i8(int32_t batch, int32_t m, int32_t n, int32_t k,
  * = cusolverDnZgetrf + Zgetrs against the identity (src/gpuroutines.cu:
  * 449-523) and zinv (src/inversions.F90:807-839).  `work` is a device buffer
  * of negf_b200_zinv_work_bytes(batch, n) bytes; info[b] = 0 or the 1-based
- * column of the first zero pivot. */
+ * column of the first zero pivot.  Gauss-Jordan is not backward stable: each
+ * inverse is checked by a residual probe, max |A (X v) - v| for a fixed v,
+ * and gets up to two Newton steps X + X (I - A X) where it exceeds 1e-7 (the
+ * residual of a backward-stable inverse).  For n <= 64 `work` may be NULL:
+ * the probe is then skipped. */
 size_t negf_b200_zinv_work_bytes(int32_t batch, int32_t n);
 int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A,
                            double* Ainv, int32_t* info, void* work,

@@ -1072,9 +1072,9 @@ static int run_lockstep(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_ids, 
   int st = sync_descs(ctx);
   if (st) return st;
   const int n = sh.n;
-  // the mixed form: two waves of resident Ozaki tiles plus a margin (512 on a
-  // B200); the small form: the whole call at once up to 8192 points
-  int batch = std::min<int>(npts, slices ? 2 * std::max(ctx->sms, 1) + 216 : 8192);
+  // the mixed form: two full waves of the inversion (one CTA per matrix, two
+  // per SM: 592 on a B200); the small form: the whole call at once up to 8192
+  int batch = std::min<int>(npts, slices ? 4 * std::max(ctx->sms, 1) : 8192);
   if (ctx->ws_limit) batch = std::min(batch, negf::mixed_batch_for(ctx->ws_limit, n, slices));
   if (batch < 1) return fail(ctx, NEGF_B200_ERR_ADMISSION, "the workspace limit is below one point of lock step");
   for (;;) {
@@ -1639,7 +1639,8 @@ int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A, double* Ai
                            void* stream) {
   if (batch < 0 || n < 0 || n > negf::kMaxOrder) return NEGF_B200_ERR_BAD_ARG;
   if (batch == 0 || n == 0) return NEGF_B200_OK;
-  if (!A || !Ainv || (negf::zinv_batched_work_elems(n) > 0 && !work)) return NEGF_B200_ERR_BAD_ARG;
+  // work may be null where the inversion needs no buffers of its own (n <= 64): the residual probe is skipped
+  if (!A || !Ainv || (negf::zinv_batched_work_elems(n) > 2 * (size_t)n * n && !work)) return NEGF_B200_ERR_BAD_ARG;
   cudaError_t e = negf::launch_zinv_batched(batch, n, (const double2*)A, (double2*)Ainv, info, (double2*)work,
                                             (cudaStream_t)stream);
   return e == cudaSuccess ? NEGF_B200_OK : NEGF_B200_ERR_CUDA;

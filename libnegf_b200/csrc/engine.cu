@@ -49,13 +49,13 @@ __device__ __forceinline__ int zinv(int n, const double2* A, double2* out, doubl
 
 // zinv, then the residual probe and up to two Newton steps
 // X <- X + X (I - A X) where the probe exceeds kInvProbeTol (the engine's
-// refine block); R and Xn are n x n scratch.
+// refine block); R and Xn are n x n scratch (R null: no probe).
 __device__ __noinline__ int zinv_refined(int n, const double2* A, double2* X, double2* ws, double2* R, double2* Xn,
                                          SmemMap& sm) {
   const int bad = zinv(n, A, X, ws, sm);
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0);
   const int nn = n * n;
-  for (int k = 0; k < 2; ++k) {
+  for (int k = 0; k < 2 && R; ++k) {
     const double e = cta_inv_probe(n, A, X, sm.main, sm.red);
     if (!(e > kInvProbeTol) || !(e <= 1.7976931348623157e308)) break;
     for (int q = threadIdx.x; q < nn; q += blockDim.x) R[q] = make_double2((q % n) == (q / n) ? 1.0 : 0.0, 0.0);
@@ -237,9 +237,9 @@ __global__ void __launch_bounds__(kThreads, 2)
   sm.tr.acc = nullptr;
   const int b = blockIdx.x;
   const int64_t nn = (int64_t)n * n;
-  double2* wb = work + b * wstride;
-  double2* R = wb + zinv_ws_elems(n, kSmemMain);
-  int inf = zinv_refined(n, A + b * nn, Ainv + b * nn, wb, R, R + nn, sm);
+  double2* wb = work ? work + b * wstride : nullptr;
+  double2* R = work ? wb + zinv_ws_elems(n, kSmemMain) : nullptr;
+  int inf = zinv_refined(n, A + b * nn, Ainv + b * nn, wb, R, R ? R + nn : nullptr, sm);
   if (threadIdx.x == 0 && info) info[b] = inf;
 }
 
