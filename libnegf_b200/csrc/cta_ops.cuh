@@ -588,7 +588,10 @@ __device__ __forceinline__ double cta_max(double v, double* red) {
 // resonance) its residual can exceed the broadening eta that selects the
 // retarded solution, which the iteration then loses.  Backward-stable
 // inverses probe at 1e-14 .. 1e-10.
-constexpr double kInvProbeTol = 1e-7;
+#ifndef NEGF_INV_PROBE_TOL
+#define NEGF_INV_PROBE_TOL 1e-7
+#endif
+constexpr double kInvProbeTol = NEGF_INV_PROBE_TOL;
 
 // The fixed probe vector of cta_inv_probe: v_k = (1 + (k mod 7) / 8) - i (k mod 5) / 8.
 __device__ __forceinline__ double2 probe_v(int k) { return make_double2(1.0 + 0.125 * (k % 7), -0.125 * (k % 5)); }

@@ -252,6 +252,43 @@ __global__ void k_trace(int n, const double2* Gam, const double2* G, const doubl
   }
 }
 
+// Points whose surface Green's function left the retarded solution: the
+// diagonal of -Im gs must be >= 0 (up to 1e-6 of the largest |gs_ii|); a
+// converged fixed point of the wrong kind, or one that is not finite, marks
+// the point for the engine (redo[p] = 1).  One CTA per point.
+__global__ void k_retarded_check(int n, const double2* gs, int64_t Q, int* redo) {
+  const int p = blockIdx.x;
+  double lo = 1.7976931348623157e308, hi = 0.0;
+  int bad = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const double2 g = gs[p * Q + (int64_t)i * (n + 1)];
+    const double v = -g.y, h = sqrt(g.x * g.x + g.y * g.y);
+    if (!(h <= 1.7976931348623157e308)) bad = 1;
+    else {
+      lo = fmin(lo, v);
+      hi = fmax(hi, h);
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  __shared__ double slo[32], shi[32];
+  __shared__ int sbad[32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { slo[w] = lo; shi[w] = hi; sbad[w] = bad; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) {
+      lo = fmin(lo, slo[q]);
+      hi = fmax(hi, shi[q]);
+      bad |= sbad[q];
+    }
+    if (bad || (hi > 0.0 && lo < -1e-6 * hi)) redo[p] = 1;
+  }
+}
+
 __global__ void k_iota(int n, int* v, int* count) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) v[b] = b;
   if (count && blockIdx.x == 0 && threadIdx.x == 0) *count = n;
@@ -273,7 +310,7 @@ struct Carver {
 struct Ws {
   double2* blk[kBlocks];
   double* mx;
-  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst;
+  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst, *redo;
   double* tb;
   double2* zwork;
   void* oz;
@@ -294,6 +331,7 @@ Ws carve(void* base, int P, int n, int slices, size_t* total) {
   w.info = c.take<int>(P);
   w.pst = c.take<int>(P);
   w.tb = c.take<double>(P);
+  w.redo = c.take<int>(P);
   const bool small = slices == 0;        // the lock-step FP64 form: one-warp kernels, no splitting
   w.zwork = c.take<double2>(small ? 1 : (size_t)P * zinv_batched_work_elems(n) + 1);
   w.oz = small ? nullptr : c.take<uint8_t>(ozaki_layout(P, n, n, n, slices).total);
@@ -395,6 +433,7 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
     const int* ids = a.d_ids + p0;
     const double* E = a.d_E + p0;
     MCK(cudaMemsetAsync(w.pst, 0, sizeof(int) * P, s), "memset status");
+    MCK(cudaMemsetAsync(w.redo, 0, sizeof(int) * P, s), "memset redo");
     // ---- surface Green's function of each contact (B9 left, B10 right)
     for (int side = 0; side < 2; ++side) {
       const int c = side == 0 ? a.left : a.right;
@@ -470,6 +509,9 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
         k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
         ++nl;
       }
+      if (a.eta > 0.0) {
+        k_retarded_check<<<P, 128, 0, s>>>(n, B[9 + side], Q, w.redo); ++nl;
+      }
     }
     // ---- self-energies Sigma_c = Tlc gs Tcl (B11 left, B12 right)
     for (int side = 0; side < 2; ++side) {
@@ -505,6 +547,13 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
     MCK(prod64(P, g, B[0], B[2]), "G Gam");
     k_trace<<<P, 512, 0, s>>>(n, B[0], g, B[1], B[2], w.tb, Q); ++nl;
     MCK(cudaGetLastError(), "trace");
+    if (a.redo) {
+      std::vector<int> h(P);
+      MCK(cudaMemcpyAsync(h.data(), w.redo, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "redo");
+      MCK(cudaStreamSynchronize(s), "sync");
+      for (int p = 0; p < P; ++p)
+        if (h[p]) a.redo->push_back(p0 + p);
+    }
     k_finish<<<(P + 255) / 256, 256, 0, s>>>(P, w.ncl, w.ncr, w.pst, w.tb, a.d_T + p0,
                                              a.d_ncyc ? a.d_ncyc + p0 : nullptr,
                                              a.d_status ? a.d_status + p0 : nullptr); ++nl;

@@ -118,7 +118,20 @@ enum OpKind : int {
   K_SUBCOPY,   // C(flag + r, flag + c) = A(r, c), A m x m, C leading dimension ldc
   K_RESPROBE,  // res[slot] = max_i |(A (B v))_i - v_i|, order m (cta_inv_probe: B a computed inverse of A)
   K_EYE,       // C = identity, order m
+  K_RETCHECK,  // res[slot] = min_i s Im A_ii / max_i |A_ii|, order m, s = -sign of the energy's imaginary part
 };
+
+// The retarded surface Green's function has a negative semidefinite
+// anti-Hermitian part, so -Im gs_ii >= 0 on every diagonal entry (checked
+// to 1e-6 of the largest |gs_ii|, far above rounding).  At a
+// nearly singular decimation (a lead resonance at small eta) FP64 rounding
+// can steer Sancho-Rubio to another fixed point of its equation, with
+// diagonal entries of the wrong sign; the decimation is then run again from
+// inputs moved by a few units in the last place (the energy times
+// 1 + k 2^-50, k = 1..kDecRetries), which keeps its result within the FP64
+// scatter of the reference path.
+constexpr double kRetardedTol = 1e-6;
+constexpr int kDecRetries = 6;
 
 
 struct Op {
@@ -317,6 +330,25 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       for (int q = tid; q < o.m * o.m; q += blockDim.x)
         o.C[q] = make_double2((q % o.m) == (q / o.m) ? 1.0 : 0.0, 0.0);
       break;
+    case K_RETCHECK: {
+      // -Inf when a diagonal entry is not finite
+      double lo = 1.7976931348623157e308, hi = 0.0, bad = 0.0;
+      for (int i = tid; i < o.m; i += blockDim.x) {
+        const double2 a = o.A[(size_t)i * (o.m + 1)];
+        const double v = o.scal * a.y, h = cabs(a);
+        if (!(h <= 1.7976931348623157e308)) bad = 1.0;
+        else {
+          lo = fmin(lo, v);
+          hi = fmax(hi, h);
+        }
+      }
+      lo = -cta_max(-lo, sm.red);
+      hi = cta_max(hi, sm.red);
+      bad = cta_max(bad, sm.red);
+      if (tid == 0)
+        sm.res[o.slot] = (bad > 0.0) ? -__longlong_as_double(0x7ff0000000000000LL) : ((hi > 0.0) ? lo / hi : 0.0);
+      break;
+    }
     case K_ACCUM:
       for (int q = tid; q < o.m; q += blockDim.x) {
         const double2 v = cmul(o.alpha, o.A[q]);
@@ -341,6 +373,8 @@ struct Prog {
   double2 ec, ecs;      // ES-H energy, contact energy
   // contacts / decimation
   int c, L, ncb, it, ok, done, ib, ix, ic, ic1;
+  int att;              // decimation attempt (retarded-branch retries)
+  double2 ecd;          // contact energy of the attempt
   // inverse refinement (the `refine` block): matrix, its computed inverse, order, return point
   const double2* rA;
   double2* rX;
@@ -461,14 +495,17 @@ dispatch:
           PT_EMIT(s);
           goto sgf_ready;
         }
+        s.att = 0;
+      decimation_attempt:
+        s.ecd = (s.att == 0) ? s.ecs : cscale(1.0 + s.att * 0x1p-50, s.ecs);
         set_esh(o, w.slot(0), s.L, s.L, s.d->h00 + s.d->olead[s.c], s.d->has_s00 ? s.d->s00 + s.d->olead[s.c] : nullptr,
-                s.ecs, 1, nullptr, nullptr, OP_N);                                          // Ao
+                s.ecd, 1, nullptr, nullptr, OP_N);                                          // Ao
         PT_EMIT(s);
         set_esh(o, w.slot(2), s.L, s.L, s.d->h01 + s.d->olead[s.c], s.d->has_s01 ? s.d->s01 + s.d->olead[s.c] : nullptr,
-                s.ecs, 0, nullptr, nullptr, OP_N);                                          // Bo
+                s.ecd, 0, nullptr, nullptr, OP_N);                                          // Bo
         PT_EMIT(s);
         set_esh(o, w.slot(3), s.L, s.L, s.d->h01 + s.d->olead[s.c], s.d->has_s01 ? s.d->s01 + s.d->olead[s.c] : nullptr,
-                cconj(s.ecs), 0, nullptr, nullptr, OP_C);                                   // Co = (E* S01 - H01)^dag
+                cconj(s.ecd), 0, nullptr, nullptr, OP_C);                                   // Co = (E* S01 - H01)^dag
         PT_EMIT(s);
         // ---- decimation (src/contselfenergy.F90:271-340): Ao 0, Aos 1, Go 4, Sf 6
         set_simple(o, K_COPY, s.L * s.L, w.slot(0), w.slot(1));
@@ -503,12 +540,24 @@ dispatch:
           PT_EMIT(s);                                                                    // Ao -= Co GoXBo
           { int t = s.ib; s.ib = s.ix; s.ix = t; t = s.ic; s.ic = s.ic1; s.ic1 = t; }   // Bo = B1, Co = C1
         }
-        if (!s.done) put_status(s.st, ST_NOT_CONVERGED);
-        s.ncyc += s.done ? s.it : a.sgf_max_iter + 1;
         o.kind = K_ZINV; o.m = s.L; o.A = w.slot(1); o.C = w.slot(4);
         PT_EMIT(s);                                                                      // gs = Ao_s^-1
         if (sm.ires[0]) put_status(s.st, ST_SINGULAR);
         PT_REFINE(s, w.slot(1), w.slot(4), s.L);
+        if (s.ecs.y != 0.0) {
+          o.kind = K_RETCHECK; o.m = s.L; o.A = w.slot(4); o.slot = 6; o.scal = (s.ecs.y > 0.0) ? -1.0 : 1.0;
+          PT_EMIT(s);
+          // a converged fixed point of the wrong kind, or an iteration that ran off to Inf / NaN
+          const bool wrong = (s.done && !(sm.res[6] >= -kRetardedTol)) ||
+                             sm.res[6] == -__longlong_as_double(0x7ff0000000000000LL);
+          if (wrong && s.att < kDecRetries) {
+            ++s.att;
+            goto decimation_attempt;
+          }
+          if (wrong) s.done = 0;   // no retarded solution reached: NOT_CONVERGED
+        }
+        if (!s.done) put_status(s.st, ST_NOT_CONVERGED);
+        s.ncyc += s.done ? s.it : a.sgf_max_iter + 1;
         if (a.sgf_out && a.sgf_out[(int64_t)s.p * a.ncont_max + s.c] >= 0) {
           // surface_green's add (:251-256)
           set_simple(o, K_COPY, s.L * s.L, w.slot(4), a.sgf_arena + a.sgf_out[(int64_t)s.p * a.ncont_max + s.c]);
