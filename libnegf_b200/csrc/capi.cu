@@ -1064,63 +1064,6 @@ static int engine_only(negf_b200_ctx* ctx, const char* what) {
   return NEGF_B200_OK;
 }
 
-// The points of a lock-step call whose decimation left the retarded solution
-// (rare: a lead resonance at small eta, where FP64 rounding can steer
-// Sancho-Rubio to another fixed point) are solved again by the persistent
-// engine, which retries such a decimation from inputs a few units in the last
-// place away; their T, ncyc and status replace the lock-step ones.
-static int redo_on_engine(negf_b200_ctx* ctx, const std::vector<int>& redo, int32_t npts, const int32_t* d_ids,
-                          const double* d_E, double eta, double* d_T, int32_t* d_ncyc, int32_t* d_status,
-                          cudaStream_t s) {
-  const int nr = (int)redo.size();
-  std::vector<int32_t> hid(npts), rid(nr);
-  std::vector<double> hE(npts), rE(nr);
-  CK(cudaMemcpyAsync(hid.data(), d_ids, sizeof(int32_t) * npts, cudaMemcpyDeviceToHost, s));
-  CK(cudaMemcpyAsync(hE.data(), d_E, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
-  CK(cudaStreamSynchronize(s));
-  for (int k = 0; k < nr; ++k) {
-    rid[k] = hid[redo[k]];
-    rE[k] = hE[redo[k]];
-  }
-  LaunchShape sh;
-  int st = shape_of(ctx, nr, rid.data(), sh);
-  if (st) return st;
-  // a separate staging block: the caller's arrays may live in the context's io buffer
-  void* buf = nullptr;
-  const size_t bytes = (size_t)nr * (4 + 8 + 8 + 4 + 4) + 256;
-  CK(cudaMalloc(&buf, bytes));
-  char* b = static_cast<char*>(buf);
-  int32_t* r_id = reinterpret_cast<int32_t*>(b);
-  double* r_E = reinterpret_cast<double*>(b + ((size_t)nr * 4 + 15) / 16 * 16);
-  double* r_T = r_E + nr;
-  int32_t* r_nc = reinterpret_cast<int32_t*>(r_T + nr);
-  int32_t* r_st = r_nc + nr;
-  cudaMemcpyAsync(r_id, rid.data(), sizeof(int32_t) * nr, cudaMemcpyHostToDevice, s);
-  cudaMemcpyAsync(r_E, rE.data(), sizeof(double) * nr, cudaMemcpyHostToDevice, s);
-  negf::EngineArgs ea = base_args(ctx, negf::MODE_T, nr);
-  ea.dev_id = r_id; ea.energy = r_E; ea.eta = eta; ea.ni = 1; ea.nf = 2;
-  ea.T = r_T; ea.ncyc = r_nc; ea.status = r_st;
-  st = run_device(ctx, ea, sh, s);
-  std::vector<double> hT(nr);
-  std::vector<int32_t> hnc(nr), hst(nr);
-  if (st == NEGF_B200_OK) {
-    cudaMemcpyAsync(hT.data(), r_T, sizeof(double) * nr, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(hnc.data(), r_nc, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost, s);
-    cudaMemcpyAsync(hst.data(), r_st, sizeof(int32_t) * nr, cudaMemcpyDeviceToHost, s);
-    if (cudaStreamSynchronize(s) != cudaSuccess) st = NEGF_B200_ERR_CUDA;
-  }
-  cudaFree(buf);
-  if (st) return st;
-  for (int k = 0; k < nr; ++k) {
-    const int p = redo[k];
-    CK(cudaMemcpyAsync(d_T + p, &hT[k], sizeof(double), cudaMemcpyHostToDevice, s));
-    if (d_ncyc) CK(cudaMemcpyAsync(d_ncyc + p, &hnc[k], sizeof(int32_t), cudaMemcpyHostToDevice, s));
-    if (d_status) CK(cudaMemcpyAsync(d_status + p, &hst[k], sizeof(int32_t), cudaMemcpyHostToDevice, s));
-  }
-  CK(cudaStreamSynchronize(s));   // the host vectors go out of scope
-  return NEGF_B200_OK;
-}
-
 // Runs a lock-step form on device arrays of ids and energies// Runs a lock-step form on device arrays of ids and energies: sizes the batch
 // to the workspace and calls negf::mixed_run.
 static int run_lockstep(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_ids, const double* d_E, double eta,
@@ -1146,12 +1089,9 @@ static int run_lockstep(negf_b200_ctx* ctx, int32_t npts, const int32_t* d_ids, 
   a.sgf_tol = ctx->opt.sgf_tol; a.sgf_max_iter = ctx->opt.sgf_max_iter; a.slices = slices;
   a.d_T = d_T; a.d_ncyc = d_ncyc; a.d_status = d_status;
   a.launches = &ctx->launches;
-  std::vector<int> redo;
-  a.redo = &redo;
   std::string msg;
   st = negf::mixed_run(a, ctx->ws, batch, s, &msg);
   if (st) return fail(ctx, st, (slices ? "mixed form: " : "lock step: ") + msg);
-  if (!redo.empty()) return redo_on_engine(ctx, redo, npts, d_ids, d_E, eta, d_T, d_ncyc, d_status, s);
   return NEGF_B200_OK;
 }
 

@@ -9,6 +9,11 @@ namespace negf {
 constexpr int kMaxCont = 10;           // MAXNCONT (src/api/lnParams.h:10)
 constexpr int kMaxOrder = 1024;        // largest PL / contact PL size supported
 constexpr int kSmemMain = 100 * 1024;  // GEMM staging ring / inversion panel region
+// A decimation that reaches a fixed point other than the retarded surface
+// Green's function (or runs off to Inf / NaN) runs again from the contact
+// energy times 1 + k 2^-50, k = 1..kDecRetries; after that the point
+// reports NOT_CONVERGED.
+constexpr int kDecRetries = 6;
 
 enum Mode : int { MODE_T = 0, MODE_DOS = 1, MODE_GN = 2, MODE_RHO = 3 };
 

@@ -35,12 +35,13 @@ __device__ __forceinline__ double2 cmulm(double2 a, double2 b) {
 }
 __device__ __forceinline__ double2 conjm(double2 a) { return make_double2(a.x, -a.y); }
 
-// Ao = Ec S00 - H00, Aos = Ao, Bo = Ec S01 - H01, Co = (conj(Ec) S01 - H01)^dag
-__global__ void k_lead_init(int n, int c, const int* ids, const double* E, double eta, const DevDesc* descs,
-                            double2* Ao, double2* Aos, double2* Bo, double2* Co, int64_t Q) {
-  const int p = blockIdx.y;
+// Ao = Ec S00 - H00, Aos = Ao, Bo = Ec S01 - H01, Co = (conj(Ec) S01 - H01)^dag,
+// Ec = (E + i eta) scale, for the points map[b] (map null: b)
+__global__ void k_lead_init(int n, int c, const int* ids, const double* E, double eta, double scale, const int* map,
+                            const DevDesc* descs, double2* Ao, double2* Aos, double2* Bo, double2* Co, int64_t Q) {
+  const int p = map ? map[blockIdx.y] : blockIdx.y;
   const DevDesc& d = descs[ids[p]];
-  const double2 ec = make_double2(E[p], eta);
+  const double2 ec = make_double2(E[p] * scale, eta * scale);
   const int64_t ol = d.olead[c], nn = (int64_t)n * n;
   for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < nn; q += (int64_t)gridDim.x * blockDim.x) {
     const int i = (int)(q % n), j = (int)(q / n);
@@ -256,8 +257,8 @@ __global__ void k_trace(int n, const double2* Gam, const double2* G, const doubl
 // diagonal of -Im gs must be >= 0 (up to 1e-6 of the largest |gs_ii|); a
 // converged fixed point of the wrong kind, or one that is not finite, marks
 // the point for the engine (redo[p] = 1).  One CTA per point.
-__global__ void k_retarded_check(int n, const double2* gs, int64_t Q, int* redo) {
-  const int p = blockIdx.x;
+__global__ void k_retarded_check(int n, const double2* gs, int64_t Q, const int* map, int* redo) {
+  const int p = map ? map[blockIdx.x] : blockIdx.x;
   double lo = 1.7976931348623157e308, hi = 0.0;
   int bad = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -289,10 +290,28 @@ __global__ void k_retarded_check(int n, const double2* gs, int64_t Q, int* redo)
   }
 }
 
-__global__ void k_iota(int n, int* v, int* count) {
-  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) v[b] = b;
-  if (count && blockIdx.x == 0 && threadIdx.x == 0) *count = n;
+// Start of a decimation for the points map[b], b < nsub (map null: b):
+// ok = 0, max = 0, ncyc = 0, the active list = the points, its count.
+__global__ void k_dec_start(int nsub, const int* map, int* ok, double* mx, int* ncyc_c, int* list, int* count) {
+  for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsub; b += gridDim.x * blockDim.x) {
+    const int p = map ? map[b] : b;
+    ok[p] = 0;
+    mx[p] = 0.0;
+    ncyc_c[p] = 0;
+    list[b] = p;
+  }
+  if (count && blockIdx.x == 0 && threadIdx.x == 0) *count = nsub;
 }
+
+// Points still flagged after the last retry: NOT_CONVERGED, ncyc = cap + 1.
+__global__ void k_flag_unresolved(int P, const int* redo, int* ncyc_c, int* status, int max_iter) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < P; p += gridDim.x * blockDim.x)
+    if (redo[p]) {
+      ncyc_c[p] = max_iter + 1;
+      if (status[p] == 0) status[p] = NEGF_B200_ERR_NOT_CONVERGED;
+    }
+}
+
 
 size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
 
@@ -310,7 +329,7 @@ struct Carver {
 struct Ws {
   double2* blk[kBlocks];
   double* mx;
-  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst, *redo;
+  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst, *redo, *sub;
   double* tb;
   double2* zwork;
   void* oz;
@@ -332,6 +351,7 @@ Ws carve(void* base, int P, int n, int slices, size_t* total) {
   w.pst = c.take<int>(P);
   w.tb = c.take<double>(P);
   w.redo = c.take<int>(P);
+  w.sub = c.take<int>(P);
   const bool small = slices == 0;        // the lock-step FP64 form: one-warp kernels, no splitting
   w.zwork = c.take<double2>(small ? 1 : (size_t)P * zinv_batched_work_elems(n) + 1);
   w.oz = small ? nullptr : c.take<uint8_t>(ozaki_layout(P, n, n, n, slices).total);
@@ -433,22 +453,22 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
     const int* ids = a.d_ids + p0;
     const double* E = a.d_E + p0;
     MCK(cudaMemsetAsync(w.pst, 0, sizeof(int) * P, s), "memset status");
-    MCK(cudaMemsetAsync(w.redo, 0, sizeof(int) * P, s), "memset redo");
     // ---- surface Green's function of each contact (B9 left, B10 right)
-    for (int side = 0; side < 2; ++side) {
+    // decimation of contact `side` for the points sub[b], b < nsub (sub null:
+    // all P), the contact energy scaled by `scale`; then gs = Aos^-1 and the
+    // retarded-branch check (redo[p] = 1 where it fails)
+    auto decimate = [&](int side, const int* sub, int nsub, double scale) -> int {
       const int c = side == 0 ? a.left : a.right;
       int* ncyc_c = side == 0 ? w.ncl : w.ncr;
       double2 *Ao = B[0], *Aos = B[1], *Bo = B[2], *Co = B[3], *Go = B[4], *X = B[5], *C1 = B[6], *Y = B[7],
               *B1 = B[8];
-      k_lead_init<<<dim3(gx, P), eb, 0, s>>>(n, c, ids, E, a.eta, a.d_descs, Ao, Aos, Bo, Co, Q); ++nl;
+      k_lead_init<<<dim3(gx, nsub), eb, 0, s>>>(n, c, ids, E, a.eta, scale, sub, a.d_descs, Ao, Aos, Bo, Co, Q);
+      ++nl;
       MCK(cudaGetLastError(), "lead init");
-      MCK(cudaMemsetAsync(w.ok, 0, sizeof(int) * P, s), "memset ok");
-      MCK(cudaMemsetAsync(w.mx, 0, sizeof(double) * P, s), "memset mx");
-      MCK(cudaMemsetAsync(ncyc_c, 0, sizeof(int) * P, s), "memset ncyc");
       int* cnt_cur = small ? w.count : nullptr;        // device active counts (small form)
       int* cnt_nxt = small ? w.count + 1 : nullptr;
-      k_iota<<<(P + 255) / 256, 256, 0, s>>>(P, w.list0, cnt_cur); ++nl;
-      int na = P;                                      // host bound of the active list
+      k_dec_start<<<(nsub + 255) / 256, 256, 0, s>>>(nsub, sub, w.ok, w.mx, ncyc_c, w.list0, cnt_cur); ++nl;
+      int na = nsub;                                   // host bound of the active list
       int* cur = w.list0;
       int* nxt = w.list1;
       int it = 1;
@@ -501,16 +521,45 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
         MCK(cudaMemcpyAsync(&na, cnt_cur, sizeof(int), cudaMemcpyDeviceToHost, s), "count");
         MCK(cudaStreamSynchronize(s), "sync");
       }
-      if (na > 0)
-        k_not_converged<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, ncyc_c, w.pst, a.sgf_max_iter); ++nl;
-      // gs = Aos^-1 for every point
-      MCK(inv(P, nullptr, nullptr, Aos, B[9 + side]), "gs");
+      if (na > 0) {
+        k_not_converged<<<(na + 255) / 256, 256, 0, s>>>(na, cnt_cur, cur, ncyc_c, w.pst, a.sgf_max_iter);
+        ++nl;
+      }
+      MCK(inv(nsub, sub, nullptr, Aos, B[9 + side]), "gs");
       if (!small) {
-        k_info_to_status<<<(P + 255) / 256, 256, 0, s>>>(P, nullptr, nullptr, w.info, w.pst, NEGF_B200_ERR_SINGULAR);
+        k_info_to_status<<<(nsub + 255) / 256, 256, 0, s>>>(nsub, nullptr, sub, w.info, w.pst,
+                                                              NEGF_B200_ERR_SINGULAR);
         ++nl;
       }
       if (a.eta > 0.0) {
-        k_retarded_check<<<P, 128, 0, s>>>(n, B[9 + side], Q, w.redo); ++nl;
+        k_retarded_check<<<nsub, 128, 0, s>>>(n, B[9 + side], Q, sub, w.redo);
+        ++nl;
+      }
+      return 0;
+    };
+    for (int side = 0; side < 2; ++side) {
+      MCK(cudaMemsetAsync(w.redo, 0, sizeof(int) * P, s), "memset redo");
+      if (int r = decimate(side, nullptr, P, 1.0)) return r;
+      if (!(a.eta > 0.0)) continue;
+      // decimations that reached another fixed point run again, in lock step over
+      // just those points, from the contact energy times 1 + k 2^-50
+      std::vector<int> h(P), again;
+      for (int att = 1;; ++att) {
+        MCK(cudaMemcpyAsync(h.data(), w.redo, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "redo");
+        MCK(cudaStreamSynchronize(s), "sync");
+        again.clear();
+        for (int p = 0; p < P; ++p)
+          if (h[p]) again.push_back(p);
+        if (again.empty()) break;
+        if (att > kDecRetries) {
+          k_flag_unresolved<<<(P + 255) / 256, 256, 0, s>>>(P, w.redo, side == 0 ? w.ncl : w.ncr, w.pst,
+                                                              a.sgf_max_iter);
+          ++nl;
+          break;
+        }
+        MCK(cudaMemcpyAsync(w.sub, again.data(), sizeof(int) * again.size(), cudaMemcpyHostToDevice, s), "sub");
+        MCK(cudaMemsetAsync(w.redo, 0, sizeof(int) * P, s), "memset redo");
+        if (int r = decimate(side, w.sub, (int)again.size(), 1.0 + att * 0x1p-50)) return r;
       }
     }
     // ---- self-energies Sigma_c = Tlc gs Tcl (B11 left, B12 right)
@@ -547,13 +596,6 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
     MCK(prod64(P, g, B[0], B[2]), "G Gam");
     k_trace<<<P, 512, 0, s>>>(n, B[0], g, B[1], B[2], w.tb, Q); ++nl;
     MCK(cudaGetLastError(), "trace");
-    if (a.redo) {
-      std::vector<int> h(P);
-      MCK(cudaMemcpyAsync(h.data(), w.redo, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "redo");
-      MCK(cudaStreamSynchronize(s), "sync");
-      for (int p = 0; p < P; ++p)
-        if (h[p]) a.redo->push_back(p0 + p);
-    }
     k_finish<<<(P + 255) / 256, 256, 0, s>>>(P, w.ncl, w.ncr, w.pst, w.tb, a.d_T + p0,
                                              a.d_ncyc ? a.d_ncyc + p0 : nullptr,
                                              a.d_status ? a.d_status + p0 : nullptr); ++nl;

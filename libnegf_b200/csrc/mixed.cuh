@@ -5,7 +5,6 @@
 #pragma once
 #include <cstdint>
 #include <string>
-#include <vector>
 
 #include <cuda_runtime.h>
 
@@ -29,9 +28,6 @@ struct MixedArgs {
   int* d_ncyc;               // decimation iterations summed over the contacts
   int* d_status;
   uint64_t* launches = nullptr;  // host counter of kernels launched (may be null)
-  // points (indices into the call) whose decimation left the retarded
-  // solution, for the engine to solve again (may be null)
-  std::vector<int>* redo = nullptr;
 };
 
 // bytes of workspace for a batch of `batch` points of order n

@@ -128,10 +128,9 @@ enum OpKind : int {
 // can steer Sancho-Rubio to another fixed point of its equation, with
 // diagonal entries of the wrong sign; the decimation is then run again from
 // inputs moved by a few units in the last place (the energy times
-// 1 + k 2^-50, k = 1..kDecRetries), which keeps its result within the FP64
-// scatter of the reference path.
+// 1 + k 2^-50, k = 1..kDecRetries, engine.cuh), which keeps its result
+// within the FP64 scatter of the reference path.
 constexpr double kRetardedTol = 1e-6;
-constexpr int kDecRetries = 6;
 
 
 struct Op {
