@@ -95,6 +95,7 @@ __device__ __noinline__ int cta_decimation(int L, const Ws& w, double tol, int m
     gemm(L, L, L, opN(Go, L), opN(Co, L), X, L, one, zero, sm);            // GoXCo
     gemm(L, L, L, opN(Co, L), opN(X, L), C1, L, one, zero, sm, true);      // C1 = Co GoXCo
     const double mx = *sm.maxv;
+    if (!(mx <= 1.7976931348623157e308)) break;   // Inf / NaN: will not converge (NOT_CONVERGED)
     if (mx <= tol) {
       if (ok) { done = true; break; }
       ok = true;

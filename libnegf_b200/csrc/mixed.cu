@@ -86,7 +86,7 @@ __global__ void k_sub_self(int64_t nn, const int* list, const int* count, const 
 // that go on (and zeroes their max for the next iteration).  One CTA.  The
 // list's length is na, or *count when count is given.
 __global__ void k_dec_check(int na, const int* count, const int* list, double* mx, int* ok, int* ncyc_c, double tol,
-                            int it, int* next, int* next_count) {
+                            int it, int* next, int* next_count, int* redo) {
   __shared__ int cnt;
   if (count) na = *count;
   if (threadIdx.x == 0) cnt = 0;
@@ -95,7 +95,11 @@ __global__ void k_dec_check(int na, const int* count, const int* list, double* m
     const int p = list[b];
     const double m = mx[p];
     bool go = true;
-    if (m <= tol) {
+    if (!(m <= 1.7976931348623157e308)) {   // Inf / NaN: this decimation will not converge; run it again
+      go = false;
+      ncyc_c[p] = it;
+      redo[p] = 1;
+    } else if (m <= tol) {
       if (ok[p]) {
         go = false;
         ncyc_c[p] = it;
@@ -478,7 +482,7 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
           // the rest of the iteration in two fused launches, one CTA per point
           MCK(cudaMemsetAsync(cnt_nxt, 0, sizeof(int), s), "memset count");
           MCK(launch_small_dec_a(na, n, cur, cnt_cur, Go, Co, Bo, C1, Ao, Aos, Q, w.ok, ncyc_c, a.sgf_tol, it, nxt,
-                                 cnt_nxt, s), "decimation a");
+                                 cnt_nxt, w.redo, s), "decimation a");
           MCK(launch_small_dec_b(na, n, nxt, cnt_nxt, Go, Bo, Co, B1, Ao, Q, s), "decimation b");
           nl += 2;
           std::swap(cur, nxt);
@@ -497,7 +501,8 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
         ++nl;
         MCK(prod(na, cur, nullptr, one, Go, Co, zero, X, nullptr), "GoXCo");
         MCK(prod(na, cur, nullptr, one, Co, X, zero, C1, w.mx), "C1");
-        k_dec_check<<<1, 1024, 0, s>>>(na, nullptr, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt, w.count); ++nl;
+        k_dec_check<<<1, 1024, 0, s>>>(na, nullptr, cur, w.mx, w.ok, ncyc_c, a.sgf_tol, it, nxt, w.count, w.redo);
+        ++nl;
         MCK(cudaGetLastError(), "check");
         std::swap(cur, nxt);
         {

@@ -373,6 +373,7 @@ struct Prog {
   // contacts / decimation
   int c, L, ncb, it, ok, done, ib, ix, ic, ic1;
   int att;              // decimation attempt (retarded-branch retries)
+  int diverged;         // the attempt's max|C1| went Inf / NaN
   double2 ecd;          // contact energy of the attempt
   // inverse refinement (the `refine` block): matrix, its computed inverse, order, return point
   const double2* rA;
@@ -509,7 +510,7 @@ dispatch:
         // ---- decimation (src/contselfenergy.F90:271-340): Ao 0, Aos 1, Go 4, Sf 6
         set_simple(o, K_COPY, s.L * s.L, w.slot(0), w.slot(1));
         PT_EMIT(s);
-        s.ok = 0; s.done = 0; s.ib = 2; s.ix = 5; s.ic = 3; s.ic1 = 7;
+        s.ok = 0; s.done = 0; s.diverged = 0; s.ib = 2; s.ix = 5; s.ic = 3; s.ic1 = 7;
         for (s.it = 1; s.it <= a.sgf_max_iter; ++s.it) {
           o.kind = K_ZINV; o.m = s.L; o.A = w.slot(0); o.C = w.slot(4);
           PT_EMIT(s);
@@ -521,6 +522,10 @@ dispatch:
                    zero, 1);
           PT_EMIT(s);                                                                    // C1 = Co GoXCo
           mx = *sm.maxv;
+          if (!(mx <= 1.7976931348623157e308)) {   // Inf / NaN: this iteration will not converge
+            s.diverged = 1;
+            break;
+          }
           if (mx <= a.sgf_tol) {
             if (s.ok) { s.done = 1; break; }
             s.ok = 1;
@@ -547,7 +552,7 @@ dispatch:
           o.kind = K_RETCHECK; o.m = s.L; o.A = w.slot(4); o.slot = 6; o.scal = (s.ecs.y > 0.0) ? -1.0 : 1.0;
           PT_EMIT(s);
           // a converged fixed point of the wrong kind, or an iteration that ran off to Inf / NaN
-          const bool wrong = (s.done && !(sm.res[6] >= -kRetardedTol)) ||
+          const bool wrong = (s.done && !(sm.res[6] >= -kRetardedTol)) || s.diverged ||
                              sm.res[6] == -__longlong_as_double(0x7ff0000000000000LL);
           if (wrong && s.att < kDecRetries) {
             ++s.att;

@@ -251,7 +251,7 @@ template <int N>
 __global__ void __launch_bounds__(kWarps * 32)
     k_small_dec_a(int n, const int* list, const int* count, int P, const double2* Go, const double2* Co,
                   const double2* Bo, double2* C1, double2* Ao, double2* Aos, int64_t Q, int* ok, int* ncyc_c,
-                  double tol, int it, int* next, int* next_count) {
+                  double tol, int it, int* next, int* next_count, int* redo) {
   constexpr int CW = N / kWarps;
   extern __shared__ __align__(16) double2 sdec[];
   double2* sG = sdec;
@@ -298,7 +298,11 @@ __global__ void __launch_bounds__(kWarps * 32)
     double m = smx[0];
     for (int q = 1; q < kWarps; ++q) m = (m != m || smx[q] != smx[q]) ? m + smx[q] : fmax(m, smx[q]);
     bool go = true;
-    if (m <= tol) {
+    if (!(m <= 1.7976931348623157e308)) {   // Inf / NaN: will not converge; run it again
+      go = false;
+      ncyc_c[p] = it;
+      if (redo) redo[p] = 1;
+    } else if (m <= tol) {
       if (ok[p]) {
         go = false;
         ncyc_c[p] = it;
@@ -484,7 +488,7 @@ cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, 
 cudaError_t launch_small_dec_a(int P, int n, const int* list, const int* count, const double2* Go,
                                const double2* Co, const double2* Bo, double2* C1, double2* Ao, double2* Aos,
                                int64_t Q, int* ok, int* ncyc_c, double tol, int it, int* next, int* next_count,
-                               cudaStream_t s) {
+                               int* redo, cudaStream_t s) {
   if (P <= 0) return cudaSuccess;
   if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
   static std::mutex mu;
@@ -494,13 +498,13 @@ cudaError_t launch_small_dec_a(int P, int n, const int* list, const int* count, 
     cudaError_t e = opt_in(k_small_dec_a<16>, smem, done16, mu);
     if (e != cudaSuccess) return e;
     k_small_dec_a<16><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, Ao, Aos, Q, ok, ncyc_c, tol,
-                                                   it, next, next_count);
+                                                   it, next, next_count, redo);
   } else {
     const size_t smem = 4 * 32 * 32 * sizeof(double2);
     cudaError_t e = opt_in(k_small_dec_a<32>, smem, done32, mu);
     if (e != cudaSuccess) return e;
     k_small_dec_a<32><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, Ao, Aos, Q, ok, ncyc_c, tol,
-                                                   it, next, next_count);
+                                                   it, next, next_count, redo);
   }
   return cudaGetLastError();
 }
