@@ -476,8 +476,9 @@ int negf_b200_zgemm_batched_i8(int32_t batch, int32_t m, int32_t n, int32_t k,
  * of negf_b200_zinv_work_bytes(batch, n) bytes; info[b] = 0 or the 1-based
  * column of the first zero pivot.  Gauss-Jordan is not backward stable: each
  * inverse is checked by a residual probe, max |A (X v) - v| for a fixed v,
- * and gets up to two Newton steps X + X (I - A X) where it exceeds 1e-7 (the
- * residual of a backward-stable inverse).  For n <= 64 `work` may be NULL:
+ * and gets up to two Newton steps X + X (I - A X) where it exceeds 1e-5
+ * (well-conditioned inverses probe at 1e-14 .. 1e-7; a Gauss-Jordan inverse
+ * of a matrix of condition 1e8 and up can reach 1e-4).  For n <= 64 `work` may be NULL:
  * the probe is then skipped. */
 size_t negf_b200_zinv_work_bytes(int32_t batch, int32_t n);
 int negf_b200_zinv_batched(int32_t batch, int32_t n, const double* A,

@@ -51,13 +51,15 @@ __device__ __forceinline__ int zinv(int n, const double2* A, double2* out, doubl
 // X <- X + X (I - A X) where the probe exceeds kInvProbeTol (the engine's
 // refine block); R and Xn are n x n scratch (R null: no probe).
 __device__ __noinline__ int zinv_refined(int n, const double2* A, double2* X, double2* ws, double2* R, double2* Xn,
-                                         SmemMap& sm) {
+                                         SmemMap& sm, bool* refined = nullptr) {
   const int bad = zinv(n, A, X, ws, sm);
+  if (refined) *refined = false;
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0);
   const int nn = n * n;
   for (int k = 0; k < 2 && R; ++k) {
     const double e = cta_inv_probe(n, A, X, sm.main, sm.red);
     if (!(e > kInvProbeTol) || !(e <= 1.7976931348623157e308)) break;
+    if (refined) *refined = true;
     for (int q = threadIdx.x; q < nn; q += blockDim.x) R[q] = make_double2((q % n) == (q / n) ? 1.0 : 0.0, 0.0);
     __syncthreads();
     gemm(n, n, n, opN(A, n), opN(X, n), R, n, mone, one, sm);     // R = I - A X
@@ -258,7 +260,7 @@ cudaError_t launch_zinv_batched(int batch, int n, const double2* A, double2* Ain
 // info[map[b]] gets the zgetrf-style singular column (0 = none).
 __global__ void __launch_bounds__(kThreads, 2)
     k_zinv_mapped(int n, const double2* A, int64_t sA, double2* X, int64_t sX, const int* map, int* info,
-                  double2* work, int64_t wstride) {
+                  double2* work, int64_t wstride, int* sens) {
   extern __shared__ __align__(16) char smem_raw[];
   SmemMap sm = map_smem(smem_raw, n);
   sm.tr.acc = nullptr;
@@ -266,18 +268,20 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int p = map ? map[b] : b;
   double2* wb = work + (int64_t)b * wstride;
   double2* R = wb + zinv_ws_elems(n, kSmemMain);
-  int inf = zinv_refined(n, A + (int64_t)p * sA, X + (int64_t)p * sX, wb, R, R + (int64_t)n * n, sm);
+  bool refined = false;
+  int inf = zinv_refined(n, A + (int64_t)p * sA, X + (int64_t)p * sX, wb, R, R + (int64_t)n * n, sm, &refined);
   if (threadIdx.x == 0 && info) info[p] = inf;
+  if (threadIdx.x == 0 && sens && refined) sens[p] = 1;
 }
 
 cudaError_t launch_zinv_mapped(int batch, int n, const double2* A, int64_t sA, double2* X, int64_t sX,
-                               const int* map, int* info, double2* work, cudaStream_t s) {
+                               const int* map, int* info, double2* work, cudaStream_t s, int* sens) {
   if (batch <= 0) return cudaSuccess;
   const size_t smem = engine_smem_bytes(n);
   cudaError_t e = cudaFuncSetAttribute(k_zinv_mapped, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   k_zinv_mapped<<<batch, kThreads, smem, s>>>(n, A, sA, X, sX, map, info, work,
-                                              (int64_t)zinv_batched_work_elems(n));
+                                              (int64_t)zinv_batched_work_elems(n), sens);
   return cudaGetLastError();
 }
 

@@ -28,7 +28,7 @@
 namespace negf {
 namespace {
 
-constexpr int kBlocks = 13;   // n x n complex work blocks per point
+constexpr int kBlocks = 14;   // n x n complex work blocks per point (the 14th: a kept surface GF)
 
 __device__ __forceinline__ double2 cmulm(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
@@ -295,16 +295,49 @@ __global__ void k_retarded_check(int n, const double2* gs, int64_t Q, const int*
 }
 
 // Start of a decimation for the points map[b], b < nsub (map null: b):
-// ok = 0, max = 0, ncyc = 0, the active list = the points, its count.
-__global__ void k_dec_start(int nsub, const int* map, int* ok, double* mx, int* ncyc_c, int* list, int* count) {
+// ok = 0, max = 0, ncyc = 0, sensitivity 0, the active list = the points,
+// its count.
+__global__ void k_dec_start(int nsub, const int* map, int* ok, double* mx, int* ncyc_c, int* list, int* count,
+                            int* sens) {
   for (int b = blockIdx.x * blockDim.x + threadIdx.x; b < nsub; b += gridDim.x * blockDim.x) {
     const int p = map ? map[b] : b;
     ok[p] = 0;
+    sens[p] = 0;
     mx[p] = 0.0;
     ncyc_c[p] = 0;
     list[b] = p;
   }
   if (count && blockIdx.x == 0 && threadIdx.x == 0) *count = nsub;
+}
+
+// kept_p = gs_p for the points map[b], b < nsub; one CTA per point.
+__global__ void k_keep(int64_t nn, const int* map, const double2* gs, double2* kept, int64_t Q) {
+  const int p = map[blockIdx.x];
+  for (int64_t q = threadIdx.x; q < nn; q += blockDim.x) kept[p * Q + q] = gs[p * Q + q];
+}
+
+// agree[p] = max |gs_p - kept_p| <= tol max |kept_p| for the points map[b]; one CTA per point.
+__global__ void k_agree(int64_t nn, const int* map, const double2* gs, const double2* kept, int64_t Q, double tol,
+                        int* agree) {
+  const int p = map[blockIdx.x];
+  double d = 0.0, m = 0.0;
+  for (int64_t q = threadIdx.x; q < nn; q += blockDim.x) {
+    const double2 a = gs[p * Q + q], b = kept[p * Q + q];
+    d = fmax(d, hypot(a.x - b.x, a.y - b.y));
+    m = fmax(m, hypot(b.x, b.y));
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d = fmax(d, __shfl_xor_sync(0xffffffffu, d, o));
+    m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  }
+  __shared__ double sd[32], sm[32];
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) { sd[w] = d; sm[w] = m; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int q = 1; q < (int)(blockDim.x >> 5); ++q) { d = fmax(d, sd[q]); m = fmax(m, sm[q]); }
+    agree[p] = (d <= tol * m) ? 1 : 0;
+  }
 }
 
 // Points still flagged after the last retry: NOT_CONVERGED, ncyc = cap + 1.
@@ -333,7 +366,7 @@ struct Carver {
 struct Ws {
   double2* blk[kBlocks];
   double* mx;
-  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst, *redo, *sub;
+  int *ok, *ncl, *ncr, *list0, *list1, *count, *info, *pst, *redo, *sub, *sens, *agree;
   double* tb;
   double2* zwork;
   void* oz;
@@ -356,6 +389,8 @@ Ws carve(void* base, int P, int n, int slices, size_t* total) {
   w.tb = c.take<double>(P);
   w.redo = c.take<int>(P);
   w.sub = c.take<int>(P);
+  w.sens = c.take<int>(P);
+  w.agree = c.take<int>(P);
   const bool small = slices == 0;        // the lock-step FP64 form: one-warp kernels, no splitting
   w.zwork = c.take<double2>(small ? 1 : (size_t)P * zinv_batched_work_elems(n) + 1);
   w.oz = small ? nullptr : c.take<uint8_t>(ozaki_layout(P, n, n, n, slices).total);
@@ -437,9 +472,9 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       cudaError_t e = launch_small_zinv(nb, n, A, X, Q, map, count, w.info, w.pst, NEGF_B200_ERR_SINGULAR, s);
       if (e != cudaSuccess) return e;
       ++nl;
-      return launch_small_refine(nb, n, A, X, Q, map, count, s);
+      return launch_small_refine(nb, n, A, X, Q, map, count, s, w.sens);
     }
-    return launch_zinv_mapped(nb, n, A, Q, X, Q, map, w.info, w.zwork, s);   // probe and refinement inside
+    return launch_zinv_mapped(nb, n, A, Q, X, Q, map, w.info, w.zwork, s, w.sens);   // probe and refinement inside
   };
   // FP64 products of the trace (the one-warp kernel at small orders, else the DMMA product)
   auto prod64 = [&](int nb, const double2* A, const double2* Bm, double2* C) -> cudaError_t {
@@ -471,7 +506,8 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       MCK(cudaGetLastError(), "lead init");
       int* cnt_cur = small ? w.count : nullptr;        // device active counts (small form)
       int* cnt_nxt = small ? w.count + 1 : nullptr;
-      k_dec_start<<<(nsub + 255) / 256, 256, 0, s>>>(nsub, sub, w.ok, w.mx, ncyc_c, w.list0, cnt_cur); ++nl;
+      k_dec_start<<<(nsub + 255) / 256, 256, 0, s>>>(nsub, sub, w.ok, w.mx, ncyc_c, w.list0, cnt_cur, w.sens);
+      ++nl;
       int na = nsub;                                   // host bound of the active list
       int* cur = w.list0;
       int* nxt = w.list1;
@@ -546,25 +582,56 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       MCK(cudaMemsetAsync(w.redo, 0, sizeof(int) * P, s), "memset redo");
       if (int r = decimate(side, nullptr, P, 1.0)) return r;
       if (!(a.eta > 0.0)) continue;
-      // decimations that reached another fixed point run again, in lock step over
-      // just those points, from the contact energy times 1 + k 2^-50
-      std::vector<int> h(P), again;
+      // Decimations that reached another fixed point (or ran off to Inf / NaN) run
+      // again, in lock step over just those points, from the contact energy times
+      // 1 + k 2^-50.  A sensitive decimation (one of its inverses needed a Newton
+      // step: a nearly singular Ao) is accepted once two attempts reach the same gs.
+      std::vector<int> hredo(P), hsens(P), hagree(P), kept(P, 0), done(P, 0), cur_sub, again, cmp, keep;
+      cur_sub.resize(P);
+      for (int p = 0; p < P; ++p) cur_sub[p] = p;
+      double2* gs = B[9 + side];
       for (int att = 1;; ++att) {
-        MCK(cudaMemcpyAsync(h.data(), w.redo, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "redo");
+        MCK(cudaMemcpyAsync(hredo.data(), w.redo, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "redo");
+        MCK(cudaMemcpyAsync(hsens.data(), w.sens, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "sens");
         MCK(cudaStreamSynchronize(s), "sync");
+        cmp.clear();
+        for (int p : cur_sub)
+          if (!hredo[p] && hsens[p] && kept[p]) cmp.push_back(p);
+        if (!cmp.empty()) {
+          MCK(cudaMemcpyAsync(w.sub, cmp.data(), sizeof(int) * cmp.size(), cudaMemcpyHostToDevice, s), "cmp");
+          k_agree<<<(int)cmp.size(), 256, 0, s>>>(Q, w.sub, gs, B[13], Q, 1e-2, w.agree); ++nl;
+          MCK(cudaMemcpyAsync(hagree.data(), w.agree, sizeof(int) * P, cudaMemcpyDeviceToHost, s), "agree");
+          MCK(cudaStreamSynchronize(s), "sync");
+        }
         again.clear();
-        for (int p = 0; p < P; ++p)
-          if (h[p]) again.push_back(p);
+        keep.clear();
+        for (int p : cur_sub) {
+          if (hredo[p]) { again.push_back(p); continue; }                  // wrong fixed point: run again
+          if (!hsens[p]) continue;                                          // settled
+          if (kept[p] && hagree[p]) continue;                               // two attempts agree
+          keep.push_back(p);                                                // keep this gs, run again
+          again.push_back(p);
+        }
         if (again.empty()) break;
         if (att > kDecRetries) {
+          for (int p : again) hredo[p] = 1;
+          MCK(cudaMemcpyAsync(w.redo, hredo.data(), sizeof(int) * P, cudaMemcpyHostToDevice, s), "redo");
           k_flag_unresolved<<<(P + 255) / 256, 256, 0, s>>>(P, w.redo, side == 0 ? w.ncl : w.ncr, w.pst,
                                                               a.sgf_max_iter);
           ++nl;
+          MCK(cudaStreamSynchronize(s), "sync");
           break;
+        }
+        if (!keep.empty()) {
+          MCK(cudaMemcpyAsync(w.sub, keep.data(), sizeof(int) * keep.size(), cudaMemcpyHostToDevice, s), "keep");
+          k_keep<<<(int)keep.size(), 256, 0, s>>>(Q, w.sub, gs, B[13], Q); ++nl;
+          for (int p : keep) kept[p] = 1;
         }
         MCK(cudaMemcpyAsync(w.sub, again.data(), sizeof(int) * again.size(), cudaMemcpyHostToDevice, s), "sub");
         MCK(cudaMemsetAsync(w.redo, 0, sizeof(int) * P, s), "memset redo");
         if (int r = decimate(side, w.sub, (int)again.size(), 1.0 + att * 0x1p-50)) return r;
+        cur_sub = again;
+        MCK(cudaStreamSynchronize(s), "sync");   // the host vectors above are reused next round
       }
     }
     // ---- self-energies Sigma_c = Tlc gs Tcl (B11 left, B12 right)

@@ -119,6 +119,7 @@ enum OpKind : int {
   K_RESPROBE,  // res[slot] = max_i |(A (B v))_i - v_i|, order m (cta_inv_probe: B a computed inverse of A)
   K_EYE,       // C = identity, order m
   K_RETCHECK,  // res[slot] = min_i s Im A_ii / max_i |A_ii|, order m, s = -sign of the energy's imaginary part
+  K_RELDIFF,   // res[slot] = max |A(q) - B(q)| / max |B(q)|, m elements
 };
 
 // The retarded surface Green's function has a negative semidefinite
@@ -348,6 +349,17 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
         sm.res[o.slot] = (bad > 0.0) ? -__longlong_as_double(0x7ff0000000000000LL) : ((hi > 0.0) ? lo / hi : 0.0);
       break;
     }
+    case K_RELDIFF: {
+      double d = 0.0, b = 0.0;
+      for (int q = tid; q < o.m; q += blockDim.x) {
+        d = fmax(d, cabs(csub(o.A[q], o.B[q])));
+        b = fmax(b, cabs(o.B[q]));
+      }
+      d = cta_max(d, sm.red);
+      b = cta_max(b, sm.red);
+      if (tid == 0) sm.res[o.slot] = (b > 0.0) ? d / b : d;
+      break;
+    }
     case K_ACCUM:
       for (int q = tid; q < o.m; q += blockDim.x) {
         const double2 v = cmul(o.alpha, o.A[q]);
@@ -374,6 +386,9 @@ struct Prog {
   int c, L, ncb, it, ok, done, ib, ix, ic, ic1;
   int att;              // decimation attempt (retarded-branch retries)
   int diverged;         // the attempt's max|C1| went Inf / NaN
+  int sens;             // the attempt needed a refined inverse (a nearly singular Ao): sensitive to rounding
+  int kept;             // a previous sensitive attempt's gs is kept for comparison
+  int in_dec;           // inside a decimation (refinements mark it sensitive)
   double2 ecd;          // contact energy of the attempt
   // inverse refinement (the `refine` block): matrix, its computed inverse, order, return point
   const double2* rA;
@@ -496,8 +511,11 @@ dispatch:
           goto sgf_ready;
         }
         s.att = 0;
+        s.kept = 0;
       decimation_attempt:
         s.ecd = (s.att == 0) ? s.ecs : cscale(1.0 + s.att * 0x1p-50, s.ecs);
+        s.sens = 0;
+        s.in_dec = 1;
         set_esh(o, w.slot(0), s.L, s.L, s.d->h00 + s.d->olead[s.c], s.d->has_s00 ? s.d->s00 + s.d->olead[s.c] : nullptr,
                 s.ecd, 1, nullptr, nullptr, OP_N);                                          // Ao
         PT_EMIT(s);
@@ -559,7 +577,27 @@ dispatch:
             goto decimation_attempt;
           }
           if (wrong) s.done = 0;   // no retarded solution reached: NOT_CONVERGED
+          // a sensitive decimation (one of its inverses needed refinement) is accepted once
+          // two attempts reach the same gs: a fixed point other than the retarded one can
+          // pass the diagonal test, and the retarded one is the common outcome
+          if (!wrong && s.sens) {
+            if (s.kept) {
+              o.kind = K_RELDIFF; o.m = s.L * s.L; o.A = w.slot(4); o.B = w.slot(10); o.slot = 5;
+              PT_EMIT(s);
+            }
+            if (!s.kept || !(sm.res[5] <= 1e-2)) {
+              if (s.att < kDecRetries) {
+                set_simple(o, K_COPY, s.L * s.L, w.slot(4), w.slot(10));
+                PT_EMIT(s);
+                s.kept = 1;
+                ++s.att;
+                goto decimation_attempt;
+              }
+              s.done = 0;          // no two attempts agree: NOT_CONVERGED
+            }
+          }
         }
+        s.in_dec = 0;
         if (!s.done) put_status(s.st, ST_NOT_CONVERGED);
         s.ncyc += s.done ? s.it : a.sgf_max_iter + 1;
         if (a.sgf_out && a.sgf_out[(int64_t)s.p * a.ncont_max + s.c] >= 0) {
@@ -1168,6 +1206,7 @@ dispatch:
         o.kind = K_RESPROBE; o.m = s.rm; o.A = s.rA; o.B = s.rX; o.slot = 7;
         PT_EMIT(s);
         if (!(sm.res[7] > kInvProbeTol) || !(sm.res[7] <= 1.7976931348623157e308)) break;   // fine, or non-finite
+        if (s.in_dec) s.sens = 1;
         o.kind = K_EYE; o.m = s.rm; o.C = w.slot(S_INV);
         PT_EMIT(s);
         set_gemm(o, s.rm, s.rm, s.rm, s.rA, s.rm, OP_N, s.rX, s.rm, OP_N, w.slot(S_INV), s.rm, mone, one);

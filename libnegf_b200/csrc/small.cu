@@ -391,7 +391,8 @@ cudaError_t opt_in(K kernel, size_t smem, bool (&done)[64], std::mutex& mu) {
 // products and leaves X untouched.
 template <int N>
 __global__ void __launch_bounds__(kWarps * 32)
-    k_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count) {
+    k_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count,
+                   int* sens) {
   extern __shared__ __align__(16) double2 sref[];
   double2* sA = sref;
   double2* sX = sA + N * N;
@@ -455,19 +456,21 @@ __global__ void __launch_bounds__(kWarps * 32)
     __syncthreads();
     changed = true;
   }
-  if (changed)
+  if (changed) {
     for (int q = threadIdx.x; q < nn; q += kWarps * 32) Xp[q] = sX[q];
+    if (sens && threadIdx.x == 0) sens[p] = 1;
+  }
 }
 
 }  // namespace
 
 cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
-                                const int* count, cudaStream_t s) {
+                                const int* count, cudaStream_t s, int* sens) {
   if (batch <= 0) return cudaSuccess;
   if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
   if (n <= 16) {
     const size_t smem = (3 * 16 * 16 + 16) * sizeof(double2);
-    k_small_refine<16><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count);
+    k_small_refine<16><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count, sens);
   } else {
     const size_t smem = (3 * 32 * 32 + 32) * sizeof(double2);   // above the 48 KB default: opt in per device
     static std::mutex mu;
@@ -480,7 +483,7 @@ cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, 
       if (e != cudaSuccess) return e;
       if (dev >= 0 && dev < 64) attr[dev] = true;
     }
-    k_small_refine<32><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count);
+    k_small_refine<32><<<batch, kWarps * 32, smem, s>>>(batch, n, A, X, Q, map, count, sens);
   }
   return cudaGetLastError();
 }
