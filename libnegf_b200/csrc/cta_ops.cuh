@@ -605,22 +605,37 @@ __device__ __forceinline__ double2 probe_v(int k) { return make_double2(1.0 + 0.
 // stable, far above it where the inversion lost accuracy (Gauss-Jordan on a
 // nearly singular matrix).  Two matrix-vector products; y is an n-element
 // shared-memory buffer.  NaN or Inf anywhere gives +Inf.
-__device__ __forceinline__ double cta_inv_probe(int n, const double2* A, const double2* X, double2* y, double* red) {
+// *kappa (optional): max_i sum_j |A_ij| |(Xv)_j|, an estimate of the
+// condition number of A (|v_k| ~ 1): about 1e4 .. 1e6 for the decimation's
+// Ao away from a lead resonance, 1e8 and up near one.
+__device__ __forceinline__ double cta_inv_probe(int n, const double2* A, const double2* X, double2* y, double* red,
+                                                double* kappa = nullptr) {
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     double2 acc = make_double2(0.0, 0.0);
     for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(X[(size_t)r + (size_t)c * n], probe_v(c)));
     y[r] = acc;
   }
   __syncthreads();
-  double e = 0.0;
+  double e = 0.0, k = 0.0;
   for (int r = threadIdx.x; r < n; r += blockDim.x) {
     double2 acc = make_double2(0.0, 0.0);
-    for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(A[(size_t)r + (size_t)c * n], y[c]));
+    double sa = 0.0;
+    for (int c = 0; c < n; ++c) {
+      const double2 a = A[(size_t)r + (size_t)c * n];
+      acc = cadd(acc, cmul(a, y[c]));
+      sa += cabs1(a) * cabs1(y[c]);
+    }
     const double d = cabs(csub(acc, probe_v(r)));
     e = (d <= 1.7976931348623157e308) ? fmax(e, d) : __longlong_as_double(0x7ff0000000000000LL);
+    k = fmax(k, sa);
   }
+  if (kappa) *kappa = cta_max(k, red);
   return cta_max(e, red);
 }
+
+// A decimation whose Ao reaches this estimated condition number is sensitive
+// to rounding (see the agreement rule of the decimations).
+constexpr double kSensitiveCond = 1e7;
 
 // Re Tr(X Y) = sum_{i,j} Re(X(i,j) Y(j,i)); op applies to Y (OP_C: Y = Z^dag)
 __device__ __forceinline__ double cta_re_trace_prod(const double2* X, const double2* Y, int n, int opY, double* red,

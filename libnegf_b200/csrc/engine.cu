@@ -50,16 +50,19 @@ __device__ __forceinline__ int zinv(int n, const double2* A, double2* out, doubl
 // zinv, then the residual probe and up to two Newton steps
 // X <- X + X (I - A X) where the probe exceeds kInvProbeTol (the engine's
 // refine block); R and Xn are n x n scratch (R null: no probe).
+// *nearly_singular (optional): the probe's condition estimate exceeds
+// kSensitiveCond.
 __device__ __noinline__ int zinv_refined(int n, const double2* A, double2* X, double2* ws, double2* R, double2* Xn,
-                                         SmemMap& sm, bool* refined = nullptr) {
+                                         SmemMap& sm, bool* nearly_singular = nullptr) {
   const int bad = zinv(n, A, X, ws, sm);
-  if (refined) *refined = false;
+  if (nearly_singular) *nearly_singular = false;
   const double2 one = make_double2(1, 0), mone = make_double2(-1, 0);
   const int nn = n * n;
   for (int k = 0; k < 2 && R; ++k) {
-    const double e = cta_inv_probe(n, A, X, sm.main, sm.red);
+    double kap = 0.0;
+    const double e = cta_inv_probe(n, A, X, sm.main, sm.red, &kap);
+    if (k == 0 && nearly_singular && kap > kSensitiveCond) *nearly_singular = true;
     if (!(e > kInvProbeTol) || !(e <= 1.7976931348623157e308)) break;
-    if (refined) *refined = true;
     for (int q = threadIdx.x; q < nn; q += blockDim.x) R[q] = make_double2((q % n) == (q / n) ? 1.0 : 0.0, 0.0);
     __syncthreads();
     gemm(n, n, n, opN(A, n), opN(X, n), R, n, mone, one, sm);     // R = I - A X
@@ -268,10 +271,10 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int p = map ? map[b] : b;
   double2* wb = work + (int64_t)b * wstride;
   double2* R = wb + zinv_ws_elems(n, kSmemMain);
-  bool refined = false;
-  int inf = zinv_refined(n, A + (int64_t)p * sA, X + (int64_t)p * sX, wb, R, R + (int64_t)n * n, sm, &refined);
+  bool near_sing = false;
+  int inf = zinv_refined(n, A + (int64_t)p * sA, X + (int64_t)p * sX, wb, R, R + (int64_t)n * n, sm, &near_sing);
   if (threadIdx.x == 0 && info) info[p] = inf;
-  if (threadIdx.x == 0 && sens && refined) sens[p] = 1;
+  if (threadIdx.x == 0 && sens && near_sing) sens[p] = 1;
 }
 
 cudaError_t launch_zinv_mapped(int batch, int n, const double2* A, int64_t sA, double2* X, int64_t sX,

@@ -133,8 +133,8 @@ cudaError_t launch_zgemm_batched(int batch, int m, int n, int k, double2 alpha, 
 cudaError_t launch_zinv_batched(int batch, int n, const double2* A, double2* Ainv, int* info, double2* work,
                                 cudaStream_t s);
 size_t zinv_batched_work_elems(int n);
-// sens (optional): sens[map[b]] = 1 where the inverse needed a Newton step
-// (its residual probe showed a nearly singular matrix)
+// sens (optional): sens[map[b]] = 1 where the matrix is nearly singular
+// (its condition estimate from the residual probe exceeds kSensitiveCond)
 cudaError_t launch_zinv_mapped(int batch, int n, const double2* A, int64_t sA, double2* X, int64_t sX,
                                const int* map, int* info, double2* work, cudaStream_t s, int* sens = nullptr);
 cudaError_t launch_decimation_batched(int batch, int n, const double2* Ao, const double2* Bo, const double2* Co,

@@ -46,7 +46,7 @@ __device__ __forceinline__ SmemMap map_smem(char* base, int nmax) {
   char* p = base + kSmemMain;
   m.red = reinterpret_cast<double*>(p); p += 32 * sizeof(double);
   m.maxv = reinterpret_cast<double*>(p); p += 2 * sizeof(double);
-  m.res = reinterpret_cast<double*>(p); p += 8 * sizeof(double);
+  m.res = reinterpret_cast<double*>(p); p += 12 * sizeof(double);
   m.inv.redv = reinterpret_cast<double*>(p); p += 32 * sizeof(double);
   m.inv.redi = reinterpret_cast<int*>(p); p += 32 * sizeof(int);
   m.inv.flag = reinterpret_cast<int*>(p); p += 4 * sizeof(int);
@@ -62,7 +62,7 @@ __device__ __forceinline__ SmemMap map_smem(char* base, int nmax) {
 }
 
 inline size_t smem_bytes_for(int nmax) {
-  return kSmemMain + 32 * 8 + 2 * 8 + 8 * 8 + 32 * 8 + 32 * 4 + 4 * 4 + 4 * 4 + 4 * 4 + 3 * (size_t)nmax * 4 + 8 +
+  return kSmemMain + 32 * 8 + 2 * 8 + 12 * 8 + 32 * 8 + 32 * 4 + 4 * 4 + 4 * 4 + 4 * 4 + 3 * (size_t)nmax * 4 + 8 +
          TR_NPHASE * 8;
 }
 
@@ -116,7 +116,7 @@ enum OpKind : int {
   K_LDOS,      // out[k] = sum over LDOS set k of dos[i-1] (A = dos row as doubles, device sets)
   K_ACCUM,     // C[q] += alpha * A[q], q < m (atomic: C is shared by all CTAs)
   K_SUBCOPY,   // C(flag + r, flag + c) = A(r, c), A m x m, C leading dimension ldc
-  K_RESPROBE,  // res[slot] = max_i |(A (B v))_i - v_i|, order m (cta_inv_probe: B a computed inverse of A)
+  K_RESPROBE,  // res[slot] = max_i |(A (B v))_i - v_i|, res[8] = the condition estimate, order m (cta_inv_probe)
   K_EYE,       // C = identity, order m
   K_RETCHECK,  // res[slot] = min_i s Im A_ii / max_i |A_ii|, order m, s = -sign of the energy's imaginary part
   K_RELDIFF,   // res[slot] = max |A(q) - B(q)| / max |B(q)|, m elements
@@ -322,8 +322,12 @@ __device__ __forceinline__ void exec_light(const Op& o, SmemMap& sm) {
       }
       break;
     case K_RESPROBE: {
-      const double e = cta_inv_probe(o.m, o.A, o.B, sm.main, sm.red);
-      if (tid == 0) sm.res[o.slot] = e;
+      double k = 0.0;
+      const double e = cta_inv_probe(o.m, o.A, o.B, sm.main, sm.red, &k);
+      if (tid == 0) {
+        sm.res[o.slot] = e;
+        sm.res[8] = k;
+      }
       break;
     }
     case K_EYE:
@@ -386,7 +390,7 @@ struct Prog {
   int c, L, ncb, it, ok, done, ib, ix, ic, ic1;
   int att;              // decimation attempt (retarded-branch retries)
   int diverged;         // the attempt's max|C1| went Inf / NaN
-  int sens;             // the attempt needed a refined inverse (a nearly singular Ao): sensitive to rounding
+  int sens;             // the attempt met a nearly singular Ao (condition estimate above kSensitiveCond)
   int kept;             // a previous sensitive attempt's gs is kept for comparison
   int in_dec;           // inside a decimation (refinements mark it sensitive)
   double2 ecd;          // contact energy of the attempt
@@ -1205,8 +1209,8 @@ dispatch:
       for (s.rk = 0; s.rk < 2; ++s.rk) {
         o.kind = K_RESPROBE; o.m = s.rm; o.A = s.rA; o.B = s.rX; o.slot = 7;
         PT_EMIT(s);
+        if (s.in_dec && s.rk == 0 && sm.res[8] > kSensitiveCond) s.sens = 1;
         if (!(sm.res[7] > kInvProbeTol) || !(sm.res[7] <= 1.7976931348623157e308)) break;   // fine, or non-finite
-        if (s.in_dec) s.sens = 1;
         o.kind = K_EYE; o.m = s.rm; o.C = w.slot(S_INV);
         PT_EMIT(s);
         set_gemm(o, s.rm, s.rm, s.rm, s.rA, s.rm, OP_N, s.rX, s.rm, OP_N, w.slot(S_INV), s.rm, mone, one);

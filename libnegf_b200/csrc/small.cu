@@ -398,7 +398,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   double2* sX = sA + N * N;
   double2* sR = sX + N * N;
   double2* y = sR + N * N;
-  __shared__ double red[kWarps];
+  __shared__ double red[kWarps], redk[kWarps];
   const int b = blockIdx.x;
   if (b >= batch_limit(batch, count)) return;
   const int p = map ? map[b] : b;
@@ -419,19 +419,35 @@ __global__ void __launch_bounds__(kWarps * 32)
       y[r] = acc;
     }
     __syncthreads();
-    double e = 0.0;
+    double e = 0.0, kap = 0.0;
     for (int r = threadIdx.x; r < n; r += kWarps * 32) {
       double2 acc = make_double2(0.0, 0.0);
-      for (int c = 0; c < n; ++c) acc = cadd(acc, cmul(sA[r + c * n], y[c]));
+      double sa = 0.0;
+      for (int c = 0; c < n; ++c) {
+        acc = cadd(acc, cmul(sA[r + c * n], y[c]));
+        sa += cabs1(sA[r + c * n]) * cabs1(y[c]);
+      }
       const double d = cabs(csub(acc, probe_v(r)));
       e = (d <= 1.7976931348623157e308) ? fmax(e, d) : __longlong_as_double(0x7ff0000000000000LL);
+      kap = fmax(kap, sa);
     }
-    for (int o = 16; o > 0; o >>= 1) e = fmax(e, __shfl_xor_sync(kFull, e, o));
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+    for (int o = 16; o > 0; o >>= 1) {
+      e = fmax(e, __shfl_xor_sync(kFull, e, o));
+      kap = fmax(kap, __shfl_xor_sync(kFull, kap, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      red[threadIdx.x >> 5] = e;
+      redk[threadIdx.x >> 5] = kap;
+    }
     __syncthreads();
-    double em = 0.0;
-    for (int q = 0; q < kWarps; ++q) em = fmax(em, red[q]);
+    double em = 0.0, km = 0.0;
+    for (int q = 0; q < kWarps; ++q) {
+      em = fmax(em, red[q]);
+      km = fmax(km, redk[q]);
+    }
     __syncthreads();
+    // the condition estimate of the unrefined inverse marks a nearly singular matrix
+    if (round == 0 && km > kSensitiveCond && sens && threadIdx.x == 0) sens[p] = 1;
     if (!(em > kInvProbeTol) || !(em <= 1.7976931348623157e308)) break;
     // R = I - A X
     for (int q = threadIdx.x; q < nn; q += kWarps * 32) {
@@ -456,10 +472,8 @@ __global__ void __launch_bounds__(kWarps * 32)
     __syncthreads();
     changed = true;
   }
-  if (changed) {
+  if (changed)
     for (int q = threadIdx.x; q < nn; q += kWarps * 32) Xp[q] = sX[q];
-    if (sens && threadIdx.x == 0) sens[p] = 1;
-  }
 }
 
 }  // namespace

@@ -50,7 +50,8 @@ cudaError_t launch_small_dec_b(int P, int n, const int* list, const int* count, 
 // The residual probe of each inverse X_p of A_p (same problem selection) and
 // up to two Newton steps X <- X + X (I - A X) where it shows a loss of
 // accuracy (kInvProbeTol); X_p is left untouched where it does not.
-// sens (optional): sens[p] = 1 where a Newton step ran.
+// sens (optional): sens[p] = 1 where the probe's condition estimate of A
+// exceeds kSensitiveCond (a nearly singular matrix).
 cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map,
                                 const int* count, cudaStream_t s, int* sens = nullptr);
 
