@@ -105,110 +105,118 @@ __global__ void __launch_bounds__(kWarps * 32)
   }
 }
 
-// In-place Gauss-Jordan on the rows held by the lanes.  Rows are never moved
-// between lanes: each lane carries the logical (pivot-order) index of its
-// row, the pivot of column k is the unused row with the largest |Re|+|Im|
-// (lowest logical index on a tie), and the column interchanges that undo the
-// row order are applied to the store addresses at the end.  Per step the
-// pivot row is published through shared memory; the pivot row becomes
-// row * d (d = 1 / pivot, entry k = d), every other row r - (r_k d) * row
-// (entry k = -(r_k d)), the update order of the engine's Gauss-Jordan.
+// In-place Gauss-Jordan, one CTA (4 warps) per matrix: lane i holds row i,
+// warp w the columns [w CW, (w + 1) CW).  Rows never move between lanes:
+// each lane carries the logical (pivot-order) index of its row, identical in
+// every warp.  Per step the warp owning column k picks the pivot (the unused
+// row with the largest |Re|+|Im|, lowest logical index on a tie: izamax) by
+// integer warp reductions on the bit pattern and publishes column k and the
+// pivot's lane in shared memory (double-buffered by step parity: one barrier
+// per step); every warp then updates its columns, taking the pivot row's
+// entries from the pivot lane by shuffle.  The pivot row becomes row * d
+// (d = 1 / pivot, entry k = d), every other row r - (r_k d) * row (entry
+// k = -(r_k d)), the update order of the engine's Gauss-Jordan.  The column
+// interchanges that undo the row order are applied to the store addresses.
 template <int N>
 __global__ void __launch_bounds__(kWarps * 32)
     k_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count,
                  int* info, int* status, int singular_code) {
-  __shared__ double2 prow[kWarps][N];
-  __shared__ int sidx[kWarps][N];
-  __shared__ int scm[kWarps][N];
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int b = blockIdx.x * kWarps + w;
+  constexpr int CW = N / kWarps;
+  __shared__ double2 colk[2][N];
+  __shared__ int sbl[2];
+  __shared__ int sidx[N];
+  __shared__ int scm[N];
+  const int b = blockIdx.x;
   if (b >= batch_limit(batch, count)) return;
   const int p = map ? map[b] : b;
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const double2* Ap = A + p * Q;
-  double2 r[N];
+  double2 r[CW];
 #pragma unroll
-  for (int c = 0; c < N; ++c)
-    r[c] = (lane < n && c < n) ? Ap[lane + (int64_t)c * n] : make_double2(0.0, 0.0);
+  for (int cc = 0; cc < CW; ++cc) {
+    const int c = w * CW + cc;
+    r[cc] = (lane < n && c < n) ? Ap[lane + (int64_t)c * n] : make_double2(0.0, 0.0);
+  }
   int lg = lane;
   bool used = lane >= n;
   int inf = 0;
-  // the step loop stays rolled (a fully unrolled N x N body overflows the
-  // instruction cache); the register row is indexed by the unrolled column
-  // loop only, the pivot column picked out with selects
-#pragma unroll 1
   for (int k = 0; k < n; ++k) {
-    double2 rk = r[0];
+    const int ow = k / CW, ck = k % CW, par = k & 1;
+    if (w == ow) {
+      double2 rk = r[0];
 #pragma unroll
-    for (int c = 1; c < N; ++c)
-      if (c == k) rk = r[c];
-    // pivot search by integer warp reductions on the bit pattern of
-    // |Re|+|Im| (non-negative doubles order as their bits), + 1 so that an
-    // unused row with a zero entry still beats the used rows (key 0); NaN
-    // ranks above everything, so every lane sees one total order and a NaN
-    // spreads to the whole inverse rather than being skipped
-    double v = cabs1(rk);
-    if (v != v) v = __longlong_as_double(0x7ff0000000000000LL);
-    const unsigned long long key = used ? 0ull : (unsigned long long)__double_as_longlong(v) + 1ull;
-    const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
-    const unsigned mhi = __reduce_max_sync(kFull, hi);
-    const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
-    const bool cand = hi == mhi && lo == mlo;
-    const int blg = (int)__reduce_min_sync(kFull, cand ? (unsigned)lg : 0xffffffffu);
-    const int bl = __ffs(__ballot_sync(kFull, cand && lg == blg)) - 1;
-    if (lane == bl) {
-#pragma unroll
-      for (int c = 0; c < N; ++c)
-        if (c < n) prow[w][c] = r[c];
+      for (int cc = 1; cc < CW; ++cc)
+        if (cc == ck) rk = r[cc];
+      // |Re|+|Im| orders as its bit pattern; + 1 puts an unused row with a zero entry
+      // above the used rows (key 0); NaN ranks highest so all lanes see one order
+      double v = cabs1(rk);
+      if (v != v) v = __longlong_as_double(0x7ff0000000000000LL);
+      const unsigned long long key = used ? 0ull : (unsigned long long)__double_as_longlong(v) + 1ull;
+      const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+      const unsigned mhi = __reduce_max_sync(kFull, hi);
+      const unsigned mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+      const bool cand = hi == mhi && lo == mlo;
+      const int blg = (int)__reduce_min_sync(kFull, cand ? (unsigned)lg : 0xffffffffu);
+      const int bl = __ffs(__ballot_sync(kFull, cand && lg == blg)) - 1;
+      colk[par][lane] = rk;
+      if (lane == 0) {
+        sbl[par] = bl;
+        sidx[k] = blg;
+      }
     }
-    __syncwarp();
-    const double2 pv = prow[w][k];
+    __syncthreads();
+    const int bl = sbl[par];
+    const int blg = sidx[k];
+    const double2 pv = colk[par][bl];
     if (pv.x == 0.0 && pv.y == 0.0 && inf == 0) inf = k + 1;
     const double2 d = crecip(pv);
-    if (lane == bl) {
+    const double2 fd = cmul(colk[par][lane], d);
 #pragma unroll
-      for (int c = 0; c < N; ++c) r[c] = (c == k) ? d : cmul(r[c], d);
-    } else {
-      const double2 fd = cmul(rk, d);
-#pragma unroll
-      for (int c = 0; c < N; ++c) {
-        if (c == k) {
-          r[c] = make_double2(-fd.x, -fd.y);
-        } else if (c < n) {
-          r[c] = csub(r[c], cmul(fd, prow[w][c]));
-        }
-      }
+    for (int cc = 0; cc < CW; ++cc) {
+      const int c = w * CW + cc;
+      double2 pc;
+      pc.x = __shfl_sync(kFull, r[cc].x, bl);
+      pc.y = __shfl_sync(kFull, r[cc].y, bl);
+      if (lane == bl)
+        r[cc] = (c == k) ? d : cmul(pc, d);
+      else if (c == k)
+        r[cc] = make_double2(-fd.x, -fd.y);
+      else if (c < n)
+        r[cc] = csub(r[cc], cmul(fd, pc));
     }
     if (lg == k) lg = blg;
     if (lane == bl) {
       lg = k;
       used = true;
     }
-    if (lane == 0) sidx[w][k] = blg;
-    __syncwarp();
   }
-  // column interchanges in reverse pivot order: output column dest[c] takes
-  // internal column c
-  if (lane == 0) {
-    for (int j = 0; j < n; ++j) scm[w][j] = j;
+  // column interchanges in reverse pivot order: output column dest[c] takes internal column c
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < n; ++j) scm[j] = j;
     for (int l = n - 1; l >= 0; --l) {
-      const int il = sidx[w][l];
+      const int il = sidx[l];
       if (il != l) {
-        const int t = scm[w][il];
-        scm[w][il] = scm[w][l];
-        scm[w][l] = t;
+        const int t = scm[il];
+        scm[il] = scm[l];
+        scm[l] = t;
       }
     }
-    for (int j = 0; j < n; ++j) sidx[w][scm[w][j]] = j;
+    for (int j = 0; j < n; ++j) sidx[scm[j]] = j;
   }
-  __syncwarp();
+  __syncthreads();
   if (lane < n) {
     double2* Xp = X + p * Q;
 #pragma unroll
-    for (int c = 0; c < N; ++c)
-      if (c < n) Xp[lg + (int64_t)sidx[w][c] * n] = r[c];
+    for (int cc = 0; cc < CW; ++cc) {
+      const int c = w * CW + cc;
+      if (c < n) Xp[lg + (int64_t)sidx[c] * n] = r[cc];
+    }
   }
-  if (lane == 0 && info) info[p] = inf;
-  if (lane == 0 && status && inf != 0 && status[p] == 0) status[p] = singular_code;
+  if (threadIdx.x == 0) {
+    if (info) info[p] = inf;
+    if (status && inf != 0 && status[p] == 0) status[p] = singular_code;
+  }
 }
 
 // ---------------------------------------------------------------- decimation steps
@@ -563,11 +571,10 @@ cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, in
                               const int* count, int* info, int* status, int singular_code, cudaStream_t s) {
   if (batch <= 0) return cudaSuccess;
   if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
-  const int grid = (batch + kWarps - 1) / kWarps;
   if (n <= 16)
-    k_small_zinv<16><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info, status, singular_code);
+    k_small_zinv<16><<<batch, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info, status, singular_code);
   else
-    k_small_zinv<32><<<grid, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info, status, singular_code);
+    k_small_zinv<32><<<batch, kWarps * 32, 0, s>>>(batch, n, A, X, Q, map, count, info, status, singular_code);
   return cudaGetLastError();
 }
 
