@@ -122,7 +122,7 @@ __global__ void __launch_bounds__(kWarps * 32)
     k_small_zinv(int batch, int n, const double2* A, double2* X, int64_t Q, const int* map, const int* count,
                  int* info, int* status, int singular_code) {
   constexpr int CW = N / kWarps;
-  __shared__ double2 colk[2][N];
+  __shared__ double2 colk[2][32];  // one entry per lane: rows >= N exist as lanes too
   __shared__ int sbl[2];
   __shared__ int sidx[N];
   __shared__ int scm[N];
