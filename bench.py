@@ -38,7 +38,9 @@ WORKLOADS = {
     # name: (nbl, n, nE, emin, emax, nk, eta, dos)
     "c1": dict(nbl=100, n=256, nE=2048, emin=-2.0, emax=2.0, nk=16, eta=1e-6, dos=True, gen="c1"),
     # the CPU-runnable config states its surface Green's functions converged to 1e-12
-    "c0": dict(nbl=20, n=32, nE=512, emin=-3.0, emax=3.0, nk=1, eta=1e-6, dos=False, gen="c0", sgf_tol=1e-12),
+    # one step = the whole 512-energy grid
+    "c0": dict(nbl=20, n=32, nE=512, emin=-3.0, emax=3.0, nk=1, eta=1e-6, dos=False, gen="c0", sgf_tol=1e-12,
+               pps=512),
     "c2": dict(nbl=60, n=512, nE=1024, emin=-2.0, emax=2.0, nk=8, eta=1e-6, dos=False, gen="c1"),
     # elastic-dephasing SCBA: dephasing coupling 0.1 eV (D = 0.01 eV^2) on every orbital, bias 0.2 eV
     # symmetric, 300 K leads; linear mixing 0.5 until the contact-1 current changes by < 1e-8, at most
