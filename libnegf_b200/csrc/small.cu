@@ -38,9 +38,25 @@ __global__ void __launch_bounds__(kWarps * 32)
   const int nn = n * n;
   const double2* Ap = A + p * Q;
   const double2* Bp = B + p * Q;
-  for (int q = threadIdx.x; q < nn; q += kWarps * 32) {
-    sA[q] = __ldg(Ap + q);
-    sB[q] = __ldg(Bp + q);
+  {
+    constexpr int R = (N * N + kWarps * 32 - 1) / (kWarps * 32);
+    double2 va[R], vb[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int q = threadIdx.x + i * kWarps * 32;
+      if (q < nn) {
+        va[i] = __ldg(Ap + q);
+        vb[i] = __ldg(Bp + q);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int q = threadIdx.x + i * kWarps * 32;
+      if (q < nn) {
+        sA[q] = va[i];
+        sB[q] = vb[i];
+      }
+    }
   }
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -171,18 +187,19 @@ __global__ void __launch_bounds__(kWarps * 32)
     if (pv.x == 0.0 && pv.y == 0.0 && inf == 0) inf = k + 1;
     const double2 d = crecip(pv);
     const double2 fd = cmul(colk[par][lane], d);
+    // both candidate values for every lane, then selects: no divergent path for the pivot lane
+    const bool isp = lane == bl;
 #pragma unroll
     for (int cc = 0; cc < CW; ++cc) {
       const int c = w * CW + cc;
       double2 pc;
       pc.x = __shfl_sync(kFull, r[cc].x, bl);
       pc.y = __shfl_sync(kFull, r[cc].y, bl);
-      if (lane == bl)
-        r[cc] = (c == k) ? d : cmul(pc, d);
-      else if (c == k)
-        r[cc] = make_double2(-fd.x, -fd.y);
-      else if (c < n)
-        r[cc] = csub(r[cc], cmul(fd, pc));
+      const double2 prow = cmul(pc, d);
+      const double2 upd = csub(r[cc], cmul(fd, pc));
+      double2 v = isp ? prow : (c < n ? upd : r[cc]);
+      if (c == k) v = isp ? d : make_double2(-fd.x, -fd.y);
+      r[cc] = v;
     }
     if (lg == k) lg = blg;
     if (lane == bl) {
@@ -245,9 +262,32 @@ __device__ __forceinline__ void mm_rows(int n, const double2* sA, const double2*
   }
 }
 
+// Three n x n operands into shared memory: every thread issues all of its
+// global loads before its first shared store (one memory latency, not three).
 template <int N>
-__device__ __forceinline__ void stage(int n, double2* dst, const double2* src) {
-  for (int q = threadIdx.x; q < n * n; q += kWarps * 32) dst[q] = src[q];
+__device__ __forceinline__ void stage3(int n, double2* d0, const double2* s0, double2* d1, const double2* s1,
+                                       double2* d2, const double2* s2) {
+  constexpr int R = (N * N + kWarps * 32 - 1) / (kWarps * 32);
+  const int nn = n * n;
+  double2 v0[R], v1[R], v2[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int q = threadIdx.x + i * kWarps * 32;
+    if (q < nn) {
+      v0[i] = __ldg(s0 + q);
+      v1[i] = __ldg(s1 + q);
+      v2[i] = __ldg(s2 + q);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int q = threadIdx.x + i * kWarps * 32;
+    if (q < nn) {
+      d0[q] = v0[i];
+      d1[q] = v1[i];
+      d2[q] = v2[i];
+    }
+  }
 }
 
 // First half of a decimation iteration (src/contselfenergy.F90:271-340) for
@@ -272,9 +312,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   if (b >= min(*count, P)) return;
   const int p = list[b];
   const int64_t o = p * Q;
-  stage<N>(n, sG, Go + o);
-  stage<N>(n, sC, Co + o);
-  stage<N>(n, sB, Bo + o);
+  stage3<N>(n, sG, Go + o, sC, Co + o, sB, Bo + o);
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 acc[CW];
@@ -353,9 +391,7 @@ __global__ void __launch_bounds__(kWarps * 32)
   if (b >= min(*count, P)) return;
   const int p = list[b];
   const int64_t o = p * Q;
-  stage<N>(n, sG, Go + o);
-  stage<N>(n, sB, Bo + o);
-  stage<N>(n, sC, Co + o);
+  stage3<N>(n, sG, Go + o, sB, Bo + o, sC, Co + o);
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 acc[CW];
