@@ -515,12 +515,11 @@ int mixed_run(const MixedArgs& a, void* ws, int batch, cudaStream_t s, std::stri
       for (; it <= a.sgf_max_iter && na > 0; ++it) {
         MCK(inv(na, cur, cnt_cur, Ao, Go), "zinv");
         if (small) {
-          // the rest of the iteration in two fused launches, one CTA per point
+          // the rest of the iteration in one fused launch, one CTA per point
           MCK(cudaMemsetAsync(cnt_nxt, 0, sizeof(int), s), "memset count");
-          MCK(launch_small_dec_a(na, n, cur, cnt_cur, Go, Co, Bo, C1, Ao, Aos, Q, w.ok, ncyc_c, a.sgf_tol, it, nxt,
-                                 cnt_nxt, w.redo, s), "decimation a");
-          MCK(launch_small_dec_b(na, n, nxt, cnt_nxt, Go, Bo, Co, B1, Ao, Q, s), "decimation b");
-          nl += 2;
+          MCK(launch_small_dec(na, n, cur, cnt_cur, Go, Co, Bo, C1, B1, Ao, Aos, Q, w.ok, ncyc_c, a.sgf_tol, it,
+                               nxt, cnt_nxt, w.redo, s), "decimation");
+          ++nl;
           std::swap(cur, nxt);
           std::swap(cnt_cur, cnt_nxt);
           std::swap(B[2], B[8]);

@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(kWarps * 32)
 
 // ---------------------------------------------------------------- decimation steps
 // Row `lane` of columns [w CW, (w + 1) CW) of A B, A and B n x n in shared
-// memory (the product of k_small_zgemm, for the fused steps below).
+// memory (the product of k_small_zgemm, for the fused decimation iteration below).
 template <int N>
 __device__ __forceinline__ void mm_rows(int n, const double2* sA, const double2* sB, double2 (&acc)[N / kWarps]) {
   constexpr int CW = N / kWarps;
@@ -290,16 +290,18 @@ __device__ __forceinline__ void stage3(int n, double2* d0, const double2* s0, do
   }
 }
 
-// First half of a decimation iteration (src/contselfenergy.F90:271-340) for
-// the points list[b], b < *count, one CTA each: X = Go Co, C1 = Co X, the
-// CPU convergence rule on max|C1| (a point is done on its second
-// consecutive max|C1| <= tol: ncyc = it; the others go on to next[]), and
-// for the points that go on Self = Bo X, Ao -= Self, Aos -= Self.
+// One decimation iteration (src/contselfenergy.F90:271-340) for the points
+// list[b], b < *count, one CTA each, with Go, Co and Bo staged in shared
+// memory once: X = Go Co, C1 = Co X, the CPU convergence rule on max|C1| (a
+// point is done on its second consecutive max|C1| <= tol: ncyc = it; the
+// others go on to next[]), and for the points that go on Self = Bo X,
+// Ao -= Self, Aos -= Self, then Y = Go Bo (in X's place), B1 = Bo Y,
+// Ao -= Co Y.
 template <int N>
 __global__ void __launch_bounds__(kWarps * 32)
-    k_small_dec_a(int n, const int* list, const int* count, int P, const double2* Go, const double2* Co,
-                  const double2* Bo, double2* C1, double2* Ao, double2* Aos, int64_t Q, int* ok, int* ncyc_c,
-                  double tol, int it, int* next, int* next_count, int* redo) {
+    k_small_dec(int n, const int* list, const int* count, int P, const double2* Go, const double2* Co,
+                const double2* Bo, double2* C1, double2* B1, double2* Ao, double2* Aos, int64_t Q, int* ok,
+                int* ncyc_c, double tol, int it, int* next, int* next_count, int* redo) {
   constexpr int CW = N / kWarps;
   extern __shared__ __align__(16) double2 sdec[];
   double2* sG = sdec;
@@ -373,40 +375,19 @@ __global__ void __launch_bounds__(kWarps * 32)
         Aos[q] = csub(Aos[q], acc[jj]);
       }
     }
-}
-
-// Second half, for the points that go on (list, count): Y = Go Bo,
-// B1 = Bo Y, Ao -= Co Y (Co before this iteration's update).
-template <int N>
-__global__ void __launch_bounds__(kWarps * 32)
-    k_small_dec_b(int n, const int* list, const int* count, int P, const double2* Go, const double2* Bo,
-                  const double2* Co, double2* B1, double2* Ao, int64_t Q) {
-  constexpr int CW = N / kWarps;
-  extern __shared__ __align__(16) double2 sdec[];
-  double2* sG = sdec;
-  double2* sB = sG + N * N;
-  double2* sC = sB + N * N;
-  double2* sY = sC + N * N;
-  const int b = blockIdx.x;
-  if (b >= min(*count, P)) return;
-  const int p = list[b];
-  const int64_t o = p * Q;
-  stage3<N>(n, sG, Go + o, sB, Bo + o, sC, Co + o);
-  __syncthreads();
-  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double2 acc[CW];
+  __syncthreads();                                 // X is read; Y takes its place
   mm_rows<N>(n, sG, sB, acc);                      // Y = Go Bo
   if (lane < n)
 #pragma unroll
     for (int jj = 0; jj < CW; ++jj)
-      if (w * CW + jj < n) sY[lane + (w * CW + jj) * n] = acc[jj];
+      if (w * CW + jj < n) sX[lane + (w * CW + jj) * n] = acc[jj];
   __syncthreads();
-  mm_rows<N>(n, sB, sY, acc);                      // B1 = Bo Y
+  mm_rows<N>(n, sB, sX, acc);                      // B1 = Bo Y
   if (lane < n)
 #pragma unroll
     for (int jj = 0; jj < CW; ++jj)
       if (w * CW + jj < n) B1[o + lane + (w * CW + jj) * n] = acc[jj];
-  mm_rows<N>(n, sC, sY, acc);                      // Ao -= Co Y
+  mm_rows<N>(n, sC, sX, acc);                      // Ao -= Co Y
   if (lane < n)
 #pragma unroll
     for (int jj = 0; jj < CW; ++jj) {
@@ -546,47 +527,25 @@ cudaError_t launch_small_refine(int batch, int n, const double2* A, double2* X, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_small_dec_a(int P, int n, const int* list, const int* count, const double2* Go,
-                               const double2* Co, const double2* Bo, double2* C1, double2* Ao, double2* Aos,
-                               int64_t Q, int* ok, int* ncyc_c, double tol, int it, int* next, int* next_count,
-                               int* redo, cudaStream_t s) {
+cudaError_t launch_small_dec(int P, int n, const int* list, const int* count, const double2* Go, const double2* Co,
+                             const double2* Bo, double2* C1, double2* B1, double2* Ao, double2* Aos, int64_t Q, int* ok,
+                             int* ncyc_c, double tol, int it, int* next, int* next_count, int* redo, cudaStream_t s) {
   if (P <= 0) return cudaSuccess;
   if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
   static std::mutex mu;
   static bool done16[64] = {false}, done32[64] = {false};
   if (n <= 16) {
     const size_t smem = 4 * 16 * 16 * sizeof(double2);
-    cudaError_t e = opt_in(k_small_dec_a<16>, smem, done16, mu);
+    cudaError_t e = opt_in(k_small_dec<16>, smem, done16, mu);
     if (e != cudaSuccess) return e;
-    k_small_dec_a<16><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, Ao, Aos, Q, ok, ncyc_c, tol,
-                                                   it, next, next_count, redo);
+    k_small_dec<16><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, B1, Ao, Aos, Q, ok, ncyc_c, tol,
+                                                 it, next, next_count, redo);
   } else {
     const size_t smem = 4 * 32 * 32 * sizeof(double2);
-    cudaError_t e = opt_in(k_small_dec_a<32>, smem, done32, mu);
+    cudaError_t e = opt_in(k_small_dec<32>, smem, done32, mu);
     if (e != cudaSuccess) return e;
-    k_small_dec_a<32><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, Ao, Aos, Q, ok, ncyc_c, tol,
-                                                   it, next, next_count, redo);
-  }
-  return cudaGetLastError();
-}
-
-cudaError_t launch_small_dec_b(int P, int n, const int* list, const int* count, const double2* Go,
-                               const double2* Bo, const double2* Co, double2* B1, double2* Ao, int64_t Q,
-                               cudaStream_t s) {
-  if (P <= 0) return cudaSuccess;
-  if (n < 1 || n > kSmallMax) return cudaErrorInvalidValue;
-  static std::mutex mu;
-  static bool done16[64] = {false}, done32[64] = {false};
-  if (n <= 16) {
-    const size_t smem = 4 * 16 * 16 * sizeof(double2);
-    cudaError_t e = opt_in(k_small_dec_b<16>, smem, done16, mu);
-    if (e != cudaSuccess) return e;
-    k_small_dec_b<16><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Bo, Co, B1, Ao, Q);
-  } else {
-    const size_t smem = 4 * 32 * 32 * sizeof(double2);
-    cudaError_t e = opt_in(k_small_dec_b<32>, smem, done32, mu);
-    if (e != cudaSuccess) return e;
-    k_small_dec_b<32><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Bo, Co, B1, Ao, Q);
+    k_small_dec<32><<<P, kWarps * 32, smem, s>>>(n, list, count, P, Go, Co, Bo, C1, B1, Ao, Aos, Q, ok, ncyc_c, tol,
+                                                 it, next, next_count, redo);
   }
   return cudaGetLastError();
 }

@@ -32,20 +32,16 @@ cudaError_t launch_small_zinv(int batch, int n, const double2* A, double2* X, in
                               const int* count, int* info, int* status, int singular_code, cudaStream_t s);
 
 // One decimation iteration (src/contselfenergy.F90:271-340) for the points
-// of list[], b < *count, in two launches, one CTA per point (operands
-// staged in shared memory).  dec_a: X = Go Co, C1 = Co X, the CPU
-// convergence rule on max|C1| (ok[], ncyc_c[], iteration `it`; the points
-// that go on are appended to next[] / *next_count, in no fixed order), and
-// for those Self = Bo X, Ao -= Self, Aos -= Self; a point whose max|C1| is
-// Inf / NaN leaves the list with redo[p] = 1.  dec_b, over next[]:
-// Y = Go Bo, B1 = Bo Y, Ao -= Co Y.  P bounds the list length.
-cudaError_t launch_small_dec_a(int P, int n, const int* list, const int* count, const double2* Go,
-                               const double2* Co, const double2* Bo, double2* C1, double2* Ao, double2* Aos,
-                               int64_t Q, int* ok, int* ncyc_c, double tol, int it, int* next, int* next_count,
-                               int* redo, cudaStream_t s);
-cudaError_t launch_small_dec_b(int P, int n, const int* list, const int* count, const double2* Go,
-                               const double2* Bo, const double2* Co, double2* B1, double2* Ao, int64_t Q,
-                               cudaStream_t s);
+// of list[], b < *count, in one launch, one CTA per point (Go, Co, Bo
+// staged in shared memory once): X = Go Co, C1 = Co X, the CPU convergence
+// rule on max|C1| (ok[], ncyc_c[], iteration `it`; the points that go on are
+// appended to next[] / *next_count, in no fixed order), and for those
+// Self = Bo X, Ao -= Self, Aos -= Self, Y = Go Bo, B1 = Bo Y, Ao -= Co Y; a
+// point whose max|C1| is Inf / NaN leaves the list with redo[p] = 1.  P
+// bounds the list length.
+cudaError_t launch_small_dec(int P, int n, const int* list, const int* count, const double2* Go, const double2* Co,
+                             const double2* Bo, double2* C1, double2* B1, double2* Ao, double2* Aos, int64_t Q, int* ok,
+                             int* ncyc_c, double tol, int it, int* next, int* next_count, int* redo, cudaStream_t s);
 
 // The residual probe of each inverse X_p of A_p (same problem selection) and
 // up to two Newton steps X <- X + X (I - A X) where it shows a loss of
