@@ -938,7 +938,7 @@ def main():
             "e2e": {"value": e2e, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": gpu_launches,
             "schedule": ("lock step: every point of a step through each batched block operation at once, one "
-                         "CTA per point and operation, one warp per inversion (n <= 32)") if gpu_launches > args.steps else
+                         "CTA of 4 warps per point and operation (n <= 32)") if gpu_launches > args.steps else
                         "persistent engine: one launch per step, one CTA per point",
             "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,

@@ -148,7 +148,7 @@ typedef struct negf_b200_options {
    * _dev; single pair, no SGF cache) are scheduled under precision = 0:
    *   1 = the persistent engine: one CTA per point, its whole solve;
    *   2 = lock step: every point of the call through the same block
-   *       operation at once, one warp per point and operation (orders
+   *       operation at once, one CTA per point and operation (orders
    *       n <= 32; the call needs the shape rules of the mixed form);
    *   0 (default) = lock step when the call's points all fit it and n <= 32
    *       (for _dev calls: every device the context holds) and the stream is

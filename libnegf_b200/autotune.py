@@ -8,7 +8,7 @@ for a given device shape is the schedule:
   (one CTA's latency-bound inversion steps overlap the other's products) or
   1 (a CTA gets the whole L2 share and tensor pipe of an SM);
 - lock step (options.schedule = 2; 2-contact transmission, n <= 32): every
-  point through each batched block operation at once, one warp per point.
+  point through each batched block operation at once, one CTA per point.
 
 `tune` times each candidate that the device shape admits on a sample of the
 caller's own points, applies the fastest on top of the caller's other
