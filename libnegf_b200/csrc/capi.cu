@@ -111,6 +111,8 @@ struct negf_b200_ctx {
   size_t ws_bytes = 0;
   void* io = nullptr;
   size_t io_bytes = 0;
+  void* pin = nullptr;     // pinned staging of large read-backs (ReadBack)
+  size_t pin_bytes = 0;
   int sms = 0;
   bool trace = false;
   unsigned long long* d_trace = nullptr;
@@ -151,6 +153,57 @@ int grow(negf_b200_ctx* ctx, void** p, size_t* cap, size_t need) {
   *cap = need;
   return NEGF_B200_OK;
 }
+
+// The device-to-host copies of one call's results.  A pageable destination
+// makes the driver stage the copy through its own small pinned chunks, one
+// synchronous round trip each (about 0.2 s for a 121 MB DOS array); results
+// of 1 MiB and more therefore go through the context's pinned staging
+// buffer at full link speed and are copied to the caller's memory after the
+// stream synchronisation (finish()).  Without a staging buffer (cudaHostAlloc
+// failed) they are copied directly.
+struct ReadBack {
+  static constexpr size_t kStageMin = 1 << 20;
+  struct Item {
+    void* dst;
+    size_t off, bytes;
+  };
+  negf_b200_ctx* ctx;
+  cudaStream_t s;
+  char* pin = nullptr;
+  size_t used = 0;
+  std::vector<Item> staged;
+
+  // reserve: the sum of the staged sizes of this call (one allocation, grown once)
+  ReadBack(negf_b200_ctx* c, cudaStream_t st, size_t reserve) : ctx(c), s(st) {
+    if (reserve == 0) return;
+    if (ctx->pin_bytes < reserve) {
+      if (ctx->pin) cudaFreeHost(ctx->pin);
+      ctx->pin = nullptr;
+      ctx->pin_bytes = 0;
+      if (cudaHostAlloc(&ctx->pin, reserve, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->pin = nullptr;
+        return;
+      }
+      ctx->pin_bytes = reserve;
+    }
+    pin = static_cast<char*>(ctx->pin);
+  }
+  static size_t staged_size(size_t bytes) { return bytes >= kStageMin ? (bytes + 255) / 256 * 256 : 0; }
+  cudaError_t copy(void* dst, const void* src, size_t bytes) {
+    if (!dst || bytes == 0) return cudaSuccess;
+    if (pin && bytes >= kStageMin) {
+      cudaError_t e = cudaMemcpyAsync(pin + used, src, bytes, cudaMemcpyDeviceToHost, s);
+      staged.push_back({dst, used, bytes});
+      used += staged_size(bytes);
+      return e;
+    }
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+  }
+  void finish() {   // after the stream synchronisation
+    for (const Item& it : staged) std::memcpy(it.dst, pin + it.off, it.bytes);
+  }
+};
 
 int sync_descs(negf_b200_ctx* ctx) {
   if (!ctx->descs_dirty) return NEGF_B200_OK;
@@ -394,6 +447,7 @@ int negf_b200_ctx_destroy(negf_b200_ctx* ctx) {
   if (ctx->d_descs) cudaFree(ctx->d_descs);
   if (ctx->ws) cudaFree(ctx->ws);
   if (ctx->io) cudaFree(ctx->io);
+  if (ctx->pin) cudaFreeHost(ctx->pin);
   if (ctx->d_trace) cudaFree(ctx->d_trace);
   if (ctx->sgf.arena) cudaFree(ctx->sgf.arena);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -1213,19 +1267,27 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   st = run_device(ctx, a, sh, s);
   if (st) return st;
   std::vector<int32_t> hst(npts);
-  if (T) CK(cudaMemcpyAsync(T, d_T, (size_t)npts * npairs * 8, cudaMemcpyDeviceToHost, s));
-  if (ledos && nldos_pts > 0)
-    CK(cudaMemcpyAsync(ledos, d_ldos, (size_t)npts * nldos_pts * 8, cudaMemcpyDeviceToHost, s));
+  const size_t b_T = T ? (size_t)npts * npairs * 8 : 0;
+  const size_t b_ledos = (ledos && nldos_pts > 0) ? (size_t)npts * nldos_pts * 8 : 0;
+  const size_t b_dos = dos ? (size_t)npts * norb_pts * 8 : 0;
+  const size_t b_curr = curr ? (size_t)npts * ncont_pts * 8 : 0;
+  const size_t b_lcurr = lcurr ? (size_t)npts * std::max(1, nbl_pts - 1) * 8 : 0;
+  const size_t b_ldens = ldens ? (size_t)npts * nbl_pts * 8 : 0;
+  ReadBack rb(ctx, s, ReadBack::staged_size(b_T) + ReadBack::staged_size(b_ledos) + ReadBack::staged_size(b_dos) +
+                          ReadBack::staged_size(b_curr) + ReadBack::staged_size(b_lcurr) +
+                          ReadBack::staged_size(b_ldens));
+  CK(rb.copy(T, d_T, b_T));
+  CK(rb.copy(ledos, d_ldos, b_ledos));
   if (ncyc) CK(cudaMemcpyAsync(ncyc, d_ncyc, npts * 4, cudaMemcpyDeviceToHost, s));
   CK(cudaMemcpyAsync(hst.data(), d_st, npts * 4, cudaMemcpyDeviceToHost, s));
-  if (dos) CK(cudaMemcpyAsync(dos, d_dos, (size_t)npts * norb_pts * 8, cudaMemcpyDeviceToHost, s));
-  if (curr) CK(cudaMemcpyAsync(curr, d_curr, (size_t)npts * ncont_pts * 8, cudaMemcpyDeviceToHost, s));
-  if (lcurr)
-    CK(cudaMemcpyAsync(lcurr, d_lcurr, (size_t)npts * std::max(1, nbl_pts - 1) * 8, cudaMemcpyDeviceToHost, s));
-  if (ldens) CK(cudaMemcpyAsync(ldens, d_ldens, (size_t)npts * nbl_pts * 8, cudaMemcpyDeviceToHost, s));
+  CK(rb.copy(dos, d_dos, b_dos));
+  CK(rb.copy(curr, d_curr, b_curr));
+  CK(rb.copy(lcurr, d_lcurr, b_lcurr));
+  CK(rb.copy(ldens, d_ldens, b_ldens));
   if (scba_iter) CK(cudaMemcpyAsync(scba_iter, d_it, npts * 4, cudaMemcpyDeviceToHost, s));
   if (scba_err) CK(cudaMemcpyAsync(scba_err, d_err, npts * 8, cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
+  rb.finish();
   if (status) std::memcpy(status, hst.data(), npts * 4);
   return first_status(hst.data(), npts);
 }

@@ -95,3 +95,42 @@ def test_device_solve_replays_from_a_cuda_graph(gpu_ctx):
         del g
     finally:
         gpu_ctx.release(did)
+
+
+@pytest.mark.gpu
+def test_large_host_read_back_matches_the_device_call(gpu_ctx):
+    """A DOS result of 1 MiB or more reaches the caller's (pageable) array
+    through the context's pinned staging buffer: bit for bit what the
+    device-buffer call leaves on the device, on a first call (the buffer is
+    allocated) and a second one into an array that already holds data."""
+    torch = pytest.importorskip("torch")
+    from libnegf_b200 import native
+    dev = G.transport_c0(nbl=4, n=128, seed=3)
+    E = np.linspace(-2.0, 2.0, 300)                   # 300 x 512 doubles = 1.2 MB of DOS
+    did = gpu_ctx.upload(dev)
+    L = native.load()
+    try:
+        n = E.size
+        assert n * dev.norb * 8 >= 1 << 20
+        gpu_ctx.set_options(schedule=1)
+        d_ids = torch.full((n,), did, dtype=torch.int32, device="cuda")
+        d_E = torch.from_numpy(E).cuda()
+        d_T = torch.zeros(n, dtype=torch.float64, device="cuda")
+        d_dos = torch.zeros((n, dev.norb), dtype=torch.float64, device="cuda")
+        d_nc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        d_st = torch.zeros(n, dtype=torch.int32, device="cuda")
+        s = torch.cuda.Stream()
+        rc = L.negf_b200_transmission_dos_dev(gpu_ctx.handle, n, d_ids.data_ptr(), d_E.data_ptr(), 1e-4, 1e-4, 1, 2,
+                                              d_T.data_ptr(), d_dos.data_ptr(), dev.norb, d_nc.data_ptr(),
+                                              d_st.data_ptr(), ctypes.c_void_p(s.cuda_stream))
+        assert rc == 0
+        torch.cuda.synchronize()
+        T_dev, dos_dev = d_T.cpu().numpy(), d_dos.cpu().numpy()
+        T1, dos1, nc1, st1 = gpu_ctx.transmission_dos(did, E, eta=1e-4, dos_delta=1e-4)
+        assert np.array_equal(T1, T_dev) and np.array_equal(dos1, dos_dev)
+        assert np.array_equal(nc1, d_nc.cpu().numpy()) and not st1.any()
+        T2, dos2, _, _ = gpu_ctx.transmission_dos(did, E[::-1].copy(), eta=1e-4, dos_delta=1e-4)
+        assert np.array_equal(T2, T_dev[::-1]) and np.array_equal(dos2, dos_dev[::-1])
+    finally:
+        gpu_ctx.set_options()
+        gpu_ctx.release(did)
