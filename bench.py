@@ -66,7 +66,8 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
     p.add_argument("--points-per-step", type=int, default=0, help="0 = 2 x resident CTAs")
-    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--e2e-steps", type=int, default=0, help="host-buffer steps timed for e2e (0 = --steps: the "
+                   "same batches as the device-timed steps)")
     p.add_argument("--cpu-sample", type=int, default=0, help="CPU baseline points (0 = auto)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--trace", action="store_true", help="one extra untimed step with per-phase cycle tracing")
@@ -903,7 +904,7 @@ def main():
 
     # e2e: same batches through the host-buffer C-ABI call, after one untimed
     # call of it (the context's host staging buffer is allocated on first use)
-    e2e_steps = max(1, args.e2e_steps)
+    e2e_steps = args.e2e_steps if args.e2e_steps > 0 else args.steps
     h_ids = np.asarray(dids, dtype=np.int32)[ids_run]
     torch.cuda.synchronize()
     if dist:
