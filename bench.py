@@ -203,6 +203,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.rows = []
+        self.times = []
+        self.window = None      # (t0, t1): keep only the samples taken inside it
         self.proc = None
 
     def __enter__(self):
@@ -221,6 +223,7 @@ class ClockSampler:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) == 8:
                 self.rows.append(parts)
+                self.times.append(time.perf_counter())
 
     def __exit__(self, *exc):
         if self.proc:
@@ -231,14 +234,17 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.rows:
+        rows = self.rows
+        if self.window is not None:
+            rows = [r for r, t in zip(self.rows, self.times) if self.window[0] <= t <= self.window[1]]
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[4 + i].lower() == "active"})
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(rows)}
 
 
 def fp64_peak_tflops(torch, dev):
@@ -846,19 +852,23 @@ def main():
         if rc != 0:
             raise RuntimeError("solve failed: %d %s" % (rc, ctx.last_error()))
 
-    for s in range(args.warmup):
-        step(s)
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    # small orders (c0): a step's device blocks and workspace can sit in the L2, so the L2 is flushed
-    # (256 MB written on the solve's stream) before every timed step, outside its events
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if wl["n"] <= 64 else None
-    ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    nl0 = ctx.launch_count()
-    with ClockSampler(local) as clk:
+    # the clock sampler starts before the warm-up steps (starting nvidia-smi slowed the
+    # step it overlapped by up to 0.3 s) and reports only the samples of the timed region
+    clk = ClockSampler(local).__enter__()
+    try:
+        for s in range(args.warmup):
+            step(s)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        # small orders (c0): a step's device blocks and workspace can sit in the L2, so the L2 is flushed
+        # (256 MB written on the solve's stream) before every timed step, outside its events
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda") if wl["n"] <= 64 else None
+        ev0 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ev1 = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        nl0 = ctx.launch_count()
+        t_on = time.perf_counter()
         for j in range(args.steps):
             if flush is not None:
                 with torch.cuda.stream(stream):
@@ -867,6 +877,9 @@ def main():
             step(args.warmup + j)
             ev1[j].record(stream)
         torch.cuda.synchronize()
+        clk.window = (t_on, time.perf_counter())
+    finally:
+        clk.__exit__(None, None, None)
     gpu_launches = ctx.launch_count() - nl0
     per_step = [ev0[j].elapsed_time(ev1[j]) for j in range(args.steps)]
     ms = sum(per_step)
