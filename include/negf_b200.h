@@ -217,7 +217,10 @@ int negf_b200_device_bytes(const negf_b200_ctx* ctx, int32_t device_id,
  * the return value is the first non-OK point status (or a call error).
  * `ncyc` (npts, optional) receives the total decimation iteration count over
  * all contacts at that point (src/integrations.F90:1751 prints the average
- * over contacts). */
+ * over contacts).  Results of 1 MiB and more (DOS, LDOS, layer rows of large
+ * calls) are read back through a pinned host staging buffer that the context
+ * allocates on first use, sized to the largest such call, and frees in
+ * negf_b200_ctx_destroy; the caller's arrays may be pageable. */
 
 /* Coherent transmission T(E) between contacts ni -> nf (1-based).
  * Replaces compute_contacts(E+i*eta) + calculate_transmissions(E)
