@@ -540,18 +540,20 @@ def serve_stream(rate, seconds, blocks, layers, grid, lanes, policy):
         npts = int(np.exp(rng.uniform(np.log(g0), np.log(g1))))
         kind = "ldos" if rng.random() < 0.3 else "T"
         gen = "c1" if rng.random() < 0.5 else "c0"
-        plan.append((t, n, nbl, npts, kind, gen, int(rng.integers(1 << 30))))
+        # FP64 or mixed precision: half of the T requests in the mixed form (8 int8 digits)
+        prec = 8 if kind == "T" and rng.random() < 0.5 else 0
+        plan.append((t, n, nbl, npts, kind, gen, int(rng.integers(1 << 30)), prec))
     srv = Server(lanes=lanes, sgf_cache_bytes=1 << 30, policy=policy)
     reqs = []
     with ClockSampler(0) as clk:
         t0 = time.perf_counter()
-        for (ta, n, nbl, npts, kind, gen, seed) in plan:
+        for (ta, n, nbl, npts, kind, gen, seed, prec) in plan:
             dev = (G.transport_c1(nbl=nbl, n=n, seed=seed, density=0.1) if gen == "c1"
                    else G.transport_c0(nbl=nbl, n=n, seed=seed))
             E = np.sort(np.random.default_rng(seed).uniform(-2.0, 2.0, npts))
             r = Request(dev, E, eta=1e-4, ldos=(kind == "ldos"), dos_delta=1e-4,
                         dos_proj=[list(range(1, n + 1)), list(range(dev.norb - n + 1, dev.norb + 1))]
-                        if kind == "ldos" else None)
+                        if kind == "ldos" else None, precision=prec)
             while time.perf_counter() - t0 < ta:
                 time.sleep(0.001)
             reqs.append(srv.submit(r))
@@ -572,11 +574,14 @@ def serve_stream(rate, seconds, blocks, layers, grid, lanes, policy):
                                "grids %d-%d log-uniform, 30%% LDOS requests, c0/c1 generators"
                                % (rate, seconds, blocks, lo, hi, g0, g1),
                    "lanes": lanes, "policy": policy, "eta": 1e-4,
-                   "precision": "complex FP64 (plain form)"},
+                   "precision": "FP64 or mixed: half of the T requests in the mixed form (8 int8 digits), "
+                                "the rest complex FP64"},
         "latency_s": {"p50": float(np.percentile(lat, 50)) if lat.size else None,
                       "p99": float(np.percentile(lat, 99)) if lat.size else None,
                       "max": float(lat.max()) if lat.size else None},
         "requests": len(reqs), "rejected": len(reqs) - len(ok), "points": pts, "gpu_launches": srv.launches,
+        "mixed_requests": int(sum(1 for r in reqs if r.precision)),
+        "mixed_points": int(sum(r.energies.size for r in ok if r.precision)),
         "status_counts": {str(k): int(v) for k, v in
                           zip(*np.unique(np.concatenate([r.status for r in reqs]), return_counts=True))},
         "clocks": clk.summary(),

@@ -130,7 +130,10 @@ typedef struct negf_b200_options {
    * FP64, all points of a call in lock step.  1 = the mixed form with 8
    * digits.  The mixed form needs two
    * contacts on blocks 1 and nbl, one PL size for every layer and both leads,
-   * no tun_proj; other solves return NEGF_B200_ERR_BAD_ARG under it. */
+   * the same shape for every point of a call, a single contact pair and no
+   * tun_proj; other solves return NEGF_B200_ERR_BAD_ARG under it.  It
+   * neither reads nor fills the SGF cache (a context that keeps one still
+   * runs it). */
   int32_t precision;
   /* Resident CTAs per SM for the persistent point engine (0 = auto). */
   int32_t ctas_per_sm;

@@ -1084,10 +1084,14 @@ static bool lockstep_choice(negf_b200_ctx* ctx, int32_t npts, const int32_t* h_i
     *st = fail(ctx, NEGF_B200_ERR_BAD_ARG, std::string(form) + " cannot run under stream capture");
     return true;
   }
-  if (!single_pair || ctx->sgf.mode) {
+  // the mixed form neither reads nor fills the SGF cache, so a context that keeps
+  // one (a serving lane) runs it too; the FP64 lock step leaves such calls to the
+  // engine, which uses the cache
+  if (!single_pair || (ctx->sgf.mode && !mixed)) {
     if (!forced) return false;
     *st = fail(ctx, NEGF_B200_ERR_BAD_ARG,
-               std::string(form) + " covers single-pair transmission solves without the SGF cache");
+               std::string(form) + (mixed ? " covers single-pair transmission solves"
+                                          : " covers single-pair transmission solves without the SGF cache"));
     return true;
   }
   std::string why;
@@ -1228,20 +1232,23 @@ static int solve_host(negf_b200_ctx* ctx, int mode, int32_t npts, const int32_t*
   if (d_cpl) CK(cudaMemcpyAsync(d_cpl, coupling, (size_t)norb_pts * 8, cudaMemcpyHostToDevice, s));
   if (d_pni) CK(cudaMemcpyAsync(d_pni, pni, (size_t)npairs * 4, cudaMemcpyHostToDevice, s));
   if (d_pnf) CK(cudaMemcpyAsync(d_pnf, pnf, (size_t)npairs * 4, cudaMemcpyHostToDevice, s));
-  std::vector<int64_t> sgf_in, sgf_out;
-  if (ctx->sgf.mode) {
-    plan_sgf(ctx, npts, ids, E, eta, sh.ncont_max, sgf_in, sgf_out);
-    CK(cudaMemcpyAsync(d_sgf_in, sgf_in.data(), sgf_in.size() * 8, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(d_sgf_out, sgf_out.data(), sgf_out.size() * 8, cudaMemcpyHostToDevice, s));
-  }
   LockShape lsh;
   int lslices = 0;
   if (mode != negf::MODE_T) {
     st = engine_only(ctx, "this solve");
     if (st) return st;
   }
-  if (mode == negf::MODE_T && lockstep_choice(ctx, npts, ids, npairs == 1, &lsh, &lslices, &st, s)) {
-    if (st) return st;
+  const bool lock = mode == negf::MODE_T && lockstep_choice(ctx, npts, ids, npairs == 1, &lsh, &lslices, &st, s);
+  if (lock && st) return st;
+  // the cache plan (which points read a cached gs, which fill a slot) only for
+  // the engine: a lock-step form would leave the planned slots unfilled
+  std::vector<int64_t> sgf_in, sgf_out;
+  if (ctx->sgf.mode && !lock) {
+    plan_sgf(ctx, npts, ids, E, eta, sh.ncont_max, sgf_in, sgf_out);
+    CK(cudaMemcpyAsync(d_sgf_in, sgf_in.data(), sgf_in.size() * 8, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(d_sgf_out, sgf_out.data(), sgf_out.size() * 8, cudaMemcpyHostToDevice, s));
+  }
+  if (lock) {
     st = run_lockstep(ctx, npts, d_ids, d_E, eta, d_T, d_ncyc, d_st, s, lsh, lslices);
     if (st) return st;
     std::vector<int32_t> hst(npts);

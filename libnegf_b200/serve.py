@@ -11,8 +11,10 @@ feeds the GPU from a pool of pending energy points:
   stream and workspace; a lane runs one persistent launch at a time, and
   the launches of different lanes run concurrently on the SMs;
 - batching: whenever a lane is free it takes pending points of one solve
-  kind (T or T+LDOS, same eta, dos_delta and pairs), whatever request they
-  belong to, up to `points_per_launch`; points of requests that arrived
+  kind (T or T+LDOS, same eta, dos_delta, pairs and precision; for the mixed
+  form also the same block order and layer count, since its lock-step call
+  needs one shape), whatever request they belong to, up to
+  `points_per_launch`; a lane sets its `precision` option per batch; points of requests that arrived
   while other launches were running join the next launch of any free lane
   (continuous batching, not a queue of whole requests).  The order is
   `policy`: "fifo" (default) takes the oldest points first; "srpt" takes
@@ -58,6 +60,10 @@ class Request:
     tun_proj: Optional[Sequence[int]] = None
     dos_proj: Optional[Sequence[Sequence[int]]] = None
     key: Optional[object] = None          # device identity for reuse across requests (default: the object)
+    # 0: complex FP64; 1 or 4..8: the mixed form (int8 tensor-core products with
+    # that many digits, 1 = 8), for single-pair T requests (no LDOS, no tun_proj)
+    # on devices with 2 contacts on blocks 1 and nbl and one PL size
+    precision: int = 0
     # filled by the server
     T: Optional[np.ndarray] = None
     ledos: Optional[np.ndarray] = None
@@ -151,9 +157,26 @@ class Server:
         req.status = np.zeros(npts, dtype=np.int32)
         req._left = npts
         with self._cv:
+            why = self._mixed_refusal(req)
+            if why:                                   # the mixed form cannot take it: fails at once
+                req.error = why
+                req.status[:] = native.BAD_ARG
+                self._finish(req)
+                return req
             self._arrivals.append(req)
             self._cv.notify_all()
         return req
+
+    @staticmethod
+    def _mixed_refusal(req) -> Optional[str]:
+        p = int(req.precision)
+        if p == 0:
+            return None
+        if p != 1 and not 4 <= p <= 8:
+            return "precision must be 0, 1 or 4..8"
+        if req.ldos or len(req.pairs) != 1 or req.tun_proj is not None:
+            return "the mixed form serves single-pair T requests without LDOS or tun_proj"
+        return None
 
     def close(self):
         with self._cv:
@@ -222,7 +245,9 @@ class Server:
     # ---------------------------------------------------------------- batching
     @staticmethod
     def _group(req):
-        return (bool(req.ldos), float(req.eta), float(req.dos_delta) if req.ldos else 0.0, tuple(req.pairs))
+        p = int(req.precision)
+        shape = (max(req.device.pl_size), int(req.device.nbl)) if p else None
+        return (bool(req.ldos), float(req.eta), float(req.dos_delta) if req.ldos else 0.0, tuple(req.pairs), p, shape)
 
     @staticmethod
     def _point_cost(req) -> float:
@@ -260,6 +285,7 @@ class Server:
 
     def _lane_loop(self, lane):
         ctx = self.lanes[lane]
+        precision = 0                                      # the lane's current option
         while True:
             with self._cv:
                 while not self._stop and not self._pending:
@@ -271,6 +297,9 @@ class Server:
             req0 = batch[0][0]
             E = np.array([r.energies[i] for r, i in batch])
             try:
+                if int(req0.precision) != precision:
+                    ctx.update_options(precision=int(req0.precision))
+                    precision = int(req0.precision)
                 T, led, nc, st = ctx.transmissions(ids, E, req0.pairs, eta=req0.eta, ldos=req0.ldos,
                                                    dos_delta=req0.dos_delta, check=False)
                 err = None

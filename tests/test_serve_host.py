@@ -19,9 +19,15 @@ class FakeContext:
         self.next_id = 0
         self.launches = []
         self.released = []
+        self.precision = 0
+        self.shapes = []           # per launch: (precision option, {(block order, layers)} of its devices)
         self.lock = threading.Lock()
 
     def set_options(self, **kw): pass
+
+    def update_options(self, **kw):
+        self.precision = kw.get("precision", self.precision)
+
     def set_workspace_limit(self, n): pass
     def set_sgf_cache(self, mode, n=0): pass
     def set_tun_proj(self, did, p): pass
@@ -44,6 +50,8 @@ class FakeContext:
         ids = np.asarray(ids)
         with self.lock:
             self.launches.append((tuple(sorted(set(ids.tolist()))), len(E), ldos))
+            self.shapes.append((self.precision, {(max(self.devices[int(i)].pl_size), self.devices[int(i)].nbl)
+                                                 for i in set(ids.tolist())}))
         time.sleep(0.01)
         T = np.stack([E * (ids + 1) + q for q in range(len(pairs))], axis=1)
         led = np.stack([E, -E], axis=1) if ldos else None
@@ -153,3 +161,35 @@ def test_out_of_order_completion():
         assert small.t_done < big.t_done
     finally:
         srv.close()
+
+
+def test_mixed_precision_requests_batch_by_precision_and_shape():
+    """Mixed-form requests share a launch only with requests of the same
+    precision, block order and layer count (the lock-step call needs one
+    shape); the lane sets its precision option per batch; FP64 requests of any
+    shape still mix.  A mixed request the form cannot take (LDOS) fails at
+    submission with BAD_ARG."""
+    from libnegf_b200 import native
+    ctxs = [FakeContext(), FakeContext()]
+    srv = Server(contexts=ctxs, sms=4, points_per_launch=16, hbm_budget=1 << 34, sgf_cache_bytes=0)
+    reqs = []
+    for q, (n, nbl, prec) in enumerate([(8, 4, 8), (8, 4, 8), (16, 4, 8), (8, 5, 7), (8, 4, 0), (16, 5, 0),
+                                        (8, 4, 1)]):
+        dev = G.transport_c0(nbl=nbl, n=n, seed=q)
+        reqs.append(srv.submit(Request(dev, np.linspace(-1, 1, 20 + q), precision=prec)))
+    bad = srv.submit(Request(G.transport_c0(nbl=4, n=8, seed=9), np.linspace(-1, 1, 5), precision=8, ldos=True,
+                             dos_proj=[[1, 2]]))
+    assert bad.wait(1) and bad.error and np.all(bad.status == native.BAD_ARG)
+    for r in reqs:
+        assert r.wait(30) and r.error is None
+    srv.close()
+    for r in reqs:                                     # every point solved once, in its own request
+        did = srv._resident[srv._key(r)].ids[0]
+        assert np.array_equal(r.T[:, 0], r.energies * (did + 1)) and not r.status.any()
+    shapes = [sh for c in ctxs for sh in c.shapes]
+    assert sum(len(c.launches) for c in ctxs) == srv.launches
+    for prec, devs in shapes:
+        if prec:
+            assert len(devs) == 1, devs                # one shape per mixed launch
+    precs = {p for p, _ in shapes}
+    assert {0, 1, 7, 8} <= precs

@@ -5,7 +5,7 @@ import time
 import numpy as np
 import pytest
 
-from conftest import assert_T_close, oracle_spread
+from conftest import assert_parity, assert_T_close, oracle_spread
 from libnegf_b200 import generators as G
 from oracle import oracle as O
 
@@ -167,5 +167,51 @@ def test_admission_rejects_a_device_over_budget():
         assert big.wait(60) and small.wait(60)
         assert big.error is not None and np.all(big.status == native.ADMISSION)
         assert small.error is None and np.all(small.status == 0)
+    finally:
+        srv.close()
+
+
+@pytest.mark.gpu
+def test_mixed_precision_requests_in_the_mix():
+    """Mixed-form requests (8 int8 digits) served beside FP64 requests, on
+    lanes that keep an SGF cache: each is bitwise the direct mixed-form call
+    on the same points (whatever the batch cut) and within the mixed form's
+    bound, max(1e-8 |T|, 1e-11), of the oracle; the FP64 requests beside them
+    keep their alone results."""
+    from libnegf_b200 import native
+    from libnegf_b200.serve import Request, Server
+    devs = [G.transport_c0(nbl=4, n=128, seed=21), G.transport_c0(nbl=5, n=16, seed=22)]
+    Es = [np.linspace(-2.0, 2.0, 20), np.linspace(-2.5, 2.5, 40)]
+    direct = []
+    with native.Context(0) as ctx:
+        ctx.set_options(precision=8)
+        for dev, E in zip(devs, Es):
+            did = ctx.upload(dev)
+            direct.append(ctx.transmission(did, E, eta=1e-4, check=False))
+            ctx.release(did)
+    alone = []
+    srv = Server(lanes=2, points_per_launch=24, hbm_budget=8 << 30, sgf_cache_bytes=64 << 20)
+    try:
+        for r in _requests()[:2]:
+            srv.submit(r)
+            assert r.wait(120) and r.error is None
+            alone.append(r.T.copy())
+    finally:
+        srv.close()
+    srv = Server(lanes=2, points_per_launch=24, hbm_budget=8 << 30, sgf_cache_bytes=64 << 20)
+    try:
+        mixed = [Request(d, E, eta=1e-4, precision=8) for d, E in zip(devs, Es)]
+        plain = _requests()[:2]
+        for r in plain[:1] + mixed + plain[1:]:
+            srv.submit(r)
+        for r in mixed + plain:
+            assert r.wait(120) and r.error is None and np.all(r.status == 0)
+        for r, T0 in zip(plain, alone):
+            assert np.array_equal(r.T, T0)
+        for r, (T, nc, st) in zip(mixed, direct):
+            assert not st.any()
+            assert np.array_equal(r.T[:, 0], T) and np.array_equal(r.ncyc, nc)
+            ref, spread = oracle_spread(lambda d: O.transmission(d, r.energies, eta=1e-4)[0], r.device, nsamp=2)
+            assert_parity(r.T[:, 0], ref, np.maximum(1e-8 * np.abs(ref), 1e-11), spread=spread, what="served mixed T")
     finally:
         srv.close()
