@@ -43,3 +43,20 @@ def test_parity_summary_applies_the_test_bound():
     off[3] += 1e-3                                        # far beyond rounding and the oracle's spread
     bad = bench.parity_summary(wl, devs, ids, E, off, Tc, cores=2)
     assert not bad["all_within_test_bound"] and bad["beyond_1e-10"] == 1
+
+
+def test_clock_summary_keeps_the_timed_window():
+    """The sampler runs from before the warm-up steps; its summary counts only
+    the samples taken inside the timed region, so a throttle reason seen
+    during warm-up alone does not mark the timed number."""
+    clk = bench.ClockSampler(0)
+    row = lambda mhz, cap: [str(mhz), "1965", "900", "0x0", "Not Active", "Not Active", "Not Active",
+                            "Active" if cap else "Not Active"]
+    clk.rows = [row(1500, True), row(1965, False), row(1965, False), row(1800, True)]
+    clk.times = [1.0, 2.0, 3.0, 4.0]
+    assert clk.summary()["samples"] == 4 and clk.summary()["reasons"] == ["sw_power_cap"]
+    clk.window = (1.5, 3.5)
+    s = clk.summary()
+    assert s["samples"] == 2 and s["sm_mhz"] == 1965.0 and s["reasons"] == []
+    clk.window = (10.0, 11.0)
+    assert clk.summary()["reasons"] == ["unsampled"]
