@@ -14,9 +14,10 @@ feeds the GPU from a pool of pending energy points:
   kind (T or T+LDOS, same eta, dos_delta, pairs and precision; for the mixed
   form also the same block order and layer count, since its lock-step call
   needs one shape), whatever request they belong to, up to
-  `points_per_launch`; a lane sets its `precision` option per batch; points of requests that arrived
-  while other launches were running join the next launch of any free lane
-  (continuous batching, not a queue of whole requests).  The order is
+  `points_per_launch`, and sets its `precision` option for the batch;
+  points of requests that arrived while other launches were running join
+  the next launch of any free lane (continuous batching, not a queue of
+  whole requests).  The order is
   `policy`: "fifo" (default) takes the oldest points first; "srpt" takes
   first the points of the request with the least estimated remaining work
   (pending points x a per-point cost of (layers + 80) x block order^3, the
@@ -285,7 +286,7 @@ class Server:
 
     def _lane_loop(self, lane):
         ctx = self.lanes[lane]
-        precision = 0                                      # the lane's current option
+        precision = int(getattr(ctx, "options", {}).get("precision", 0))   # the lane's current option
         while True:
             with self._cv:
                 while not self._stop and not self._pending:
